@@ -1,0 +1,389 @@
+"""Benchmark of the B200 space-charge step (one JSON line on rank 0).
+
+Workload (the headline configuration): free-space IGF solve on a 128x128x256 grid with
+10^7 particles from a seeded Gaussian, sigma = (0.5, 0.5, 2) mm truncated at 4 sigma,
+total charge 1 nC, gamma = 5 MeV / m_e c^2, mesh from the reference's test-path rule
+(get_mesh_quantities).  One step = CIC deposit of all particles + E on the grid (Green
+spectrum cached, fixed mesh) + interpolation of E at every particle, device-resident.
+
+`value` is FP32-path solves/s summed over ranks; the same step on the plain FP64 GPU
+path (the reference algorithm restated on the GPU) is timed beside it, and the FP32
+field at the particles is compared with it.  `e2e` drives the same step through the C
+ABI with pinned host buffers (copies inside the timed region).  `--impl reference` times
+the FP64 CPU port of the reference algorithm (oracle/) on the host cores.
+
+Multi-GPU: the single-grid solve does not shard; `--gpus N` runs N independent replicas
+(one per rank) and reports the aggregate ("scaling": "weak").
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "solves/s at 128x128x256, 1e7 ptcl: FP32 vs FP64 GPU path at rel err<=1e-5"
+GRID = (128, 128, 256)
+NPART = 10_000_000
+SIGMA = (0.5e-3, 0.5e-3, 2e-3)
+CUTOFF = 4.0
+QTOT = 1e-9
+GAMMA = 5e6 / 0.510998910e6
+SEED = 1
+WORKLOAD = ("free-space IGF space-charge step: CIC deposit + E on a 128x128x256 grid (doubled FFT "
+            "256x256x512) + interpolation at 1e7 particles; Gaussian sigma=(0.5,0.5,2) mm cut at 4 sigma, "
+            "1 nC, gamma=9.785; Green spectrum cached, fixed mesh")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--np", type=int, default=NPART, help="particles (default: the headline 1e7)")
+    ap.add_argument("--grid", type=str, default="", help="nx,ny,nz (default 128,128,256)")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    return ap.parse_args()
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    return ws, rank, local, pg
+
+
+def make_bunch(npart):
+    from openspacecharge_b200.bunch import gendist
+    return gendist(npart, sigma=SIGMA, cutoff=CUTOFF, disttype=1, seed=SEED)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                if out.returncode == 0 and out.stdout.strip():
+                    self.samples.append([s.strip() for s in out.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for i, nm in enumerate(names):
+                if len(s) > 5 + i and s[5 + i].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+# ---------------------------------------------------------------------------------------
+# algorithmic bytes per launch of each kernel of the FP32 step (inputs read once, outputs
+# written once; f64 particle coordinates, f64 E at particles, complex64 spectra)
+def kernel_bytes(nx, ny, nz, npart, at_cathode=False):
+    nxh = nx + 1
+    Nx, Ny, Nz = 2 * nx, 2 * ny, 2 * nz
+    N = nx * ny * nz
+    c8 = 8
+    nout = 3
+    g_bytes = 3 * 4 * nxh * (ny + 1) * (nz + 1)
+    return {
+        "deposit_f32": 24 * npart + 4 * N,
+        "fft_x_r2c": 4 * N + c8 * nxh * ny * nz,
+        "fft_y_fwd": c8 * nxh * ny * nz + c8 * nxh * Ny * nz,
+        "fft_z_conv": c8 * nxh * Ny * nz + g_bytes + nout * c8 * nxh * Ny * nz,
+        "fft_y_inv": nout * c8 * nxh * Ny * nz + nout * c8 * nxh * ny * nz,
+        "fft_x_c2r": nout * c8 * nxh * ny * nz + 16 * N,
+        "interp_f32": 24 * npart + 16 * N + 24 * npart,
+    }
+
+
+def run_ours(args, ws, rank, local, dist):
+    import torch
+    import openspacecharge_b200 as osc
+    from openspacecharge_b200 import native
+
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    grid = tuple(int(v) for v in args.grid.split(",")) if args.grid else GRID
+    npart = args.np
+    x, y, z = make_bunch(npart)
+    ctx = osc.Context(local)
+    stream = torch.cuda.Stream(device=dev)
+    ctx.set_stream(stream.cuda_stream)
+    delta, umin = osc.get_mesh_quantities(ctx, x, y, z, (1, 1, 1), grid, 0)
+    umax = umin + (np.array(grid) - 1) * delta
+    mesh = osc.Mesh3D(nlo=(1, 1, 1), nhi=grid, min=umin, max=umax, delta=delta, gamma=GAMMA)
+    tx = torch.from_numpy(x).to(dev)
+    ty = torch.from_numpy(y).to(dev)
+    tz = torch.from_numpy(z).to(dev)
+    E = torch.empty((npart, 3), dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+
+    def step(prec, out=E):
+        osc.space_charge_step_dev(ctx, mesh, tx, ty, tz, out, total_charge=QTOT, resize_mesh=False,
+                                  precision=prec)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def timed(prec, k, w):
+        for _ in range(w):
+            step(prec)
+        ctx.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        l0 = ctx.launch_count()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k):
+            step(prec)
+        e1.record(stream)
+        e1.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / k
+        if dist is not None:
+            t = torch.tensor([ms], dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, ctx.launch_count() - l0
+
+    # headline: FP32 path
+    with ClockSampler(local) as clk:
+        ms32, launches = timed(osc.PREC_FP32, args.steps, max(3, args.warmup))
+    E32 = E.clone()
+    value = ws * 1000.0 / ms32
+
+    # plain FP64 GPU path (the reference algorithm on the GPU) and the error of FP32 vs it
+    fp64 = None
+    err = None
+    if not args.no_fp64:
+        E64 = torch.empty_like(E)
+        step(osc.PREC_FP64_PLAIN, E64)
+        ctx.synchronize()
+        k64 = max(3, min(args.steps, 10))
+        ms64, _ = timed(osc.PREC_FP64_PLAIN, k64, 1)
+        step(osc.PREC_FP64_PLAIN, E64)
+        ctx.synchronize()
+        d = (E32 - E64).abs()
+        ref = E64.abs()
+        mx = float((d.amax(0) / ref.amax(0)).max())
+        rms = float((torch.sqrt((d * d).mean(0)) / torch.sqrt((E64 * E64).mean(0))).max())
+        err = {"max": mx, "rms": rms, "against": "plain FP64 GPU path (reference algorithm)",
+               "definition": "per component max|E-E_ref|/max|E_ref| and RMS ratio, at all particles"}
+        fp64 = {"value": ws * 1000.0 / ms64, "ms_per_step": ms64, "steps": k64,
+                "speedup_fp32_over_fp64": ms64 / ms32}
+
+    # per-kernel profile of the FP32 step: CUDA events around each launch on the stream
+    ctx.set_option(osc.OPT_PROFILE, 1)
+    ctx.profile_reset()
+    nprof = max(3, min(args.steps, 10))
+    for _ in range(nprof):
+        step(osc.PREC_FP32)
+    prof = ctx.profile()
+    ctx.set_option(osc.OPT_PROFILE, 0)
+    kb = kernel_bytes(*grid, npart)
+    kernels = {}
+    for name, (cnt, tot) in prof.items():
+        avg = tot / max(cnt, 1)
+        ent = {"launches": cnt, "avg_ms": avg, "share": tot / max(1e-12, sum(v[1] for v in prof.values()))}
+        if name in kb:
+            ent["alg_bytes"] = kb[name]
+            ent["gbs"] = kb[name] / (avg * 1e-3) / 1e9
+        kernels[name] = ent
+    dom = max((k for k in kernels if k in kb), key=lambda k: kernels[k]["share"], default=None)
+    roof = None
+    if dom:
+        ach = kernels[dom]["gbs"]
+        roof = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
+                "frac": ach / hbm_peak, "peak_source": peak_src + " (MEASURED_PEAKS.json hbm_gbs)",
+                "traffic": None, "alg_bytes_per_launch": kb[dom]}
+    step_bytes = sum(kb.values())
+    step_gbs = step_bytes / (ms32 * 1e-3) / 1e9
+
+    # end to end through the C ABI with pinned host buffers, copies inside the timed region
+    e2e = None
+    if not args.no_e2e:
+        px = torch.from_numpy(x).pin_memory()
+        py = torch.from_numpy(y).pin_memory()
+        pz = torch.from_numpy(z).pin_memory()
+        pE = torch.empty((npart, 3), dtype=torch.float64).pin_memory()
+        import ctypes
+        m = mesh.to_c()
+        tc = ctypes.c_double(QTOT)
+
+        def host_step():
+            ctx.call("osc_space_charge_step", ctypes.byref(m), ctypes.c_int64(npart),
+                     ctypes.c_void_p(px.data_ptr()), ctypes.c_void_p(py.data_ptr()),
+                     ctypes.c_void_p(pz.data_ptr()), None, ctypes.byref(tc), 0, 0, osc.PREC_FP32,
+                     ctypes.c_void_p(pE.data_ptr()), None)
+
+        for _ in range(2):
+            host_step()
+        barrier()
+        ke = max(3, min(args.steps, 10))
+        t0 = time.perf_counter()
+        for _ in range(ke):
+            host_step()
+        te = (time.perf_counter() - t0) / ke
+        if dist is not None:
+            t = torch.tensor([te], dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            te = float(t.item())
+        e2e = {"value": ws / te, "unit": "solves/s", "h2d_bytes_per_step": 3 * 8 * npart,
+               "d2h_bytes_per_step": 3 * 8 * npart, "ms_per_step": te * 1e3,
+               "api": "osc_space_charge_step (C ABI, pinned host buffers)"}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        cpu = cpu_baseline(x, y, z, grid, umin, umax, delta)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": ms32, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "grid": list(grid), "particles": npart, "precision": "fp32",
+                       "particle_dtype": "f64 coordinates in, f64 E out",
+                       "l2": "inputs larger than L2 (240 MB of particle coordinates per step)",
+                       "parallelism": f"{ws} independent replica(s)"},
+            "fp64_plain": fp64, "rel_err_vs_fp64": err,
+            "step_alg_bytes": step_bytes, "step_alg_gbs": step_gbs,
+            "kernels": kernels, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": launches, "clocks": clk.summary(),
+        }
+        print(json.dumps(line))
+    ctx.close()
+
+
+def cpu_baseline(x, y, z, grid, umin, umax, delta):
+    """One full step of the FP64 CPU port (oracle/) on the host cores."""
+    from oracle import oracle as O
+    O.build()
+    m = O.make_mesh((1, 1, 1), grid, (1, 1, 1), umin, umax, delta, GAMMA)
+    t0 = time.perf_counter()
+    rho, _ = O.deposit_particles(x, y, z, m, total_charge=QTOT, resize_mesh=False)
+    ef, _ = O.space_charge_3d(m, rho)
+    O.interpolate_field(m, ef, x, y, z)
+    dt = time.perf_counter() - t0
+    return {"value": 1.0 / dt, "unit": "solves/s", "cores": O.num_threads(), "kind": "port",
+            "sample": "1 full step (deposit + solve + interpolation, 1e7 particles, 128x128x256) of the FP64 C++ "
+                      "restatement of the reference algorithm (7 full complex FFTs, G rebuilt), OpenMP"}
+
+
+def run_reference(args, ws, rank):
+    """The reference's CPU algorithm (FP64 port in oracle/, all host threads), same workload."""
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    O.build()
+    grid = tuple(int(v) for v in args.grid.split(",")) if args.grid else GRID
+    x, y, z = make_bunch(args.np)
+    delta, umin = O.get_mesh_quantities(x, y, z, (1, 1, 1), grid, 0)
+    umax = umin + (np.array(grid) - 1) * delta
+    m = O.make_mesh((1, 1, 1), grid, (1, 1, 1), umin, umax, delta, GAMMA)
+
+    def step():
+        rho, _ = O.deposit_particles(x, y, z, m, total_charge=QTOT, resize_mesh=False)
+        ef, _ = O.space_charge_3d(m, rho)
+        O.interpolate_field(m, ef, x, y, z)
+
+    budget = 240.0
+    t0 = time.perf_counter()
+    step()  # warm-up
+    t1 = time.perf_counter() - t0
+    nwarm = min(max(0, args.warmup - 1), int(max(0.0, budget * 0.2 - t1) / max(t1, 1e-9)))
+    for _ in range(nwarm):
+        step()
+    k = max(1, min(args.steps, int(budget * 0.8 / max(t1, 1e-9))))
+    t0 = time.perf_counter()
+    for _ in range(k):
+        step()
+    dt = (time.perf_counter() - t0) / k
+    val = 1.0 / dt
+    line = {
+        "metric": METRIC, "impl": "reference", "value": val, "unit": "solves/s", "n_gpus": ws,
+        "steps": k, "warmup": 1 + nwarm, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "grid": list(grid), "particles": args.np, "precision": "fp64"},
+        "cpu_baseline": {"value": val, "unit": "solves/s", "cores": O.num_threads(), "kind": "port",
+                         "sample": f"{k} of {args.steps} requested full steps timed (240 s cap); FP64 C++ "
+                                   f"restatement of the reference algorithm with OpenMP"},
+        "e2e": {"value": val, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    ws, rank, local, dist = dist_init()
+    try:
+        if args.impl == "reference":
+            run_reference(args, ws, rank)
+        else:
+            run_ours(args, ws, rank, local, dist)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

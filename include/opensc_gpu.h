@@ -1,0 +1,206 @@
+/*
+ * opensc_gpu.h -- C ABI of the B200 space-charge library (libopensc_b200.so).
+ *
+ * Each entry point replaces one routine of OpenSpaceCharge's Fortran module API
+ * (RobertRyne/OpenSpaceCharge, code/open_spacecharge_mod.f90 and
+ * code/open_spacecharge_core_mod.f90); the routine it replaces is cited above it.  The
+ * Fortran host binds these with iso_c_binding (fortran/open_spacecharge_mod.f90).
+ *
+ * Conventions
+ *   - Every function returns an int status: OSC_OK (0) or an OSC_E_* code.  Nothing exits,
+ *     aborts or traps; osc_last_error() gives a message for the last failure on a context.
+ *   - Grids are Fortran column-major, x fastest: a(i,j,k) at i + nx*(j + ny*k).  Field
+ *     grids are [3][nz][ny][nx] (efield(:,:,:,1:3), component slowest).  Particle fields
+ *     are [np][3] (a Fortran E(3,np) array).
+ *   - Host-pointer entry points take REAL64 host arrays, like the Fortran module; *_dev
+ *     entry points take device pointers and do no host<->device copies.
+ *   - A context owns one CUDA stream, its workspaces and the Green-spectrum cache.  One
+ *     context per host thread; calls on one context are serialised by the caller.
+ */
+#ifndef OPENSC_GPU_H
+#define OPENSC_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define OSC_API __attribute__((visibility("default")))
+#else
+#define OSC_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------------------- */
+#define OSC_OK 0
+#define OSC_E_INVALID 1     /* bad argument: null pointer, non-positive size, bad enum */
+#define OSC_E_BOUNDS 2      /* particles outside the mesh while strict bounds are on */
+#define OSC_E_FFT_SIZE 3    /* a doubled grid length is not 2^a 3^b 5^c or exceeds 2048 */
+#define OSC_E_ALLOC 4       /* device or pinned-host allocation failed */
+#define OSC_E_CUDA 5        /* a CUDA runtime call failed */
+#define OSC_E_TIMEOUT 6     /* a bounded device wait gave up */
+#define OSC_E_NAN 7         /* non-finite particle coordinate or charge */
+#define OSC_E_NOCHARGE 8    /* neither qa nor total_charge given (reference prints, returns) */
+#define OSC_E_UNSUPPORTED 9 /* combination the reference rejects (e.g. direct E in a pipe) */
+#define OSC_E_STATE 10      /* call order violated (e.g. pipe solve before its Green set) */
+
+/* ---- precision / path ------------------------------------------------------------ */
+#define OSC_PREC_FP32 0       /* complex64 convolution, FP64 Green build, cached spectra */
+#define OSC_PREC_FP64 1       /* same pipeline in FP64 / complex128 */
+#define OSC_PREC_FP64_PLAIN 2 /* the reference algorithm on the GPU in FP64: full complex
+                                 zero-padded FFTs, Green function rebuilt on every call */
+
+/* ---- deposition modes ------------------------------------------------------------ */
+#define OSC_DEPOSIT_ATOMIC 0 /* unsorted input, FP32/FP64 atomics, warp-aggregated */
+#define OSC_DEPOSIT_SORTED 1 /* cell-sorted, compensated, bit-reproducible run to run */
+
+/* ---- context options (osc_ctx_set_option) ---------------------------------------- */
+#define OSC_OPT_PRECISION 1      /* default precision for host entry points */
+#define OSC_OPT_DEPOSIT_MODE 2   /* OSC_DEPOSIT_* */
+#define OSC_OPT_STRICT_BOUNDS 3  /* 1: out-of-mesh particles make deposit return OSC_E_BOUNDS */
+#define OSC_OPT_GREEN_CACHE_MB 4 /* byte budget of the Green-spectrum cache (default 4096) */
+#define OSC_OPT_PROFILE 5        /* 1: time every kernel with CUDA events (osc_profile_*) */
+#define OSC_OPT_CHECK_FINITE 6   /* 1: deposit rejects non-finite coordinates (OSC_E_NAN) */
+
+typedef struct osc_ctx osc_ctx;
+
+/* Scalar members of mesh3d_struct (code/open_spacecharge_mod.f90:14-27), laid out so a
+ * Fortran bind(C) derived type with the same members maps onto it. */
+typedef struct osc_mesh3d {
+    int32_t nlo[3];    /* lowest grid index per axis (Fortran lbound) */
+    int32_t nhi[3];    /* highest grid index per axis */
+    int32_t npad[3];   /* padding of the legacy cyclic convolution */
+    double min[3];     /* grid origin (m) */
+    double max[3];     /* grid end (m) */
+    double delta[3];   /* grid spacing (m) */
+    double gamma;      /* relativistic gamma */
+    double charge;     /* total charge on the mesh (C) */
+} osc_mesh3d;
+
+/* ---- context ------------------------------------------------------------------------
+ * No reference counterpart: the reference keeps module-global Green arrays
+ * (code/open_spacecharge_core_mod.f90:22-23) and is not re-entrant. */
+OSC_API int osc_ctx_create(int device, osc_ctx **out);
+OSC_API int osc_ctx_destroy(osc_ctx *ctx);
+OSC_API const char *osc_last_error(const osc_ctx *ctx);
+OSC_API int osc_ctx_set_stream(osc_ctx *ctx, void *cuda_stream); /* NULL: the context's own stream */
+OSC_API int osc_ctx_set_option(osc_ctx *ctx, int option, int64_t value);
+OSC_API int osc_ctx_get_option(osc_ctx *ctx, int option, int64_t *value);
+OSC_API int osc_ctx_synchronize(osc_ctx *ctx);
+OSC_API int osc_clear_green_cache(osc_ctx *ctx);
+OSC_API const char *osc_version(void);
+/* Kernel profile (OSC_OPT_PROFILE=1): per kernel name, launches and summed ms. */
+OSC_API int osc_profile_reset(osc_ctx *ctx);
+OSC_API int osc_profile_count(osc_ctx *ctx, int *n);
+OSC_API int osc_profile_entry(osc_ctx *ctx, int i, const char **name, int64_t *launches, double *ms);
+/* Number of kernels this library launched on the context since creation. */
+OSC_API int osc_launch_count(osc_ctx *ctx, int64_t *n);
+
+/* ---- deposition -------------------------------------------------------------------
+ * Replaces deposit_particles (code/open_spacecharge_mod.f90:156-288).  qa may be NULL, then
+ * total_charge must be non-NULL (else OSC_E_NOCHARGE, rho untouched, like the reference's
+ * print-and-return).  resize_mesh != 0 refits min/max/delta to the bunch with the
+ * reference's 1e-6*delta padding.  mesh->charge is set.  rho is [nz][ny][nx] REAL64.
+ * Particles whose 2x2x2 stencil leaves the mesh are skipped and counted in *n_outside
+ * (the reference writes out of bounds there). */
+OSC_API int osc_deposit_particles(osc_ctx *ctx, int64_t np, const double *xa, const double *ya,
+                          const double *za, const double *qa, const double *total_charge,
+                          int resize_mesh, osc_mesh3d *mesh, double *rho, int64_t *n_outside);
+OSC_API int osc_deposit_particles_dev(osc_ctx *ctx, int64_t np, const double *d_x, const double *d_y,
+                              const double *d_z, const double *d_q, const double *total_charge,
+                              int resize_mesh, osc_mesh3d *mesh, double *d_rho,
+                              int64_t *n_outside);
+
+/* Replaces get_mesh_quantities (code/test_mod.f90:288-358), the test-path mesh rule:
+ * delta=(max-min)/(n-3), min=bunch_min-delta; isetzmin=1 pins zmin=1e-9 for cathodes. */
+OSC_API int osc_get_mesh_quantities(osc_ctx *ctx, int64_t np, const double *xa, const double *ya,
+                            const double *za, const int32_t nlo[3], const int32_t nhi[3],
+                            int isetzmin, double delta[3], double umin[3]);
+/* Replaces depose_rho_scalar (code/test_mod.f90:410-474).  lostflag may be NULL; rho is
+ * scaled by chrgpermacro; *ifail counts skipped (out-of-mesh) particles. */
+OSC_API int osc_depose_rho_scalar(osc_ctx *ctx, int64_t np, const double *xa, const double *ya,
+                          const double *za, const double *lostflag, double chrgpermacro,
+                          const int32_t nlo[3], const int32_t nhi[3], const double delta[3],
+                          const double umin[3], double *rho, int64_t *ifail);
+
+/* ---- field solves ------------------------------------------------------------------
+ * Replaces space_charge_3d (code/open_spacecharge_mod.f90:431-489): IGF free-space field
+ * (and the cathode image when at_cathode != 0), optional B.  offset may be NULL. */
+OSC_API int osc_space_charge_3d(osc_ctx *ctx, const osc_mesh3d *mesh, const double *rho,
+                        const double *offset, int at_cathode, int calc_bfield, int precision,
+                        double *efield, double *bfield);
+OSC_API int osc_space_charge_3d_dev(osc_ctx *ctx, const osc_mesh3d *mesh, const double *d_rho,
+                            const double *offset, int at_cathode, int calc_bfield,
+                            int precision, double *d_efield, double *d_bfield);
+/* Replaces osc_freespace_solver2 (code/open_spacecharge_mod.f90:535-597); phi (the
+ * icomp=0 branch) and efield are each optional (NULL). */
+OSC_API int osc_freespace_solver2(osc_ctx *ctx, const int32_t n[3], const double *rho, double gamma,
+                          const double delta[3], const double *offset, int precision,
+                          double *efield, double *phi);
+/* Replaces space_charge_freespace (code/open_spacecharge_mod.f90:60-75), which runs the
+ * legacy osc_freespace_solver (code/open_spacecharge_core_mod.f90:30-138). */
+OSC_API int osc_space_charge_freespace(osc_ctx *ctx, const osc_mesh3d *mesh, const double *rho,
+                               int direct_field_calc, int integrated_green_function,
+                               int precision, double *phi, double *efield, double *bfield);
+/* Replaces space_charge_cathodeimages (code/open_spacecharge_mod.f90:83-103) ->
+ * osc_cathodeimages_solver (code/open_spacecharge_core_mod.f90:905-1083).  image_method 1
+ * (convolution/correlation) or 2 (shifted Green function).  Method 2 leaves rho flipped in
+ * z on return, as the reference does. */
+OSC_API int osc_space_charge_cathodeimages(osc_ctx *ctx, const osc_mesh3d *mesh, double *rho,
+                                   int direct_field_calc, int integrated_green_function,
+                                   int image_method, int precision, double *phi,
+                                   double *efield, double *bfield);
+
+/* ---- rectangular pipe ----------------------------------------------------------------
+ * Replaces osc_alloc_rectpipe_arrays + osc_getgrnpipe (code/open_spacecharge_core_mod.f90:
+ * 876-898, 632-715): builds and caches the four transformed pipe Green arrays on the
+ * context (the reference's module-global cgrn1..4).  umin is the mesh origin. */
+OSC_API int osc_rectpipe_green(osc_ctx *ctx, const osc_mesh3d *mesh, double apipe, double bpipe,
+                       int precision);
+/* Replaces space_charge_rectpipe (code/open_spacecharge_mod.f90:110-127) ->
+ * osc_rectpipe_solver (core:536-624).  direct_field_calc must be 0 (the reference prints
+ * an error otherwise: OSC_E_UNSUPPORTED).  Needs osc_rectpipe_green first (OSC_E_STATE). */
+OSC_API int osc_space_charge_rectpipe(osc_ctx *ctx, const osc_mesh3d *mesh, const double *rho,
+                              double apipe, double bpipe, int direct_field_calc,
+                              int integrated_green_function, int precision, double *phi,
+                              double *efield, double *bfield);
+/* Replace osc_write_rectpipe_grn / osc_read_rectpipe_grn (core:825-870): a header record
+ * and cgrn1..4 as complex128, Fortran unformatted sequential layout. */
+OSC_API int osc_write_rectpipe_grn(osc_ctx *ctx, const char *path, double apipe, double bpipe,
+                           const osc_mesh3d *mesh);
+OSC_API int osc_read_rectpipe_grn(osc_ctx *ctx, const char *path, const osc_mesh3d *mesh,
+                          double *apipe, double *bpipe);
+
+/* ---- interpolation -------------------------------------------------------------------
+ * Replaces interpolate_field (code/open_spacecharge_mod.f90:311-390), batched over np
+ * points.  efield/bfield are grids ([3][nz][ny][nx]); either may be NULL together with
+ * its output.  E and B are [np][3].  Out-of-range points are clamped to cells [1,nhi-1]
+ * as in the reference and counted in *n_clamped (the reference prints them). */
+OSC_API int osc_interpolate_field(osc_ctx *ctx, const osc_mesh3d *mesh, const double *efield,
+                          const double *bfield, int64_t np, const double *x, const double *y,
+                          const double *z, double *E, double *B, int64_t *n_clamped);
+OSC_API int osc_interpolate_field_dev(osc_ctx *ctx, const osc_mesh3d *mesh, const double *d_efield,
+                              const double *d_bfield, int64_t np, const double *d_x,
+                              const double *d_y, const double *d_z, double *d_E, double *d_B,
+                              int64_t *n_clamped);
+
+/* ---- fused step ------------------------------------------------------------------------
+ * deposit_particles + space_charge_3d + interpolate_field at every particle in one call
+ * (code/test_opensc.f90:156-228 does the same three steps).  Host buffers; *_dev takes
+ * device pointers.  If resize_mesh is 0 the mesh geometry is used as given and the Green
+ * spectrum is reused from the cache.  E is [np][3]; B may be NULL. */
+OSC_API int osc_space_charge_step(osc_ctx *ctx, osc_mesh3d *mesh, int64_t np, const double *x,
+                          const double *y, const double *z, const double *q,
+                          const double *total_charge, int resize_mesh, int at_cathode,
+                          int precision, double *E, double *B);
+OSC_API int osc_space_charge_step_dev(osc_ctx *ctx, osc_mesh3d *mesh, int64_t np, const double *d_x,
+                              const double *d_y, const double *d_z, const double *d_q,
+                              const double *total_charge, int resize_mesh, int at_cathode,
+                              int precision, double *d_E, double *d_B);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OPENSC_GPU_H */

@@ -1,0 +1,698 @@
+// abi.cu -- extern "C" entry points of libopensc_b200.so (declared in include/opensc_gpu.h).
+#include <cmath>
+#include <cstring>
+#include <new>
+
+#include "../../include/opensc_gpu.h"
+#include "solver.cuh"
+
+using namespace osc;
+
+#define TRY(...)             \
+    do {                     \
+        int rc_ = (__VA_ARGS__); \
+        if (rc_) return rc_; \
+    } while (0)
+#define CK(call, what) TRY(cuda_check(ctx, (call), what))
+
+namespace {
+
+int bad(osc_ctx *ctx, const char *what) { return set_err(ctx, OSC_E_INVALID, "invalid argument: %s", what); }
+
+int mesh_dims(osc_ctx *ctx, const osc_mesh3d *m, int n[3]) {
+    if (!m) return bad(ctx, "mesh is NULL");
+    for (int d = 0; d < 3; ++d) {
+        n[d] = m->nhi[d] - m->nlo[d] + 1;
+        if (n[d] < 2) return set_err(ctx, OSC_E_INVALID, "mesh axis %d has %d nodes (need >= 2)", d, n[d]);
+    }
+    return OSC_OK;
+}
+
+int check_prec(osc_ctx *ctx, int p) {
+    if (p < 0 || p > 2) return bad(ctx, "precision must be OSC_PREC_FP32, OSC_PREC_FP64 or OSC_PREC_FP64_PLAIN");
+    return OSC_OK;
+}
+
+int h2d(osc_ctx *ctx, void *d, const void *h, size_t bytes) {
+    return cuda_check(ctx, cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, ctx->stream), "H2D copy");
+}
+int d2h(osc_ctx *ctx, void *h, const void *d, size_t bytes) {
+    return cuda_check(ctx, cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, ctx->stream), "D2H copy");
+}
+int sync(osc_ctx *ctx) { return cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "stream synchronize"); }
+
+// Stage a host array on the device under a workspace name.
+template <typename T> int stage_in(osc_ctx *ctx, const char *name, const T *h, size_t n, T **d) {
+    if (!h) {
+        *d = nullptr;
+        return OSC_OK;
+    }
+    TRY(ws_get(ctx, name, sizeof(T) * n, (void **)d));
+    return h2d(ctx, *d, h, sizeof(T) * n);
+}
+
+// Reference mesh refit of deposit_particles (code/open_spacecharge_mod.f90:176-189) from
+// the particle bounding box computed on the device.
+int refit_mesh(osc_ctx *ctx, int64_t np, const double *x, const double *y, const double *z, osc_mesh3d *mesh) {
+    if (np <= 0) return set_err(ctx, OSC_E_INVALID, "resize_mesh needs at least one particle");
+    double *bb;
+    TRY(ws_get(ctx, "bbox", sizeof(double) * 8, (void **)&bb));
+    {
+        Launch L_(ctx, "bbox", 3);
+        TRY(launch_bbox(np, x, y, z, ctx->d_small + 8, bb, ctx->d_small + 16, ctx->stream) ? set_err(ctx, OSC_E_CUDA, "bbox") : 0);
+    }
+    double hb[6];
+    TRY(d2h(ctx, hb, bb, sizeof(hb)));
+    TRY(d2h(ctx, ctx->h_small + 16, ctx->d_small + 16, sizeof(unsigned long long)));
+    TRY(sync(ctx));
+    if (ctx->h_small[16]) return set_err(ctx, OSC_E_NAN, "%llu non-finite particle coordinates", ctx->h_small[16]);
+    double mn[3] = {hb[0], hb[2], hb[4]}, mx[3] = {hb[1], hb[3], hb[5]}, delta[3];
+    for (int d = 0; d < 3; ++d) delta[d] = (mx[d] - mn[d]) / (double)(mesh->nhi[d] - mesh->nlo[d]);
+    for (int d = 0; d < 3; ++d) {
+        mn[d] = mn[d] - 1.0e-6 * delta[d];
+        mx[d] = mx[d] + 1.0e-6 * delta[d];
+    }
+    for (int d = 0; d < 3; ++d) delta[d] = (mx[d] - mn[d]) / (double)(mesh->nhi[d] - mesh->nlo[d]);
+    for (int d = 0; d < 3; ++d) {
+        mesh->min[d] = mn[d];
+        mesh->max[d] = mx[d];
+        mesh->delta[d] = delta[d];
+    }
+    return OSC_OK;
+}
+
+int set_charge(osc_ctx *ctx, int64_t np, const double *q, const double *total_charge, osc_mesh3d *mesh,
+               double *charge1) {
+    if (q) {
+        double *out;
+        TRY(ws_get(ctx, "qsum", sizeof(double), (void **)&out));
+        {
+            Launch L_(ctx, "charge_sum", 2);
+            if (launch_sum(np, q, ctx->d_partials, out, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "charge sum");
+        }
+        double s = 0;
+        TRY(d2h(ctx, &s, out, sizeof(double)));
+        TRY(sync(ctx));
+        mesh->charge = s;
+        *charge1 = 0;
+    } else if (total_charge) {
+        mesh->charge = *total_charge;
+        *charge1 = *total_charge / (double)np;
+    } else {
+        return set_err(ctx, OSC_E_NOCHARGE, "Error, must specify qa or total_charge");
+    }
+    return OSC_OK;
+}
+
+DepositArgs deposit_args(const osc_mesh3d *m, const int n[3], int64_t np, const double *x, const double *y,
+                         const double *z, const double *q, double charge1, int check_finite) {
+    DepositArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.np = np;
+    a.x = x; a.y = y; a.z = z; a.q = q; a.lost = nullptr;
+    a.xmin = m->min[0]; a.ymin = m->min[1]; a.zmin = m->min[2];
+    a.dx = m->delta[0]; a.dy = m->delta[1]; a.dz = m->delta[2];
+    a.dxi = 1.0 / a.dx; a.dyi = 1.0 / a.dy; a.dzi = 1.0 / a.dz;
+    for (int d = 0; d < 3; ++d) {
+        a.nlo[d] = m->nlo[d];
+        a.nhi[d] = m->nhi[d];
+        a.nlogbl[d] = m->nlo[d];
+    }
+    a.nx = n[0]; a.ny = n[1]; a.nz = n[2];
+    a.mode = 0;
+    a.charge1 = charge1;
+    a.check_finite = check_finite;
+    return a;
+}
+
+InterpArgs interp_args(const osc_mesh3d *m, const int n[3], int64_t np, const double *x, const double *y,
+                       const double *z) {
+    InterpArgs a;
+    a.np = np;
+    a.x = x; a.y = y; a.z = z;
+    for (int d = 0; d < 3; ++d) {
+        a.min[d] = m->min[d];
+        a.delta[d] = m->delta[d];
+        a.hinv[d] = 1.0 / m->delta[d];
+        a.nlo[d] = m->nlo[d];
+        a.nhi[d] = m->nhi[d];
+    }
+    a.nx = n[0]; a.ny = n[1]; a.nz = n[2];
+    return a;
+}
+
+int counters_reset(osc_ctx *ctx) {
+    return cuda_check(ctx, cudaMemsetAsync(ctx->d_small, 0, sizeof(unsigned long long) * 8, ctx->stream), "memset counters");
+}
+// counters: [0] outside, [1] non-finite, [2] clamped
+int counters_read(osc_ctx *ctx, unsigned long long out[3]) {
+    TRY(d2h(ctx, ctx->h_small, ctx->d_small, sizeof(unsigned long long) * 3));
+    TRY(sync(ctx));
+    for (int i = 0; i < 3; ++i) out[i] = ctx->h_small[i];
+    return OSC_OK;
+}
+
+FreeSpaceJob fs_job(const osc_mesh3d *mesh, const int n[3], const double *offset, int at_cathode, int calc_b) {
+    FreeSpaceJob j;
+    j.nx = n[0]; j.ny = n[1]; j.nz = n[2];
+    for (int d = 0; d < 3; ++d) {
+        j.delta[d] = mesh->delta[d];
+        j.offset[d] = offset ? offset[d] : 0.0;
+    }
+    j.gamma = mesh->gamma;
+    j.at_cathode = at_cathode ? 1 : 0;
+    // offset0(3) + 2*min(3) + (max(3)-min(3)) (code/open_spacecharge_mod.f90:472)
+    j.img_zoff = 2 * mesh->min[2] + (mesh->max[2] - mesh->min[2]);
+    j.calc_b = calc_b ? 1 : 0;
+    if (calc_b) {
+        const double beta = std::sqrt(1 - 1 / (mesh->gamma * mesh->gamma));
+        j.bcoef = beta / c_light_sc3d();
+    }
+    return j;
+}
+
+int run_freespace(osc_ctx *ctx, const FreeSpaceJob &j, const double *d_rho, int precision) {
+    switch (precision) {
+    case OSC_PREC_FP32: return freespace_opt<float, double>(ctx, j, d_rho);
+    case OSC_PREC_FP64: return freespace_opt<double, double>(ctx, j, d_rho);
+    default: return freespace_plain(ctx, j, d_rho);
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *osc_version(void) { return "opensc_b200 0.1.0 (sm_100a)"; }
+
+int osc_ctx_create(int device, osc_ctx **out) {
+    if (!out) return OSC_E_INVALID;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+        cudaGetLastError();
+        return OSC_E_CUDA;
+    }
+    if (device < 0 || device >= ndev) return OSC_E_INVALID;
+    osc_ctx *ctx = new (std::nothrow) osc_ctx();
+    if (!ctx) return OSC_E_ALLOC;
+    ctx->device = device;
+    if (cudaSetDevice(device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc(&ctx->d_small, sizeof(unsigned long long) * 64) != cudaSuccess ||
+        cudaMallocHost(&ctx->h_small, sizeof(unsigned long long) * 64) != cudaSuccess ||
+        cudaMalloc(&ctx->d_partials, sizeof(double) * 1024) != cudaSuccess) {
+        cudaGetLastError();
+        osc_ctx_destroy(ctx);
+        return OSC_E_CUDA;
+    }
+    ctx->stream = ctx->own_stream;
+    *out = ctx;
+    return OSC_OK;
+}
+
+int osc_ctx_destroy(osc_ctx *ctx) {
+    if (!ctx) return OSC_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (auto &kv : ctx->ws) cudaFree(kv.second.p);
+    for (auto &kv : ctx->tw32) cudaFree(kv.second.p);
+    for (auto &kv : ctx->tw64) cudaFree(kv.second.p);
+    for (auto &g : ctx->gcache)
+        for (int i = 0; i < g.nspec; ++i) cudaFree(g.buf[i].p);
+    for (int t = 0; t < 4; ++t) cudaFree(ctx->pipe.g[t].p);
+    cudaFree(ctx->pipe.comb.p);
+    for (auto &r : ctx->prof_pending) {
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    for (auto e : ctx->ev_pool) cudaEventDestroy(e);
+    if (ctx->d_small) cudaFree(ctx->d_small);
+    if (ctx->h_small) cudaFreeHost(ctx->h_small);
+    if (ctx->d_partials) cudaFree(ctx->d_partials);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+    return OSC_OK;
+}
+
+const char *osc_last_error(const osc_ctx *ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+int osc_ctx_set_stream(osc_ctx *ctx, void *s) {
+    if (!ctx) return OSC_E_INVALID;
+    ctx->stream = s ? (cudaStream_t)s : ctx->own_stream;
+    return OSC_OK;
+}
+
+int osc_ctx_set_option(osc_ctx *ctx, int option, int64_t v) {
+    if (!ctx) return OSC_E_INVALID;
+    switch (option) {
+    case OSC_OPT_PRECISION: TRY(check_prec(ctx, (int)v)); ctx->precision = (int)v; return OSC_OK;
+    case OSC_OPT_DEPOSIT_MODE:
+        if (v != OSC_DEPOSIT_ATOMIC && v != OSC_DEPOSIT_SORTED) return bad(ctx, "deposit mode");
+        ctx->deposit_mode = (int)v;
+        return OSC_OK;
+    case OSC_OPT_STRICT_BOUNDS: ctx->strict_bounds = v ? 1 : 0; return OSC_OK;
+    case OSC_OPT_GREEN_CACHE_MB: ctx->gcache_budget = (size_t)(v < 0 ? 0 : v) << 20; return OSC_OK;
+    case OSC_OPT_PROFILE: ctx->profile = v ? 1 : 0; return OSC_OK;
+    case OSC_OPT_CHECK_FINITE: ctx->check_finite = v ? 1 : 0; return OSC_OK;
+    default: return bad(ctx, "unknown option");
+    }
+}
+
+int osc_ctx_get_option(osc_ctx *ctx, int option, int64_t *v) {
+    if (!ctx || !v) return OSC_E_INVALID;
+    switch (option) {
+    case OSC_OPT_PRECISION: *v = ctx->precision; return OSC_OK;
+    case OSC_OPT_DEPOSIT_MODE: *v = ctx->deposit_mode; return OSC_OK;
+    case OSC_OPT_STRICT_BOUNDS: *v = ctx->strict_bounds; return OSC_OK;
+    case OSC_OPT_GREEN_CACHE_MB: *v = (int64_t)(ctx->gcache_budget >> 20); return OSC_OK;
+    case OSC_OPT_PROFILE: *v = ctx->profile; return OSC_OK;
+    case OSC_OPT_CHECK_FINITE: *v = ctx->check_finite; return OSC_OK;
+    default: return bad(ctx, "unknown option");
+    }
+}
+
+int osc_ctx_synchronize(osc_ctx *ctx) {
+    if (!ctx) return OSC_E_INVALID;
+    return sync(ctx);
+}
+
+int osc_clear_green_cache(osc_ctx *ctx) {
+    if (!ctx) return OSC_E_INVALID;
+    TRY(sync(ctx));
+    for (auto &g : ctx->gcache)
+        for (int i = 0; i < g.nspec; ++i) cudaFree(g.buf[i].p);
+    ctx->gcache.clear();
+    return OSC_OK;
+}
+
+int osc_profile_reset(osc_ctx *ctx) {
+    if (!ctx) return OSC_E_INVALID;
+    prof_flush(ctx);
+    ctx->prof.clear();
+    return OSC_OK;
+}
+int osc_profile_count(osc_ctx *ctx, int *n) {
+    if (!ctx || !n) return OSC_E_INVALID;
+    prof_flush(ctx);
+    *n = (int)ctx->prof.size();
+    return OSC_OK;
+}
+int osc_profile_entry(osc_ctx *ctx, int i, const char **name, int64_t *launches, double *ms) {
+    if (!ctx) return OSC_E_INVALID;
+    prof_flush(ctx);
+    if (i < 0 || i >= (int)ctx->prof.size()) return OSC_E_INVALID;
+    auto it = ctx->prof.begin();
+    std::advance(it, i);
+    if (name) *name = it->first.c_str();
+    if (launches) *launches = it->second.launches;
+    if (ms) *ms = it->second.ms;
+    return OSC_OK;
+}
+int osc_launch_count(osc_ctx *ctx, int64_t *n) {
+    if (!ctx || !n) return OSC_E_INVALID;
+    *n = ctx->launches;
+    return OSC_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+int osc_deposit_particles_dev(osc_ctx *ctx, int64_t np, const double *x, const double *y, const double *z,
+                              const double *q, const double *total_charge, int resize_mesh, osc_mesh3d *mesh,
+                              double *rho, int64_t *n_outside) {
+    if (!ctx) return OSC_E_INVALID;
+    if (np < 0 || (np > 0 && (!x || !y || !z)) || !rho) return bad(ctx, "deposit arrays");
+    int n[3];
+    TRY(mesh_dims(ctx, mesh, n));
+    if (resize_mesh) TRY(refit_mesh(ctx, np, x, y, z, mesh));
+    double charge1 = 0;
+    if (np == 0 && !q && total_charge) {
+        mesh->charge = *total_charge;
+    } else {
+        TRY(set_charge(ctx, np, q, total_charge, mesh, &charge1));
+    }
+    const int64_t N = (int64_t)n[0] * n[1] * n[2];
+    CK(cudaMemsetAsync(rho, 0, sizeof(double) * N, ctx->stream), "memset rho");
+    TRY(counters_reset(ctx));
+    DepositArgs a = deposit_args(mesh, n, np, x, y, z, q, charge1, ctx->check_finite);
+    {
+        Launch L_(ctx, "deposit_f64");
+        if (launch_deposit<double>(a, rho, ctx->d_small, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "deposit");
+    }
+    if (n_outside || ctx->strict_bounds || ctx->check_finite) {
+        unsigned long long cnt[3];
+        TRY(counters_read(ctx, cnt));
+        if (n_outside) *n_outside = (int64_t)cnt[0];
+        if (ctx->check_finite && cnt[1]) return set_err(ctx, OSC_E_NAN, "%llu non-finite particles", cnt[1]);
+        if (ctx->strict_bounds && cnt[0]) return set_err(ctx, OSC_E_BOUNDS, "%llu particles outside the mesh", cnt[0]);
+    }
+    return OSC_OK;
+}
+
+int osc_deposit_particles(osc_ctx *ctx, int64_t np, const double *xa, const double *ya, const double *za,
+                          const double *qa, const double *total_charge, int resize_mesh, osc_mesh3d *mesh,
+                          double *rho, int64_t *n_outside) {
+    if (!ctx) return OSC_E_INVALID;
+    if (np < 0 || (np > 0 && (!xa || !ya || !za)) || !rho) return bad(ctx, "deposit arrays");
+    int n[3];
+    TRY(mesh_dims(ctx, mesh, n));
+    if (!qa && !total_charge) return set_err(ctx, OSC_E_NOCHARGE, "Error, must specify qa or total_charge");
+    const int64_t N = (int64_t)n[0] * n[1] * n[2];
+    double *dx, *dy, *dz, *dq, *drho;
+    TRY(stage_in(ctx, "h_x", xa, np, &dx));
+    TRY(stage_in(ctx, "h_y", ya, np, &dy));
+    TRY(stage_in(ctx, "h_z", za, np, &dz));
+    TRY(stage_in(ctx, "h_q", qa, np, &dq));
+    TRY(ws_get(ctx, "h_rho", sizeof(double) * N, (void **)&drho));
+    int64_t nout = 0;
+    TRY(osc_deposit_particles_dev(ctx, np, dx, dy, dz, dq, total_charge, resize_mesh, mesh, drho, &nout));
+    TRY(d2h(ctx, rho, drho, sizeof(double) * N));
+    TRY(sync(ctx));
+    if (n_outside) *n_outside = nout;
+    return OSC_OK;
+}
+
+int osc_get_mesh_quantities(osc_ctx *ctx, int64_t np, const double *xa, const double *ya, const double *za,
+                            const int32_t nlo[3], const int32_t nhi[3], int isetzmin, double delta[3],
+                            double umin[3]) {
+    if (!ctx) return OSC_E_INVALID;
+    if (np < 0 || (np > 0 && (!xa || !ya || !za)) || !nlo || !nhi || !delta || !umin) return bad(ctx, "mesh quantities");
+    // getbeamboundingbox (code/test_mod.f90:366): host min/max, as the arrays are host arrays
+    double sml[3], big[3];
+    const double *p[3] = {xa, ya, za};
+    for (int d = 0; d < 3; ++d) {
+        if (np > 0) {
+            double lo = p[d][0], hi = p[d][0];
+            for (int64_t m = 1; m < np; ++m) {
+                if (p[d][m] < lo) lo = p[d][m];
+                if (p[d][m] > hi) hi = p[d][m];
+            }
+            sml[d] = lo;
+            big[d] = hi;
+        } else {
+            sml[d] = 9999999.;
+            big[d] = -9999999.;
+        }
+    }
+    const double eps = 1.e-13;
+    for (int d = 0; d < 3; ++d) {
+        big[d] = big[d] * (1.0 + std::copysign(1.0, big[d]) * eps);
+        sml[d] = sml[d] * (1.0 - std::copysign(1.0, sml[d]) * eps);
+        const int nn = nhi[d] - nlo[d] + 1;
+        if (nn <= 3) return set_err(ctx, OSC_E_INVALID, "get_mesh_quantities needs more than 3 nodes per axis");
+        delta[d] = (big[d] - sml[d]) / (double)(nn - 3);
+        umin[d] = sml[d] - delta[d];
+    }
+    if (isetzmin == 1) {
+        const int nz = nhi[2] - nlo[2] + 1;
+        const double zsml = 1.e-9;
+        delta[2] = (big[2] - zsml) / (double)(nz - 1);
+        umin[2] = zsml;
+    }
+    return OSC_OK;
+}
+
+int osc_depose_rho_scalar(osc_ctx *ctx, int64_t np, const double *xa, const double *ya, const double *za,
+                          const double *lostflag, double chrgpermacro, const int32_t nlo[3], const int32_t nhi[3],
+                          const double delta[3], const double umin[3], double *rho, int64_t *ifail) {
+    if (!ctx) return OSC_E_INVALID;
+    if (np < 0 || (np > 0 && (!xa || !ya || !za)) || !rho || !nlo || !nhi || !delta || !umin) return bad(ctx, "depose");
+    osc_mesh3d m;
+    std::memset(&m, 0, sizeof(m));
+    for (int d = 0; d < 3; ++d) {
+        m.nlo[d] = nlo[d];
+        m.nhi[d] = nhi[d];
+        m.min[d] = umin[d];
+        m.delta[d] = delta[d];
+    }
+    int n[3];
+    TRY(mesh_dims(ctx, &m, n));
+    const int64_t N = (int64_t)n[0] * n[1] * n[2];
+    double *dx, *dy, *dz, *dl, *drho;
+    TRY(stage_in(ctx, "h_x", xa, np, &dx));
+    TRY(stage_in(ctx, "h_y", ya, np, &dy));
+    TRY(stage_in(ctx, "h_z", za, np, &dz));
+    TRY(stage_in(ctx, "h_q", lostflag, np, &dl));
+    TRY(ws_get(ctx, "h_rho", sizeof(double) * N, (void **)&drho));
+    CK(cudaMemsetAsync(drho, 0, sizeof(double) * N, ctx->stream), "memset rho");
+    TRY(counters_reset(ctx));
+    DepositArgs a = deposit_args(&m, n, np, dx, dy, dz, nullptr, 1.0, 0);
+    a.lost = dl;
+    a.mode = 1;
+    {
+        Launch L_(ctx, "deposit_f64");
+        if (launch_deposit<double>(a, drho, ctx->d_small, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "deposit");
+    }
+    {
+        Launch L_(ctx, "scale");
+        if (launch_scale(drho, chrgpermacro, N, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "scale");
+    }
+    TRY(d2h(ctx, rho, drho, sizeof(double) * N));
+    unsigned long long cnt[3];
+    TRY(counters_read(ctx, cnt));
+    if (ifail) *ifail = (int64_t)cnt[0];
+    return OSC_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+int osc_space_charge_3d_dev(osc_ctx *ctx, const osc_mesh3d *mesh, const double *d_rho, const double *offset,
+                            int at_cathode, int calc_bfield, int precision, double *d_efield, double *d_bfield) {
+    if (!ctx) return OSC_E_INVALID;
+    int n[3];
+    TRY(mesh_dims(ctx, mesh, n));
+    TRY(check_prec(ctx, precision));
+    if (!d_rho || !d_efield || (calc_bfield && !d_bfield)) return bad(ctx, "space_charge_3d arrays");
+    if (!(mesh->gamma >= 1.0)) return set_err(ctx, OSC_E_INVALID, "gamma must be >= 1");
+    FreeSpaceJob j = fs_job(mesh, n, offset, at_cathode, calc_bfield);
+    j.E = d_efield;
+    j.B = calc_bfield ? d_bfield : nullptr;
+    return run_freespace(ctx, j, d_rho, precision);
+}
+
+int osc_space_charge_3d(osc_ctx *ctx, const osc_mesh3d *mesh, const double *rho, const double *offset,
+                        int at_cathode, int calc_bfield, int precision, double *efield, double *bfield) {
+    if (!ctx) return OSC_E_INVALID;
+    int n[3];
+    TRY(mesh_dims(ctx, mesh, n));
+    if (!rho || !efield || (calc_bfield && !bfield)) return bad(ctx, "space_charge_3d arrays");
+    const int64_t N = (int64_t)n[0] * n[1] * n[2];
+    double *drho, *dE, *dB = nullptr;
+    TRY(stage_in(ctx, "h_rho", rho, N, &drho));
+    TRY(ws_get(ctx, "h_E", sizeof(double) * 3 * N, (void **)&dE));
+    if (calc_bfield) TRY(ws_get(ctx, "h_B", sizeof(double) * 3 * N, (void **)&dB));
+    TRY(osc_space_charge_3d_dev(ctx, mesh, drho, offset, at_cathode, calc_bfield, precision, dE, dB));
+    TRY(d2h(ctx, efield, dE, sizeof(double) * 3 * N));
+    if (calc_bfield) TRY(d2h(ctx, bfield, dB, sizeof(double) * 3 * N));
+    return sync(ctx);
+}
+
+int osc_freespace_solver2(osc_ctx *ctx, const int32_t n3[3], const double *rho, double gamma, const double delta[3],
+                          const double *offset, int precision, double *efield, double *phi) {
+    if (!ctx) return OSC_E_INVALID;
+    if (!n3 || !rho || !delta || (!efield && !phi)) return bad(ctx, "freespace_solver2 arguments");
+    TRY(check_prec(ctx, precision));
+    osc_mesh3d m;
+    std::memset(&m, 0, sizeof(m));
+    for (int d = 0; d < 3; ++d) {
+        m.nlo[d] = 1;
+        m.nhi[d] = n3[d];
+        m.delta[d] = delta[d];
+    }
+    m.gamma = gamma;
+    int n[3];
+    TRY(mesh_dims(ctx, &m, n));
+    const int64_t N = (int64_t)n[0] * n[1] * n[2];
+    double *drho, *dE = nullptr, *dP = nullptr;
+    TRY(stage_in(ctx, "h_rho", rho, N, &drho));
+    if (efield) TRY(ws_get(ctx, "h_E", sizeof(double) * 3 * N, (void **)&dE));
+    if (phi) TRY(ws_get(ctx, "h_phi", sizeof(double) * N, (void **)&dP));
+    FreeSpaceJob j = fs_job(&m, n, offset, 0, 0);
+    j.want_phi = phi ? 1 : 0;
+    j.want_e = efield ? 1 : 0;
+    j.E = dE;
+    j.phi = dP;
+    TRY(run_freespace(ctx, j, drho, precision));
+    if (efield) TRY(d2h(ctx, efield, dE, sizeof(double) * 3 * N));
+    if (phi) TRY(d2h(ctx, phi, dP, sizeof(double) * N));
+    return sync(ctx);
+}
+
+// ---------------------------------------------------------------------------------------
+int osc_interpolate_field_dev(osc_ctx *ctx, const osc_mesh3d *mesh, const double *d_efield, const double *d_bfield,
+                              int64_t np, const double *x, const double *y, const double *z, double *E, double *B,
+                              int64_t *n_clamped) {
+    if (!ctx) return OSC_E_INVALID;
+    int n[3];
+    TRY(mesh_dims(ctx, mesh, n));
+    if (np < 0 || (np > 0 && (!x || !y || !z))) return bad(ctx, "interpolate arrays");
+    if ((d_efield && !E) || (d_bfield && !B)) return bad(ctx, "interpolate outputs");
+    TRY(counters_reset(ctx));
+    InterpArgs a = interp_args(mesh, n, np, x, y, z);
+    if (d_efield && E) {
+        Launch L_(ctx, "interp_f64");
+        if (launch_interp_planes(a, d_efield, E, ctx->d_small + 2, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "interp");
+    }
+    if (d_bfield && B) {
+        Launch L_(ctx, "interp_f64");
+        if (launch_interp_planes(a, d_bfield, B, ctx->d_small + 3, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "interp");
+    }
+    if (n_clamped) {
+        unsigned long long cnt[3];
+        TRY(counters_read(ctx, cnt));
+        *n_clamped = (int64_t)cnt[2];
+    }
+    return OSC_OK;
+}
+
+int osc_interpolate_field(osc_ctx *ctx, const osc_mesh3d *mesh, const double *efield, const double *bfield,
+                          int64_t np, const double *x, const double *y, const double *z, double *E, double *B,
+                          int64_t *n_clamped) {
+    if (!ctx) return OSC_E_INVALID;
+    int n[3];
+    TRY(mesh_dims(ctx, mesh, n));
+    if (np < 0 || (np > 0 && (!x || !y || !z))) return bad(ctx, "interpolate arrays");
+    const int64_t N = (int64_t)n[0] * n[1] * n[2];
+    double *dx, *dy, *dz, *dE = nullptr, *dB = nullptr, *oE = nullptr, *oB = nullptr;
+    TRY(stage_in(ctx, "h_x", x, np, &dx));
+    TRY(stage_in(ctx, "h_y", y, np, &dy));
+    TRY(stage_in(ctx, "h_z", z, np, &dz));
+    if (efield && E) {
+        TRY(stage_in(ctx, "h_E", efield, 3 * N, &dE));
+        TRY(ws_get(ctx, "h_pE", sizeof(double) * 3 * (size_t)np, (void **)&oE));
+    }
+    if (bfield && B) {
+        TRY(stage_in(ctx, "h_B", bfield, 3 * N, &dB));
+        TRY(ws_get(ctx, "h_pB", sizeof(double) * 3 * (size_t)np, (void **)&oB));
+    }
+    int64_t ncl = 0;
+    TRY(osc_interpolate_field_dev(ctx, mesh, dE, dB, np, dx, dy, dz, oE, oB, &ncl));
+    if (oE) TRY(d2h(ctx, E, oE, sizeof(double) * 3 * np));
+    if (oB) TRY(d2h(ctx, B, oB, sizeof(double) * 3 * np));
+    TRY(sync(ctx));
+    if (n_clamped) *n_clamped = ncl;
+    return OSC_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+int osc_space_charge_step_dev(osc_ctx *ctx, osc_mesh3d *mesh, int64_t np, const double *x, const double *y,
+                              const double *z, const double *q, const double *total_charge, int resize_mesh,
+                              int at_cathode, int precision, double *E, double *B) {
+    if (!ctx) return OSC_E_INVALID;
+    int n[3];
+    TRY(mesh_dims(ctx, mesh, n));
+    TRY(check_prec(ctx, precision));
+    if (np <= 0 || !x || !y || !z || !E) return bad(ctx, "step arrays");
+    if (!q && !total_charge) return set_err(ctx, OSC_E_NOCHARGE, "Error, must specify qa or total_charge");
+    if (!(mesh->gamma >= 1.0)) return set_err(ctx, OSC_E_INVALID, "gamma must be >= 1");
+    if (resize_mesh) TRY(refit_mesh(ctx, np, x, y, z, mesh));
+    double charge1 = 0;
+    if (q) TRY(set_charge(ctx, np, q, total_charge, mesh, &charge1));
+    else {
+        mesh->charge = *total_charge;
+        charge1 = *total_charge / (double)np;
+    }
+    const int64_t N = (int64_t)n[0] * n[1] * n[2];
+    TRY(counters_reset(ctx));
+    DepositArgs da = deposit_args(mesh, n, np, x, y, z, q, charge1, ctx->check_finite);
+    InterpArgs ia = interp_args(mesh, n, np, x, y, z);
+    FreeSpaceJob j = fs_job(mesh, n, nullptr, at_cathode, B != nullptr);
+    if (precision == OSC_PREC_FP64_PLAIN) {
+        double *rho, *Eg, *Bg = nullptr;
+        TRY(ws_get(ctx, "st_rho64", sizeof(double) * N, (void **)&rho));
+        TRY(ws_get(ctx, "st_Eg", sizeof(double) * 3 * N, (void **)&Eg));
+        if (B) TRY(ws_get(ctx, "st_Bg", sizeof(double) * 3 * N, (void **)&Bg));
+        CK(cudaMemsetAsync(rho, 0, sizeof(double) * N, ctx->stream), "memset rho");
+        {
+            Launch L_(ctx, "deposit_f64");
+            if (launch_deposit<double>(da, rho, ctx->d_small, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "deposit");
+        }
+        j.E = Eg;
+        j.B = Bg;
+        TRY(freespace_plain(ctx, j, rho));
+        {
+            Launch L_(ctx, "interp_f64");
+            if (launch_interp_planes(ia, Eg, E, ctx->d_small + 2, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "interp");
+        }
+        if (B) {
+            Launch L_(ctx, "interp_f64");
+            if (launch_interp_planes(ia, Bg, B, ctx->d_small + 3, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "interp");
+        }
+        return OSC_OK;
+    }
+    if (precision == OSC_PREC_FP32) {
+        float *rho;
+        void *E4, *B4 = nullptr;
+        TRY(ws_get(ctx, "st_rho32", sizeof(float) * N, (void **)&rho));
+        TRY(ws_get(ctx, "st_E4", sizeof(float4) * N, &E4));
+        if (B) TRY(ws_get(ctx, "st_B4", sizeof(float4) * N, &B4));
+        CK(cudaMemsetAsync(rho, 0, sizeof(float) * N, ctx->stream), "memset rho");
+        {
+            Launch L_(ctx, "deposit_f32");
+            if (launch_deposit<float>(da, rho, ctx->d_small, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "deposit");
+        }
+        j.E4 = E4;
+        j.B = nullptr;
+        if (B) {
+            // B grid as a second vec4 grid: computed through the plane destinations below
+            double *Bg;
+            TRY(ws_get(ctx, "st_Bg", sizeof(double) * 3 * N, (void **)&Bg));
+            j.B = Bg;
+        }
+        TRY(freespace_opt<float, float>(ctx, j, rho));
+        {
+            Launch L_(ctx, "interp_f32");
+            if (launch_interp_vec4<float>(ia, E4, E, ctx->d_small + 2, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "interp");
+        }
+        if (B) {
+            Launch L_(ctx, "interp_f64");
+            if (launch_interp_planes(ia, j.B, B, ctx->d_small + 3, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "interp");
+        }
+        return OSC_OK;
+    }
+    // OSC_PREC_FP64: optimised pipeline in double
+    double *rho;
+    void *E4;
+    TRY(ws_get(ctx, "st_rho64", sizeof(double) * N, (void **)&rho));
+    TRY(ws_get(ctx, "st_E4d", sizeof(double4) * N, &E4));
+    CK(cudaMemsetAsync(rho, 0, sizeof(double) * N, ctx->stream), "memset rho");
+    {
+        Launch L_(ctx, "deposit_f64");
+        if (launch_deposit<double>(da, rho, ctx->d_small, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "deposit");
+    }
+    j.E4 = E4;
+    if (B) {
+        double *Bg;
+        TRY(ws_get(ctx, "st_Bg", sizeof(double) * 3 * N, (void **)&Bg));
+        j.B = Bg;
+    }
+    TRY(freespace_opt<double, double>(ctx, j, rho));
+    {
+        Launch L_(ctx, "interp_f64");
+        if (launch_interp_vec4<double>(ia, E4, E, ctx->d_small + 2, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "interp");
+    }
+    if (B) {
+        Launch L_(ctx, "interp_f64");
+        if (launch_interp_planes(ia, j.B, B, ctx->d_small + 3, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "interp");
+    }
+    return OSC_OK;
+}
+
+int osc_space_charge_step(osc_ctx *ctx, osc_mesh3d *mesh, int64_t np, const double *x, const double *y,
+                          const double *z, const double *q, const double *total_charge, int resize_mesh,
+                          int at_cathode, int precision, double *E, double *B) {
+    if (!ctx) return OSC_E_INVALID;
+    if (np <= 0 || !x || !y || !z || !E) return bad(ctx, "step arrays");
+    double *dx, *dy, *dz, *dq, *dE, *dB = nullptr;
+    TRY(stage_in(ctx, "h_x", x, np, &dx));
+    TRY(stage_in(ctx, "h_y", y, np, &dy));
+    TRY(stage_in(ctx, "h_z", z, np, &dz));
+    TRY(stage_in(ctx, "h_q", q, np, &dq));
+    TRY(ws_get(ctx, "h_pE", sizeof(double) * 3 * (size_t)np, (void **)&dE));
+    if (B) TRY(ws_get(ctx, "h_pB", sizeof(double) * 3 * (size_t)np, (void **)&dB));
+    TRY(osc_space_charge_step_dev(ctx, mesh, np, dx, dy, dz, dq, total_charge, resize_mesh, at_cathode, precision, dE,
+                                  dB));
+    TRY(d2h(ctx, E, dE, sizeof(double) * 3 * np));
+    if (B) TRY(d2h(ctx, B, dB, sizeof(double) * 3 * np));
+    return sync(ctx);
+}
+
+}  // extern "C"

@@ -1,0 +1,106 @@
+// context.cuh -- per-context state: stream, workspaces, Green-spectrum cache, profiling.
+#pragma once
+
+#include <cstdarg>
+#include <cstdio>
+#include <list>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "fft_kernels.cuh"
+
+struct osc_ctx;
+
+namespace osc {
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+};
+
+// One cached Green spectrum set: the stored spectra of all components of one geometry.
+struct GreenSet {
+    std::string key;
+    int nspec = 0;
+    DevBuf buf[8];
+    GSpecDev spec[8];
+    size_t bytes = 0;
+    uint64_t stamp = 0;
+};
+
+struct ProfRec {
+    std::string name;
+    cudaEvent_t a, b;
+};
+struct ProfSum {
+    int64_t launches = 0;
+    double ms = 0;
+};
+
+// Transformed pipe Green arrays (the reference's module-global cgrn1..4, core:22-23).
+struct PipeGreen {
+    bool valid = false;
+    int nlo[3], nhi[3], npad[3], period[3];
+    double apipe = 0, bpipe = 0, gamma = 0, delta[3], umin[3], umax[3];
+    DevBuf g[4];          // complex128 full spectra in the reference layout (FP64 plain path)
+    DevBuf comb;          // combined single-kernel spectrum for the optimised path
+    int comb_prec = -1;
+    GSpecDev comb_spec;
+};
+
+}  // namespace osc
+
+struct osc_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    std::string err;
+    // options
+    int precision = 0;
+    int deposit_mode = 0;
+    int strict_bounds = 0;
+    int profile = 0;
+    int check_finite = 0;
+    size_t gcache_budget = (size_t)4096 << 20;
+    // workspaces by name
+    std::map<std::string, osc::DevBuf> ws;
+    std::map<int, osc::DevBuf> tw32, tw64;
+    std::list<osc::GreenSet> gcache;
+    uint64_t stamp = 0;
+    // small device/pinned scratch for counters and reductions
+    unsigned long long *d_small = nullptr;  // 64 words
+    unsigned long long *h_small = nullptr;  // pinned 64 words
+    double *d_partials = nullptr;           // 1024 doubles
+    // profiling
+    std::vector<osc::ProfRec> prof_pending;
+    std::map<std::string, osc::ProfSum> prof;
+    std::vector<cudaEvent_t> ev_pool;
+    int64_t launches = 0;
+    osc::PipeGreen pipe;
+};
+
+namespace osc {
+
+int set_err(osc_ctx *c, int code, const char *fmt, ...);
+int cuda_check(osc_ctx *c, cudaError_t e, const char *what);
+// Named device workspace of at least `bytes` (grown by reallocation; contents not kept).
+int ws_get(osc_ctx *c, const char *name, size_t bytes, void **out);
+template <typename T> int twiddles(osc_ctx *c, int L, const cplx<T> **out);
+
+// Kernel-launch bookkeeping and optional per-kernel CUDA-event timing.
+struct Launch {
+    osc_ctx *c;
+    const char *name;
+    int nk;
+    cudaEvent_t a = nullptr;
+    Launch(osc_ctx *c_, const char *name_, int nk_ = 1);
+    ~Launch();
+};
+int prof_flush(osc_ctx *c);
+
+// Green-spectrum cache.
+GreenSet *gcache_find(osc_ctx *c, const std::string &key);
+GreenSet *gcache_insert(osc_ctx *c, GreenSet &&g);
+
+}  // namespace osc

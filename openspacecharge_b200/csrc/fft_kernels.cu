@@ -1,0 +1,387 @@
+// fft_kernels.cu -- batched shared-memory FFT kernels for the IGF convolution (sm_100a).
+//
+// The free-space solve runs as five kernels over HBM (FP32 path, G spectra cached):
+//   k_r2c_rows  x: real rho rows -> half spectra (two rows packed per complex line)
+//   k_lines     y: forward C2C along y (input window [0,ny))
+//   k_zconv     z: forward along z, multiply by the stored Green spectra, inverse along z
+//   k_lines     y: inverse C2C along y (output window [0,ny))
+//   k_c2r_rows  x: inverse to real rows, epilogue scatters E (and B) to their layouts
+// Zero padding of the doubled grid is never stored: loads past the physical window are
+// zeros in shared memory and stores cover only the physical window.
+#include <cstdio>
+#include <type_traits>
+
+#include "fft_kernels.cuh"
+
+namespace osc {
+
+bool make_fft_plan(int L, FFTPlan &p) {
+    if (L < 1 || L > FFT_MAX_LEN) return false;
+    p.L = L;
+    p.nst = 0;
+    int m = L;
+    while (m % 8 == 0) { p.radix[p.nst++] = 8; m /= 8; }
+    while (m % 4 == 0) { p.radix[p.nst++] = 4; m /= 4; }
+    while (m % 2 == 0) { p.radix[p.nst++] = 2; m /= 2; }
+    while (m % 3 == 0) { p.radix[p.nst++] = 3; m /= 3; }
+    while (m % 5 == 0) { p.radix[p.nst++] = 5; m /= 5; }
+    if (m != 1 || p.nst > FFT_MAX_STAGES) return false;
+    return L % 2 == 0;  // every length used here is a doubled grid edge
+}
+
+// Largest lines-per-CTA NL <= nl_max such that the CTA has a whole number of threads
+// (L*NL divisible by FFT_EPT), at most 1024 threads, and nbuf line buffers fit in budget.
+int pick_nl(int L, int nl_max, size_t elem_bytes, int nbuf, size_t budget) {
+    for (int nl = nl_max; nl >= 2; nl /= 2) {
+        if ((L * nl) % FFT_EPT != 0) continue;
+        if (fft_threads(L, nl) > 512) continue;
+        if ((size_t)nbuf * L * (nl + 1) * elem_bytes + L * elem_bytes > budget && nl > 2) continue;
+        return nl;
+    }
+    return 0;
+}
+
+// ------------------------------------------------------------------------------------
+template <typename T, int NL, bool ROW, class E>
+__global__ void __launch_bounds__(E::kMaxThreads) k_lines(const cplx<T> *in, cplx<T> *out, LineArgs a,
+                                                          const cplx<T> *__restrict__ twg) {
+    typedef cplx<T> V;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V *tw = reinterpret_cast<V *>(smem_raw);
+    const int L = E::kLen ? E::kLen : a.p.L;
+    V *buf = tw + L;
+    constexpr int lstr = NL + 1;
+    const int nthreads = blockDim.x, tid = threadIdx.x;
+    const int col0 = blockIdx.x * NL;
+    const V *src = in + (int64_t)blockIdx.z * a.in_zstride + (int64_t)blockIdx.y * a.in_pstride;
+    V *dst = out + (int64_t)blockIdx.z * a.out_zstride + (int64_t)blockIdx.y * a.out_pstride;
+    load_twiddles(tw, twg, L);
+    const int nld = NL * L;
+    for (int idx = tid; idx < nld; idx += nthreads) {
+        int e, c;
+        if (ROW) { c = idx / L; e = idx - c * L; }
+        else { e = idx / NL; c = idx - e * NL; }
+        V v = mk<T>(0, 0);
+        const int col = col0 + c;
+        if (e < a.in_len && col < a.ncols) v = src[(int64_t)col * a.in_cstride + (int64_t)e * a.in_estride];
+        buf[e * lstr + c] = v;
+    }
+    __syncthreads();
+    E::template run<V, NL>(buf, a.p, tw, a.sign);
+    const int nst = NL * a.out_len;
+    const T sc = (T)a.scale;
+    for (int idx = tid; idx < nst; idx += nthreads) {
+        int e, c;
+        if (ROW) { c = idx / a.out_len; e = idx - c * a.out_len; }
+        else { e = idx / NL; c = idx - e * NL; }
+        const int col = col0 + c;
+        if (col < a.ncols)
+            dst[(int64_t)col * a.out_cstride + (int64_t)e * a.out_estride] = cscale(buf[(e + a.out_lo) * lstr + c], sc);
+    }
+}
+
+// ------------------------------------------------------------------------------------
+template <typename T, typename TIn, int NL, class E>
+__global__ void __launch_bounds__(E::kMaxThreads) k_r2c_rows(const TIn *__restrict__ in, cplx<T> *__restrict__ out,
+                                                             R2CArgs a, const cplx<T> *__restrict__ twg) {
+    typedef cplx<T> V;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V *tw = reinterpret_cast<V *>(smem_raw);
+    const int L = E::kLen ? E::kLen : a.p.L;
+    V *buf = tw + L;
+    constexpr int lstr = NL + 1;
+    const int nthreads = blockDim.x, tid = threadIdx.x;
+    const int64_t row0 = (int64_t)blockIdx.x * (2 * NL);
+    load_twiddles(tw, twg, L);
+    for (int idx = tid; idx < 2 * NL * L; idx += nthreads) {
+        const int rr = idx / L, e = idx - rr * L;
+        const int64_t row = row0 + rr;
+        T v = 0;
+        if (row < a.nrows && e < a.nin) v = (T)in[row * a.in_rstride + e];
+        T *slot = reinterpret_cast<T *>(&buf[e * lstr + (rr >> 1)]);
+        slot[rr & 1] = v;
+    }
+    __syncthreads();
+    E::template run<V, NL>(buf, a.p, tw, +1);
+    const int nh = L / 2 + 1;
+    for (int idx = tid; idx < 2 * NL * nh; idx += nthreads) {
+        const int rr = idx / nh, k = idx - rr * nh;
+        const int64_t row = row0 + rr;
+        if (row >= a.nrows) continue;
+        const int line = rr >> 1;
+        const V Z = buf[k * lstr + line];
+        const V Zm = buf[((L - k) % L) * lstr + line];
+        V r;
+        if ((rr & 1) == 0) {  // (Z + conj Zm)/2
+            r.x = (T)0.5 * (Z.x + Zm.x);
+            r.y = (T)0.5 * (Z.y - Zm.y);
+        } else {  // (Z - conj Zm)/(2i)
+            r.x = (T)0.5 * (Z.y + Zm.y);
+            r.y = (T)0.5 * (Zm.x - Z.x);
+        }
+        out[row * a.out_rstride + k] = r;
+    }
+}
+
+// ------------------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void write_dest(const OutDest &d, int64_t gidx, T val) {
+    if (d.kind == 0) reinterpret_cast<T *>(d.ptr)[gidx * 4 + d.slot] = (T)(d.coef * val);
+    else if (d.kind == 1) reinterpret_cast<double *>(d.ptr)[gidx] = d.coef * (double)val;
+    else reinterpret_cast<T *>(d.ptr)[gidx] = (T)(d.coef * val);
+}
+
+template <typename T, int NL, class E>
+__global__ void __launch_bounds__(E::kMaxThreads) k_c2r_rows(const cplx<T> *__restrict__ in, C2RArgs a,
+                                                             const cplx<T> *__restrict__ twg) {
+    typedef cplx<T> V;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V *tw = reinterpret_cast<V *>(smem_raw);
+    const int L = E::kLen ? E::kLen : a.p.L;
+    V *buf = tw + L;
+    constexpr int lstr = NL + 1;
+    const int nthreads = blockDim.x, tid = threadIdx.x;
+    const int64_t row0 = (int64_t)blockIdx.x * (2 * NL);
+    const int half = L / 2;
+    load_twiddles(tw, twg, L);
+    for (int c = 0; c < a.ncomp; ++c) {
+        const V *src = in + (int64_t)c * a.in_cstride;
+        for (int idx = tid; idx < NL * L; idx += nthreads) {
+            const int line = idx / L, k = idx - line * L;
+            const int64_t ra = row0 + 2 * line, rb = ra + 1;
+            const int kk = k <= half ? k : L - k;
+            V A = mk<T>(0, 0), B = mk<T>(0, 0);
+            if (ra < a.nrows) A = src[ra * a.in_rstride + kk];
+            if (rb < a.nrows) B = src[rb * a.in_rstride + kk];
+            if (k == 0 || k == half) { A.y = 0; B.y = 0; }
+            if (k > half) { A.y = -A.y; B.y = -B.y; }
+            buf[k * lstr + line] = mk<T>(A.x - B.y, A.y + B.x);
+        }
+        __syncthreads();
+        E::template run<V, NL>(buf, a.p, tw, -1);
+        for (int idx = tid; idx < 2 * NL * a.nout; idx += nthreads) {
+            const int rr = idx / a.nout, x = idx - rr * a.nout;
+            const int64_t row = row0 + rr;
+            if (row >= a.nrows) continue;
+            const V z = buf[x * lstr + (rr >> 1)];
+            const T val = (rr & 1) ? z.y : z.x;
+            const int64_t gidx = row * a.nout + x;
+            for (int d = 0; d < a.ndest[c]; ++d) write_dest<T>(a.dest[c][d], gidx, val);
+        }
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ cplx<T> g_lookup(const GSpecDev &g, int kx, int ky, int kz, int nxh,
+                                            int Ny, int ny, int Nz, int nz) {
+    int yy = ky, zz = kz;
+    bool neg = false;
+    if (g.sym_y && ky > ny) { yy = Ny - ky; neg ^= (g.par_y < 0); }
+    if (g.sym_z && kz > nz) { zz = Nz - kz; neg ^= (g.par_z < 0); }
+    const int64_t idx = ((int64_t)zz * g.dimy + yy) * nxh + kx;
+    if (g.real_valued) {
+        T s = __ldg(reinterpret_cast<const T *>(g.data) + idx);
+        if (neg) s = -s;
+        return g.imag_unit ? mk<T>(0, s) : mk<T>(s, 0);
+    }
+    cplx<T> v = __ldg(reinterpret_cast<const cplx<T> *>(g.data) + idx);
+    if (neg) { v.x = -v.x; v.y = -v.y; }
+    return v;
+}
+
+template <typename T, int NL, class E>
+__global__ void __launch_bounds__(E::kMaxThreads) k_zconv(const cplx<T> *__restrict__ in, cplx<T> *__restrict__ out,
+                                                          ZConvArgs a, const cplx<T> *__restrict__ twg) {
+    typedef cplx<T> V;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V *tw = reinterpret_cast<V *>(smem_raw);
+    const int L = E::kLen ? E::kLen : a.p.L;
+    V *rhat = tw + L;
+    constexpr int lstr = NL + 1;
+    V *buf = rhat + L * lstr;
+    const int nthreads = blockDim.x, tid = threadIdx.x;
+    const int col0 = blockIdx.x * NL;
+    load_twiddles(tw, twg, L);
+    for (int idx = tid; idx < NL * L; idx += nthreads) {
+        const int e = idx / NL, c = idx - e * NL;
+        const int col = col0 + c;
+        V v = mk<T>(0, 0);
+        if (e < a.nz && col < a.ncols) v = in[(int64_t)e * a.in_estride + col];
+        rhat[e * lstr + c] = v;
+    }
+    __syncthreads();
+    E::template run<V, NL>(rhat, a.p, tw, +1);
+    for (int o = 0; o < a.nout; ++o) {
+        const int gd = a.gdir[o], gi = a.gimg[o];
+        const T icoef = (T)a.img_coef[o];
+        for (int idx = tid; idx < NL * L; idx += nthreads) {
+            const int e = idx / NL, c = idx - e * NL;
+            const int col = min(col0 + c, a.ncols - 1);
+            const int ky = col / a.nxh, kx = col - ky * a.nxh;
+            V S = mk<T>(0, 0);
+            if (gd >= 0) S = cmul(rhat[e * lstr + c], g_lookup<T>(a.g[gd], kx, ky, e, a.nxh, a.Ny, a.ny, L, a.nz));
+            if (gi >= 0) {
+                // spectrum of -rho flipped in z: -w^((nz-1) kz) * rho_hat(-kz)
+                const V rm = rhat[((L - e) % L) * lstr + c];
+                const V ph = tw[(int)(((int64_t)a.img_phase_mul * e) % L)];
+                V ri = cmul(ph, rm);
+                ri.x = -ri.x * icoef;
+                ri.y = -ri.y * icoef;
+                S = cadd(S, cmul(ri, g_lookup<T>(a.g[gi], kx, ky, e, a.nxh, a.Ny, a.ny, L, a.nz)));
+            }
+            buf[e * lstr + c] = S;
+        }
+        __syncthreads();
+        E::template run<V, NL>(buf, a.p, tw, -1);
+        V *dst = out + (int64_t)o * a.out_cstride;
+        for (int idx = tid; idx < NL * a.nz; idx += nthreads) {
+            const int e = idx / NL, c = idx - e * NL;
+            const int col = col0 + c;
+            if (col < a.ncols) dst[(int64_t)e * a.out_estride + col] = buf[e * lstr + c];
+        }
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// Launchers.  Shared memory above 48 KB needs the opt-in attribute, set per kernel.
+template <typename K> static int set_smem(K kern, size_t bytes) {
+    if (bytes > 227 * 1024) return OSC_E_INVALID;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    return e == cudaSuccess ? OSC_OK : OSC_E_CUDA;
+}
+static inline int launch_ok() { return cudaGetLastError() == cudaSuccess ? OSC_OK : OSC_E_CUDA; }
+
+// Runtime-engine NL: a whole number of threads, <= 256 threads, buffers within budget.
+static int pick_nl_rt(int L, int nl_max, size_t elem, int nbuf) {
+    for (int nl = nl_max; nl >= 2; nl /= 2) {
+        if ((L * nl) % FFT_EPT != 0 || fft_threads(L, nl) > FftRuntime::kMaxThreads) continue;
+        if ((size_t)nbuf * L * (nl + 1) * elem + L * elem > 110 * 1024 && nl > 2) continue;
+        return nl;
+    }
+    return 0;
+}
+
+// Calls f(std::integral_constant<int, NL>) for the engine's lines-per-CTA.
+template <typename T, class E, class F> static int with_nl(int L, int nbuf, int nl_max, int nl_req, F &&f) {
+    if constexpr (E::kLen > 0) {
+        (void)L;
+        (void)nl_req;
+        constexpr int NL = nl_static(E::kLen, sizeof(T) == 4 ? 16 : 8, (int)sizeof(cplx<T>), 2);
+        constexpr int NL1 = nl_static(E::kLen, sizeof(T) == 4 ? 16 : 8, (int)sizeof(cplx<T>), 1);
+        if (nbuf >= 2) return f(std::integral_constant<int, (NL < 8 ? NL : 8)>{});
+        return f(std::integral_constant<int, NL1>{});
+    } else {
+        int nl = nl_req > 0 ? nl_req : pick_nl_rt(L, nl_max, sizeof(cplx<T>), nbuf);
+        switch (nl) {
+        case 16: return f(std::integral_constant<int, 16>{});
+        case 8: return f(std::integral_constant<int, 8>{});
+        case 4: return f(std::integral_constant<int, 4>{});
+        case 2: return f(std::integral_constant<int, 2>{});
+        default: return OSC_E_FFT_SIZE;
+        }
+    }
+}
+
+template <typename T>
+int launch_lines(const cplx<T> *in, cplx<T> *out, const LineArgs &a, int nplanes, int ncomp,
+                 bool row_mode, const cplx<T> *tw, cudaStream_t st) {
+    const int L = a.p.L;
+    return dispatch_fft_len(L, [&](auto eng) -> int {
+        using E = decltype(eng);
+        return with_nl<T, E>(L, 1, sizeof(T) == 4 ? 16 : 8, 0, [&](auto nlc) -> int {
+            constexpr int NL = decltype(nlc)::value;
+            const int nt = fft_threads(L, NL);
+            if (nt < 1 || nt > E::kMaxThreads || (L * NL) % FFT_EPT) return OSC_E_FFT_SIZE;
+            const size_t sm = sizeof(cplx<T>) * ((size_t)L + (size_t)L * (NL + 1));
+            dim3 grid((unsigned)ceil_div(a.ncols, NL), (unsigned)nplanes, (unsigned)ncomp);
+            if (row_mode) {
+                auto kern = k_lines<T, NL, true, E>;
+                int rc = set_smem(kern, sm);
+                if (rc) return rc;
+                kern<<<grid, nt, sm, st>>>(in, out, a, tw);
+            } else {
+                auto kern = k_lines<T, NL, false, E>;
+                int rc = set_smem(kern, sm);
+                if (rc) return rc;
+                kern<<<grid, nt, sm, st>>>(in, out, a, tw);
+            }
+            return launch_ok();
+        });
+    });
+}
+
+template <typename T, typename TIn>
+int launch_r2c_rows(const TIn *in, cplx<T> *out, const R2CArgs &a, const cplx<T> *tw, cudaStream_t st) {
+    const int L = a.p.L;
+    return dispatch_fft_len(L, [&](auto eng) -> int {
+        using E = decltype(eng);
+        return with_nl<T, E>(L, 1, sizeof(T) == 4 ? 16 : 8, 0, [&](auto nlc) -> int {
+            constexpr int NL = decltype(nlc)::value;
+            const int nt = fft_threads(L, NL);
+            if (nt < 1 || nt > E::kMaxThreads || (L * NL) % FFT_EPT) return OSC_E_FFT_SIZE;
+            const size_t sm = sizeof(cplx<T>) * ((size_t)L + (size_t)L * (NL + 1));
+            auto kern = k_r2c_rows<T, TIn, NL, E>;
+            int rc = set_smem(kern, sm);
+            if (rc) return rc;
+            kern<<<(unsigned)ceil_div(a.nrows, 2 * NL), nt, sm, st>>>(in, out, a, tw);
+            return launch_ok();
+        });
+    });
+}
+
+template <typename T>
+int launch_c2r_rows(const cplx<T> *in, const C2RArgs &a, const cplx<T> *tw, cudaStream_t st) {
+    const int L = a.p.L;
+    return dispatch_fft_len(L, [&](auto eng) -> int {
+        using E = decltype(eng);
+        return with_nl<T, E>(L, 1, sizeof(T) == 4 ? 16 : 8, 0, [&](auto nlc) -> int {
+            constexpr int NL = decltype(nlc)::value;
+            const int nt = fft_threads(L, NL);
+            if (nt < 1 || nt > E::kMaxThreads || (L * NL) % FFT_EPT) return OSC_E_FFT_SIZE;
+            const size_t sm = sizeof(cplx<T>) * ((size_t)L + (size_t)L * (NL + 1));
+            auto kern = k_c2r_rows<T, NL, E>;
+            int rc = set_smem(kern, sm);
+            if (rc) return rc;
+            kern<<<(unsigned)ceil_div(a.nrows, 2 * NL), nt, sm, st>>>(in, a, tw);
+            return launch_ok();
+        });
+    });
+}
+
+template <typename T>
+int launch_zconv(const cplx<T> *in, cplx<T> *out, const ZConvArgs &a, const cplx<T> *tw, int nl,
+                 cudaStream_t st) {
+    const int L = a.p.L;
+    return dispatch_fft_len(L, [&](auto eng) -> int {
+        using E = decltype(eng);
+        return with_nl<T, E>(L, 2, sizeof(T) == 4 ? 8 : 4, nl, [&](auto nlc) -> int {
+            constexpr int NL = decltype(nlc)::value;
+            const int nt = fft_threads(L, NL);
+            if (nt < 1 || nt > E::kMaxThreads || (L * NL) % FFT_EPT) return OSC_E_FFT_SIZE;
+            const size_t sm = sizeof(cplx<T>) * ((size_t)L + 2 * (size_t)L * (NL + 1));
+            auto kern = k_zconv<T, NL, E>;
+            int rc = set_smem(kern, sm);
+            if (rc) return rc;
+            kern<<<(unsigned)ceil_div(a.ncols, NL), nt, sm, st>>>(in, out, a, tw);
+            return launch_ok();
+        });
+    });
+}
+
+// Explicit instantiations.
+template int launch_lines<float>(const cplx<float> *, cplx<float> *, const LineArgs &, int, int, bool,
+                                 const cplx<float> *, cudaStream_t);
+template int launch_lines<double>(const cplx<double> *, cplx<double> *, const LineArgs &, int, int, bool,
+                                  const cplx<double> *, cudaStream_t);
+template int launch_r2c_rows<float, float>(const float *, cplx<float> *, const R2CArgs &, const cplx<float> *, cudaStream_t);
+template int launch_r2c_rows<float, double>(const double *, cplx<float> *, const R2CArgs &, const cplx<float> *, cudaStream_t);
+template int launch_r2c_rows<double, double>(const double *, cplx<double> *, const R2CArgs &, const cplx<double> *, cudaStream_t);
+template int launch_c2r_rows<float>(const cplx<float> *, const C2RArgs &, const cplx<float> *, cudaStream_t);
+template int launch_c2r_rows<double>(const cplx<double> *, const C2RArgs &, const cplx<double> *, cudaStream_t);
+template int launch_zconv<float>(const cplx<float> *, cplx<float> *, const ZConvArgs &, const cplx<float> *, int, cudaStream_t);
+template int launch_zconv<double>(const cplx<double> *, cplx<double> *, const ZConvArgs &, const cplx<double> *, int, cudaStream_t);
+
+}  // namespace osc

@@ -1,0 +1,98 @@
+// fft_kernels.cuh -- argument blocks and launchers of the FFT-based convolution kernels.
+#pragma once
+
+#include "osc_fft.cuh"
+
+namespace osc {
+
+// Generic batched C2C transform of lines along one axis, with zero-padded input window
+// [0, in_len) and output window [out_lo, out_lo + out_len).  Element (plane, col, e) sits at
+// plane*pstride + col*cstride + e*estride; blockIdx.z selects one of several component
+// arrays (zstride apart).  ROW=true: lines are contiguous rows (global accesses walk e);
+// ROW=false: lines are adjacent columns (global accesses walk col).
+struct LineArgs {
+    FFTPlan p;
+    int sign;
+    int ncols;
+    int in_len, out_lo, out_len;
+    int64_t in_pstride, in_cstride, in_estride, in_zstride;
+    int64_t out_pstride, out_cstride, out_estride, out_zstride;
+    double scale;
+};
+
+// Forward transform of real rows (length nin, zero-padded to L) packed two per complex
+// line; writes the L/2+1 non-negative frequencies of every row.
+struct R2CArgs {
+    FFTPlan p;
+    int nin;
+    int64_t nrows;
+    int64_t in_rstride;   // elements between rows of the real input
+    int64_t out_rstride;  // complex elements between output rows
+};
+
+// Where the real result of one inverse component goes.
+struct OutDest {
+    void *ptr;        // nullptr = unused
+    int kind;         // 0: slot of a vec4<T> grid, 1: double plane, 2: T plane
+    int slot;         // vec4 component (kind 0)
+    double coef;      // multiplier
+};
+constexpr int MAX_OUT = 6;
+constexpr int MAX_DEST = 3;
+
+// Inverse transform of Hermitian rows (L/2+1 stored frequencies) to real rows, keeping
+// x in [0, nout), for ncomp component arrays; each component's result goes to up to
+// MAX_DEST destinations (grid index = row*nout + x, i.e. [z][y][x]).
+struct C2RArgs {
+    FFTPlan p;
+    int nout;
+    int64_t nrows;
+    int64_t in_rstride, in_cstride;
+    int ncomp;
+    int ndest[MAX_OUT];
+    OutDest dest[MAX_OUT][MAX_DEST];
+};
+
+// Stored Green spectrum of one kernel component on the half-spectrum grid
+// kx in [0, nx], ky in [0, Ny), kz in [0, Nz).  Axes with sym_* hold only k <= n and the
+// value at N-k is par_* times the value at k.  real_valued spectra store one T per point
+// meaning s (imag_unit=0) or i*s (imag_unit=1); others store cplx<T>.
+struct GSpecDev {
+    const void *data;
+    int real_valued, imag_unit;
+    int sym_y, sym_z, par_y, par_z;
+    int dimy, dimz;
+};
+
+// Fused z pass of the free-space convolution: forward transform of each (kx,ky) column
+// (nz non-zero planes, length Nz), multiply by stored Green spectra (optionally adding the
+// mirrored-image term), inverse transform, keep z in [0, nz) of every output.
+struct ZConvArgs {
+    FFTPlan p;       // length Nz
+    int nz;
+    int ncols;       // (nx+1)*Ny
+    int nxh, Ny, ny;
+    int64_t in_estride;   // complex elements between z planes of the input (= ncols)
+    int64_t out_estride;  // between z planes of the output
+    int64_t out_cstride;  // between output components
+    int nout;
+    int gdir[MAX_OUT];    // index into g[] of the direct term (-1 none)
+    int gimg[MAX_OUT];    // index into g[] of the image term (-1 none)
+    double img_coef[MAX_OUT];
+    int img_phase_mul;    // image spectrum = -w^(img_phase_mul*kz) * rho_hat(-kz)
+    int ng;
+    GSpecDev g[8];
+};
+
+template <typename T>
+int launch_lines(const cplx<T> *in, cplx<T> *out, const LineArgs &a, int nplanes, int ncomp,
+                 bool row_mode, const cplx<T> *tw, cudaStream_t st);
+template <typename T, typename TIn>
+int launch_r2c_rows(const TIn *in, cplx<T> *out, const R2CArgs &a, const cplx<T> *tw, cudaStream_t st);
+template <typename T>
+int launch_c2r_rows(const cplx<T> *in, const C2RArgs &a, const cplx<T> *tw, cudaStream_t st);
+template <typename T>
+int launch_zconv(const cplx<T> *in, cplx<T> *out, const ZConvArgs &a, const cplx<T> *tw,
+                 int nl, cudaStream_t st);
+
+}  // namespace osc

@@ -1,0 +1,309 @@
+// particle_kernels.cu -- CIC deposition, CIC interpolation, bounding box and charge sum.
+#include "particle_kernels.cuh"
+
+namespace osc {
+
+static inline int ok() { return cudaGetLastError() == cudaSuccess ? OSC_OK : OSC_E_CUDA; }
+static inline unsigned nblocks(int64_t n, int bs, int64_t cap = (1 << 20)) {
+    int64_t b = (n + bs - 1) / bs;
+    if (b < 1) b = 1;
+    if (b > cap) b = cap;
+    return (unsigned)b;
+}
+#define GRID_STRIDE(i, n) for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (n); i += (int64_t)gridDim.x * blockDim.x)
+
+__device__ __forceinline__ void atomic_add_t(float *p, double v) { atomicAdd(p, (float)v); }
+__device__ __forceinline__ void atomic_add_t(double *p, double v) { atomicAdd(p, v); }
+
+// Warp-aggregated counter increment.
+__device__ __forceinline__ void count_one(unsigned long long *c, bool pred) {
+    const unsigned mask = __ballot_sync(__activemask(), pred);
+    if (pred && (threadIdx.x & 31) == __ffs(mask) - 1) atomicAdd(c, (unsigned long long)__popc(mask));
+}
+
+template <typename TA>
+__global__ void __launch_bounds__(256) k_deposit(DepositArgs a, TA *__restrict__ rho,
+                                                 unsigned long long *__restrict__ counters) {
+    const int64_t plane = (int64_t)a.nx * a.ny;
+    GRID_STRIDE(m, a.np) {
+        bool skip = false, outside = false, nonfinite = false;
+        if (a.lost && a.lost[m] != 0.0) skip = true;
+        const double xm = a.x[m], ym = a.y[m], zm = a.z[m];
+        if (!skip && a.check_finite && !(isfinite(xm) && isfinite(ym) && isfinite(zm))) {
+            nonfinite = true;
+            skip = true;
+        }
+        double fx, fy, fz, ab, de, gh;
+        int i = 0, j = 0, k = 0;
+        if (!skip) {
+            if (a.mode == 0) {
+                fx = floor((xm - a.xmin) * a.dxi + 1);
+                fy = floor((ym - a.ymin) * a.dyi + 1);
+                fz = floor((zm - a.zmin) * a.dzi + 1);
+                ab = ((a.xmin - xm) + fx * a.dx) * a.dxi;
+                de = ((a.ymin - ym) + fy * a.dy) * a.dyi;
+                gh = ((a.zmin - zm) + fz * a.dz) * a.dzi;
+                // array offsets; the 2x2x2 stencil must lie inside the array
+                outside = !(fx >= a.nlo[0] && fx + 1 <= a.nhi[0] && fy >= a.nlo[1] && fy + 1 <= a.nhi[1] &&
+                            fz >= a.nlo[2] && fz + 1 <= a.nhi[2]);
+            } else {
+                fx = floor((xm - a.xmin) * a.dxi + a.nlogbl[0]);
+                fy = floor((ym - a.ymin) * a.dyi + a.nlogbl[1]);
+                fz = floor((zm - a.zmin) * a.dzi + a.nlogbl[2]);
+                ab = ((a.xmin - xm) + (fx - a.nlogbl[0] + 1) * a.dx) * a.dxi;
+                de = ((a.ymin - ym) + (fy - a.nlogbl[1] + 1) * a.dy) * a.dyi;
+                gh = ((a.zmin - zm) + (fz - a.nlogbl[2] + 1) * a.dz) * a.dzi;
+                // reference check (ip < ilo or ip > size) and the array bound of ip+1
+                outside = !(fx >= a.nlo[0] && fx <= a.nx && fy >= a.nlo[1] && fy <= a.ny && fz >= a.nlo[2] &&
+                            fz <= a.nz) ||
+                          !(fx - a.nlo[0] + 1 < a.nx && fy - a.nlo[1] + 1 < a.ny && fz - a.nlo[2] + 1 < a.nz);
+            }
+            if (!outside) {
+                i = (int)fx - a.nlo[0];
+                j = (int)fy - a.nlo[1];
+                k = (int)fz - a.nlo[2];
+            }
+        }
+        count_one(&counters[0], !skip && outside);
+        count_one(&counters[1], nonfinite);
+        if (skip || outside) continue;
+        const double c = a.mode == 0 ? (a.q ? a.q[m] : a.charge1) : 1.0;
+        const double omab = 1. - ab, omde = 1. - de, omgh = 1. - gh;
+        TA *r0 = rho + i + (int64_t)a.nx * j + plane * k;
+        atomic_add_t(r0, ab * de * gh * c);
+        atomic_add_t(r0 + a.nx, ab * omde * gh * c);
+        atomic_add_t(r0 + a.nx + plane, ab * omde * omgh * c);
+        atomic_add_t(r0 + plane, ab * de * omgh * c);
+        atomic_add_t(r0 + 1 + plane, omab * de * omgh * c);
+        atomic_add_t(r0 + 1 + a.nx + plane, omab * omde * omgh * c);
+        atomic_add_t(r0 + 1 + a.nx, omab * omde * gh * c);
+        atomic_add_t(r0 + 1, omab * de * gh * c);
+    }
+}
+
+template <typename TA>
+int launch_deposit(const DepositArgs &a, TA *rho, unsigned long long *counters, cudaStream_t st) {
+    if (a.np <= 0) return OSC_OK;
+    k_deposit<TA><<<nblocks(a.np, 256, 148 * 64), 256, 0, st>>>(a, rho, counters);
+    return ok();
+}
+template int launch_deposit<float>(const DepositArgs &, float *, unsigned long long *, cudaStream_t);
+template int launch_deposit<double>(const DepositArgs &, double *, unsigned long long *, cudaStream_t);
+
+// ------------------------------------------------------------------------------------
+struct Cell {
+    int i, j, k;
+    double ab, de, gh;
+};
+
+__device__ __forceinline__ bool locate(const InterpArgs &a, double x, double y, double z, Cell &c) {
+    const double pos[3] = {x, y, z};
+    int idx[3];
+    double w[3];
+    bool flag = false;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        double f = floor((pos[d] - a.min[d]) * a.hinv[d] + 1);
+        const double hi = (double)(a.nhi[d] - 1);
+        if (!(f >= 1.0 && f <= hi)) {  // NaN lands here too
+            flag = true;
+            f = (f < 1.0 || f != f) ? 1.0 : hi;
+        }
+        const double lo_arr = (double)a.nlo[d];
+        if (f < lo_arr) { flag = true; f = lo_arr; }
+        w[d] = ((a.min[d] - pos[d]) + f * a.delta[d]) * a.hinv[d];
+        idx[d] = (int)f - a.nlo[d];
+    }
+    c.i = idx[0]; c.j = idx[1]; c.k = idx[2];
+    c.ab = w[0]; c.de = w[1]; c.gh = w[2];
+    return flag;
+}
+
+template <typename T>
+__device__ __forceinline__ void load_node(const vec4<T> *g, int64_t n, double &a, double &b, double &c) {
+    const vec4<T> v = g[n];
+    a = (double)v.x;
+    b = (double)v.y;
+    c = (double)v.z;
+}
+
+template <typename T, typename TO>
+__global__ void __launch_bounds__(256) k_interp_vec4(InterpArgs a, const vec4<T> *__restrict__ g, TO *__restrict__ E,
+                                                     unsigned long long *__restrict__ nclamp) {
+    const int64_t plane = (int64_t)a.nx * a.ny;
+    GRID_STRIDE(m, a.np) {
+        Cell c;
+        const bool fl = locate(a, a.x[m], a.y[m], a.z[m], c);
+        count_one(nclamp, fl);
+        const int64_t n0 = c.i + (int64_t)a.nx * c.j + plane * c.k;
+        const double ab = c.ab, de = c.de, gh = c.gh;
+        const double omab = 1. - ab, omde = 1. - de, omgh = 1. - gh;
+        const int64_t nodes[8] = {n0, n0 + a.nx, n0 + a.nx + plane, n0 + plane,
+                                  n0 + 1 + plane, n0 + 1 + a.nx + plane, n0 + 1 + a.nx, n0 + 1};
+        const double wts[8] = {ab * de * gh, ab * omde * gh, ab * omde * omgh, ab * de * omgh,
+                               omab * de * omgh, omab * omde * omgh, omab * omde * gh, omab * de * gh};
+        double ex = 0, ey = 0, ez = 0;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            double vx, vy, vz;
+            load_node<T>(g, nodes[q], vx, vy, vz);
+            ex = ex + vx * wts[q];
+            ey = ey + vy * wts[q];
+            ez = ez + vz * wts[q];
+        }
+        E[3 * m] = (TO)ex;
+        E[3 * m + 1] = (TO)ey;
+        E[3 * m + 2] = (TO)ez;
+    }
+}
+
+template <typename T>
+int launch_interp_vec4(const InterpArgs &a, const void *E4, double *E, unsigned long long *nclamp, cudaStream_t st) {
+    if (a.np <= 0) return OSC_OK;
+    k_interp_vec4<T, double><<<nblocks(a.np, 256, 148 * 64), 256, 0, st>>>(a, reinterpret_cast<const vec4<T> *>(E4),
+                                                                            E, nclamp);
+    return ok();
+}
+template <typename T>
+int launch_interp_vec4_any(const InterpArgs &a, const void *E4, void *E, int out_f32, unsigned long long *nclamp,
+                           cudaStream_t st) {
+    if (a.np <= 0) return OSC_OK;
+    if (out_f32)
+        k_interp_vec4<T, float><<<nblocks(a.np, 256, 148 * 64), 256, 0, st>>>(
+            a, reinterpret_cast<const vec4<T> *>(E4), reinterpret_cast<float *>(E), nclamp);
+    else
+        k_interp_vec4<T, double><<<nblocks(a.np, 256, 148 * 64), 256, 0, st>>>(
+            a, reinterpret_cast<const vec4<T> *>(E4), reinterpret_cast<double *>(E), nclamp);
+    return ok();
+}
+template int launch_interp_vec4<float>(const InterpArgs &, const void *, double *, unsigned long long *, cudaStream_t);
+template int launch_interp_vec4<double>(const InterpArgs &, const void *, double *, unsigned long long *, cudaStream_t);
+template int launch_interp_vec4_any<float>(const InterpArgs &, const void *, void *, int, unsigned long long *, cudaStream_t);
+template int launch_interp_vec4_any<double>(const InterpArgs &, const void *, void *, int, unsigned long long *, cudaStream_t);
+
+// Three double planes [3][N], reference order of the 8-term sum per component.
+__global__ void __launch_bounds__(256) k_interp_planes(InterpArgs a, const double *__restrict__ F,
+                                                       double *__restrict__ out,
+                                                       unsigned long long *__restrict__ nclamp) {
+    const int64_t plane = (int64_t)a.nx * a.ny;
+    const int64_t N = plane * a.nz;
+    GRID_STRIDE(m, a.np) {
+        Cell c;
+        const bool fl = locate(a, a.x[m], a.y[m], a.z[m], c);
+        count_one(nclamp, fl);
+        const int64_t n0 = c.i + (int64_t)a.nx * c.j + plane * c.k;
+        const double ab = c.ab, de = c.de, gh = c.gh;
+#pragma unroll
+        for (int comp = 0; comp < 3; ++comp) {
+            const double *A = F + comp * N;
+            double v = A[n0] * ab * de * gh;
+            v = v + A[n0 + a.nx] * ab * (1. - de) * gh;
+            v = v + A[n0 + a.nx + plane] * ab * (1. - de) * (1. - gh);
+            v = v + A[n0 + plane] * ab * de * (1. - gh);
+            v = v + A[n0 + 1 + plane] * (1. - ab) * de * (1. - gh);
+            v = v + A[n0 + 1 + a.nx + plane] * (1. - ab) * (1. - de) * (1. - gh);
+            v = v + A[n0 + 1 + a.nx] * (1. - ab) * (1. - de) * gh;
+            v = v + A[n0 + 1] * (1. - ab) * de * gh;
+            out[3 * m + comp] = v;
+        }
+    }
+}
+int launch_interp_planes(const InterpArgs &a, const double *F, double *out, unsigned long long *nclamp,
+                         cudaStream_t st) {
+    if (a.np <= 0) return OSC_OK;
+    k_interp_planes<<<nblocks(a.np, 256, 148 * 64), 256, 0, st>>>(a, F, out, nclamp);
+    return ok();
+}
+
+// ------------------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long ord_key(double v) {
+    const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+    return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double ord_val(unsigned long long u) {
+    const unsigned long long b = (u >> 63) ? (u & 0x7fffffffffffffffull) : ~u;
+    return __longlong_as_double((long long)b);
+}
+
+__global__ void k_bbox_init(unsigned long long *keys, unsigned long long *nonfinite) {
+    if (threadIdx.x < 6) keys[threadIdx.x] = (threadIdx.x & 1) ? 0ull : ~0ull;
+    if (threadIdx.x == 0) *nonfinite = 0;
+}
+__global__ void __launch_bounds__(256) k_bbox(int64_t np, const double *__restrict__ x, const double *__restrict__ y,
+                                              const double *__restrict__ z, unsigned long long *keys,
+                                              unsigned long long *nonfinite) {
+    unsigned long long lo[3] = {~0ull, ~0ull, ~0ull}, hi[3] = {0, 0, 0};
+    unsigned long long bad = 0;
+    const double *p[3] = {x, y, z};
+    GRID_STRIDE(m, np) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const double v = p[d][m];
+            if (!isfinite(v)) { ++bad; continue; }
+            const unsigned long long k = ord_key(v);
+            lo[d] = k < lo[d] ? k : lo[d];
+            hi[d] = k > hi[d] ? k : hi[d];
+        }
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        for (int off = 16; off; off >>= 1) {
+            const unsigned long long a = __shfl_xor_sync(0xffffffffu, lo[d], off);
+            const unsigned long long b = __shfl_xor_sync(0xffffffffu, hi[d], off);
+            lo[d] = a < lo[d] ? a : lo[d];
+            hi[d] = b > hi[d] ? b : hi[d];
+        }
+    }
+    for (int off = 16; off; off >>= 1) bad += __shfl_xor_sync(0xffffffffu, bad, off);
+    if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            atomicMin(&keys[2 * d], lo[d]);
+            atomicMax(&keys[2 * d + 1], hi[d]);
+        }
+        if (bad) atomicAdd(nonfinite, bad);
+    }
+}
+__global__ void k_bbox_final(const unsigned long long *keys, double *bb) {
+    if (threadIdx.x < 6) bb[threadIdx.x] = ord_val(keys[threadIdx.x]);
+}
+int launch_bbox(int64_t np, const double *x, const double *y, const double *z, unsigned long long *keys, double *bb,
+                unsigned long long *nonfinite, cudaStream_t st) {
+    k_bbox_init<<<1, 32, 0, st>>>(keys, nonfinite);
+    if (np > 0) k_bbox<<<nblocks(np, 256, 148 * 16), 256, 0, st>>>(np, x, y, z, keys, nonfinite);
+    k_bbox_final<<<1, 32, 0, st>>>(keys, bb);
+    return ok();
+}
+
+// Deterministic two-pass sum: 1024 fixed partial sums in index order, then one block.
+__global__ void __launch_bounds__(256) k_sum_partial(int64_t n, const double *__restrict__ q, double *partials) {
+    __shared__ double sh[256];
+    double s = 0;
+    const int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
+    const int64_t beg = blockIdx.x * chunk, end = min(n, beg + chunk);
+    for (int64_t m = beg + threadIdx.x; m < end; m += blockDim.x) s += q[m];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = 128; w; w >>= 1) {
+        if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partials[blockIdx.x] = sh[0];
+}
+__global__ void k_sum_final(const double *partials, int np, double *out) {
+    __shared__ double sh[1024];
+    sh[threadIdx.x] = threadIdx.x < np ? partials[threadIdx.x] : 0.0;
+    __syncthreads();
+    for (int w = 512; w; w >>= 1) {
+        if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = sh[0];
+}
+int launch_sum(int64_t n, const double *q, double *partials, double *out, cudaStream_t st) {
+    k_sum_partial<<<1024, 256, 0, st>>>(n, q, partials);
+    k_sum_final<<<1, 1024, 0, st>>>(partials, 1024, out);
+    return ok();
+}
+
+}  // namespace osc

@@ -1,0 +1,57 @@
+// particle_kernels.cuh -- charge deposition, field interpolation and particle reductions.
+#pragma once
+
+#include "osc_common.cuh"
+
+namespace osc {
+
+// CIC deposition.  mode 0 follows deposit_particles (code/open_spacecharge_mod.f90:257-283):
+// ip = floor((x-xmin)/dx + 1), low-node weight ab = ((xmin-x) + ip*dx)/dx, charge per
+// particle.  mode 1 follows depose_rho_scalar (code/test_mod.f90:442-470): ip uses the
+// global lower index nlogbl, lost particles are skipped, weights carry no charge (the grid
+// is scaled afterwards).  Particles whose stencil leaves the array are counted, not written.
+struct DepositArgs {
+    int64_t np;
+    const double *x, *y, *z, *q, *lost;
+    double xmin, ymin, zmin, dx, dy, dz, dxi, dyi, dzi;
+    int nlo[3], nhi[3], nlogbl[3];
+    int nx, ny, nz;
+    int mode;
+    double charge1;  // charge per particle when q == nullptr (mode 0)
+    int check_finite;
+};
+// counters[0] += outside particles, counters[1] += non-finite particles
+template <typename TA>
+int launch_deposit(const DepositArgs &a, TA *rho, unsigned long long *counters, cudaStream_t st);
+
+// Transpose of interpolation for the adjoint: scatter per-particle 3-vectors w_p onto
+// three grids with the CIC weights (same stencil and clamping as interpolation).
+// CIC gather (interpolate_field, code/open_spacecharge_mod.f90:311-390): clamp cells to
+// [1, nhi-1] (and the array), weights computed after clamping, 8-node sum in the
+// reference's order.  Source: a vec4<T> interleaved grid or three double planes.
+struct InterpArgs {
+    int64_t np;
+    const double *x, *y, *z;
+    double min[3], delta[3], hinv[3];
+    int nlo[3], nhi[3];
+    int nx, ny, nz;
+};
+template <typename T>
+int launch_interp_vec4(const InterpArgs &a, const void *E4, double *E, unsigned long long *nclamp,
+                       cudaStream_t st);
+// out_f32 != 0: E is float [np][3]
+template <typename T>
+int launch_interp_vec4_any(const InterpArgs &a, const void *E4, void *E, int out_f32,
+                           unsigned long long *nclamp, cudaStream_t st);
+int launch_interp_planes(const InterpArgs &a, const double *F, double *out,
+                         unsigned long long *nclamp, cudaStream_t st);
+
+// Bounding box {xmin,xmax,ymin,ymax,zmin,zmax} of the particles, written to bb (device)
+// through order-preserving 64-bit keys; also counts non-finite coordinates.
+int launch_bbox(int64_t np, const double *x, const double *y, const double *z,
+                unsigned long long *keys /*6*/, double *bb /*6*/, unsigned long long *nonfinite,
+                cudaStream_t st);
+// Deterministic sum of q (two passes, fixed order) into *out.
+int launch_sum(int64_t n, const double *q, double *partials /*>= 1024*/, double *out, cudaStream_t st);
+
+}  // namespace osc

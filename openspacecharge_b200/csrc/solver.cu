@@ -1,0 +1,433 @@
+// solver.cu -- free-space IGF field solves: the optimised pipeline and the plain FP64 path.
+//
+// Optimised pipeline (osc_freespace_solver2 semantics, code/open_spacecharge_mod.f90:535):
+// the kernel g is stored "centred" (displacement a at index a mod 2n), which makes the
+// physical output window [0,n) in every axis -- the same linear map as the reference's
+// shifted extraction at n-1.  Its spectrum is computed once in FP64 and cached, stored as
+// a half spectrum (real input along x), and where the offset along an axis is zero the
+// kernel's parity halves the stored extent along y and z and makes the spectrum purely
+// real or imaginary.  The cathode image (-rho flipped in z) is folded into the same
+// spectral product, so the image costs one more spectrum read, not one more solve.
+#include <cstring>
+#include <sstream>
+
+#include "solver.cuh"
+
+namespace osc {
+
+#define TRY(...)                   \
+    do {                           \
+        int rc_ = (__VA_ARGS__);   \
+        if (rc_) return rc_;       \
+    } while (0)
+
+static int kerr(osc_ctx *c, int rc, const char *what) {
+    if (rc == OSC_OK) return OSC_OK;
+    if (rc == OSC_E_FFT_SIZE) return set_err(c, rc, "%s: unsupported transform length", what);
+    cudaError_t e = cudaGetLastError();
+    return set_err(c, rc, "%s: %s", what, cudaGetErrorString(e));
+}
+
+template <typename T>
+int fft3d_full(osc_ctx *c, cplx<T> *a, int Nx, int Ny, int Nz, int sx, int sy, int sz) {
+    const int Ls[3] = {Nx, Ny, Nz};
+    const int sg[3] = {sx, sy, sz};
+    for (int ax = 0; ax < 3; ++ax) {
+        if (sg[ax] == 0) continue;
+        LineArgs la;
+        if (!make_fft_plan(Ls[ax], la.p)) return set_err(c, OSC_E_FFT_SIZE, "FFT length %d unsupported", Ls[ax]);
+        const cplx<T> *tw;
+        TRY(twiddles<T>(c, Ls[ax], &tw));
+        la.sign = sg[ax];
+        la.in_len = la.out_len = Ls[ax];
+        la.out_lo = 0;
+        la.scale = 1.0;
+        la.in_zstride = la.out_zstride = 0;
+        int nplanes = 1;
+        bool row = false;
+        if (ax == 0) {
+            la.ncols = Ny * Nz;
+            la.in_pstride = la.out_pstride = 0;
+            la.in_cstride = la.out_cstride = Nx;
+            la.in_estride = la.out_estride = 1;
+            row = true;
+        } else if (ax == 1) {
+            la.ncols = Nx;
+            nplanes = Nz;
+            la.in_pstride = la.out_pstride = (int64_t)Nx * Ny;
+            la.in_cstride = la.out_cstride = 1;
+            la.in_estride = la.out_estride = Nx;
+        } else {
+            la.ncols = Nx * Ny;
+            la.in_pstride = la.out_pstride = 0;
+            la.in_cstride = la.out_cstride = 1;
+            la.in_estride = la.out_estride = (int64_t)Nx * Ny;
+        }
+        Launch L_(c, ax == 0 ? "fft_x_c2c" : (ax == 1 ? "fft_y_c2c" : "fft_z_c2c"));
+        TRY(kerr(c, launch_lines<T>(a, a, la, nplanes, 1, row, tw, c->stream), "fft3d_full"));
+    }
+    return OSC_OK;
+}
+template int fft3d_full<float>(osc_ctx *, cplx<float> *, int, int, int, int, int, int);
+template int fft3d_full<double>(osc_ctx *, cplx<double> *, int, int, int, int, int, int);
+
+// ------------------------------------------------------------------------------------
+// Green spectrum of one component (icomp 0 phi, 1..3 E) with the given offset.
+template <typename T>
+static int build_green_component(osc_ctx *c, int nx, int ny, int nz, const double delta[3], double gamma,
+                                 const double off[3], int icomp, DevBuf &store, GSpecDev &spec) {
+    const int n[3] = {nx, ny, nz};
+    const int N[3] = {2 * nx, 2 * ny, 2 * nz};
+    const int64_t M = (int64_t)N[0] * N[1] * N[2];
+    int sym[3], par[3] = {1, 1, 1}, c0[3], cd[3];
+    for (int d = 0; d < 3; ++d) sym[d] = off[d] == 0.0 ? 1 : 0;
+    if (icomp >= 1) par[icomp - 1] = -1;
+    for (int d = 0; d < 3; ++d) {
+        c0[d] = sym[d] ? n[d] - 1 : 0;
+        cd[d] = sym[d] ? n[d] + 1 : 2 * n[d];
+    }
+    double *F;
+    double2 *cg;
+    TRY(ws_get(c, "green_F", sizeof(double) * (size_t)cd[0] * cd[1] * cd[2], (void **)&F));
+    TRY(ws_get(c, "green_cg", sizeof(double2) * (size_t)M, (void **)&cg));
+    // osc_get_cgrn_freespace (code/open_spacecharge_mod.f90:648-668)
+    CornerArgs ca;
+    ca.cdx = cd[0]; ca.cdy = cd[1]; ca.cdz = cd[2];
+    ca.c0x = c0[0]; ca.c0y = c0[1]; ca.c0z = c0[2];
+    ca.dx = delta[0];
+    ca.dy = delta[1];
+    ca.dz = delta[2] * gamma;
+    ca.factor = (icomp == 1 || icomp == 2) ? gamma / (ca.dx * ca.dy * ca.dz) : 1.0 / (ca.dx * ca.dy * ca.dz);
+    ca.umin = (double)(0.5f - (float)(N[0] / 2)) * ca.dx + off[0];
+    ca.vmin = (double)(0.5f - (float)(N[1] / 2)) * ca.dy + off[1];
+    ca.wmin = (double)(0.5f - (float)(N[2] / 2)) * ca.dz + off[2] * gamma;
+    ca.icomp = icomp;
+    {
+        Launch L_(c, "green_corners");
+        TRY(kerr(c, launch_igf_corners(F, ca, c->stream), "green corners"));
+    }
+    CenterArgs ce;
+    ce.nx = nx; ce.ny = ny; ce.nz = nz;
+    ce.symx = sym[0]; ce.symy = sym[1]; ce.symz = sym[2];
+    ce.parx = par[0]; ce.pary = par[1]; ce.parz = par[2];
+    ce.c0x = c0[0]; ce.c0y = c0[1]; ce.c0z = c0[2];
+    ce.cdx = cd[0]; ce.cdy = cd[1];
+    {
+        Launch L_(c, "green_center");
+        TRY(kerr(c, launch_green_center(F, cg, ce, c->stream), "green center"));
+    }
+    TRY(fft3d_full<double>(c, reinterpret_cast<cplx<double> *>(cg), N[0], N[1], N[2], 1, 1, 1));
+    spec.real_valued = (sym[0] && sym[1] && sym[2]) ? 1 : 0;
+    spec.imag_unit = (spec.real_valued && icomp != 0) ? 1 : 0;
+    spec.sym_y = sym[1];
+    spec.sym_z = sym[2];
+    spec.par_y = par[1];
+    spec.par_z = par[2];
+    spec.dimy = sym[1] ? ny + 1 : N[1];
+    spec.dimz = sym[2] ? nz + 1 : N[2];
+    const size_t elems = (size_t)(nx + 1) * spec.dimy * spec.dimz;
+    const size_t bytes = elems * (spec.real_valued ? sizeof(T) : sizeof(cplx<T>));
+    cudaError_t e = cudaMalloc(&store.p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return set_err(c, OSC_E_ALLOC, "Green spectrum: cudaMalloc(%zu) failed", bytes);
+    }
+    store.bytes = bytes;
+    const double scale = fpei_solver2() / (double)M;
+    {
+        Launch L_(c, "green_extract");
+        TRY(kerr(c, launch_green_extract<T>(cg, store.p, nx, N[0], N[1], spec.dimy, spec.dimz, spec.real_valued,
+                                            spec.imag_unit, scale, c->stream),
+                 "green extract"));
+    }
+    spec.data = store.p;
+    return OSC_OK;
+}
+
+static std::string fs_key(const FreeSpaceJob &j, int tbytes, const int *comps, int ncomp) {
+    std::ostringstream s;
+    s.precision(17);
+    s << "fs|" << tbytes << "|" << j.nx << "," << j.ny << "," << j.nz << "|" << j.delta[0] << "," << j.delta[1]
+      << "," << j.delta[2] << "|" << j.gamma << "|" << j.offset[0] << "," << j.offset[1] << "," << j.offset[2]
+      << "|" << (j.at_cathode ? j.img_zoff : 0.0) << "|" << j.at_cathode << "|";
+    for (int i = 0; i < ncomp; ++i) s << comps[i];
+    return s.str();
+}
+
+// Cached Green set for a job: spectra [direct comps..., image comps...].
+template <typename T>
+static int green_set(osc_ctx *c, const FreeSpaceJob &j, const int *comps, int ncomp, GreenSet **out) {
+    const std::string key = fs_key(j, (int)sizeof(T), comps, ncomp);
+    if (GreenSet *g = gcache_find(c, key)) {
+        *out = g;
+        return OSC_OK;
+    }
+    GreenSet gs;
+    gs.key = key;
+    const int nsets = j.at_cathode ? 2 : 1;
+    for (int s = 0; s < nsets; ++s) {
+        double off[3] = {j.offset[0], j.offset[1], j.offset[2]};
+        if (s == 1) off[2] = off[2] + j.img_zoff;
+        for (int i = 0; i < ncomp; ++i) {
+            const int k = gs.nspec;
+            int rc = build_green_component<T>(c, j.nx, j.ny, j.nz, j.delta, j.gamma, off, comps[i], gs.buf[k], gs.spec[k]);
+            if (rc) {
+                for (int q = 0; q <= k; ++q)
+                    if (gs.buf[q].p) cudaFree(gs.buf[q].p);
+                return rc;
+            }
+            gs.bytes += gs.buf[k].bytes;
+            gs.nspec++;
+        }
+    }
+    *out = gcache_insert(c, std::move(gs));
+    return OSC_OK;
+}
+
+template <typename T, typename TIn>
+int freespace_opt(osc_ctx *c, const FreeSpaceJob &j, const TIn *rho) {
+    typedef cplx<T> V;
+    const int nx = j.nx, ny = j.ny, nz = j.nz;
+    const int Nx = 2 * nx, Ny = 2 * ny, Nz = 2 * nz, nxh = nx + 1;
+    const int64_t N = (int64_t)nx * ny * nz;
+    FFTPlan px, py, pz;
+    if (!make_fft_plan(Nx, px) || !make_fft_plan(Ny, py) || !make_fft_plan(Nz, pz))
+        return set_err(c, OSC_E_FFT_SIZE, "doubled grid %dx%dx%d: lengths must be 2^a 3^b 5^c <= %d", Nx, Ny, Nz,
+                       FFT_MAX_LEN);
+    int comps[4], ncomp = 0;
+    if (j.want_phi) comps[ncomp++] = 0;
+    if (j.want_e || j.calc_b)
+        for (int q = 1; q <= 3; ++q) comps[ncomp++] = q;
+    if (ncomp == 0) return OSC_OK;
+    GreenSet *gs;
+    TRY(green_set<T>(c, j, comps, ncomp, &gs));
+    auto spec_index = [&](int icomp, bool img) {
+        for (int i = 0; i < ncomp; ++i)
+            if (comps[i] == icomp) return img ? ncomp + i : i;
+        return -1;
+    };
+    // outputs of the z-convolution and their destinations
+    ZConvArgs za;
+    C2RArgs cr;
+    std::memset(&za, 0, sizeof(za));
+    std::memset(&cr, 0, sizeof(cr));
+    int nout = 0;
+    auto add_out = [&](int icomp, double icoef) {
+        za.gdir[nout] = spec_index(icomp, false);
+        za.gimg[nout] = j.at_cathode ? spec_index(icomp, true) : -1;
+        za.img_coef[nout] = icoef;
+        cr.ndest[nout] = 0;
+        return nout++;
+    };
+    auto add_dest = [&](int o, void *ptr, int kind, int slot, double coef) {
+        OutDest &d = cr.dest[o][cr.ndest[o]++];
+        d.ptr = ptr;
+        d.kind = kind;
+        d.slot = slot;
+        d.coef = coef;
+    };
+    if (j.want_phi && j.phi) add_dest(add_out(0, 1.0), j.phi, 1, 0, 1.0);
+    if (j.want_e || j.calc_b) {
+        for (int q = 0; q < 3; ++q) {
+            const int o = add_out(q + 1, 1.0);
+            if (j.E) add_dest(o, j.E + q * N, 1, 0, 1.0);
+            if (j.E4) add_dest(o, j.E4, 0, q, 1.0);
+            if (j.calc_b && j.B && !j.at_cathode) {
+                if (q == 1) add_dest(o, j.B, 1, 0, -j.bcoef);
+                if (q == 0) add_dest(o, j.B + N, 1, 0, j.bcoef);
+            }
+        }
+        if (j.calc_b && j.B && j.at_cathode) {
+            // image charges move the other way: B from (direct - image) fields
+            add_dest(add_out(1, -1.0), j.B + N, 1, 0, j.bcoef);
+            add_dest(add_out(2, -1.0), j.B, 1, 0, -j.bcoef);
+        }
+    }
+    if (j.calc_b && j.B) TRY(cuda_check(c, cudaMemsetAsync(j.B + 2 * N, 0, sizeof(double) * N, c->stream), "memset B"));
+
+    V *X1, *X2, *X3, *X4;
+    TRY(ws_get(c, "fs_x1", sizeof(V) * (size_t)nxh * ny * nz, (void **)&X1));
+    TRY(ws_get(c, "fs_x2", sizeof(V) * (size_t)nxh * Ny * nz, (void **)&X2));
+    TRY(ws_get(c, "fs_x3", sizeof(V) * (size_t)nout * nxh * Ny * nz, (void **)&X3));
+    TRY(ws_get(c, "fs_x4", sizeof(V) * (size_t)nout * nxh * ny * nz, (void **)&X4));
+    const V *twx, *twy, *twz;
+    TRY(twiddles<T>(c, Nx, &twx));
+    TRY(twiddles<T>(c, Ny, &twy));
+    TRY(twiddles<T>(c, Nz, &twz));
+
+    // x: real rows -> half spectra, [z][y][kx]
+    R2CArgs ra;
+    ra.p = px;
+    ra.nin = nx;
+    ra.nrows = (int64_t)ny * nz;
+    ra.in_rstride = nx;
+    ra.out_rstride = nxh;
+    {
+        Launch L_(c, "fft_x_r2c");
+        TRY(kerr(c, launch_r2c_rows<T, TIn>(rho, X1, ra, twx, c->stream), "x r2c"));
+    }
+    // y forward: [z][y][kx] -> [z][ky][kx]
+    LineArgs ly;
+    ly.p = py;
+    ly.sign = +1;
+    ly.ncols = nxh;
+    ly.in_len = ny;
+    ly.out_lo = 0;
+    ly.out_len = Ny;
+    ly.in_pstride = (int64_t)nxh * ny;
+    ly.in_cstride = 1;
+    ly.in_estride = nxh;
+    ly.in_zstride = 0;
+    ly.out_pstride = (int64_t)nxh * Ny;
+    ly.out_cstride = 1;
+    ly.out_estride = nxh;
+    ly.out_zstride = 0;
+    ly.scale = 1.0;
+    {
+        Launch L_(c, "fft_y_fwd");
+        TRY(kerr(c, launch_lines<T>(X1, X2, ly, nz, 1, false, twy, c->stream), "y forward"));
+    }
+    // z: forward, spectral product, inverse
+    za.p = pz;
+    za.nz = nz;
+    za.ncols = nxh * Ny;
+    za.nxh = nxh;
+    za.Ny = Ny;
+    za.ny = ny;
+    za.in_estride = (int64_t)nxh * Ny;
+    za.out_estride = (int64_t)nxh * Ny;
+    za.out_cstride = (int64_t)nxh * Ny * nz;
+    za.nout = nout;
+    za.img_phase_mul = nz - 1;
+    za.ng = gs->nspec;
+    for (int i = 0; i < gs->nspec; ++i) za.g[i] = gs->spec[i];
+    {
+        Launch L_(c, "fft_z_conv");
+        TRY(kerr(c, launch_zconv<T>(X2, X3, za, twz, 0, c->stream), "z convolution"));
+    }
+    // y inverse, window [0,ny)
+    LineArgs li = ly;
+    li.sign = -1;
+    li.in_len = Ny;
+    li.out_len = ny;
+    li.in_pstride = (int64_t)nxh * Ny;
+    li.in_zstride = (int64_t)nxh * Ny * nz;
+    li.out_pstride = (int64_t)nxh * ny;
+    li.out_zstride = (int64_t)nxh * ny * nz;
+    {
+        Launch L_(c, "fft_y_inv");
+        TRY(kerr(c, launch_lines<T>(X3, X4, li, nz, nout, false, twy, c->stream), "y inverse"));
+    }
+    // x: half spectra -> real rows [0,nx), scattered to the outputs
+    cr.p = px;
+    cr.nout = nx;
+    cr.nrows = (int64_t)ny * nz;
+    cr.in_rstride = nxh;
+    cr.in_cstride = (int64_t)nxh * ny * nz;
+    cr.ncomp = nout;
+    {
+        Launch L_(c, "fft_x_c2r");
+        TRY(kerr(c, launch_c2r_rows<T>(X4, cr, twx, c->stream), "x c2r"));
+    }
+    return OSC_OK;
+}
+template int freespace_opt<float, float>(osc_ctx *, const FreeSpaceJob &, const float *);
+template int freespace_opt<float, double>(osc_ctx *, const FreeSpaceJob &, const double *);
+template int freespace_opt<double, double>(osc_ctx *, const FreeSpaceJob &, const double *);
+
+// ------------------------------------------------------------------------------------
+// osc_freespace_solver2 restated on the GPU in FP64, one call = one solve: zero-padded
+// complex rho, full 3D transforms, G built and transformed for every component.
+static int solver2_plain(osc_ctx *c, int nx, int ny, int nz, const double delta[3], double gamma, const double off[3],
+                         const double *rho, double rho_sign, int flipz, double *phi, double *E, int accumulate) {
+    const int Nx = 2 * nx, Ny = 2 * ny, Nz = 2 * nz;
+    const int64_t M = (int64_t)Nx * Ny * Nz, N = (int64_t)nx * ny * nz;
+    double2 *crho, *cgrn;
+    double *F;
+    TRY(ws_get(c, "plain_crho", sizeof(double2) * (size_t)M, (void **)&crho));
+    TRY(ws_get(c, "plain_cgrn", sizeof(double2) * (size_t)M, (void **)&cgrn));
+    TRY(ws_get(c, "plain_F", sizeof(double) * (size_t)M, (void **)&F));
+    {
+        Launch L_(c, "plain_pad");
+        TRY(kerr(c, launch_pad_rho(rho, crho, nx, ny, nz, Nx, Ny, Nz, rho_sign, flipz, c->stream), "pad"));
+    }
+    TRY(fft3d_full<double>(c, reinterpret_cast<cplx<double> *>(crho), Nx, Ny, Nz, 1, 1, 1));
+    const double factr = fpei_solver2() / ((double)Nx * Ny * Nz);
+    for (int icomp = 0; icomp <= 3; ++icomp) {
+        if (icomp == 0 && !phi) continue;
+        if (icomp == 1 && !E) break;
+        CornerArgs ca;
+        ca.cdx = Nx; ca.cdy = Ny; ca.cdz = Nz;
+        ca.c0x = ca.c0y = ca.c0z = 0;
+        ca.dx = delta[0];
+        ca.dy = delta[1];
+        ca.dz = delta[2] * gamma;
+        ca.factor = (icomp == 1 || icomp == 2) ? gamma / (ca.dx * ca.dy * ca.dz) : 1.0 / (ca.dx * ca.dy * ca.dz);
+        ca.umin = (double)(0.5f - (float)(Nx / 2)) * ca.dx + off[0];
+        ca.vmin = (double)(0.5f - (float)(Ny / 2)) * ca.dy + off[1];
+        ca.wmin = (double)(0.5f - (float)(Nz / 2)) * ca.dz + off[2] * gamma;
+        ca.icomp = icomp;
+        {
+            Launch L_(c, "plain_green_corners");
+            TRY(kerr(c, launch_igf_corners(F, ca, c->stream), "plain corners"));
+        }
+        {
+            Launch L_(c, "plain_green_diff");
+            TRY(kerr(c, launch_igf_diff_ref(F, cgrn, Nx, Ny, Nz, c->stream), "plain diff"));
+        }
+        TRY(fft3d_full<double>(c, reinterpret_cast<cplx<double> *>(cgrn), Nx, Ny, Nz, 1, 1, 1));
+        {
+            Launch L_(c, "plain_cmul");
+            TRY(kerr(c, launch_cmul(cgrn, crho, M, c->stream), "plain cmul"));
+        }
+        TRY(fft3d_full<double>(c, reinterpret_cast<cplx<double> *>(cgrn), Nx, Ny, Nz, -1, -1, -1));
+        double *out = icomp == 0 ? phi : E + (int64_t)(icomp - 1) * N;
+        {
+            Launch L_(c, "plain_extract");
+            TRY(kerr(c, launch_extract_re(cgrn, Nx, Ny, nx - 1, ny - 1, nz - 1, nx, ny, nz, factr, out, accumulate,
+                                          c->stream),
+                     "plain extract"));
+        }
+    }
+    return OSC_OK;
+}
+
+// space_charge_3d (code/open_spacecharge_mod.f90:431-489) in the plain FP64 path.
+int freespace_plain(osc_ctx *c, const FreeSpaceJob &j, const double *rho) {
+    const int64_t N = (int64_t)j.nx * j.ny * j.nz;
+    double *Eout = j.E;
+    if (!Eout && (j.want_e || j.calc_b)) TRY(ws_get(c, "plain_E", sizeof(double) * 3 * N, (void **)&Eout));
+    TRY(solver2_plain(c, j.nx, j.ny, j.nz, j.delta, j.gamma, j.offset, rho, 1.0, 0, j.want_phi ? j.phi : nullptr,
+                      (j.want_e || j.calc_b) ? Eout : nullptr, 0));
+    if (j.calc_b && j.B) {
+        Launch L_(c, "plain_bfield");
+        TRY(kerr(c, launch_bfield(Eout, j.B, N, j.bcoef, 0, c->stream), "bfield"));
+    }
+    if (j.at_cathode) {
+        double off[3] = {j.offset[0], j.offset[1], j.offset[2] + j.img_zoff};
+        double *img, *phimg = nullptr;
+        TRY(ws_get(c, "plain_img", sizeof(double) * 3 * N, (void **)&img));
+        if (j.want_phi && j.phi) TRY(ws_get(c, "plain_phimg", sizeof(double) * N, (void **)&phimg));
+        TRY(solver2_plain(c, j.nx, j.ny, j.nz, j.delta, j.gamma, off, rho, -1.0, 1, phimg,
+                          (j.want_e || j.calc_b) ? img : nullptr, 0));
+        if (j.calc_b && j.B) {
+            Launch L_(c, "plain_bfield");
+            TRY(kerr(c, launch_bfield(img, j.B, N, -j.bcoef, 1, c->stream), "bfield image"));
+        }
+        if (Eout) {
+            Launch L_(c, "plain_axpy");
+            TRY(kerr(c, launch_axpy(Eout, img, 1.0, 3 * N, c->stream), "image add"));
+        }
+        if (phimg) {
+            Launch L_(c, "plain_axpy");
+            TRY(kerr(c, launch_axpy(j.phi, phimg, 1.0, N, c->stream), "image phi add"));
+        }
+    }
+    if (j.E4) {
+        // the plain path hands interpolation the field as three planes; callers use E
+        return set_err(c, OSC_E_INVALID, "plain path writes E planes only");
+    }
+    return OSC_OK;
+}
+
+}  // namespace osc

@@ -1,0 +1,65 @@
+// solver.cuh -- field-solve pipelines on one context.
+#pragma once
+
+#include "context.cuh"
+#include "grid_kernels.cuh"
+#include "particle_kernels.cuh"
+
+namespace osc {
+
+// 1/(4 pi eps0) of osc_freespace_solver2: `299792458.0**2*1.00000000055d-7` squares a
+// single-precision literal (code/open_spacecharge_mod.f90:547).
+inline double fpei_solver2() {
+    const float c = 299792458.0f;
+    return (double)(c * c) * 1.00000000055e-7;
+}
+// c_light of space_charge_3d, also a single-precision literal (code/open_spacecharge_mod.f90:436).
+inline double c_light_sc3d() { return (double)299792458.0f; }
+// Legacy core module constants (code/open_spacecharge_core_mod.f90:51, :515).
+inline double fpei_legacy() { return 299792458.0 * 299792458.0 * 1.0e-7; }
+const double CLIGHT_CORE = 299792458.0;
+// fftconvcorr3d's single-precision `299792458.**2*1.e-7` (core:783).
+inline double fpei_pipe() {
+    const float c = 299792458.0f;
+    float v = c * c;
+    v = v * 1.0e-7f;
+    return (double)v;
+}
+
+struct FreeSpaceJob {
+    int nx = 0, ny = 0, nz = 0;
+    double delta[3] = {0, 0, 0}, gamma = 1, offset[3] = {0, 0, 0};
+    int at_cathode = 0;
+    double img_zoff = 0;  // 2*min(3) + (max(3)-min(3))
+    int want_phi = 0, want_e = 1;
+    int calc_b = 0;
+    double bcoef = 0;     // beta/c_light
+    double *phi = nullptr;  // device f64 [N]
+    double *E = nullptr;    // device f64 [3][N]
+    double *B = nullptr;    // device f64 [3][N]
+    void *E4 = nullptr;     // device vec4<T> [N]
+};
+
+// Optimised IGF convolution (cached half-spectra, pruned transforms) in precision T.
+template <typename T, typename TIn>
+int freespace_opt(osc_ctx *c, const FreeSpaceJob &job, const TIn *rho);
+// The reference algorithm in FP64 (full zero-padded complex FFTs, G rebuilt per call).
+int freespace_plain(osc_ctx *c, const FreeSpaceJob &job, const double *rho);
+
+// Full in-place C2C transform of an (Nx,Ny,Nz) array with per-axis signs.
+template <typename T>
+int fft3d_full(osc_ctx *c, cplx<T> *a, int Nx, int Ny, int Nz, int sx, int sy, int sz);
+
+// Legacy solvers (FP64, reference algorithms).
+int legacy_freespace(osc_ctx *c, const int nlo[3], const int nhi[3], const int npad[3],
+                     const double delta[3], double gam0, const double *rho, int direct, int igf,
+                     double *phi, double *E, double *B);
+int legacy_cathode(osc_ctx *c, const int nlo[3], const int nhi[3], const int npad[3],
+                   const double umin[3], const double delta[3], double gam0, double *rho,
+                   int direct, int igf, int imethod, double *phi, double *E, double *B);
+int pipe_green_build(osc_ctx *c, const int nlo[3], const int nhi[3], const int npad[3],
+                     const double delta[3], const double umin[3], double gam, double a, double b);
+int pipe_solve(osc_ctx *c, int precision, const double delta[3], double gam0, const double *rho,
+               double *phi, double *E, double *B);
+
+}  // namespace osc
