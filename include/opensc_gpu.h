@@ -113,6 +113,24 @@ OSC_API int osc_deposit_particles_dev(osc_ctx *ctx, int64_t np, const double *d_
                               int resize_mesh, osc_mesh3d *mesh, double *d_rho,
                               int64_t *n_outside);
 
+/* No counterpart in the reference.  Charge deposition for callers that may not allocate
+ * device memory (inside another framework's memory pool, in loops that cannot absorb the
+ * synchronisation of cudaMalloc/cudaFree, or without a library context, whose creation
+ * allocates).  It needs no context and allocates nothing: the caller passes a stream, the
+ * mesh and device buffers; the deposit accumulates in FP32 in a fixed array compiled into
+ * the library (OSC_NOALLOC_MAX_NODES floats, 16 MiB, held on every GPU that loads the
+ * library until the process exits) and writes REAL64 rho.  Meshes with more nodes are
+ * rejected with OSC_E_INVALID.  Charges are d_q per particle, or total_charge/np when d_q
+ * is NULL; the mesh is not refitted and mesh->charge is not touched.  The first call on a
+ * device looks up the array's device address once (make that first call before any stream
+ * capture).  All calls share the one array, so calls whose work overlaps on the GPU race.
+ * errbuf (optional, errlen bytes) receives a message. */
+#define OSC_NOALLOC_MAX_NODES 4194304
+OSC_API int osc_deposit_particles_dev_noalloc(void *cuda_stream, const osc_mesh3d *mesh, int64_t np,
+                                              const double *d_x, const double *d_y, const double *d_z,
+                                              const double *d_q, double total_charge, double *d_rho,
+                                              int64_t *n_outside, char *errbuf, size_t errlen);
+
 /* Replaces get_mesh_quantities (code/test_mod.f90:288-358), the test-path mesh rule:
  * delta=(max-min)/(n-3), min=bunch_min-delta; isetzmin=1 pins zmin=1e-9 for cathodes. */
 OSC_API int osc_get_mesh_quantities(osc_ctx *ctx, int64_t np, const double *xa, const double *ya,

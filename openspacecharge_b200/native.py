@@ -93,6 +93,8 @@ SIGNATURES = {
     "osc_launch_count": [_P, _PI64],
     "osc_deposit_particles": [_P, _I64, _P, _P, _P, _P, _P, _I, _PM, _P, _PI64],
     "osc_deposit_particles_dev": [_P, _I64, _P, _P, _P, _P, _P, _I, _PM, _P, _PI64],
+    "osc_deposit_particles_dev_noalloc": [_P, _PM, _I64, _P, _P, _P, _P, _D, _P, _PI64, ctypes.c_char_p,
+                                          ctypes.c_size_t],
     "osc_get_mesh_quantities": [_P, _I64, _P, _P, _P, _P, _P, _I, _P, _P],
     "osc_depose_rho_scalar": [_P, _I64, _P, _P, _P, _P, _D, _P, _P, _P, _P, _P, _PI64],
     "osc_space_charge_3d": [_P, _PM, _P, _P, _I, _I, _I, _P, _P],
