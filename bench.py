@@ -135,13 +135,16 @@ def kernel_bytes(nx, ny, nz, npart, at_cathode=False):
     nout = 3
     g_bytes = 3 * 4 * nxh * (ny + 1) * (nz + 1)
     return {
-        "deposit_f32": 24 * npart + 4 * N,
+        # CIC weights into per-cell corner sums (8 floats per cell), then gathered to nodes
+        "deposit_f32": 24 * npart + 32 * N,
+        "cells_to_nodes": 32 * N + 4 * N,
         "fft_x_r2c": 4 * N + c8 * nxh * ny * nz,
         "fft_y_fwd": c8 * nxh * ny * nz + c8 * nxh * Ny * nz,
         "fft_z_conv": c8 * nxh * Ny * nz + g_bytes + nout * c8 * nxh * Ny * nz,
         "fft_y_inv": nout * c8 * nxh * Ny * nz + nout * c8 * nxh * ny * nz,
-        "fft_x_c2r": nout * c8 * nxh * ny * nz + 16 * N,
-        "interp_f32": 24 * npart + 16 * N + 24 * npart,
+        # E written as the x-pair grid (two float4 per node)
+        "fft_x_c2r": nout * c8 * nxh * ny * nz + 32 * N,
+        "interp_f32": 24 * npart + 32 * N + 24 * npart,
     }
 
 

@@ -619,20 +619,27 @@ int osc_space_charge_step_dev(osc_ctx *ctx, osc_mesh3d *mesh, int64_t np, const 
         return OSC_OK;
     }
     if (precision == OSC_PREC_FP32) {
-        float *rho;
-        void *E4, *B4 = nullptr;
+        // deposit: per-cell corner sums (two float4 atomics per particle), then a gather
+        // to nodes; field: E written as an x-pair grid; interpolation: 4 sectors/particle
+        float *rho, *acc;
+        void *E8;
         TRY(ws_get(ctx, "st_rho32", sizeof(float) * N, (void **)&rho));
-        TRY(ws_get(ctx, "st_E4", sizeof(float4) * N, &E4));
-        if (B) TRY(ws_get(ctx, "st_B4", sizeof(float4) * N, &B4));
-        CK(cudaMemsetAsync(rho, 0, sizeof(float) * N, ctx->stream), "memset rho");
+        TRY(ws_get(ctx, "st_cells", sizeof(float) * 8 * N, (void **)&acc));
+        TRY(ws_get(ctx, "st_E8", sizeof(float4) * 2 * N, &E8));
+        CK(cudaMemsetAsync(acc, 0, sizeof(float) * 8 * N, ctx->stream), "memset cells");
         {
             Launch L_(ctx, "deposit_f32");
-            if (launch_deposit<float>(da, rho, ctx->d_small, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "deposit");
+            if (launch_deposit_cells(da, acc, ctx->d_small, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "deposit");
         }
-        j.E4 = E4;
+        {
+            Launch L_(ctx, "cells_to_nodes");
+            if (launch_cells_to_nodes(acc, rho, n[0], n[1], n[2], ctx->stream))
+                return set_err(ctx, OSC_E_CUDA, "cells to nodes");
+        }
+        j.E4 = E8;
+        j.e4_pairs = 1;
         j.B = nullptr;
         if (B) {
-            // B grid as a second vec4 grid: computed through the plane destinations below
             double *Bg;
             TRY(ws_get(ctx, "st_Bg", sizeof(double) * 3 * N, (void **)&Bg));
             j.B = Bg;
@@ -640,7 +647,8 @@ int osc_space_charge_step_dev(osc_ctx *ctx, osc_mesh3d *mesh, int64_t np, const 
         TRY(freespace_opt<float, float>(ctx, j, rho));
         {
             Launch L_(ctx, "interp_f32");
-            if (launch_interp_vec4<float>(ia, E4, E, ctx->d_small + 2, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "interp");
+            if (launch_interp_pairs(ia, reinterpret_cast<const float4 *>(E8), E, ctx->d_small + 2, ctx->stream))
+                return set_err(ctx, OSC_E_CUDA, "interp");
         }
         if (B) {
             Launch L_(ctx, "interp_f64");

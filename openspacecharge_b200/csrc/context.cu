@@ -47,51 +47,91 @@ int ws_get(osc_ctx *c, const char *name, size_t bytes, void **out) {
     return OSC_OK;
 }
 
-template <typename T> int twiddles(osc_ctx *c, int L, const cplx<T> **out) {
-    auto &tab = sizeof(T) == 4 ? c->tw32 : c->tw64;
-    auto it = tab.find(L);
-    if (it != tab.end()) {
-        *out = reinterpret_cast<const cplx<T> *>(it->second.p);
-        return OSC_OK;
+// exp(+2 pi i m/n) in FP64, reducing the angle to one octant so every entry is as exact as
+// the FP64 sin/cos of an angle in [0, pi/4].
+static void cis_exact(int64_t m, int64_t n, double &cs, double &sn) {
+    m %= n;
+    if (m < 0) m += n;
+    const int64_t num = 8 * m;  // angle = 2*pi*num/(8n)
+    const int oct = (int)(num / n);
+    const double rem = (double)(num - (int64_t)oct * n) / (double)n;
+    const double qpi = 0.78539816339744830961566084581988;  // pi/4
+    const double a = rem * qpi;
+    const double ca = std::cos(a), sa = std::sin(a);
+    const double h2 = 0.70710678118654752440084436210485;
+    switch (oct) {  // rotate by oct*pi/4
+    case 0: cs = ca; sn = sa; break;
+    case 1: cs = h2 * (ca - sa); sn = h2 * (ca + sa); break;
+    case 2: cs = -sa; sn = ca; break;
+    case 3: cs = -h2 * (ca + sa); sn = h2 * (ca - sa); break;
+    case 4: cs = -ca; sn = -sa; break;
+    case 5: cs = -h2 * (ca - sa); sn = -h2 * (ca + sa); break;
+    case 6: cs = sa; sn = -ca; break;
+    default: cs = h2 * (ca + sa); sn = -h2 * (ca - sa); break;
     }
-    std::vector<cplx<T>> h(L);
-    // exp(+2 pi i m/L) in FP64, using the octant symmetry so every entry is as exact as
-    // the FP64 sin/cos of an angle in [0, pi/4]
-    for (int m = 0; m < L; ++m) {
-        // reduce m/L to [0,1/8] turns
-        const int64_t num = (int64_t)8 * m;  // angle = 2*pi*num/(8L)
-        const int oct = (int)(num / L);      // octant 0..7
-        const double rem = (double)(num - (int64_t)oct * L) / (double)L;  // fraction of an octant
-        double cs, sn;
-        const double qpi = 0.78539816339744830961566084581988;  // pi/4
-        const double a = rem * qpi;
-        const double ca = std::cos(a), sa = std::sin(a);
-        const double h2 = 0.70710678118654752440084436210485;
-        // rotate by oct*pi/4
-        switch (oct) {
-        case 0: cs = ca; sn = sa; break;
-        case 1: cs = h2 * (ca - sa); sn = h2 * (ca + sa); break;
-        case 2: cs = -sa; sn = ca; break;
-        case 3: cs = -h2 * (ca + sa); sn = h2 * (ca - sa); break;
-        case 4: cs = -ca; sn = -sa; break;
-        case 5: cs = -h2 * (ca - sa); sn = -h2 * (ca + sa); break;
-        case 6: cs = sa; sn = -ca; break;
-        default: cs = h2 * (ca + sa); sn = -h2 * (ca - sa); break;
-        }
-        h[m] = mk<T>((T)cs, (T)sn);
-    }
-    DevBuf b;
-    cudaError_t e = cudaMalloc(&b.p, sizeof(cplx<T>) * L);
+}
+
+template <typename T> static int upload(osc_ctx *c, const std::vector<cplx<T>> &h, DevBuf &b) {
+    cudaError_t e = cudaMalloc(&b.p, sizeof(cplx<T>) * h.size());
     if (e != cudaSuccess) return cuda_check(c, e, "twiddle table");
-    b.bytes = sizeof(cplx<T>) * L;
+    b.bytes = sizeof(cplx<T>) * h.size();
     e = cudaMemcpy(b.p, h.data(), b.bytes, cudaMemcpyHostToDevice);
-    if (e != cudaSuccess) return cuda_check(c, e, "twiddle upload");
-    tab[L] = b;
-    *out = reinterpret_cast<const cplx<T> *>(b.p);
+    return e == cudaSuccess ? OSC_OK : cuda_check(c, e, "twiddle upload");
+}
+
+template <typename T> int twiddles(osc_ctx *c, int L, TwPair<cplx<T>> *out) {
+    auto &tab = sizeof(T) == 4 ? c->tw32 : c->tw64;
+    // runtime table under key L, per-stage static table under key -L
+    if (tab.find(L) == tab.end()) {
+        std::vector<cplx<T>> h(L);
+        for (int m = 0; m < L; ++m) {
+            double cs, sn;
+            cis_exact(m, L, cs, sn);
+            h[m] = mk<T>((T)cs, (T)sn);
+        }
+        DevBuf b;
+        int rc = upload<T>(c, h, b);
+        if (rc) return rc;
+        tab[L] = b;
+    }
+    if (tab.find(-L) == tab.end()) {
+        // stage s (Ns = product of earlier radices, radix R): entry (Ns-1) + k*(R-1) + (r-1)
+        // holds exp(2 pi i r k/(Ns R)) for k < Ns, 1 <= r < R; L-1 entries in all
+        std::vector<cplx<T>> h(L, mk<T>((T)1, (T)0));
+        const bool has_static = dispatch_fft_len(L, [&](auto eng) -> int {
+            using E = decltype(eng);
+            if constexpr (E::kLen > 0) {
+                int Ns = 1;
+                for (int s = 0; s < E::kNst; ++s) {
+                    const int R = E::kRad[s];
+                    for (int k = 0; k < Ns; ++k)
+                        for (int r = 1; r < R; ++r) {
+                            double cs, sn;
+                            cis_exact((int64_t)r * k, (int64_t)Ns * R, cs, sn);
+                            h[(Ns - 1) + k * (R - 1) + (r - 1)] = mk<T>((T)cs, (T)sn);
+                        }
+                    Ns *= R;
+                }
+                return 1;
+            }
+            return 0;
+        });
+        if (has_static) {
+            DevBuf b;
+            int rc = upload<T>(c, h, b);
+            if (rc) return rc;
+            tab[-L] = b;
+        } else {
+            tab[-L] = DevBuf{nullptr, 0};
+        }
+    }
+    out->rt = reinterpret_cast<const cplx<T> *>(tab[L].p);
+    const DevBuf &s = tab[-L];
+    out->st = s.p ? reinterpret_cast<const cplx<T> *>(s.p) : out->rt;
     return OSC_OK;
 }
-template int twiddles<float>(osc_ctx *, int, const cplx<float> **);
-template int twiddles<double>(osc_ctx *, int, const cplx<double> **);
+template int twiddles<float>(osc_ctx *, int, TwPair<cplx<float>> *);
+template int twiddles<double>(osc_ctx *, int, TwPair<cplx<double>> *);
 
 static cudaEvent_t ev_get(osc_ctx *c) {
     if (!c->ev_pool.empty()) {

@@ -86,7 +86,9 @@ int set_err(osc_ctx *c, int code, const char *fmt, ...);
 int cuda_check(osc_ctx *c, cudaError_t e, const char *what);
 // Named device workspace of at least `bytes` (grown by reallocation; contents not kept).
 int ws_get(osc_ctx *c, const char *name, size_t bytes, void **out);
-template <typename T> int twiddles(osc_ctx *c, int L, const cplx<T> **out);
+// Twiddle tables of length L (runtime table and, when L has a static engine, its
+// per-stage table), built once per context in FP64.
+template <typename T> int twiddles(osc_ctx *c, int L, TwPair<cplx<T>> *out);
 
 // Kernel-launch bookkeeping and optional per-kernel CUDA-event timing.
 struct Launch {

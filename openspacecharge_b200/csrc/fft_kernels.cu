@@ -7,7 +7,7 @@
 //   k_lines     y: inverse C2C along y (output window [0,ny))
 //   k_c2r_rows  x: inverse to real rows, epilogue scatters E (and B) to their layouts
 // Zero padding of the doubled grid is never stored: loads past the physical window are
-// zeros in shared memory and stores cover only the physical window.
+// zeros (or, for the static engines, not read at all) and stores cover only the window.
 #include <cstdio>
 #include <type_traits>
 
@@ -16,7 +16,7 @@
 namespace osc {
 
 bool make_fft_plan(int L, FFTPlan &p) {
-    if (L < 1 || L > FFT_MAX_LEN) return false;
+    if (L < 2 || L > FFT_MAX_LEN || (L % 2) != 0) return false;
     p.L = L;
     p.nst = 0;
     int m = L;
@@ -25,24 +25,18 @@ bool make_fft_plan(int L, FFTPlan &p) {
     while (m % 2 == 0) { p.radix[p.nst++] = 2; m /= 2; }
     while (m % 3 == 0) { p.radix[p.nst++] = 3; m /= 3; }
     while (m % 5 == 0) { p.radix[p.nst++] = 5; m /= 5; }
-    if (m != 1 || p.nst > FFT_MAX_STAGES) return false;
-    return L % 2 == 0;  // every length used here is a doubled grid edge
+    return m == 1 && p.nst <= FFT_MAX_STAGES;
 }
 
-// Largest lines-per-CTA NL <= nl_max such that the CTA has a whole number of threads
-// (L*NL divisible by FFT_EPT), at most 1024 threads, and nbuf line buffers fit in budget.
-int pick_nl(int L, int nl_max, size_t elem_bytes, int nbuf, size_t budget) {
-    for (int nl = nl_max; nl >= 2; nl /= 2) {
-        if ((L * nl) % FFT_EPT != 0) continue;
-        if (fft_threads(L, nl) > 512) continue;
-        if ((size_t)nbuf * L * (nl + 1) * elem_bytes + L * elem_bytes > budget && nl > 2) continue;
-        return nl;
-    }
-    return 0;
+// Engine-specific twiddle table in global memory.
+template <class E, typename V> __host__ __device__ inline const V *eng_tw(const TwPair<V> &t) {
+    return E::kLen > 0 ? t.st : t.rt;
 }
 
 // ------------------------------------------------------------------------------------
-template <typename T, int NL, bool ROW, class E>
+// MODE 0: full transform; 1: input window is the lower half (static engines skip it);
+// 2: output window is the lower half and is not flipped (static engines skip the rest).
+template <typename T, int NL, bool ROW, class E, int MODE>
 __global__ void __launch_bounds__(E::kMaxThreads) k_lines(const cplx<T> *in, cplx<T> *out, LineArgs a,
                                                           const cplx<T> *__restrict__ twg) {
     typedef cplx<T> V;
@@ -56,10 +50,11 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_lines(const cplx<T> *in, cpl
     const V *src = in + (int64_t)blockIdx.z * a.in_zstride + (int64_t)blockIdx.y * a.in_pstride;
     V *dst = out + (int64_t)blockIdx.z * a.out_zstride + (int64_t)blockIdx.y * a.out_pstride;
     load_twiddles(tw, twg, L);
-    const int nld = NL * L;
+    const int ld_len = (E::kLen > 0 && MODE == 1) ? a.in_len : L;  // the static first stage skips zeros
+    const int nld = NL * ld_len;
     for (int idx = tid; idx < nld; idx += nthreads) {
         int e, c;
-        if (ROW) { c = idx / L; e = idx - c * L; }
+        if (ROW) { c = idx / ld_len; e = idx - c * ld_len; }
         else { e = idx / NL; c = idx - e * NL; }
         V v = mk<T>(0, 0);
         const int col = col0 + c;
@@ -67,7 +62,7 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_lines(const cplx<T> *in, cpl
         buf[e * lstr + c] = v;
     }
     __syncthreads();
-    E::template run<V, NL>(buf, a.p, tw, a.sign);
+    E::template run<V, NL, MODE == 1, MODE == 2>(buf, a.p, tw, a.sign);
     const int nst = NL * a.out_len;
     const T sc = (T)a.scale;
     for (int idx = tid; idx < nst; idx += nthreads) {
@@ -75,13 +70,14 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_lines(const cplx<T> *in, cpl
         if (ROW) { c = idx / a.out_len; e = idx - c * a.out_len; }
         else { e = idx / NL; c = idx - e * NL; }
         const int col = col0 + c;
+        const int src_e = ((a.flip_mask >> blockIdx.z) & 1u) ? (L - (e + a.out_lo)) % L : e + a.out_lo;
         if (col < a.ncols)
-            dst[(int64_t)col * a.out_cstride + (int64_t)e * a.out_estride] = cscale(buf[(e + a.out_lo) * lstr + c], sc);
+            dst[(int64_t)col * a.out_cstride + (int64_t)e * a.out_estride] = cscale(buf[src_e * lstr + c], sc);
     }
 }
 
 // ------------------------------------------------------------------------------------
-template <typename T, typename TIn, int NL, class E>
+template <typename T, typename TIn, int NL, class E, bool HIN>
 __global__ void __launch_bounds__(E::kMaxThreads) k_r2c_rows(const TIn *__restrict__ in, cplx<T> *__restrict__ out,
                                                              R2CArgs a, const cplx<T> *__restrict__ twg) {
     typedef cplx<T> V;
@@ -93,8 +89,9 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_r2c_rows(const TIn *__restri
     const int nthreads = blockDim.x, tid = threadIdx.x;
     const int64_t row0 = (int64_t)blockIdx.x * (2 * NL);
     load_twiddles(tw, twg, L);
-    for (int idx = tid; idx < 2 * NL * L; idx += nthreads) {
-        const int rr = idx / L, e = idx - rr * L;
+    const int ld_len = (E::kLen > 0 && HIN) ? a.nin : L;
+    for (int idx = tid; idx < 2 * NL * ld_len; idx += nthreads) {
+        const int rr = idx / ld_len, e = idx - rr * ld_len;
         const int64_t row = row0 + rr;
         T v = 0;
         if (row < a.nrows && e < a.nin) v = (T)in[row * a.in_rstride + e];
@@ -102,7 +99,7 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_r2c_rows(const TIn *__restri
         slot[rr & 1] = v;
     }
     __syncthreads();
-    E::template run<V, NL>(buf, a.p, tw, +1);
+    E::template run<V, NL, HIN, false>(buf, a.p, tw, +1);
     const int nh = L / 2 + 1;
     for (int idx = tid; idx < 2 * NL * nh; idx += nthreads) {
         const int rr = idx / nh, k = idx - rr * nh;
@@ -125,13 +122,38 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_r2c_rows(const TIn *__restri
 
 // ------------------------------------------------------------------------------------
 template <typename T>
-__device__ __forceinline__ void write_dest(const OutDest &d, int64_t gidx, T val) {
-    if (d.kind == 0) reinterpret_cast<T *>(d.ptr)[gidx * 4 + d.slot] = (T)(d.coef * val);
-    else if (d.kind == 1) reinterpret_cast<double *>(d.ptr)[gidx] = d.coef * (double)val;
-    else reinterpret_cast<T *>(d.ptr)[gidx] = (T)(d.coef * val);
+__device__ __forceinline__ void write_dest(const OutDest &d, int64_t gidx, int x, T val) {
+    // vec4 grids also write their unused 4th slot, so every 32-byte sector is written whole
+    switch (d.kind) {
+    case 0: {
+        T *p = reinterpret_cast<T *>(d.ptr) + gidx * 4;
+        p[d.slot] = (T)(d.coef * val);
+        if (d.slot == 2) p[3] = (T)0;
+        break;
+    }
+    case 1: reinterpret_cast<double *>(d.ptr)[gidx] = d.coef * (double)val; break;
+    case 3: reinterpret_cast<double *>(d.ptr)[gidx] += d.coef * (double)val; break;
+    case 4: {  // x-pair grid: node n holds (E(n), E(n+1)) as two vec4; the last node's
+               // second half is never read and is zeroed
+        T *p = reinterpret_cast<T *>(d.ptr);
+        const T v = (T)(d.coef * val);
+        p[gidx * 8 + d.slot] = v;
+        if (d.slot == 2) p[gidx * 8 + 3] = (T)0;
+        if (x > 0) {
+            p[(gidx - 1) * 8 + 4 + d.slot] = v;
+            if (d.slot == 2) p[(gidx - 1) * 8 + 7] = (T)0;
+        }
+        if (x == d.last_x) {
+            p[gidx * 8 + 4 + d.slot] = (T)0;
+            if (d.slot == 2) p[gidx * 8 + 7] = (T)0;
+        }
+        break;
+    }
+    default: reinterpret_cast<T *>(d.ptr)[gidx] = (T)(d.coef * val); break;
+    }
 }
 
-template <typename T, int NL, class E>
+template <typename T, int NL, class E, bool HOUT>
 __global__ void __launch_bounds__(E::kMaxThreads) k_c2r_rows(const cplx<T> *__restrict__ in, C2RArgs a,
                                                              const cplx<T> *__restrict__ twg) {
     typedef cplx<T> V;
@@ -158,15 +180,16 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_c2r_rows(const cplx<T> *__re
             buf[k * lstr + line] = mk<T>(A.x - B.y, A.y + B.x);
         }
         __syncthreads();
-        E::template run<V, NL>(buf, a.p, tw, -1);
+        E::template run<V, NL, false, HOUT>(buf, a.p, tw, -1);
         for (int idx = tid; idx < 2 * NL * a.nout; idx += nthreads) {
             const int rr = idx / a.nout, x = idx - rr * a.nout;
             const int64_t row = row0 + rr;
             if (row >= a.nrows) continue;
-            const V z = buf[x * lstr + (rr >> 1)];
+            const int xs = ((a.flip_mask >> c) & 1u) ? (L - x) % L : x;
+            const V z = buf[xs * lstr + (rr >> 1)];
             const T val = (rr & 1) ? z.y : z.x;
             const int64_t gidx = row * a.nout + x;
-            for (int d = 0; d < a.ndest[c]; ++d) write_dest<T>(a.dest[c][d], gidx, val);
+            for (int d = 0; d < a.ndest[c]; ++d) write_dest<T>(a.dest[c][d], gidx, x, val);
         }
         __syncthreads();
     }
@@ -191,9 +214,12 @@ __device__ __forceinline__ cplx<T> g_lookup(const GSpecDev &g, int kx, int ky, i
     return v;
 }
 
-template <typename T, int NL, class E>
+// HALF: nz == L/2, so the static engine's forward first stage skips the zero half and
+// its inverse last stage skips the upper half, which is never stored.
+template <typename T, int NL, class E, bool HALF>
 __global__ void __launch_bounds__(E::kMaxThreads) k_zconv(const cplx<T> *__restrict__ in, cplx<T> *__restrict__ out,
-                                                          ZConvArgs a, const cplx<T> *__restrict__ twg) {
+                                                          ZConvArgs a, const cplx<T> *__restrict__ twg,
+                                                          const cplx<T> *__restrict__ tw_rt) {
     typedef cplx<T> V;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V *tw = reinterpret_cast<V *>(smem_raw);
@@ -204,7 +230,8 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_zconv(const cplx<T> *__restr
     const int nthreads = blockDim.x, tid = threadIdx.x;
     const int col0 = blockIdx.x * NL;
     load_twiddles(tw, twg, L);
-    for (int idx = tid; idx < NL * L; idx += nthreads) {
+    const int ld_len = (E::kLen > 0 && HALF) ? a.nz : L;
+    for (int idx = tid; idx < NL * ld_len; idx += nthreads) {
         const int e = idx / NL, c = idx - e * NL;
         const int col = col0 + c;
         V v = mk<T>(0, 0);
@@ -212,7 +239,7 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_zconv(const cplx<T> *__restr
         rhat[e * lstr + c] = v;
     }
     __syncthreads();
-    E::template run<V, NL>(rhat, a.p, tw, +1);
+    E::template run<V, NL, HALF, false>(rhat, a.p, tw, +1);
     for (int o = 0; o < a.nout; ++o) {
         const int gd = a.gdir[o], gi = a.gimg[o];
         const T icoef = (T)a.img_coef[o];
@@ -225,7 +252,7 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_zconv(const cplx<T> *__restr
             if (gi >= 0) {
                 // spectrum of -rho flipped in z: -w^((nz-1) kz) * rho_hat(-kz)
                 const V rm = rhat[((L - e) % L) * lstr + c];
-                const V ph = tw[(int)(((int64_t)a.img_phase_mul * e) % L)];
+                const V ph = __ldg(tw_rt + (int)(((int64_t)a.img_phase_mul * e) % L));
                 V ri = cmul(ph, rm);
                 ri.x = -ri.x * icoef;
                 ri.y = -ri.y * icoef;
@@ -234,7 +261,7 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_zconv(const cplx<T> *__restr
             buf[e * lstr + c] = S;
         }
         __syncthreads();
-        E::template run<V, NL>(buf, a.p, tw, -1);
+        E::template run<V, NL, false, HALF>(buf, a.p, tw, -1);
         V *dst = out + (int64_t)o * a.out_cstride;
         for (int idx = tid; idx < NL * a.nz; idx += nthreads) {
             const int e = idx / NL, c = idx - e * NL;
@@ -264,14 +291,17 @@ static int pick_nl_rt(int L, int nl_max, size_t elem, int nbuf) {
     return 0;
 }
 
-// Calls f(std::integral_constant<int, NL>) for the engine's lines-per-CTA.
+// Calls f(std::integral_constant<int, NL>) for the engine's lines-per-CTA.  Static engines
+// use a compile-time NL: the widest that fits (one line buffer) or, for the two-buffer
+// z-pass, at most 4 lines in ~48 KB so several CTAs share an SM.
 template <typename T, class E, class F> static int with_nl(int L, int nbuf, int nl_max, int nl_req, F &&f) {
     if constexpr (E::kLen > 0) {
         (void)L;
         (void)nl_req;
-        constexpr int NL = nl_static(E::kLen, sizeof(T) == 4 ? 16 : 8, (int)sizeof(cplx<T>), 2);
+        (void)nl_max;
         constexpr int NL1 = nl_static(E::kLen, sizeof(T) == 4 ? 16 : 8, (int)sizeof(cplx<T>), 1);
-        if (nbuf >= 2) return f(std::integral_constant<int, (NL < 8 ? NL : 8)>{});
+        constexpr int NL2 = nl_static(E::kLen, 4, (int)sizeof(cplx<T>), 2, 64 * 1024);
+        if (nbuf >= 2) return f(std::integral_constant<int, NL2>{});
         return f(std::integral_constant<int, NL1>{});
     } else {
         int nl = nl_req > 0 ? nl_req : pick_nl_rt(L, nl_max, sizeof(cplx<T>), nbuf);
@@ -285,87 +315,122 @@ template <typename T, class E, class F> static int with_nl(int L, int nbuf, int 
     }
 }
 
+template <typename T, int NL, bool ROW, class E, int MODE>
+static int launch_lines_k(const cplx<T> *in, cplx<T> *out, const LineArgs &a, int nplanes, int ncomp, const cplx<T> *tw,
+                          cudaStream_t st) {
+    const int L = a.p.L;
+    const int nt = fft_threads(L, NL);
+    if (nt < 1 || nt > E::kMaxThreads || (L * NL) % FFT_EPT) return OSC_E_FFT_SIZE;
+    const size_t sm = sizeof(cplx<T>) * ((size_t)L + (size_t)L * (NL + 1));
+    auto kern = k_lines<T, NL, ROW, E, MODE>;
+    int rc = set_smem(kern, sm);
+    if (rc) return rc;
+    dim3 grid((unsigned)ceil_div(a.ncols, NL), (unsigned)nplanes, (unsigned)ncomp);
+    kern<<<grid, nt, sm, st>>>(in, out, a, tw);
+    return launch_ok();
+}
+
 template <typename T>
-int launch_lines(const cplx<T> *in, cplx<T> *out, const LineArgs &a, int nplanes, int ncomp,
-                 bool row_mode, const cplx<T> *tw, cudaStream_t st) {
+int launch_lines(const cplx<T> *in, cplx<T> *out, const LineArgs &a, int nplanes, int ncomp, bool row_mode,
+                 const TwPair<cplx<T>> &tw, cudaStream_t st) {
     const int L = a.p.L;
     return dispatch_fft_len(L, [&](auto eng) -> int {
         using E = decltype(eng);
+        const cplx<T> *twe = eng_tw<E>(tw);
+        return with_nl<T, E>(L, 1, sizeof(T) == 4 ? 16 : 8, 0, [&](auto nlc) -> int {
+            constexpr int NL = decltype(nlc)::value;
+            if (row_mode) return launch_lines_k<T, NL, true, E, 0>(in, out, a, nplanes, ncomp, twe, st);
+            if constexpr (E::kLen > 0) {
+                if (2 * a.in_len == L && a.out_len == L && a.out_lo == 0)
+                    return launch_lines_k<T, NL, false, E, 1>(in, out, a, nplanes, ncomp, twe, st);
+                if (a.in_len == L && 2 * a.out_len == L && a.out_lo == 0 && a.flip_mask == 0)
+                    return launch_lines_k<T, NL, false, E, 2>(in, out, a, nplanes, ncomp, twe, st);
+            }
+            return launch_lines_k<T, NL, false, E, 0>(in, out, a, nplanes, ncomp, twe, st);
+        });
+    });
+}
+
+template <typename T, typename TIn>
+int launch_r2c_rows(const TIn *in, cplx<T> *out, const R2CArgs &a, const TwPair<cplx<T>> &tw, cudaStream_t st) {
+    const int L = a.p.L;
+    return dispatch_fft_len(L, [&](auto eng) -> int {
+        using E = decltype(eng);
+        const cplx<T> *twe = eng_tw<E>(tw);
         return with_nl<T, E>(L, 1, sizeof(T) == 4 ? 16 : 8, 0, [&](auto nlc) -> int {
             constexpr int NL = decltype(nlc)::value;
             const int nt = fft_threads(L, NL);
             if (nt < 1 || nt > E::kMaxThreads || (L * NL) % FFT_EPT) return OSC_E_FFT_SIZE;
             const size_t sm = sizeof(cplx<T>) * ((size_t)L + (size_t)L * (NL + 1));
-            dim3 grid((unsigned)ceil_div(a.ncols, NL), (unsigned)nplanes, (unsigned)ncomp);
-            if (row_mode) {
-                auto kern = k_lines<T, NL, true, E>;
+            const unsigned nblk = (unsigned)ceil_div(a.nrows, 2 * NL);
+            if (E::kLen > 0 && 2 * a.nin == L) {
+                auto kern = k_r2c_rows<T, TIn, NL, E, true>;
                 int rc = set_smem(kern, sm);
                 if (rc) return rc;
-                kern<<<grid, nt, sm, st>>>(in, out, a, tw);
+                kern<<<nblk, nt, sm, st>>>(in, out, a, twe);
             } else {
-                auto kern = k_lines<T, NL, false, E>;
+                auto kern = k_r2c_rows<T, TIn, NL, E, false>;
                 int rc = set_smem(kern, sm);
                 if (rc) return rc;
-                kern<<<grid, nt, sm, st>>>(in, out, a, tw);
+                kern<<<nblk, nt, sm, st>>>(in, out, a, twe);
             }
             return launch_ok();
         });
     });
 }
 
-template <typename T, typename TIn>
-int launch_r2c_rows(const TIn *in, cplx<T> *out, const R2CArgs &a, const cplx<T> *tw, cudaStream_t st) {
+template <typename T>
+int launch_c2r_rows(const cplx<T> *in, const C2RArgs &a, const TwPair<cplx<T>> &tw, cudaStream_t st) {
     const int L = a.p.L;
     return dispatch_fft_len(L, [&](auto eng) -> int {
         using E = decltype(eng);
+        const cplx<T> *twe = eng_tw<E>(tw);
         return with_nl<T, E>(L, 1, sizeof(T) == 4 ? 16 : 8, 0, [&](auto nlc) -> int {
             constexpr int NL = decltype(nlc)::value;
             const int nt = fft_threads(L, NL);
             if (nt < 1 || nt > E::kMaxThreads || (L * NL) % FFT_EPT) return OSC_E_FFT_SIZE;
             const size_t sm = sizeof(cplx<T>) * ((size_t)L + (size_t)L * (NL + 1));
-            auto kern = k_r2c_rows<T, TIn, NL, E>;
-            int rc = set_smem(kern, sm);
-            if (rc) return rc;
-            kern<<<(unsigned)ceil_div(a.nrows, 2 * NL), nt, sm, st>>>(in, out, a, tw);
+            const unsigned nblk = (unsigned)ceil_div(a.nrows, 2 * NL);
+            if (E::kLen > 0 && 2 * a.nout == L && a.flip_mask == 0) {
+                auto kern = k_c2r_rows<T, NL, E, true>;
+                int rc = set_smem(kern, sm);
+                if (rc) return rc;
+                kern<<<nblk, nt, sm, st>>>(in, a, twe);
+            } else {
+                auto kern = k_c2r_rows<T, NL, E, false>;
+                int rc = set_smem(kern, sm);
+                if (rc) return rc;
+                kern<<<nblk, nt, sm, st>>>(in, a, twe);
+            }
             return launch_ok();
         });
     });
 }
 
 template <typename T>
-int launch_c2r_rows(const cplx<T> *in, const C2RArgs &a, const cplx<T> *tw, cudaStream_t st) {
-    const int L = a.p.L;
-    return dispatch_fft_len(L, [&](auto eng) -> int {
-        using E = decltype(eng);
-        return with_nl<T, E>(L, 1, sizeof(T) == 4 ? 16 : 8, 0, [&](auto nlc) -> int {
-            constexpr int NL = decltype(nlc)::value;
-            const int nt = fft_threads(L, NL);
-            if (nt < 1 || nt > E::kMaxThreads || (L * NL) % FFT_EPT) return OSC_E_FFT_SIZE;
-            const size_t sm = sizeof(cplx<T>) * ((size_t)L + (size_t)L * (NL + 1));
-            auto kern = k_c2r_rows<T, NL, E>;
-            int rc = set_smem(kern, sm);
-            if (rc) return rc;
-            kern<<<(unsigned)ceil_div(a.nrows, 2 * NL), nt, sm, st>>>(in, a, tw);
-            return launch_ok();
-        });
-    });
-}
-
-template <typename T>
-int launch_zconv(const cplx<T> *in, cplx<T> *out, const ZConvArgs &a, const cplx<T> *tw, int nl,
+int launch_zconv(const cplx<T> *in, cplx<T> *out, const ZConvArgs &a, const TwPair<cplx<T>> &tw, int nl,
                  cudaStream_t st) {
     const int L = a.p.L;
     return dispatch_fft_len(L, [&](auto eng) -> int {
         using E = decltype(eng);
+        const cplx<T> *twe = eng_tw<E>(tw);
         return with_nl<T, E>(L, 2, sizeof(T) == 4 ? 8 : 4, nl, [&](auto nlc) -> int {
             constexpr int NL = decltype(nlc)::value;
             const int nt = fft_threads(L, NL);
             if (nt < 1 || nt > E::kMaxThreads || (L * NL) % FFT_EPT) return OSC_E_FFT_SIZE;
             const size_t sm = sizeof(cplx<T>) * ((size_t)L + 2 * (size_t)L * (NL + 1));
-            auto kern = k_zconv<T, NL, E>;
-            int rc = set_smem(kern, sm);
-            if (rc) return rc;
-            kern<<<(unsigned)ceil_div(a.ncols, NL), nt, sm, st>>>(in, out, a, tw);
+            const unsigned nblk = (unsigned)ceil_div(a.ncols, NL);
+            if (E::kLen > 0 && 2 * a.nz == L) {
+                auto kern = k_zconv<T, NL, E, true>;
+                int rc = set_smem(kern, sm);
+                if (rc) return rc;
+                kern<<<nblk, nt, sm, st>>>(in, out, a, twe, tw.rt);
+            } else {
+                auto kern = k_zconv<T, NL, E, false>;
+                int rc = set_smem(kern, sm);
+                if (rc) return rc;
+                kern<<<nblk, nt, sm, st>>>(in, out, a, twe, tw.rt);
+            }
             return launch_ok();
         });
     });
@@ -373,15 +438,21 @@ int launch_zconv(const cplx<T> *in, cplx<T> *out, const ZConvArgs &a, const cplx
 
 // Explicit instantiations.
 template int launch_lines<float>(const cplx<float> *, cplx<float> *, const LineArgs &, int, int, bool,
-                                 const cplx<float> *, cudaStream_t);
+                                 const TwPair<cplx<float>> &, cudaStream_t);
 template int launch_lines<double>(const cplx<double> *, cplx<double> *, const LineArgs &, int, int, bool,
-                                  const cplx<double> *, cudaStream_t);
-template int launch_r2c_rows<float, float>(const float *, cplx<float> *, const R2CArgs &, const cplx<float> *, cudaStream_t);
-template int launch_r2c_rows<float, double>(const double *, cplx<float> *, const R2CArgs &, const cplx<float> *, cudaStream_t);
-template int launch_r2c_rows<double, double>(const double *, cplx<double> *, const R2CArgs &, const cplx<double> *, cudaStream_t);
-template int launch_c2r_rows<float>(const cplx<float> *, const C2RArgs &, const cplx<float> *, cudaStream_t);
-template int launch_c2r_rows<double>(const cplx<double> *, const C2RArgs &, const cplx<double> *, cudaStream_t);
-template int launch_zconv<float>(const cplx<float> *, cplx<float> *, const ZConvArgs &, const cplx<float> *, int, cudaStream_t);
-template int launch_zconv<double>(const cplx<double> *, cplx<double> *, const ZConvArgs &, const cplx<double> *, int, cudaStream_t);
+                                  const TwPair<cplx<double>> &, cudaStream_t);
+template int launch_r2c_rows<float, float>(const float *, cplx<float> *, const R2CArgs &, const TwPair<cplx<float>> &,
+                                           cudaStream_t);
+template int launch_r2c_rows<float, double>(const double *, cplx<float> *, const R2CArgs &,
+                                            const TwPair<cplx<float>> &, cudaStream_t);
+template int launch_r2c_rows<double, double>(const double *, cplx<double> *, const R2CArgs &,
+                                             const TwPair<cplx<double>> &, cudaStream_t);
+template int launch_c2r_rows<float>(const cplx<float> *, const C2RArgs &, const TwPair<cplx<float>> &, cudaStream_t);
+template int launch_c2r_rows<double>(const cplx<double> *, const C2RArgs &, const TwPair<cplx<double>> &,
+                                     cudaStream_t);
+template int launch_zconv<float>(const cplx<float> *, cplx<float> *, const ZConvArgs &, const TwPair<cplx<float>> &,
+                                 int, cudaStream_t);
+template int launch_zconv<double>(const cplx<double> *, cplx<double> *, const ZConvArgs &,
+                                  const TwPair<cplx<double>> &, int, cudaStream_t);
 
 }  // namespace osc

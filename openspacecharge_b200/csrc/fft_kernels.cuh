@@ -18,6 +18,7 @@ struct LineArgs {
     int64_t in_pstride, in_cstride, in_estride, in_zstride;
     int64_t out_pstride, out_cstride, out_estride, out_zstride;
     double scale;
+    unsigned flip_mask;  // bit z: component z stores element (L-e) mod L at e (index flip)
 };
 
 // Forward transform of real rows (length nin, zero-padded to L) packed two per complex
@@ -33,8 +34,10 @@ struct R2CArgs {
 // Where the real result of one inverse component goes.
 struct OutDest {
     void *ptr;        // nullptr = unused
-    int kind;         // 0: slot of a vec4<T> grid, 1: double plane, 2: T plane
-    int slot;         // vec4 component (kind 0)
+    int kind;         // 0: slot of a vec4<T> grid, 1: double plane, 2: T plane, 3: add to a double
+                      // plane, 4: slot of an x-pair grid (node n holds vec4 E(n), E(n+1))
+    int slot;         // vec4 component (kinds 0 and 4)
+    int last_x;       // kind 4: the last x index of a row
     double coef;      // multiplier
 };
 constexpr int MAX_OUT = 6;
@@ -49,6 +52,7 @@ struct C2RArgs {
     int64_t nrows;
     int64_t in_rstride, in_cstride;
     int ncomp;
+    unsigned flip_mask;   // bit c: component c is read at x -> (L-x) mod L (index flip)
     int ndest[MAX_OUT];
     OutDest dest[MAX_OUT][MAX_DEST];
 };
@@ -86,13 +90,13 @@ struct ZConvArgs {
 
 template <typename T>
 int launch_lines(const cplx<T> *in, cplx<T> *out, const LineArgs &a, int nplanes, int ncomp,
-                 bool row_mode, const cplx<T> *tw, cudaStream_t st);
+                 bool row_mode, const TwPair<cplx<T>> &tw, cudaStream_t st);
 template <typename T, typename TIn>
-int launch_r2c_rows(const TIn *in, cplx<T> *out, const R2CArgs &a, const cplx<T> *tw, cudaStream_t st);
+int launch_r2c_rows(const TIn *in, cplx<T> *out, const R2CArgs &a, const TwPair<cplx<T>> &tw, cudaStream_t st);
 template <typename T>
-int launch_c2r_rows(const cplx<T> *in, const C2RArgs &a, const cplx<T> *tw, cudaStream_t st);
+int launch_c2r_rows(const cplx<T> *in, const C2RArgs &a, const TwPair<cplx<T>> &tw, cudaStream_t st);
 template <typename T>
-int launch_zconv(const cplx<T> *in, cplx<T> *out, const ZConvArgs &a, const cplx<T> *tw,
+int launch_zconv(const cplx<T> *in, cplx<T> *out, const ZConvArgs &a, const TwPair<cplx<T>> &tw,
                  int nl, cudaStream_t st);
 
 }  // namespace osc

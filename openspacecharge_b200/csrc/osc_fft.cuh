@@ -9,9 +9,16 @@
 // autosorted positions.  The CTA has L*NL/FFT_EPT threads, so each thread owns FFT_EPT
 // complex values per stage and all butterflies of a stage fit in registers.
 //
-// Twiddles come from a table tw[m] = exp(+2*pi*i*m/L) computed on the host in FP64 (and
-// rounded once for FP32) and staged in shared memory; sign -1 uses the conjugate.
-// Convention: X[k] = sum_j x[j] exp(sign*2*pi*i*j*k/L), unnormalised -- the sign
+// Two engines share these stages.  FftStatic<L, R...> fixes the radix sequence at compile
+// time (every index is a shift or a constant multiply) and reads its twiddles from a
+// per-stage table laid out [stage][k][r-1], so the lanes of a warp read consecutive words.
+// Its first stage can skip the zero upper half of the input (forward transforms of the
+// zero-padded doubled grid) and its last stage can skip the upper half of the output
+// (inverse transforms whose physical window is the lower half).  FftRuntime follows a
+// runtime radix plan for any other 2^a 3^b 5^c length with the table tw[m]=exp(2 pi i m/L).
+//
+// Twiddles are computed on the host in FP64 and rounded once for FP32; sign -1 uses the
+// conjugate.  Convention: X[k] = sum_j x[j] exp(sign*2*pi*i*j*k/L), unnormalised -- the sign
 // convention of the reference's ccfft3d / Singleton sfft (code/fft_interface_mod.f90:96).
 #pragma once
 
@@ -30,11 +37,10 @@ struct FFTPlan {
 };
 
 // Host: radix plan for L = 2^a 3^b 5^c (radix 8 first, then 4, 2, 3, 5).  Returns false
-// for other lengths or L > FFT_MAX_LEN.
+// for other lengths, odd lengths or L > FFT_MAX_LEN.
 bool make_fft_plan(int L, FFTPlan &p);
 // Threads of a CTA that transforms NL lines of length L.
 inline int fft_threads(int L, int NL) { return (L * NL) / FFT_EPT; }
-int pick_nl(int L, int nl_max, size_t elem_bytes, int nbuf, size_t budget);
 
 template <typename V> __device__ __forceinline__ V tw_get(const V *tw, int m, int sign) {
     V w = tw[m];
@@ -42,10 +48,11 @@ template <typename V> __device__ __forceinline__ V tw_get(const V *tw, int m, in
     return w;
 }
 
+// Small DFTs in registers: y[q] = sum_r v[r] exp(s*2*pi*i*r*q/R).
 template <int R> struct Dft;
 
 template <> struct Dft<2> {
-    template <typename V> __device__ __forceinline__ static void run(V *v, int, const V *, int) {
+    template <typename V> __device__ __forceinline__ static void run(V *v, int) {
         V a = v[0], b = v[1];
         v[0] = cadd(a, b);
         v[1] = csub(a, b);
@@ -53,7 +60,7 @@ template <> struct Dft<2> {
 };
 
 template <> struct Dft<4> {
-    template <typename V> __device__ __forceinline__ static void run(V *v, int s, const V *, int) {
+    template <typename V> __device__ __forceinline__ static void run(V *v, int s) {
         V apc = cadd(v[0], v[2]), amc = csub(v[0], v[2]);
         V bpd = cadd(v[1], v[3]), bmd = csub(v[1], v[3]);
         V jb = cmul_si(bmd, s);
@@ -65,9 +72,9 @@ template <> struct Dft<4> {
 };
 
 template <> struct Dft<8> {
-    template <typename V> __device__ __forceinline__ static void run(V *v, int s, const V *, int) {
+    template <typename V> __device__ __forceinline__ static void run(V *v, int s) {
         typedef decltype(v[0].x) T;
-        const T h = (T)0.70710678118654752440084436210485;
+        const T h = (T)0.70710678118654752440084436210485;  // cos(pi/4)
         V a[4], b[4];
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
@@ -87,8 +94,8 @@ template <> struct Dft<8> {
             u.y = h * (-t.y + (T)s * t.x);
             b[3] = u;
         }
-        Dft<4>::run(a, s, (const V *)nullptr, 0);
-        Dft<4>::run(b, s, (const V *)nullptr, 0);
+        Dft<4>::run(a, s);
+        Dft<4>::run(b, s);
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             v[2 * q] = a[q];
@@ -98,9 +105,9 @@ template <> struct Dft<8> {
 };
 
 template <> struct Dft<3> {
-    template <typename V> __device__ __forceinline__ static void run(V *v, int s, const V *tw, int L) {
+    template <typename V> __device__ __forceinline__ static void run(V *v, int s) {
         typedef decltype(v[0].x) T;
-        const T h = tw[L / 3].y;  // sin(2*pi/3)
+        const T h = (T)0.86602540378443864676372317075294;  // sin(2 pi/3)
         V a = v[0], t = cadd(v[1], v[2]), d = csub(v[1], v[2]);
         V m;
         m.x = a.x - (T)0.5 * t.x;
@@ -115,21 +122,34 @@ template <> struct Dft<3> {
 };
 
 template <> struct Dft<5> {
-    template <typename V> __device__ __forceinline__ static void run(V *v, int s, const V *tw, int L) {
-        V out[5];
-        const int step = L / 5;
-#pragma unroll
-        for (int q = 0; q < 5; ++q) {
-            V acc = v[0];
-#pragma unroll
-            for (int r = 1; r < 5; ++r) acc = cadd(acc, cmul(v[r], tw_get(tw, ((r * q) % 5) * step, s)));
-            out[q] = acc;
-        }
-#pragma unroll
-        for (int q = 0; q < 5; ++q) v[q] = out[q];
+    template <typename V> __device__ __forceinline__ static void run(V *v, int s) {
+        typedef decltype(v[0].x) T;
+        const T c1 = (T)0.30901699437494742410229341718282;   // cos(2 pi/5)
+        const T c2 = (T)-0.80901699437494742410229341718282;  // cos(4 pi/5)
+        const T s1 = (T)0.95105651629515357211643933337938;   // sin(2 pi/5)
+        const T s2 = (T)0.58778525229247312916870595463907;   // sin(4 pi/5)
+        const V x0 = v[0];
+        const V a1 = cadd(v[1], v[4]), b1 = csub(v[1], v[4]);
+        const V a2 = cadd(v[2], v[3]), b2 = csub(v[2], v[3]);
+        V p1, p2, q1, q2;
+        p1.x = x0.x + c1 * a1.x + c2 * a2.x;
+        p1.y = x0.y + c1 * a1.y + c2 * a2.y;
+        p2.x = x0.x + c2 * a1.x + c1 * a2.x;
+        p2.y = x0.y + c2 * a1.y + c1 * a2.y;
+        q1.x = s1 * b1.x + s2 * b2.x;
+        q1.y = s1 * b1.y + s2 * b2.y;
+        q2.x = s2 * b1.x - s1 * b2.x;
+        q2.y = s2 * b1.y - s1 * b2.y;
+        const V j1 = cmul_si(q1, s), j2 = cmul_si(q2, s);
+        v[0] = cadd(x0, cadd(a1, a2));
+        v[1] = cadd(p1, j1);
+        v[4] = csub(p1, j1);
+        v[2] = cadd(p2, j2);
+        v[3] = csub(p2, j2);
     }
 };
 
+// ---- runtime-plan engine ----------------------------------------------------------------
 // One Stockham stage over NL interleaved lines; all threads of the CTA must call it.
 template <typename V, int R, int NL>
 __device__ __forceinline__ void stockham_stage(V *buf, int lstr, int L, int Ns, const V *tw, int sign) {
@@ -153,7 +173,7 @@ __device__ __forceinline__ void stockham_stage(V *buf, int lstr, int L, int Ns, 
                 if (r) x = cmul(x, tw_get(tw, r * k * tstep, sign));
                 v[q][r] = x;
             }
-            Dft<R>::run(v[q], sign, tw, L);
+            Dft<R>::run(v[q], sign);
         }
     }
     __syncthreads();
@@ -189,16 +209,19 @@ __device__ __forceinline__ void fft_smem(V *buf, int lstr, const FFTPlan &p, con
     }
 }
 
-// Compile-time version of one stage: L, Ns, R and NL are constants, so every index is a
-// shift or a multiply by a constant and all butterflies stay in registers.
-template <typename V, int R, int NL, int L, int Ns>
+// ---- compile-time engine ------------------------------------------------------------------
+// MODE 0: full stage; 1: first stage whose upper input half is zero (not read);
+// 2: last stage whose upper output half is not needed (not written).
+template <typename V, int R, int NL, int L, int Ns, int MODE>
 __device__ __forceinline__ void stage_ct(V *buf, const V *tw, int sign) {
     constexpr int lstr = NL + 1;
     constexpr int MAXB = (FFT_EPT + R - 1) / R;
     constexpr int nb = L / R;
     constexpr int total = nb * NL;
-    constexpr int tstep = L / (Ns * R);
     constexpr int nthreads = L * NL / FFT_EPT;
+    constexpr int toff = Ns - 1;  // this stage's block of the per-stage twiddle table
+    constexpr bool half_in = MODE == 1 && (R % 2 == 0);
+    constexpr bool half_out = MODE == 2 && (R % 2 == 0);
     const int tid = threadIdx.x;
     V v[MAXB][R];
 #pragma unroll
@@ -208,11 +231,17 @@ __device__ __forceinline__ void stage_ct(V *buf, const V *tw, int sign) {
             const int line = b % NL, j = b / NL, k = j % Ns;
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-                V x = buf[(j + r * nb) * lstr + line];
-                if (r && Ns > 1) x = cmul(x, tw_get(tw, r * k * tstep, sign));
+                V x;
+                if (half_in && r >= R / 2) {
+                    x.x = 0;
+                    x.y = 0;
+                } else {
+                    x = buf[(j + r * nb) * lstr + line];
+                    if (r && Ns > 1) x = cmul(x, tw_get(tw, toff + k * (R - 1) + (r - 1), sign));
+                }
                 v[q][r] = x;
             }
-            Dft<R>::run(v[q], sign, tw, L);
+            Dft<R>::run(v[q], sign);
         }
     }
     __syncthreads();
@@ -223,25 +252,29 @@ __device__ __forceinline__ void stage_ct(V *buf, const V *tw, int sign) {
             const int line = b % NL, j = b / NL, k = j % Ns;
             const int idxD = (j / Ns) * Ns * R + k;
 #pragma unroll
-            for (int r = 0; r < R; ++r) buf[(idxD + r * Ns) * lstr + line] = v[q][r];
+            for (int r = 0; r < R; ++r)
+                if (!half_out || r < R / 2) buf[(idxD + r * Ns) * lstr + line] = v[q][r];
         }
     }
     __syncthreads();
 }
 
-template <typename V, int NL, int L, int Ns, int R, int... Rest>
+template <typename V, int NL, int L, int Ns, bool HIN, bool HOUT, int R, int... Rest>
 __device__ __forceinline__ void fft_ct(V *buf, const V *tw, int sign) {
-    stage_ct<V, R, NL, L, Ns>(buf, tw, sign);
-    if constexpr (sizeof...(Rest) > 0) fft_ct<V, NL, L, Ns * R, Rest...>(buf, tw, sign);
+    constexpr bool last = sizeof...(Rest) == 0;
+    constexpr int mode = (Ns == 1 && HIN) ? 1 : ((last && HOUT) ? 2 : 0);
+    stage_ct<V, R, NL, L, Ns, mode>(buf, tw, sign);
+    if constexpr (!last) fft_ct<V, NL, L, Ns * R, false, HOUT, Rest...>(buf, tw, sign);
 }
 
-// FFT engines.  FftRuntime follows a runtime radix plan (any supported length); its
-// CTAs are capped at 256 threads so the generic stage code keeps its registers.
-// FftStatic<L, R...> is the compile-time radix sequence for one length.
+// FFT engines.  FftRuntime CTAs are capped at 256 threads so the generic stage code keeps
+// its registers; FftStatic CTAs at 512.  HIN/HOUT only change the static engine.
 struct FftRuntime {
     static constexpr int kLen = 0;
     static constexpr int kMaxThreads = 256;
-    template <typename V, int NL>
+    static constexpr int kNst = 0;
+    static constexpr int kRad[1] = {0};
+    template <typename V, int NL, bool HIN, bool HOUT>
     __device__ __forceinline__ static void run(V *buf, const FFTPlan &p, const V *tw, int sign) {
         fft_smem<V, NL>(buf, NL + 1, p, tw, sign);
     }
@@ -249,18 +282,20 @@ struct FftRuntime {
 template <int L_, int... Rs> struct FftStatic {
     static constexpr int kLen = L_;
     static constexpr int kMaxThreads = 512;
-    template <typename V, int NL>
+    static constexpr int kNst = sizeof...(Rs);
+    static constexpr int kRad[sizeof...(Rs)] = {Rs...};
+    template <typename V, int NL, bool HIN, bool HOUT>
     __device__ __forceinline__ static void run(V *buf, const FFTPlan &, const V *tw, int sign) {
-        fft_ct<V, NL, L_, 1, Rs...>(buf, tw, sign);
+        fft_ct<V, NL, L_, 1, HIN, HOUT, Rs...>(buf, tw, sign);
     }
 };
 
 // Lines per CTA for a static engine: the largest NL <= nl_max with a whole number of
-// threads, at most 512 threads, and nbuf line buffers within ~100 KB of shared memory.
-constexpr int nl_static(int L, int nl_max, int elem_bytes, int nbuf) {
+// threads, at most 512 threads, and nbuf line buffers within budget bytes of shared memory.
+constexpr int nl_static(int L, int nl_max, int elem_bytes, int nbuf, int budget = 100 * 1024) {
     int nl = nl_max;
     while (nl > 2 && ((L * nl) % FFT_EPT != 0 || (L * nl) / FFT_EPT > 512 ||
-                      nbuf * L * (nl + 1) * elem_bytes + L * elem_bytes > 100 * 1024))
+                      nbuf * L * (nl + 1) * elem_bytes + L * elem_bytes > budget))
         nl /= 2;
     return nl;
 }
@@ -280,11 +315,19 @@ template <class F> inline int dispatch_fft_len(int L, F &&f) {
     }
 }
 
-// Stage the twiddle table of length L into shared memory.
-template <typename V> __device__ __forceinline__ void load_twiddles(V *tw_s, const V *tw_g, int L) {
+// Twiddle tables of one length: rt[m] = exp(2 pi i m/L) for the runtime engine; st is the
+// per-stage table of the static engine ([stage][k][r-1], L-1 entries), or rt when the
+// length has no static engine.
+template <typename V> struct TwPair {
+    const V *rt;
+    const V *st;
+};
+
+// Stage the twiddle table of length n into shared memory.
+template <typename V> __device__ __forceinline__ void load_twiddles(V *tw_s, const V *tw_g, int n) {
     const int nthreads = blockDim.x * blockDim.y;
     const int tid = threadIdx.x + blockDim.x * threadIdx.y;
-    for (int m = tid; m < L; m += nthreads) tw_s[m] = tw_g[m];
+    for (int m = tid; m < n; m += nthreads) tw_s[m] = tw_g[m];
 }
 
 }  // namespace osc

@@ -91,6 +91,90 @@ template int launch_deposit<float>(const DepositArgs &, float *, unsigned long l
 template int launch_deposit<double>(const DepositArgs &, double *, unsigned long long *, cudaStream_t);
 
 // ------------------------------------------------------------------------------------
+// Corner q = a + 2b + 4c of a cell is node (i+a, j+b, k+c); its weight is
+// (a ? 1-ab : ab) * (b ? 1-de : de) * (c ? 1-gh : gh) times the charge, the factors of
+// deposit_particles (code/open_spacecharge_mod.f90:274-281).
+__global__ void __launch_bounds__(256) k_deposit_cells(DepositArgs a, float4 *__restrict__ acc,
+                                                       unsigned long long *__restrict__ counters) {
+    GRID_STRIDE(m, a.np) {
+        const double xm = a.x[m], ym = a.y[m], zm = a.z[m];
+        bool nonfinite = false, skip = false;
+        if (a.check_finite && !(isfinite(xm) && isfinite(ym) && isfinite(zm))) {
+            nonfinite = true;
+            skip = true;
+        }
+        const double fx = floor((xm - a.xmin) * a.dxi + 1);
+        const double fy = floor((ym - a.ymin) * a.dyi + 1);
+        const double fz = floor((zm - a.zmin) * a.dzi + 1);
+        const bool outside = !skip && !(fx >= a.nlo[0] && fx + 1 <= a.nhi[0] && fy >= a.nlo[1] &&
+                                        fy + 1 <= a.nhi[1] && fz >= a.nlo[2] && fz + 1 <= a.nhi[2]);
+        count_one(&counters[0], outside);
+        count_one(&counters[1], nonfinite);
+        if (skip || outside) continue;
+        const double ab = ((a.xmin - xm) + fx * a.dx) * a.dxi;
+        const double de = ((a.ymin - ym) + fy * a.dy) * a.dyi;
+        const double gh = ((a.zmin - zm) + fz * a.dz) * a.dzi;
+        const double c = a.q ? a.q[m] : a.charge1;
+        const double omab = 1. - ab, omde = 1. - de, omgh = 1. - gh;
+        const double lo = gh * c, hi = omgh * c;
+        const int i = (int)fx - a.nlo[0], j = (int)fy - a.nlo[1], k = (int)fz - a.nlo[2];
+        float4 *cell = acc + 2 * ((int64_t)i + (int64_t)a.nx * (j + (int64_t)a.ny * k));
+        atomicAdd(cell, make_float4((float)(ab * de * lo), (float)(omab * de * lo), (float)(ab * omde * lo),
+                                    (float)(omab * omde * lo)));
+        atomicAdd(cell + 1, make_float4((float)(ab * de * hi), (float)(omab * de * hi), (float)(ab * omde * hi),
+                                        (float)(omab * omde * hi)));
+    }
+}
+
+int launch_deposit_cells(const DepositArgs &a, float *acc, unsigned long long *counters, cudaStream_t st) {
+    if (a.np <= 0) return OSC_OK;
+    k_deposit_cells<<<nblocks(a.np, 256, 148 * 64), 256, 0, st>>>(a, reinterpret_cast<float4 *>(acc), counters);
+    return ok();
+}
+
+// rho(n) = sum over the 8 cells that have n as a corner, in a fixed order.  A CTA owns a
+// 32x4x4 tile of nodes and stages the 33x5x5 cells it needs in shared memory, one plane
+// per corner index so the reads of a warp hit consecutive words.
+constexpr int GX = 32, GY = 4, GZ = 4;
+constexpr int CX = GX + 1, CY = GY + 1, CZ = GZ + 1, NCELL = CX * CY * CZ;
+
+__global__ void __launch_bounds__(GX *GY *GZ) k_cells_to_nodes(const float4 *__restrict__ acc, float *__restrict__ rho,
+                                                               int nx, int ny, int nz) {
+    __shared__ float sm[8][NCELL];
+    const int i0 = blockIdx.x * GX, j0 = blockIdx.y * GY, k0 = blockIdx.z * GZ;
+    for (int t = threadIdx.x; t < 2 * NCELL; t += blockDim.x) {
+        const int cidx = t >> 1, half = t & 1;
+        const int cx = cidx % CX, r = cidx / CX, cy = r % CY, cz = r / CY;
+        const int i = i0 - 1 + cx, j = j0 - 1 + cy, k = k0 - 1 + cz;
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (i >= 0 && j >= 0 && k >= 0 && i < nx - 1 && j < ny - 1 && k < nz - 1)
+            v = __ldg(acc + 2 * ((int64_t)i + (int64_t)nx * (j + (int64_t)ny * k)) + half);
+        sm[4 * half + 0][cidx] = v.x;
+        sm[4 * half + 1][cidx] = v.y;
+        sm[4 * half + 2][cidx] = v.z;
+        sm[4 * half + 3][cidx] = v.w;
+    }
+    __syncthreads();
+    const int li = threadIdx.x % GX, lj = (threadIdx.x / GX) % GY, lk = threadIdx.x / (GX * GY);
+    const int i = i0 + li, j = j0 + lj, k = k0 + lk;
+    if (i >= nx || j >= ny || k >= nz) return;
+    float s = 0.f;
+#pragma unroll
+    for (int c = 0; c < 2; ++c)
+#pragma unroll
+        for (int b = 0; b < 2; ++b)
+#pragma unroll
+            for (int a = 0; a < 2; ++a) s += sm[a + 2 * b + 4 * c][(li + 1 - a) + CX * ((lj + 1 - b) + CY * (lk + 1 - c))];
+    rho[(int64_t)i + (int64_t)nx * (j + (int64_t)ny * k)] = s;
+}
+
+int launch_cells_to_nodes(const float *acc, float *rho, int nx, int ny, int nz, cudaStream_t st) {
+    dim3 grid((unsigned)ceil_div(nx, GX), (unsigned)ceil_div(ny, GY), (unsigned)ceil_div(nz, GZ));
+    k_cells_to_nodes<<<grid, GX * GY * GZ, 0, st>>>(reinterpret_cast<const float4 *>(acc), rho, nx, ny, nz);
+    return ok();
+}
+
+// ------------------------------------------------------------------------------------
 struct Cell {
     int i, j, k;
     double ab, de, gh;
@@ -208,6 +292,46 @@ __global__ void __launch_bounds__(256) k_interp_planes(InterpArgs a, const doubl
         }
     }
 }
+__global__ void __launch_bounds__(256) k_interp_pairs(InterpArgs a, const float4 *__restrict__ g8,
+                                                      double *__restrict__ E, unsigned long long *__restrict__ nclamp) {
+    const int64_t plane = (int64_t)a.nx * a.ny;
+    GRID_STRIDE(m, a.np) {
+        Cell c;
+        const bool fl = locate(a, a.x[m], a.y[m], a.z[m], c);
+        count_one(nclamp, fl);
+        const int64_t n0 = c.i + (int64_t)a.nx * c.j + plane * c.k;
+        const double ab = c.ab, de = c.de, gh = c.gh;
+        const double omab = 1. - ab, omde = 1. - de, omgh = 1. - gh;
+        // (j,k), (j+1,k), (j+1,k+1), (j,k+1) rows; each pair = nodes i and i+1
+        const int64_t rows[4] = {n0, n0 + a.nx, n0 + a.nx + plane, n0 + plane};
+        const double wy[4] = {de * gh, omde * gh, omde * omgh, de * omgh};
+        float4 lo[4], hi[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            lo[q] = __ldg(g8 + 2 * rows[q]);
+            hi[q] = __ldg(g8 + 2 * rows[q] + 1);
+        }
+        double ex = 0, ey = 0, ez = 0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const double w0 = ab * wy[q], w1 = omab * wy[q];
+            ex += (double)lo[q].x * w0 + (double)hi[q].x * w1;
+            ey += (double)lo[q].y * w0 + (double)hi[q].y * w1;
+            ez += (double)lo[q].z * w0 + (double)hi[q].z * w1;
+        }
+        E[3 * m] = ex;
+        E[3 * m + 1] = ey;
+        E[3 * m + 2] = ez;
+    }
+}
+
+int launch_interp_pairs(const InterpArgs &a, const float4 *E8, double *E, unsigned long long *nclamp,
+                        cudaStream_t st) {
+    if (a.np <= 0) return OSC_OK;
+    k_interp_pairs<<<nblocks(a.np, 256, 148 * 64), 256, 0, st>>>(a, E8, E, nclamp);
+    return ok();
+}
+
 int launch_interp_planes(const InterpArgs &a, const double *F, double *out, unsigned long long *nclamp,
                          cudaStream_t st) {
     if (a.np <= 0) return OSC_OK;

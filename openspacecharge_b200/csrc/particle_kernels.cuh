@@ -24,8 +24,13 @@ struct DepositArgs {
 template <typename TA>
 int launch_deposit(const DepositArgs &a, TA *rho, unsigned long long *counters, cudaStream_t st);
 
-// Transpose of interpolation for the adjoint: scatter per-particle 3-vectors w_p onto
-// three grids with the CIC weights (same stencil and clamping as interpolation).
+// FP32 deposition through per-cell corner sums: each particle adds its 8 CIC weights to
+// the 8 floats of its cell (two 16-byte vector atomics instead of eight scalar ones), then
+// launch_cells_to_nodes gathers every node's 8 corner contributions in a fixed order.
+// acc is [nx*ny*nz][8] floats (cell index = its low node), zeroed by the caller.
+int launch_deposit_cells(const DepositArgs &a, float *acc, unsigned long long *counters, cudaStream_t st);
+int launch_cells_to_nodes(const float *acc, float *rho, int nx, int ny, int nz, cudaStream_t st);
+
 // CIC gather (interpolate_field, code/open_spacecharge_mod.f90:311-390): clamp cells to
 // [1, nhi-1] (and the array), weights computed after clamping, 8-node sum in the
 // reference's order.  Source: a vec4<T> interleaved grid or three double planes.
@@ -45,6 +50,10 @@ int launch_interp_vec4_any(const InterpArgs &a, const void *E4, void *E, int out
                            unsigned long long *nclamp, cudaStream_t st);
 int launch_interp_planes(const InterpArgs &a, const double *F, double *out,
                          unsigned long long *nclamp, cudaStream_t st);
+// Gather from an x-pair grid: node n holds (E(n), E(n+1)) as two float4 in one 32-byte
+// sector, so the 8 nodes of a particle come from 4 sectors.
+int launch_interp_pairs(const InterpArgs &a, const float4 *E8, double *E, unsigned long long *nclamp,
+                        cudaStream_t st);
 
 // Bounding box {xmin,xmax,ymin,ymax,zmin,zmax} of the particles, written to bb (device)
 // through order-preserving 64-bit keys; also counts non-finite coordinates.

@@ -36,13 +36,14 @@ int fft3d_full(osc_ctx *c, cplx<T> *a, int Nx, int Ny, int Nz, int sx, int sy, i
         if (sg[ax] == 0) continue;
         LineArgs la;
         if (!make_fft_plan(Ls[ax], la.p)) return set_err(c, OSC_E_FFT_SIZE, "FFT length %d unsupported", Ls[ax]);
-        const cplx<T> *tw;
+        TwPair<cplx<T>> tw;
         TRY(twiddles<T>(c, Ls[ax], &tw));
         la.sign = sg[ax];
         la.in_len = la.out_len = Ls[ax];
         la.out_lo = 0;
         la.scale = 1.0;
         la.in_zstride = la.out_zstride = 0;
+        la.flip_mask = 0;
         int nplanes = 1;
         bool row = false;
         if (ax == 0) {
@@ -225,13 +226,14 @@ int freespace_opt(osc_ctx *c, const FreeSpaceJob &j, const TIn *rho) {
         d.kind = kind;
         d.slot = slot;
         d.coef = coef;
+        d.last_x = nx - 1;
     };
     if (j.want_phi && j.phi) add_dest(add_out(0, 1.0), j.phi, 1, 0, 1.0);
     if (j.want_e || j.calc_b) {
         for (int q = 0; q < 3; ++q) {
             const int o = add_out(q + 1, 1.0);
             if (j.E) add_dest(o, j.E + q * N, 1, 0, 1.0);
-            if (j.E4) add_dest(o, j.E4, 0, q, 1.0);
+            if (j.E4) add_dest(o, j.E4, j.e4_pairs ? 4 : 0, q, 1.0);
             if (j.calc_b && j.B && !j.at_cathode) {
                 if (q == 1) add_dest(o, j.B, 1, 0, -j.bcoef);
                 if (q == 0) add_dest(o, j.B + N, 1, 0, j.bcoef);
@@ -250,7 +252,7 @@ int freespace_opt(osc_ctx *c, const FreeSpaceJob &j, const TIn *rho) {
     TRY(ws_get(c, "fs_x2", sizeof(V) * (size_t)nxh * Ny * nz, (void **)&X2));
     TRY(ws_get(c, "fs_x3", sizeof(V) * (size_t)nout * nxh * Ny * nz, (void **)&X3));
     TRY(ws_get(c, "fs_x4", sizeof(V) * (size_t)nout * nxh * ny * nz, (void **)&X4));
-    const V *twx, *twy, *twz;
+    TwPair<V> twx, twy, twz;
     TRY(twiddles<T>(c, Nx, &twx));
     TRY(twiddles<T>(c, Ny, &twy));
     TRY(twiddles<T>(c, Nz, &twz));
@@ -283,6 +285,7 @@ int freespace_opt(osc_ctx *c, const FreeSpaceJob &j, const TIn *rho) {
     ly.out_estride = nxh;
     ly.out_zstride = 0;
     ly.scale = 1.0;
+    ly.flip_mask = 0;
     {
         Launch L_(c, "fft_y_fwd");
         TRY(kerr(c, launch_lines<T>(X1, X2, ly, nz, 1, false, twy, c->stream), "y forward"));

@@ -37,7 +37,8 @@ struct FreeSpaceJob {
     double *phi = nullptr;  // device f64 [N]
     double *E = nullptr;    // device f64 [3][N]
     double *B = nullptr;    // device f64 [3][N]
-    void *E4 = nullptr;     // device vec4<T> [N]
+    void *E4 = nullptr;     // device vec4<T> [N], or the x-pair grid vec4<T> [N][2]
+    int e4_pairs = 0;       // 1: E4 is the x-pair grid read by launch_interp_pairs
 };
 
 // Optimised IGF convolution (cached half-spectra, pruned transforms) in precision T.

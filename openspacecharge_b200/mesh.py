@@ -197,9 +197,11 @@ def osc_rectpipe_green(ctx, mesh3d: Mesh3D, apipe, bpipe, precision=PREC_FP32) -
              int(precision))
 
 
-def space_charge_rectpipe(ctx, mesh3d: Mesh3D, apipe, bpipe, direct_field_calc=False,
+def space_charge_rectpipe(ctx, mesh3d: Mesh3D, apipe, bpipe, direct_field_calc=True,
                           integrated_green_function=True, precision=PREC_FP32) -> None:
-    """space_charge_rectpipe (code/open_spacecharge_mod.f90:110)."""
+    """space_charge_rectpipe (code/open_spacecharge_mod.f90:110).  As in the reference, the
+    default direct_field_calc=True is rejected (the pipe solves for phi and differences it):
+    pass direct_field_calc=False."""
     ctx = _ctx(ctx)
     rho = _grid(mesh3d.rho)
     n = rho.shape
