@@ -53,6 +53,8 @@ struct C2RArgs {
     int64_t in_rstride, in_cstride;
     int ncomp;
     unsigned flip_mask;   // bit c: component c is read at x -> (L-x) mod L (index flip)
+    void *e8;             // optional x-pair grid vec4<T>[N][2] filled from components e8_comp
+    int e8_comp[3];       // components giving (Ex, Ey, Ez) of the x-pair grid
     int ndest[MAX_OUT];
     OutDest dest[MAX_OUT][MAX_DEST];
 };

@@ -1,4 +1,5 @@
-// fft_kernels.cu -- batched shared-memory FFT kernels for the IGF convolution (sm_100a).
+// fft_kernels_impl.cuh -- batched shared-memory FFT kernels for the IGF convolution (sm_100a).
+// Included by fft_kernels_f32.cu and fft_kernels_f64.cu, which instantiate one precision each.
 //
 // The free-space solve runs as five kernels over HBM (FP32 path, G spectra cached):
 //   k_r2c_rows  x: real rho rows -> half spectra (two rows packed per complex line)
@@ -8,6 +9,7 @@
 //   k_c2r_rows  x: inverse to real rows, epilogue scatters E (and B) to their layouts
 // Zero padding of the doubled grid is never stored: loads past the physical window are
 // zeros (or, for the static engines, not read at all) and stores cover only the window.
+#pragma once
 #include <cstdio>
 #include <type_traits>
 
@@ -15,6 +17,7 @@
 
 namespace osc {
 
+#ifdef OSC_FFT_DEFINE_PLAN
 bool make_fft_plan(int L, FFTPlan &p) {
     if (L < 2 || L > FFT_MAX_LEN || (L % 2) != 0) return false;
     p.L = L;
@@ -27,6 +30,7 @@ bool make_fft_plan(int L, FFTPlan &p) {
     while (m % 5 == 0) { p.radix[p.nst++] = 5; m /= 5; }
     return m == 1 && p.nst <= FFT_MAX_STAGES;
 }
+#endif
 
 // Engine-specific twiddle table in global memory.
 template <class E, typename V> __host__ __device__ inline const V *eng_tw(const TwPair<V> &t) {
@@ -50,6 +54,26 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_lines(const cplx<T> *in, cpl
     const V *src = in + (int64_t)blockIdx.z * a.in_zstride + (int64_t)blockIdx.y * a.in_pstride;
     V *dst = out + (int64_t)blockIdx.z * a.out_zstride + (int64_t)blockIdx.y * a.out_pstride;
     load_twiddles(tw, twg, L);
+    if (!ROW) {
+        // columns: the first stage reads global memory, the last stage writes it
+        __syncthreads();
+        const bool flip = (a.flip_mask >> blockIdx.z) & 1u;
+        const T sc = (T)a.scale;
+        auto ld = [&](int e, int l) -> V {
+            const int col = col0 + l;
+            V v = mk<T>(0, 0);
+            if (e < a.in_len && col < a.ncols) v = src[(int64_t)col * a.in_cstride + (int64_t)e * a.in_estride];
+            return v;
+        };
+        auto st = [&](int p, int l, const V &v) {
+            const int col = col0 + l;
+            const int e = (flip ? (L - p) % L : p) - a.out_lo;
+            if (col < a.ncols && e >= 0 && e < a.out_len)
+                dst[(int64_t)col * a.out_cstride + (int64_t)e * a.out_estride] = cscale(v, sc);
+        };
+        E::template run_io<V, NL, MODE == 1, MODE == 2>(buf, a.p, tw, a.sign, ld, st);
+        return;
+    }
     const int ld_len = (E::kLen > 0 && MODE == 1) ? a.in_len : L;  // the static first stage skips zeros
     const int nld = NL * ld_len;
     for (int idx = tid; idx < nld; idx += nthreads) {
@@ -165,6 +189,7 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_c2r_rows(const cplx<T> *__re
     const int nthreads = blockDim.x, tid = threadIdx.x;
     const int64_t row0 = (int64_t)blockIdx.x * (2 * NL);
     const int half = L / 2;
+    T *res = reinterpret_cast<T *>(buf + L * lstr);  // [3][2*NL][nout] when a.e8 is set
     load_twiddles(tw, twg, L);
     for (int c = 0; c < a.ncomp; ++c) {
         const V *src = in + (int64_t)c * a.in_cstride;
@@ -190,8 +215,41 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_c2r_rows(const cplx<T> *__re
             const T val = (rr & 1) ? z.y : z.x;
             const int64_t gidx = row * a.nout + x;
             for (int d = 0; d < a.ndest[c]; ++d) write_dest<T>(a.dest[c][d], gidx, x, val);
+            if (a.e8) {
+#pragma unroll
+                for (int q = 0; q < 3; ++q)
+                    if (a.e8_comp[q] == c) res[(q * 2 * NL + rr) * a.nout + x] = val;
+            }
         }
         __syncthreads();
+    }
+    if (a.e8) {
+        // x-pair grid rows: node n gets (E(n), E(n+1)), the row's last node (E(n), 0)
+        typedef vec4<T> V4;
+        V4 *g = reinterpret_cast<V4 *>(a.e8);
+        for (int idx = tid; idx < 2 * NL * a.nout; idx += nthreads) {
+            const int rr = idx / a.nout, x = idx - rr * a.nout;
+            const int64_t row = row0 + rr;
+            if (row >= a.nrows) continue;
+            const int64_t gidx = row * a.nout + x;
+            const T *r0 = res + rr * a.nout + x;
+            const int64_t cs = (int64_t)2 * NL * a.nout;
+            V4 lo, hi;
+            lo.x = r0[0];
+            lo.y = r0[cs];
+            lo.z = r0[2 * cs];
+            lo.w = (T)0;
+            if (x + 1 < a.nout) {
+                hi.x = r0[1];
+                hi.y = r0[cs + 1];
+                hi.z = r0[2 * cs + 1];
+            } else {
+                hi.x = hi.y = hi.z = (T)0;
+            }
+            hi.w = (T)0;
+            g[2 * gidx] = lo;
+            g[2 * gidx + 1] = hi;
+        }
     }
 }
 
@@ -215,7 +273,10 @@ __device__ __forceinline__ cplx<T> g_lookup(const GSpecDev &g, int kx, int ky, i
 }
 
 // HALF: nz == L/2, so the static engine's forward first stage skips the zero half and
-// its inverse last stage skips the upper half, which is never stored.
+// its inverse last stage skips the upper half, which is never stored.  The forward
+// transform reads the column straight from global memory into its first stage; each
+// inverse transform computes its input (spectrum times Green spectrum, plus the image term)
+// inside its first stage and writes its last stage straight to global memory.
 template <typename T, int NL, class E, bool HALF>
 __global__ void __launch_bounds__(E::kMaxThreads) k_zconv(const cplx<T> *__restrict__ in, cplx<T> *__restrict__ out,
                                                           ZConvArgs a, const cplx<T> *__restrict__ twg,
@@ -227,62 +288,56 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_zconv(const cplx<T> *__restr
     V *rhat = tw + L;
     constexpr int lstr = NL + 1;
     V *buf = rhat + L * lstr;
-    const int nthreads = blockDim.x, tid = threadIdx.x;
     const int col0 = blockIdx.x * NL;
     load_twiddles(tw, twg, L);
-    const int ld_len = (E::kLen > 0 && HALF) ? a.nz : L;
-    for (int idx = tid; idx < NL * ld_len; idx += nthreads) {
-        const int e = idx / NL, c = idx - e * NL;
-        const int col = col0 + c;
+    __syncthreads();
+    auto ld_in = [&](int e, int l) -> V {
+        const int col = col0 + l;
         V v = mk<T>(0, 0);
         if (e < a.nz && col < a.ncols) v = in[(int64_t)e * a.in_estride + col];
-        rhat[e * lstr + c] = v;
-    }
-    __syncthreads();
-    E::template run<V, NL, HALF, false>(rhat, a.p, tw, +1);
+        return v;
+    };
+    auto st_rhat = [&](int e, int l, const V &v) { rhat[e * lstr + l] = v; };
+    E::template run_io<V, NL, HALF, false>(rhat, a.p, tw, +1, ld_in, st_rhat);
     for (int o = 0; o < a.nout; ++o) {
         const int gd = a.gdir[o], gi = a.gimg[o];
         const T icoef = (T)a.img_coef[o];
-        for (int idx = tid; idx < NL * L; idx += nthreads) {
-            const int e = idx / NL, c = idx - e * NL;
-            const int col = min(col0 + c, a.ncols - 1);
+        auto ld_mul = [&](int e, int l) -> V {
+            const int col = min(col0 + l, a.ncols - 1);
             const int ky = col / a.nxh, kx = col - ky * a.nxh;
             V S = mk<T>(0, 0);
-            if (gd >= 0) S = cmul(rhat[e * lstr + c], g_lookup<T>(a.g[gd], kx, ky, e, a.nxh, a.Ny, a.ny, L, a.nz));
+            if (gd >= 0) S = cmul(rhat[e * lstr + l], g_lookup<T>(a.g[gd], kx, ky, e, a.nxh, a.Ny, a.ny, L, a.nz));
             if (gi >= 0) {
                 // spectrum of -rho flipped in z: -w^((nz-1) kz) * rho_hat(-kz)
-                const V rm = rhat[((L - e) % L) * lstr + c];
+                const V rm = rhat[((L - e) % L) * lstr + l];
                 const V ph = __ldg(tw_rt + (int)(((int64_t)a.img_phase_mul * e) % L));
                 V ri = cmul(ph, rm);
                 ri.x = -ri.x * icoef;
                 ri.y = -ri.y * icoef;
                 S = cadd(S, cmul(ri, g_lookup<T>(a.g[gi], kx, ky, e, a.nxh, a.Ny, a.ny, L, a.nz)));
             }
-            buf[e * lstr + c] = S;
-        }
-        __syncthreads();
-        E::template run<V, NL, false, HALF>(buf, a.p, tw, -1);
+            return S;
+        };
         V *dst = out + (int64_t)o * a.out_cstride;
-        for (int idx = tid; idx < NL * a.nz; idx += nthreads) {
-            const int e = idx / NL, c = idx - e * NL;
-            const int col = col0 + c;
-            if (col < a.ncols) dst[(int64_t)e * a.out_estride + col] = buf[e * lstr + c];
-        }
-        __syncthreads();
+        auto st_out = [&](int e, int l, const V &v) {
+            const int col = col0 + l;
+            if (e < a.nz && col < a.ncols) dst[(int64_t)e * a.out_estride + col] = v;
+        };
+        E::template run_io<V, NL, false, HALF>(buf, a.p, tw, -1, ld_mul, st_out);
     }
 }
 
 // ------------------------------------------------------------------------------------
 // Launchers.  Shared memory above 48 KB needs the opt-in attribute, set per kernel.
-template <typename K> static int set_smem(K kern, size_t bytes) {
+template <typename K> inline int set_smem(K kern, size_t bytes) {
     if (bytes > 227 * 1024) return OSC_E_INVALID;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     return e == cudaSuccess ? OSC_OK : OSC_E_CUDA;
 }
-static inline int launch_ok() { return cudaGetLastError() == cudaSuccess ? OSC_OK : OSC_E_CUDA; }
+inline int launch_ok() { return cudaGetLastError() == cudaSuccess ? OSC_OK : OSC_E_CUDA; }
 
 // Runtime-engine NL: a whole number of threads, <= 256 threads, buffers within budget.
-static int pick_nl_rt(int L, int nl_max, size_t elem, int nbuf) {
+inline int pick_nl_rt(int L, int nl_max, size_t elem, int nbuf) {
     for (int nl = nl_max; nl >= 2; nl /= 2) {
         if ((L * nl) % FFT_EPT != 0 || fft_threads(L, nl) > FftRuntime::kMaxThreads) continue;
         if ((size_t)nbuf * L * (nl + 1) * elem + L * elem > 110 * 1024 && nl > 2) continue;
@@ -294,7 +349,7 @@ static int pick_nl_rt(int L, int nl_max, size_t elem, int nbuf) {
 // Calls f(std::integral_constant<int, NL>) for the engine's lines-per-CTA.  Static engines
 // use a compile-time NL: the widest that fits (one line buffer) or, for the two-buffer
 // z-pass, at most 4 lines in ~48 KB so several CTAs share an SM.
-template <typename T, class E, class F> static int with_nl(int L, int nbuf, int nl_max, int nl_req, F &&f) {
+template <typename T, class E, class F> inline int with_nl(int L, int nbuf, int nl_max, int nl_req, F &&f) {
     if constexpr (E::kLen > 0) {
         (void)L;
         (void)nl_req;
@@ -316,7 +371,7 @@ template <typename T, class E, class F> static int with_nl(int L, int nbuf, int 
 }
 
 template <typename T, int NL, bool ROW, class E, int MODE>
-static int launch_lines_k(const cplx<T> *in, cplx<T> *out, const LineArgs &a, int nplanes, int ncomp, const cplx<T> *tw,
+inline int launch_lines_k(const cplx<T> *in, cplx<T> *out, const LineArgs &a, int nplanes, int ncomp, const cplx<T> *tw,
                           cudaStream_t st) {
     const int L = a.p.L;
     const int nt = fft_threads(L, NL);
@@ -389,7 +444,8 @@ int launch_c2r_rows(const cplx<T> *in, const C2RArgs &a, const TwPair<cplx<T>> &
             constexpr int NL = decltype(nlc)::value;
             const int nt = fft_threads(L, NL);
             if (nt < 1 || nt > E::kMaxThreads || (L * NL) % FFT_EPT) return OSC_E_FFT_SIZE;
-            const size_t sm = sizeof(cplx<T>) * ((size_t)L + (size_t)L * (NL + 1));
+            const size_t sm = sizeof(cplx<T>) * ((size_t)L + (size_t)L * (NL + 1)) +
+                              (a.e8 ? sizeof(T) * 3 * 2 * NL * (size_t)a.nout : 0);
             const unsigned nblk = (unsigned)ceil_div(a.nrows, 2 * NL);
             if (E::kLen > 0 && 2 * a.nout == L && a.flip_mask == 0) {
                 auto kern = k_c2r_rows<T, NL, E, true>;
@@ -435,24 +491,5 @@ int launch_zconv(const cplx<T> *in, cplx<T> *out, const ZConvArgs &a, const TwPa
         });
     });
 }
-
-// Explicit instantiations.
-template int launch_lines<float>(const cplx<float> *, cplx<float> *, const LineArgs &, int, int, bool,
-                                 const TwPair<cplx<float>> &, cudaStream_t);
-template int launch_lines<double>(const cplx<double> *, cplx<double> *, const LineArgs &, int, int, bool,
-                                  const TwPair<cplx<double>> &, cudaStream_t);
-template int launch_r2c_rows<float, float>(const float *, cplx<float> *, const R2CArgs &, const TwPair<cplx<float>> &,
-                                           cudaStream_t);
-template int launch_r2c_rows<float, double>(const double *, cplx<float> *, const R2CArgs &,
-                                            const TwPair<cplx<float>> &, cudaStream_t);
-template int launch_r2c_rows<double, double>(const double *, cplx<double> *, const R2CArgs &,
-                                             const TwPair<cplx<double>> &, cudaStream_t);
-template int launch_c2r_rows<float>(const cplx<float> *, const C2RArgs &, const TwPair<cplx<float>> &, cudaStream_t);
-template int launch_c2r_rows<double>(const cplx<double> *, const C2RArgs &, const TwPair<cplx<double>> &,
-                                     cudaStream_t);
-template int launch_zconv<float>(const cplx<float> *, cplx<float> *, const ZConvArgs &, const TwPair<cplx<float>> &,
-                                 int, cudaStream_t);
-template int launch_zconv<double>(const cplx<double> *, cplx<double> *, const ZConvArgs &,
-                                  const TwPair<cplx<double>> &, int, cudaStream_t);
 
 }  // namespace osc

@@ -267,8 +267,79 @@ __device__ __forceinline__ void fft_ct(V *buf, const V *tw, int sign) {
     if constexpr (!last) fft_ct<V, NL, L, Ns * R, false, HOUT, Rest...>(buf, tw, sign);
 }
 
+// Stage with explicit input and output functors: ld(e, line) -> V and st(e, line, V).
+// The first stage of a transform can read straight from global memory (or compute its
+// input, e.g. a spectral product) and the last stage can write straight to global memory,
+// which saves two shared-memory passes per transform.
+template <typename V, int R, int NL, int L, int Ns, bool HALF_IN, bool HALF_OUT, class LD, class ST>
+__device__ __forceinline__ void stage_io(const LD &ld, const ST &st, const V *tw, int sign) {
+    constexpr int MAXB = (FFT_EPT + R - 1) / R;
+    constexpr int nb = L / R;
+    constexpr int total = nb * NL;
+    constexpr int nthreads = L * NL / FFT_EPT;
+    constexpr int toff = Ns - 1;
+    constexpr bool half_in = HALF_IN && (R % 2 == 0);
+    constexpr bool half_out = HALF_OUT && (R % 2 == 0);
+    const int tid = threadIdx.x;
+    V v[MAXB][R];
+#pragma unroll
+    for (int q = 0; q < MAXB; ++q) {
+        const int b = tid + q * nthreads;
+        if (total % nthreads == 0 || b < total) {
+            const int line = b % NL, j = b / NL, k = j % Ns;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                V x;
+                if (half_in && r >= R / 2) {
+                    x.x = 0;
+                    x.y = 0;
+                } else {
+                    x = ld(j + r * nb, line);
+                    if (r && Ns > 1) x = cmul(x, tw_get(tw, toff + k * (R - 1) + (r - 1), sign));
+                }
+                v[q][r] = x;
+            }
+            Dft<R>::run(v[q], sign);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < MAXB; ++q) {
+        const int b = tid + q * nthreads;
+        if (total % nthreads == 0 || b < total) {
+            const int line = b % NL, j = b / NL, k = j % Ns;
+            const int idxD = (j / Ns) * Ns * R + k;
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                if (!half_out || r < R / 2) st(idxD + r * Ns, line, v[q][r]);
+        }
+    }
+    __syncthreads();
+}
+
+template <int... Rs> struct Radices {};
+
+template <typename V, int NL, int L, int Ns, bool HIN, bool HOUT, int R, int... Rest, class LD, class ST>
+__device__ __forceinline__ void fft_io_rec(Radices<R, Rest...>, V *buf, const V *tw, int sign, const LD &ld,
+                                           const ST &st) {
+    constexpr bool first = Ns == 1, last = sizeof...(Rest) == 0;
+    constexpr int lstr = NL + 1;
+    auto sld = [buf](int e, int l) -> V { return buf[e * lstr + l]; };
+    auto sst = [buf](int e, int l, const V &x) { buf[e * lstr + l] = x; };
+    if constexpr (first && last) stage_io<V, R, NL, L, Ns, HIN, HOUT>(ld, st, tw, sign);
+    else if constexpr (first) stage_io<V, R, NL, L, Ns, HIN, false>(ld, sst, tw, sign);
+    else if constexpr (last) stage_io<V, R, NL, L, Ns, false, HOUT>(sld, st, tw, sign);
+    else stage_io<V, R, NL, L, Ns, false, false>(sld, sst, tw, sign);
+    if constexpr (!last) fft_io_rec<V, NL, L, Ns * R, HIN, HOUT>(Radices<Rest...>{}, buf, tw, sign, ld, st);
+}
+
 // FFT engines.  FftRuntime CTAs are capped at 256 threads so the generic stage code keeps
 // its registers; FftStatic CTAs at 512.  HIN/HOUT only change the static engine.
+//
+// run_io(buf, plan, tw, sign, ld, st): transform with input ld(e, line) (asked only for
+// e < L/2 when HIN) and output st(e, line, v) (called only for e < L/2 when HOUT; storers
+// must themselves ignore indices outside their window).  buf is the working buffer; ld may
+// read another shared buffer.
 struct FftRuntime {
     static constexpr int kLen = 0;
     static constexpr int kMaxThreads = 256;
@@ -277,6 +348,23 @@ struct FftRuntime {
     template <typename V, int NL, bool HIN, bool HOUT>
     __device__ __forceinline__ static void run(V *buf, const FFTPlan &p, const V *tw, int sign) {
         fft_smem<V, NL>(buf, NL + 1, p, tw, sign);
+    }
+    template <typename V, int NL, bool HIN, bool HOUT, class LD, class ST>
+    __device__ __forceinline__ static void run_io(V *buf, const FFTPlan &p, const V *tw, int sign, const LD &ld,
+                                                  const ST &st) {
+        const int L = p.L, nthreads = blockDim.x, tid = threadIdx.x;
+        constexpr int lstr = NL + 1;
+        for (int idx = tid; idx < NL * L; idx += nthreads) {
+            const int e = idx / NL, l = idx - e * NL;
+            buf[e * lstr + l] = ld(e, l);
+        }
+        __syncthreads();
+        fft_smem<V, NL>(buf, lstr, p, tw, sign);
+        for (int idx = tid; idx < NL * L; idx += nthreads) {
+            const int e = idx / NL, l = idx - e * NL;
+            st(e, l, buf[e * lstr + l]);
+        }
+        __syncthreads();
     }
 };
 template <int L_, int... Rs> struct FftStatic {
@@ -287,6 +375,11 @@ template <int L_, int... Rs> struct FftStatic {
     template <typename V, int NL, bool HIN, bool HOUT>
     __device__ __forceinline__ static void run(V *buf, const FFTPlan &, const V *tw, int sign) {
         fft_ct<V, NL, L_, 1, HIN, HOUT, Rs...>(buf, tw, sign);
+    }
+    template <typename V, int NL, bool HIN, bool HOUT, class LD, class ST>
+    __device__ __forceinline__ static void run_io(V *buf, const FFTPlan &, const V *tw, int sign, const LD &ld,
+                                                  const ST &st) {
+        fft_io_rec<V, NL, L_, 1, HIN, HOUT>(Radices<Rs...>{}, buf, tw, sign, ld, st);
     }
 };
 

@@ -233,7 +233,14 @@ int freespace_opt(osc_ctx *c, const FreeSpaceJob &j, const TIn *rho) {
         for (int q = 0; q < 3; ++q) {
             const int o = add_out(q + 1, 1.0);
             if (j.E) add_dest(o, j.E + q * N, 1, 0, 1.0);
-            if (j.E4) add_dest(o, j.E4, j.e4_pairs ? 4 : 0, q, 1.0);
+            if (j.E4) {
+                if (j.e4_pairs) {  // staged in the x epilogue and written as whole pairs
+                    cr.e8 = j.E4;
+                    cr.e8_comp[q] = o;
+                } else {
+                    add_dest(o, j.E4, 0, q, 1.0);
+                }
+            }
             if (j.calc_b && j.B && !j.at_cathode) {
                 if (q == 1) add_dest(o, j.B, 1, 0, -j.bcoef);
                 if (q == 0) add_dest(o, j.B + N, 1, 0, j.bcoef);
