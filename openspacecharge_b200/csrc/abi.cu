@@ -39,7 +39,7 @@ int h2d(osc_ctx *ctx, void *d, const void *h, size_t bytes) {
 int d2h(osc_ctx *ctx, void *h, const void *d, size_t bytes) {
     return cuda_check(ctx, cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, ctx->stream), "D2H copy");
 }
-int sync(osc_ctx *ctx) { return cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "stream synchronize"); }
+int sync(osc_ctx *ctx) { return ctx_sync(ctx); }
 
 // Stage a host array on the device under a workspace name.
 template <typename T> int stage_in(osc_ctx *ctx, const char *name, const T *h, size_t n, T **d) {
@@ -201,11 +201,14 @@ int osc_ctx_create(int device, osc_ctx **out) {
         cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMalloc(&ctx->d_small, sizeof(unsigned long long) * 64) != cudaSuccess ||
         cudaMallocHost(&ctx->h_small, sizeof(unsigned long long) * 64) != cudaSuccess ||
-        cudaMalloc(&ctx->d_partials, sizeof(double) * 1024) != cudaSuccess) {
+        cudaMalloc(&ctx->d_partials, sizeof(double) * 1024) != cudaSuccess ||
+        cudaHostAlloc((void **)&ctx->h_fault, sizeof(unsigned), cudaHostAllocMapped) != cudaSuccess ||
+        cudaHostGetDevicePointer((void **)&ctx->d_fault, ctx->h_fault, 0) != cudaSuccess) {
         cudaGetLastError();
         osc_ctx_destroy(ctx);
         return OSC_E_CUDA;
     }
+    *ctx->h_fault = 0;
     ctx->stream = ctx->own_stream;
     *out = ctx;
     return OSC_OK;
@@ -230,6 +233,7 @@ int osc_ctx_destroy(osc_ctx *ctx) {
     if (ctx->d_small) cudaFree(ctx->d_small);
     if (ctx->h_small) cudaFreeHost(ctx->h_small);
     if (ctx->d_partials) cudaFree(ctx->d_partials);
+    if (ctx->h_fault) cudaFreeHost(ctx->h_fault);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return OSC_OK;

@@ -47,6 +47,17 @@ int ws_get(osc_ctx *c, const char *name, size_t bytes, void **out) {
     return OSC_OK;
 }
 
+int ctx_sync(osc_ctx *c) {
+    const int rc = cuda_check(c, cudaStreamSynchronize(c->stream), "stream synchronize");
+    if (rc) return rc;
+    if (c->h_fault && *reinterpret_cast<volatile unsigned *>(c->h_fault)) {
+        const unsigned f = *c->h_fault;
+        *reinterpret_cast<volatile unsigned *>(c->h_fault) = 0;
+        return set_err(c, OSC_E_CUDA, "device wait gave up (fault code %u): a bulk copy did not complete", f);
+    }
+    return OSC_OK;
+}
+
 // exp(+2 pi i m/n) in FP64, reducing the angle to one octant so every entry is as exact as
 // the FP64 sin/cos of an angle in [0, pi/4].
 static void cis_exact(int64_t m, int64_t n, double &cs, double &sn) {
@@ -79,9 +90,31 @@ template <typename T> static int upload(osc_ctx *c, const std::vector<cplx<T>> &
     return e == cudaSuccess ? OSC_OK : cuda_check(c, e, "twiddle upload");
 }
 
+// Per-stage table of a radix sequence: stage s (Ns = product of earlier radices, radix R)
+// has entry (Ns-1) + k*(R-1) + (r-1) = exp(2 pi i r k/(Ns R)) for k < Ns, 1 <= r < R;
+// L-1 entries in all.
+template <typename T> static std::vector<cplx<T>> stage_table(int L, const int *rad, int nst) {
+    std::vector<cplx<T>> h(L, mk<T>((T)1, (T)0));
+    int Ns = 1;
+    for (int s = 0; s < nst; ++s) {
+        const int R = rad[s];
+        for (int k = 0; k < Ns; ++k)
+            for (int r = 1; r < R; ++r) {
+                double cs, sn;
+                cis_exact((int64_t)r * k, (int64_t)Ns * R, cs, sn);
+                h[(Ns - 1) + k * (R - 1) + (r - 1)] = mk<T>((T)cs, (T)sn);
+            }
+        Ns *= R;
+    }
+    return h;
+}
+
+// Keys of the table map: L runtime table, -L static-engine stages, L + kWarpKey warp-engine
+// stages (a null entry when the length has no such engine).
+static constexpr int kWarpKey = 1 << 20;
+
 template <typename T> int twiddles(osc_ctx *c, int L, TwPair<cplx<T>> *out) {
     auto &tab = sizeof(T) == 4 ? c->tw32 : c->tw64;
-    // runtime table under key L, per-stage static table under key -L
     if (tab.find(L) == tab.end()) {
         std::vector<cplx<T>> h(L);
         for (int m = 0; m < L; ++m) {
@@ -94,40 +127,29 @@ template <typename T> int twiddles(osc_ctx *c, int L, TwPair<cplx<T>> *out) {
         if (rc) return rc;
         tab[L] = b;
     }
-    if (tab.find(-L) == tab.end()) {
-        // stage s (Ns = product of earlier radices, radix R): entry (Ns-1) + k*(R-1) + (r-1)
-        // holds exp(2 pi i r k/(Ns R)) for k < Ns, 1 <= r < R; L-1 entries in all
-        std::vector<cplx<T>> h(L, mk<T>((T)1, (T)0));
-        const bool has_static = dispatch_fft_len(L, [&](auto eng) -> int {
+    for (int which = 0; which < 2; ++which) {
+        const int key = which == 0 ? -L : L + kWarpKey;
+        if (tab.find(key) != tab.end()) continue;
+        std::vector<cplx<T>> h;
+        auto make = [&](auto eng) -> int {
             using E = decltype(eng);
-            if constexpr (E::kLen > 0) {
-                int Ns = 1;
-                for (int s = 0; s < E::kNst; ++s) {
-                    const int R = E::kRad[s];
-                    for (int k = 0; k < Ns; ++k)
-                        for (int r = 1; r < R; ++r) {
-                            double cs, sn;
-                            cis_exact((int64_t)r * k, (int64_t)Ns * R, cs, sn);
-                            h[(Ns - 1) + k * (R - 1) + (r - 1)] = mk<T>((T)cs, (T)sn);
-                        }
-                    Ns *= R;
-                }
-                return 1;
-            }
+            if constexpr (E::kLen > 0) h = stage_table<T>(L, E::kRad, E::kNst);
             return 0;
-        });
-        if (has_static) {
-            DevBuf b;
+        };
+        if (which == 0) dispatch_fft_len(L, make);
+        else dispatch_warp_len(L, make);
+        DevBuf b{nullptr, 0};
+        if (!h.empty()) {
             int rc = upload<T>(c, h, b);
             if (rc) return rc;
-            tab[-L] = b;
-        } else {
-            tab[-L] = DevBuf{nullptr, 0};
         }
+        tab[key] = b;
     }
     out->rt = reinterpret_cast<const cplx<T> *>(tab[L].p);
     const DevBuf &s = tab[-L];
     out->st = s.p ? reinterpret_cast<const cplx<T> *>(s.p) : out->rt;
+    const DevBuf &w = tab[L + kWarpKey];
+    out->wt = w.p ? reinterpret_cast<const cplx<T> *>(w.p) : out->rt;
     return OSC_OK;
 }
 template int twiddles<float>(osc_ctx *, int, TwPair<cplx<float>> *);

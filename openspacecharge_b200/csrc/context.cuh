@@ -72,6 +72,9 @@ struct osc_ctx {
     unsigned long long *d_small = nullptr;  // 64 words
     unsigned long long *h_small = nullptr;  // pinned 64 words
     double *d_partials = nullptr;           // 1024 doubles
+    // host-mapped word where kernels report bounded waits that gave up (0 = none)
+    unsigned *h_fault = nullptr;
+    unsigned *d_fault = nullptr;
     // profiling
     std::vector<osc::ProfRec> prof_pending;
     std::map<std::string, osc::ProfSum> prof;
@@ -84,6 +87,8 @@ namespace osc {
 
 int set_err(osc_ctx *c, int code, const char *fmt, ...);
 int cuda_check(osc_ctx *c, cudaError_t e, const char *what);
+// Synchronises the context stream, then reports (and clears) a fault word set by a kernel.
+int ctx_sync(osc_ctx *c);
 // Named device workspace of at least `bytes` (grown by reallocation; contents not kept).
 int ws_get(osc_ctx *c, const char *name, size_t bytes, void **out);
 // Twiddle tables of length L (runtime table and, when L has a static engine, its

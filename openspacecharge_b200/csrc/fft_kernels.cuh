@@ -62,13 +62,35 @@ struct C2RArgs {
 // Stored Green spectrum of one kernel component on the half-spectrum grid
 // kx in [0, nx], ky in [0, Ny), kz in [0, Nz).  Axes with sym_* hold only k <= n and the
 // value at N-k is par_* times the value at k.  real_valued spectra store one T per point
-// meaning s (imag_unit=0) or i*s (imag_unit=1); others store cplx<T>.
+// meaning s (imag_unit=0) or i*s (imag_unit=1); others store cplx<T>.  Layout [kz][ky][kx],
+// or [ky][kx][kz] when zinner is set (the layout of the warp-per-column z pass), with
+// columns zpitch >= dimz elements apart (a multiple of 16 bytes).
 struct GSpecDev {
     const void *data;
     int real_valued, imag_unit;
     int sym_y, sym_z, par_y, par_z;
     int dimy, dimz;
+    int zinner, zpitch;
 };
+
+// Value of a stored Green spectrum at (kx, ky, kz) of the Nx/2+1 x Ny x Nz half spectrum.
+template <typename T>
+__device__ __forceinline__ cplx<T> g_lookup(const GSpecDev &g, int kx, int ky, int kz, int nxh,
+                                            int Ny, int ny, int Nz, int nz) {
+    int yy = ky, zz = kz;
+    bool neg = false;
+    if (g.sym_y && ky > ny) { yy = Ny - ky; neg ^= (g.par_y < 0); }
+    if (g.sym_z && kz > nz) { zz = Nz - kz; neg ^= (g.par_z < 0); }
+    const int64_t idx = g.zinner ? ((int64_t)yy * nxh + kx) * g.zpitch + zz : ((int64_t)zz * g.dimy + yy) * nxh + kx;
+    if (g.real_valued) {
+        T s = __ldg(reinterpret_cast<const T *>(g.data) + idx);
+        if (neg) s = -s;
+        return g.imag_unit ? mk<T>(0, s) : mk<T>(s, 0);
+    }
+    cplx<T> v = __ldg(reinterpret_cast<const cplx<T> *>(g.data) + idx);
+    if (neg) { v.x = -v.x; v.y = -v.y; }
+    return v;
+}
 
 // Fused z pass of the free-space convolution: forward transform of each (kx,ky) column
 // (nz non-zero planes, length Nz), multiply by stored Green spectra (optionally adding the
@@ -88,6 +110,7 @@ struct ZConvArgs {
     int img_phase_mul;    // image spectrum = -w^(img_phase_mul*kz) * rho_hat(-kz)
     int ng;
     GSpecDev g[8];
+    unsigned *fault;      // host-mapped fault word (bounded waits that gave up), or null
 };
 
 template <typename T>
@@ -97,6 +120,9 @@ template <typename T, typename TIn>
 int launch_r2c_rows(const TIn *in, cplx<T> *out, const R2CArgs &a, const TwPair<cplx<T>> &tw, cudaStream_t st);
 template <typename T>
 int launch_c2r_rows(const cplx<T> *in, const C2RArgs &a, const TwPair<cplx<T>> &tw, cudaStream_t st);
+// True when the z pass of length L with nz = L/2 non-zero planes runs the warp-per-column
+// kernel, whose Green spectra must be stored with zinner set.
+bool zconv_warp_ok(int L, int nz, int elem_bytes);
 template <typename T>
 int launch_zconv(const cplx<T> *in, cplx<T> *out, const ZConvArgs &a, const TwPair<cplx<T>> &tw,
                  int nl, cudaStream_t st);

@@ -14,6 +14,7 @@
 #include <type_traits>
 
 #include "fft_kernels.cuh"
+#include "zconv_warp.cuh"
 
 namespace osc {
 
@@ -29,6 +30,11 @@ bool make_fft_plan(int L, FFTPlan &p) {
     while (m % 3 == 0) { p.radix[p.nst++] = 3; m /= 3; }
     while (m % 5 == 0) { p.radix[p.nst++] = 5; m /= 5; }
     return m == 1 && p.nst <= FFT_MAX_STAGES;
+}
+// The warp-per-column z pass holds a column's spectrum in registers: FP32 only.
+bool zconv_warp_ok(int L, int nz, int elem_bytes) {
+    if (elem_bytes != 4 || 2 * nz != L) return false;
+    return dispatch_warp_len(L, [](auto eng) -> int { return decltype(eng)::kLen > 0 ? 1 : 0; }) != 0;
 }
 #endif
 
@@ -254,24 +260,6 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_c2r_rows(const cplx<T> *__re
 }
 
 // ------------------------------------------------------------------------------------
-template <typename T>
-__device__ __forceinline__ cplx<T> g_lookup(const GSpecDev &g, int kx, int ky, int kz, int nxh,
-                                            int Ny, int ny, int Nz, int nz) {
-    int yy = ky, zz = kz;
-    bool neg = false;
-    if (g.sym_y && ky > ny) { yy = Ny - ky; neg ^= (g.par_y < 0); }
-    if (g.sym_z && kz > nz) { zz = Nz - kz; neg ^= (g.par_z < 0); }
-    const int64_t idx = ((int64_t)zz * g.dimy + yy) * nxh + kx;
-    if (g.real_valued) {
-        T s = __ldg(reinterpret_cast<const T *>(g.data) + idx);
-        if (neg) s = -s;
-        return g.imag_unit ? mk<T>(0, s) : mk<T>(s, 0);
-    }
-    cplx<T> v = __ldg(reinterpret_cast<const cplx<T> *>(g.data) + idx);
-    if (neg) { v.x = -v.x; v.y = -v.y; }
-    return v;
-}
-
 // HALF: nz == L/2, so the static engine's forward first stage skips the zero half and
 // its inverse last stage skips the upper half, which is never stored.  The forward
 // transform reads the column straight from global memory into its first stage; each
@@ -463,10 +451,59 @@ int launch_c2r_rows(const cplx<T> *in, const C2RArgs &a, const TwPair<cplx<T>> &
     });
 }
 
+template <typename T, int W, int MODE, int L, int... Rs>
+inline int launch_zconv_warp_k(const cplx<T> *in, cplx<T> *out, const ZConvArgs &a, const TwPair<cplx<T>> &tw,
+                               cudaStream_t st) {
+    const size_t sm = zconv_warp_smem<T>(L, W, MODE, a.nout, a.g[0].zpitch);
+    auto kern = k_zconv_warp<T, W, MODE, L, Rs...>;
+    int rc = set_smem(kern, sm);
+    if (rc) return rc;
+    kern<<<(unsigned)ceil_div(a.ncols, W), W * 32, sm, st>>>(in, out, a, tw.wt, tw.rt);
+    return launch_ok();
+}
+template <typename T, int MODE, int L, int... Rs>
+inline int launch_zconv_warp(WarpFft<L, Rs...>, const cplx<T> *in, cplx<T> *out, const ZConvArgs &a,
+                             const TwPair<cplx<T>> &tw, cudaStream_t st) {
+    return launch_zconv_warp_k<T, 8, MODE, L, Rs...>(in, out, a, tw, st);
+}
+
+// Staged Green columns need real spectra, even/odd in z, one common 16-byte column pitch.
+template <typename T> inline bool zconv_can_stage(const ZConvArgs &a) {
+    const int zp = a.g[0].zpitch;
+    if (zp <= 0 || (zp * sizeof(T)) % 16) return false;
+    for (int o = 0; o < a.nout; ++o) {
+        const int gd = a.gdir[o];
+        if (gd < 0 || a.gimg[o] >= 0) return false;
+        const GSpecDev &g = a.g[gd];
+        if (!g.real_valued || !g.sym_z || !g.zinner || g.zpitch != zp || g.dimz > zp) return false;
+        if (reinterpret_cast<uintptr_t>(g.data) % 16) return false;
+    }
+    return zconv_warp_smem<T>(a.p.L, 8, ZW_STAGED, a.nout, zp) <= 100 * 1024;
+}
+
 template <typename T>
 int launch_zconv(const cplx<T> *in, cplx<T> *out, const ZConvArgs &a, const TwPair<cplx<T>> &tw, int nl,
                  cudaStream_t st) {
     const int L = a.p.L;
+    if (zconv_warp_ok(L, a.nz, (int)sizeof(T))) {
+        for (int i = 0; i < a.ng; ++i)
+            if (!a.g[i].zinner) return OSC_E_INVALID;  // spectra stored for the other z pass
+        bool img = false;
+        for (int o = 0; o < a.nout; ++o) img |= a.gimg[o] >= 0;
+        if (tw.wt == tw.rt) return OSC_E_INVALID;
+        const bool staged = !img && zconv_can_stage<T>(a);
+        return dispatch_warp_len(L, [&](auto eng) -> int {
+            using E = decltype(eng);
+            if constexpr (E::kLen > 0 && sizeof(T) == 4) {
+                if (img) return launch_zconv_warp<T, ZW_IMAGE>(eng, in, out, a, tw, st);
+                if (staged) return launch_zconv_warp<T, ZW_STAGED>(eng, in, out, a, tw, st);
+                return launch_zconv_warp<T, ZW_DIRECT>(eng, in, out, a, tw, st);
+            }
+            return OSC_E_INVALID;
+        });
+    }
+    for (int i = 0; i < a.ng; ++i)
+        if (a.g[i].zinner) return OSC_E_INVALID;
     return dispatch_fft_len(L, [&](auto eng) -> int {
         using E = decltype(eng);
         const cplx<T> *twe = eng_tw<E>(tw);

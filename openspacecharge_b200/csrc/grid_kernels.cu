@@ -106,29 +106,40 @@ int launch_green_center(const double *F, double2 *cg, const CenterArgs &a, cudaS
 
 template <typename T>
 __global__ void k_green_extract(const double2 *__restrict__ ghat, void *out, int nx, int Nx, int Ny,
-                                int dimy, int dimz, int real_valued, int imag_unit, double scale) {
+                                int dimy, int dimz, int real_valued, int imag_unit, double scale, int zpitch) {
     const int nxh = nx + 1;
-    const int64_t n = (int64_t)nxh * dimy * dimz;
+    const int64_t n = (int64_t)nxh * dimy * (zpitch > 0 ? zpitch : dimz);
     GRID_STRIDE(idx, n) {
-        const int kx = (int)(idx % nxh);
-        const int64_t r = idx / nxh;
-        const int ky = (int)(r % dimy);
-        const int kz = (int)(r / dimy);
-        const double2 v = ghat[kx + (int64_t)Nx * (ky + (int64_t)Ny * kz)];
+        int kx, ky, kz;
+        if (zpitch > 0) {  // [ky][kx][kz], columns zpitch apart
+            kz = (int)(idx % zpitch);
+            const int64_t r = idx / zpitch;
+            kx = (int)(r % nxh);
+            ky = (int)(r / nxh);
+        } else {  // [kz][ky][kx]
+            kx = (int)(idx % nxh);
+            const int64_t r = idx / nxh;
+            ky = (int)(r % dimy);
+            kz = (int)(r / dimy);
+        }
+        double2 v = make_double2(0.0, 0.0);
+        if (kz < dimz) v = ghat[kx + (int64_t)Nx * (ky + (int64_t)Ny * kz)];
         if (real_valued) reinterpret_cast<T *>(out)[idx] = (T)((imag_unit ? v.y : v.x) * scale);
         else reinterpret_cast<cplx<T> *>(out)[idx] = mk<T>((T)(v.x * scale), (T)(v.y * scale));
     }
 }
 template <typename T>
 int launch_green_extract(const double2 *ghat, void *out, int nx, int Nx, int Ny, int dimy, int dimz,
-                         int real_valued, int imag_unit, double scale, cudaStream_t st) {
-    const int64_t n = (int64_t)(nx + 1) * dimy * dimz;
+                         int real_valued, int imag_unit, double scale, int zpitch, cudaStream_t st) {
+    const int64_t n = (int64_t)(nx + 1) * dimy * (zpitch > 0 ? zpitch : dimz);
     k_green_extract<T><<<nblocks(n, 256), 256, 0, st>>>(ghat, out, nx, Nx, Ny, dimy, dimz, real_valued,
-                                                        imag_unit, scale);
+                                                        imag_unit, scale, zpitch);
     return ok();
 }
-template int launch_green_extract<float>(const double2 *, void *, int, int, int, int, int, int, int, double, cudaStream_t);
-template int launch_green_extract<double>(const double2 *, void *, int, int, int, int, int, int, int, double, cudaStream_t);
+template int launch_green_extract<float>(const double2 *, void *, int, int, int, int, int, int, int, double, int,
+                                         cudaStream_t);
+template int launch_green_extract<double>(const double2 *, void *, int, int, int, int, int, int, int, double, int,
+                                          cudaStream_t);
 
 // ------------------------------------------------------------------------------------
 __global__ void k_pad_rho(const double *__restrict__ rho, double2 *__restrict__ crho, int nx, int ny, int nz,

@@ -32,10 +32,17 @@ struct CenterArgs {
 };
 int launch_green_center(const double *F, double2 *cg, const CenterArgs &a, cudaStream_t st);
 
-// Stored half-spectrum extraction: kx in [0,nx], ky in [0,dimy), kz in [0,dimz), times scale.
+// Stored half-spectrum extraction: kx in [0,nx], ky in [0,dimy), kz in [0,dimz), times scale;
+// layout [kz][ky][kx], or [ky][kx][kz] with columns zpitch elements apart when zpitch > 0
+// (padding zeroed).
 template <typename T>
 int launch_green_extract(const double2 *ghat, void *out, int nx, int Nx, int Ny, int dimy, int dimz,
-                         int real_valued, int imag_unit, double scale, cudaStream_t st);
+                         int real_valued, int imag_unit, double scale, int zpitch, cudaStream_t st);
+// Column pitch (elements) of the kz-innermost layout: dimz rounded up to 16 bytes.
+inline int green_zpitch(int dimz, size_t elem_bytes) {
+    const int q = (int)(16 / elem_bytes) > 0 ? (int)(16 / elem_bytes) : 1;
+    return (dimz + q - 1) / q * q;
+}
 
 // ---- plain (reference-algorithm) path helpers ---------------------------------------
 // crho = 0 everywhere, rho (sign * flipped-in-z if flipz) in the low octant.

@@ -339,6 +339,9 @@ template <typename T> static int pipe_comb(osc_ctx *c, const LGeom &g) {
         TRY(kchk(c, launch_green_extract<T>(reinterpret_cast<const double2 *>(p.g[t].p),
                                             reinterpret_cast<char *>(p.comb.p) + t * each, nx, g.period[0],
                                             g.period[1], g.period[1], g.period[2], 0, 0, PIPE_SIGN[t] * factr,
+                                            zconv_warp_ok(g.period[2], g.n[2], (int)sizeof(T))
+                                                ? green_zpitch(g.period[2], sizeof(cplx<T>))
+                                                : 0,
                                             c->stream),
                  "pipe extract"));
     }
@@ -407,6 +410,7 @@ template <typename T> static int pipe_phi_opt(osc_ctx *c, const LGeom &g, const 
     za.out_cstride = (int64_t)nxh * Ny * nz;
     za.nout = nout;
     za.ng = 4;
+    za.fault = c->d_fault;
     const size_t each = (size_t)nxh * Ny * Nz;
     for (int t = 0; t < 4; ++t) {
         za.gdir[t] = t;
@@ -419,6 +423,8 @@ template <typename T> static int pipe_phi_opt(osc_ctx *c, const LGeom &g, const 
         s.par_y = s.par_z = 1;
         s.dimy = Ny;
         s.dimz = Nz;
+        s.zinner = zconv_warp_ok(Nz, nz, (int)sizeof(T)) ? 1 : 0;
+        s.zpitch = s.zinner ? green_zpitch(Nz, sizeof(V)) : Nz;
     }
     {
         Launch L_(c, "fft_z_conv");
@@ -510,7 +516,7 @@ int mesh_n(osc_ctx *c, const osc_mesh3d *m, int64_t *N) {
 int cp(osc_ctx *c, void *dst, const void *src, size_t bytes, cudaMemcpyKind k) {
     return cuda_check(c, cudaMemcpyAsync(dst, src, bytes, k, c->stream), "copy");
 }
-int syncc(osc_ctx *c) { return cuda_check(c, cudaStreamSynchronize(c->stream), "synchronize"); }
+int syncc(osc_ctx *c) { return ctx_sync(c); }
 }  // namespace
 
 extern "C" {

@@ -408,12 +408,37 @@ template <class F> inline int dispatch_fft_len(int L, F &&f) {
     }
 }
 
+// Radix sequences of the warp-per-column engine of the z pass (first radix == last radix,
+// even); WarpNone for lengths without one.
+template <int L_, int... Rs> struct WarpFft {
+    static constexpr int kLen = L_;
+    static constexpr int kNst = sizeof...(Rs);
+    static constexpr int kRad[sizeof...(Rs)] = {Rs...};
+};
+struct WarpNone {
+    static constexpr int kLen = 0;
+    static constexpr int kNst = 0;
+    static constexpr int kRad[1] = {0};
+};
+template <class F> inline int dispatch_warp_len(int L, F &&f) {
+    switch (L) {
+    case 96: return f(WarpFft<96, 4, 2, 3, 4>{});
+    case 128: return f(WarpFft<128, 4, 8, 4>{});
+    case 192: return f(WarpFft<192, 4, 4, 3, 4>{});
+    case 256: return f(WarpFft<256, 8, 4, 8>{});
+    case 384: return f(WarpFft<384, 4, 8, 3, 4>{});
+    case 512: return f(WarpFft<512, 8, 8, 8>{});
+    default: return f(WarpNone{});
+    }
+}
+
 // Twiddle tables of one length: rt[m] = exp(2 pi i m/L) for the runtime engine; st is the
 // per-stage table of the static engine ([stage][k][r-1], L-1 entries), or rt when the
-// length has no static engine.
+// length has no static engine; wt the same for the warp engine of the z pass (or rt).
 template <typename V> struct TwPair {
     const V *rt;
     const V *st;
+    const V *wt;
 };
 
 // Stage the twiddle table of length n into shared memory.

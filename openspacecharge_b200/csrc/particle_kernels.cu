@@ -292,6 +292,14 @@ __global__ void __launch_bounds__(256) k_interp_planes(InterpArgs a, const doubl
         }
     }
 }
+// One x-pair (two float4, 32 bytes, 32-byte aligned) with a single 256-bit read-only load:
+// half the L1 tag lookups of two 128-bit loads for the same bytes.
+__device__ __forceinline__ void ldg_pair(const float4 *p, float4 &lo, float4 &hi) {
+    asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+        : "=f"(lo.x), "=f"(lo.y), "=f"(lo.z), "=f"(lo.w), "=f"(hi.x), "=f"(hi.y), "=f"(hi.z), "=f"(hi.w)
+        : "l"(p));
+}
+
 __global__ void __launch_bounds__(256) k_interp_pairs(InterpArgs a, const float4 *__restrict__ g8,
                                                       double *__restrict__ E, unsigned long long *__restrict__ nclamp) {
     const int64_t plane = (int64_t)a.nx * a.ny;
@@ -307,10 +315,7 @@ __global__ void __launch_bounds__(256) k_interp_pairs(InterpArgs a, const float4
         const double wy[4] = {de * gh, omde * gh, omde * omgh, de * omgh};
         float4 lo[4], hi[4];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            lo[q] = __ldg(g8 + 2 * rows[q]);
-            hi[q] = __ldg(g8 + 2 * rows[q] + 1);
-        }
+        for (int q = 0; q < 4; ++q) ldg_pair(g8 + 2 * rows[q], lo[q], hi[q]);
         double ex = 0, ey = 0, ez = 0;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
@@ -328,6 +333,7 @@ __global__ void __launch_bounds__(256) k_interp_pairs(InterpArgs a, const float4
 int launch_interp_pairs(const InterpArgs &a, const float4 *E8, double *E, unsigned long long *nclamp,
                         cudaStream_t st) {
     if (a.np <= 0) return OSC_OK;
+    if (reinterpret_cast<uintptr_t>(E8) % 32) return OSC_E_INVALID;
     k_interp_pairs<<<nblocks(a.np, 256, 148 * 64), 256, 0, st>>>(a, E8, E, nclamp);
     return ok();
 }

@@ -126,7 +126,9 @@ static int build_green_component(osc_ctx *c, int nx, int ny, int nz, const doubl
     spec.par_z = par[2];
     spec.dimy = sym[1] ? ny + 1 : N[1];
     spec.dimz = sym[2] ? nz + 1 : N[2];
-    const size_t elems = (size_t)(nx + 1) * spec.dimy * spec.dimz;
+    spec.zinner = zconv_warp_ok(N[2], nz, (int)sizeof(T)) ? 1 : 0;
+    spec.zpitch = spec.zinner ? green_zpitch(spec.dimz, spec.real_valued ? sizeof(T) : sizeof(cplx<T>)) : spec.dimz;
+    const size_t elems = (size_t)(nx + 1) * spec.dimy * spec.zpitch;
     const size_t bytes = elems * (spec.real_valued ? sizeof(T) : sizeof(cplx<T>));
     cudaError_t e = cudaMalloc(&store.p, bytes);
     if (e != cudaSuccess) {
@@ -138,7 +140,7 @@ static int build_green_component(osc_ctx *c, int nx, int ny, int nz, const doubl
     {
         Launch L_(c, "green_extract");
         TRY(kerr(c, launch_green_extract<T>(cg, store.p, nx, N[0], N[1], spec.dimy, spec.dimz, spec.real_valued,
-                                            spec.imag_unit, scale, c->stream),
+                                            spec.imag_unit, scale, spec.zinner ? spec.zpitch : 0, c->stream),
                  "green extract"));
     }
     spec.data = store.p;
@@ -310,6 +312,7 @@ int freespace_opt(osc_ctx *c, const FreeSpaceJob &j, const TIn *rho) {
     za.nout = nout;
     za.img_phase_mul = nz - 1;
     za.ng = gs->nspec;
+    za.fault = c->d_fault;
     for (int i = 0; i < gs->nspec; ++i) za.g[i] = gs->spec[i];
     {
         Launch L_(c, "fft_z_conv");

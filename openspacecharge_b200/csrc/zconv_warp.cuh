@@ -1,0 +1,293 @@
+// zconv_warp.cuh -- the z pass of the free-space convolution with one warp per column.
+//
+// A CTA of W warps owns W adjacent (kx,ky) columns.  It loads the non-zero half of the
+// columns (z in [0,nz), coalesced across the W columns) into one shared buffer per warp;
+// every warp then transforms its own column with warp-synchronous Stockham stages.  The
+// radix sequence starts and ends with the same radix, so the butterflies a lane owns in the
+// forward transform's last stage are exactly the inputs it owns in an inverse transform's
+// first stage: the forward spectrum stays in registers, the product with the cached Green
+// spectrum is formed in registers and fed straight into the inverse's first butterflies.
+// The inverse's last stage (window z < nz only) goes back to the warp buffer and the CTA
+// stores its W columns with coalesced writes.
+//
+// Warp buffers are padded by one element per sixteen (p = e + e/16) and are 2 mod 16
+// elements apart, which keeps the stride-R writes of the first stage, the unit-stride reads
+// of the others and the column-interleaved CTA loads and stores (nearly) free of
+// shared-memory bank conflicts.  The Green spectra of this kernel are stored with kz
+// innermost (GSpecDev::zinner), so the 32 lanes of a warp read 32 consecutive kz.  When
+// all spectra are real and even/odd in z (free space without images), each CTA fetches the
+// Green columns of its W columns into shared memory with bulk copies at launch, which
+// complete while the forward transforms run.
+#pragma once
+
+#include "async_copy.cuh"
+#include "fft_kernels.cuh"
+
+namespace osc {
+
+// Resident CTAs per SM the register allocation of k_zconv_warp is sized for.
+#ifndef ZW_MINB
+#define ZW_MINB 2
+#endif
+
+
+__device__ __forceinline__ int wpad(int e) { return e + (e >> 4); }
+constexpr int wbuf_len(int L) { return L + L / 16 + 2; }
+
+// One stage of one warp's transform: butterflies j = lane + 32q (j < L/R), input elements
+// j + (L/R) r, outputs (j/Ns) Ns R + j%Ns + Ns r; per-stage twiddles at (Ns-1) + k(R-1) + r-1.
+// Padded positions of a butterfly's R elements are a per-lane base plus compile-time
+// offsets wherever the padding allows it.
+template <typename V, int R, int L, int Ns> struct WStage {
+    static constexpr int nb = L / R;
+    static constexpr int Q = (nb + 31) / 32;
+    static constexpr bool full = nb % 32 == 0;
+    static constexpr bool ld_lin = nb % 16 == 0;  // wpad(j + r nb) = wpad(j) + r (nb + nb/16)
+    // store: 1 = Ns multiple of 16, 2 = Ns | 16 and 16 | Ns R, 3 = Ns R | 16, 0 = per element
+    static constexpr int st_kind =
+        Ns % 16 == 0 ? 1 : (16 % Ns == 0 && (Ns * R) % 16 == 0) ? 2 : (16 % (Ns * R) == 0) ? 3 : 0;
+    __device__ __forceinline__ static constexpr int st_off(int r) {
+        return st_kind == 1 ? r * (Ns + Ns / 16) : st_kind == 2 ? r * Ns + ((r * Ns) >> 4) : r * Ns;
+    }
+
+    __device__ __forceinline__ static void load(const V *wb, const V *tw, int sign, int lane, V (&v)[Q][R],
+                                                bool half_in) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const int j = lane + 32 * q, k = j % Ns;
+            const int pb = wpad(j);
+            if (full || j < nb) {
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    V x;
+                    if (half_in && r >= R / 2) {
+                        x.x = 0;
+                        x.y = 0;
+                    } else {
+                        x = wb[ld_lin ? pb + r * (nb + nb / 16) : wpad(j + r * nb)];
+                        if (r && Ns > 1) x = cmul(x, tw_get(tw, (Ns - 1) + k * (R - 1) + (r - 1), sign));
+                    }
+                    v[q][r] = x;
+                }
+            }
+        }
+    }
+    __device__ __forceinline__ static void dft(V (&v)[Q][R], int sign) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) Dft<R>::run(v[q], sign);
+    }
+    __device__ __forceinline__ static void store(V *wb, int lane, const V (&v)[Q][R]) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const int j = lane + 32 * q, k = j % Ns;
+            if (full || j < nb) {
+                const int idxD = (j / Ns) * Ns * R + k;
+                const int pb = wpad(idxD);
+#pragma unroll
+                for (int r = 0; r < R; ++r) wb[st_kind ? pb + st_off(r) : wpad(idxD + r * Ns)] = v[q][r];
+            }
+        }
+    }
+};
+
+// Stages strictly between the first and the last, in place in the warp buffer.
+template <typename V, int L, int Ns, int R, int... Rest>
+__device__ __forceinline__ void wfft_mid(V *wb, const V *tw, int sign, int lane) {
+    if constexpr (sizeof...(Rest) > 0) {
+        typedef WStage<V, R, L, Ns> S;
+        V v[S::Q][R];
+        S::load(wb, tw, sign, lane, v, false);
+        S::dft(v, sign);
+        __syncwarp();
+        S::store(wb, lane, v);
+        __syncwarp();
+        wfft_mid<V, L, Ns * R, Rest...>(wb, tw, sign, lane);
+    }
+}
+template <typename V, int L, int R0, int... Rest>
+__device__ __forceinline__ void wfft_mid_of(Radices<R0, Rest...>, V *wb, const V *tw, int sign, int lane) {
+    wfft_mid<V, L, R0, Rest...>(wb, tw, sign, lane);
+}
+
+// Green term modes of the kernel.
+constexpr int ZW_DIRECT = 0;  // spectra read from global memory
+constexpr int ZW_IMAGE = 1;   // as 0, plus the mirrored-image term
+constexpr int ZW_STAGED = 2;  // real, z-symmetric spectra staged in shared memory by bulk copies
+
+template <typename T, int W, int MODE, int L, int... Rs>
+__global__ void __launch_bounds__(W * 32, ZW_MINB) k_zconv_warp(const cplx<T> *__restrict__ in, cplx<T> *__restrict__ out,
+                                                       ZConvArgs a, const cplx<T> *__restrict__ twg,
+                                                       const cplx<T> *__restrict__ tw_rt) {
+    typedef cplx<T> V;
+    constexpr bool IMG = MODE == ZW_IMAGE, GS = MODE == ZW_STAGED;
+    constexpr int RF = WarpFft<L, Rs...>::kRad[0];
+    static_assert(RF == WarpFft<L, Rs...>::kRad[sizeof...(Rs) - 1], "first and last radix must match");
+    static_assert(RF % 2 == 0, "first radix must be even");
+    typedef WStage<V, RF, L, 1> S0;       // first stage
+    typedef WStage<V, RF, L, L / RF> SL;  // last stage
+    constexpr int NB = L / RF, Q = S0::Q, WB = wbuf_len(L);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ uint64_t gbar;
+    __shared__ int gfail;
+    V *tw = reinterpret_cast<V *>(smem_raw);
+    V *wbufs = tw + L;
+    V *rbufs = wbufs + W * WB;                          // IMG: forward spectra, read at mirrored kz
+    T *gst = reinterpret_cast<T *>(wbufs + W * WB);     // GS: Green columns [W][nout][zpitch]
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int col0 = blockIdx.x * W;
+    const int zp = a.g[0].zpitch;
+    V *wb = wbufs + warp * WB;
+    if (GS) {
+        if (threadIdx.x == 0) {
+            mbar_init(&gbar, 1);
+            const int ncv = min(W, a.ncols - col0);
+            mbar_arrive_expect_tx(&gbar, (unsigned)(ncv * a.nout * zp * (int)sizeof(T)));
+            for (int c = 0; c < ncv; ++c) {
+                const int col = col0 + c, ky = col / a.nxh, kx = col - ky * a.nxh;
+                for (int o = 0; o < a.nout; ++o) {
+                    const GSpecDev &g = a.g[a.gdir[o]];
+                    const int yy = (g.sym_y && ky > a.ny) ? a.Ny - ky : ky;
+                    const T *src = reinterpret_cast<const T *>(g.data) + ((int64_t)yy * a.nxh + kx) * zp;
+                    bulk_g2s(gst + (c * a.nout + o) * zp, src, (unsigned)(zp * sizeof(T)), &gbar);
+                }
+            }
+        }
+    }
+    load_twiddles(tw, twg, L);
+    for (int idx = threadIdx.x; idx < W * a.nz; idx += W * 32) {
+        const int e = idx / W, c = idx - e * W;
+        const int col = col0 + c;
+        V v = mk<T>(0, 0);
+        if (col < a.ncols) v = in[(int64_t)e * a.in_estride + col];
+        wbufs[c * WB + wpad(e)] = v;
+    }
+    __syncthreads();
+    // forward transform (sign +1) of the column; the upper half of its input is zero
+    V rh[Q][RF];
+    {
+        V v[Q][RF];
+        S0::load(wb, tw, +1, lane, v, true);
+        S0::dft(v, +1);
+        __syncwarp();
+        S0::store(wb, lane, v);
+        __syncwarp();
+        wfft_mid_of<V, L>(Radices<Rs...>{}, wb, tw, +1, lane);
+        SL::load(wb, tw, +1, lane, rh, false);
+        SL::dft(rh, +1);
+    }
+    // rh[q][r] holds the spectrum at kz = lane + 32q + NB r
+    V *rb = rbufs + warp * WB;
+    if (IMG) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const int j = lane + 32 * q;
+            if (S0::full || j < NB)
+#pragma unroll
+                for (int r = 0; r < RF; ++r) rb[wpad(j + NB * r)] = rh[q][r];
+        }
+    }
+    if (GS) {
+        if (threadIdx.x == 0) {
+            const bool ok = mbar_wait_bounded(&gbar, 0);
+            if (!ok) {
+                report_fault(a.fault, FAULT_BULK_WAIT);
+                mbar_wait_bounded(&gbar, 0);  // let copies in flight land before leaving
+            }
+            gfail = ok ? 0 : 1;
+        }
+        __syncthreads();
+        if (gfail) return;  // CTA-uniform
+    }
+    __syncwarp();
+    const int colc = min(col0 + warp, a.ncols - 1);
+    const int ky = colc / a.nxh, kx = colc - ky * a.nxh;
+    for (int o = 0; o < a.nout; ++o) {
+        const int gd = a.gdir[o], gi = a.gimg[o];
+        V v[Q][RF];
+        if (GS) {
+            const GSpecDev &g = a.g[gd];
+            const T *gc = gst + (warp * a.nout + o) * zp;
+            const bool yneg = g.sym_y && ky > a.ny && g.par_y < 0;
+            const bool zodd = g.par_z < 0, iu = g.imag_unit;
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                const int j = lane + 32 * q;
+                if (S0::full || j < NB) {
+#pragma unroll
+                    for (int r = 0; r < RF; ++r) {
+                        const int e = j + NB * r;
+                        T s;
+                        if (r < RF / 2) {
+                            s = gc[e];
+                        } else {  // kz >= nz: the value at Nz - kz, odd spectra change sign
+                            s = gc[L - e];
+                            if (zodd && e != a.nz) s = -s;
+                        }
+                        if (yneg) s = -s;
+                        const V x = rh[q][r];
+                        v[q][r] = iu ? mk<T>(-x.y * s, x.x * s) : mk<T>(x.x * s, x.y * s);
+                    }
+                }
+            }
+        } else {
+            const T icoef = (T)a.img_coef[o];
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                const int j = lane + 32 * q;
+                if (S0::full || j < NB) {
+#pragma unroll
+                    for (int r = 0; r < RF; ++r) {
+                        const int e = j + NB * r;
+                        V S = mk<T>(0, 0);
+                        if (gd >= 0)
+                            S = cmul(rh[q][r], g_lookup<T>(a.g[gd], kx, ky, e, a.nxh, a.Ny, a.ny, L, a.nz));
+                        if (IMG && gi >= 0) {
+                            // spectrum of -rho flipped in z: -w^((nz-1) kz) * rho_hat(-kz)
+                            const V rm = rb[wpad(e == 0 ? 0 : L - e)];
+                            const V ph = __ldg(tw_rt + (int)(((int64_t)a.img_phase_mul * e) % L));
+                            V ri = cmul(ph, rm);
+                            ri.x = -ri.x * icoef;
+                            ri.y = -ri.y * icoef;
+                            S = cadd(S, cmul(ri, g_lookup<T>(a.g[gi], kx, ky, e, a.nxh, a.Ny, a.ny, L, a.nz)));
+                        }
+                        v[q][r] = S;
+                    }
+                }
+            }
+        }
+        // inverse transform: first stage from registers, last stage back to the buffer
+        S0::dft(v, -1);
+        S0::store(wb, lane, v);
+        __syncwarp();
+        wfft_mid_of<V, L>(Radices<Rs...>{}, wb, tw, -1, lane);
+        SL::load(wb, tw, -1, lane, v, false);
+        SL::dft(v, -1);
+        __syncwarp();
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const int j = lane + 32 * q;
+            if (S0::full || j < NB)
+#pragma unroll
+                for (int r = 0; r < RF / 2; ++r) wb[wpad(j + NB * r)] = v[q][r];  // z = j + NB r < L/2
+        }
+        __syncthreads();
+        V *dst = out + (int64_t)o * a.out_cstride;
+        for (int idx = threadIdx.x; idx < W * a.nz; idx += W * 32) {
+            const int e = idx / W, c = idx - e * W;
+            const int col = col0 + c;
+            if (col < a.ncols) dst[(int64_t)e * a.out_estride + col] = wbufs[c * WB + wpad(e)];
+        }
+        __syncthreads();
+    }
+}
+
+// Shared memory bytes of k_zconv_warp for length L, W warps; zp = Green column pitch
+// (elements) of the staged mode.
+template <typename T> inline size_t zconv_warp_smem(int L, int W, int mode, int nout, int zp) {
+    size_t b = sizeof(cplx<T>) * ((size_t)L + (size_t)W * wbuf_len(L));
+    if (mode == ZW_IMAGE) b += sizeof(cplx<T>) * (size_t)W * wbuf_len(L);
+    if (mode == ZW_STAGED) b += sizeof(T) * (size_t)W * nout * zp;
+    return b;
+}
+
+}  // namespace osc
