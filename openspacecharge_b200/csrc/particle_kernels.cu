@@ -96,8 +96,25 @@ template int launch_deposit<double>(const DepositArgs &, double *, unsigned long
 // deposit_particles (code/open_spacecharge_mod.f90:274-281).
 __global__ void __launch_bounds__(256) k_deposit_cells(DepositArgs a, float4 *__restrict__ acc,
                                                        unsigned long long *__restrict__ counters) {
-    GRID_STRIDE(m, a.np) {
-        const double xm = a.x[m], ym = a.y[m], zm = a.z[m];
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    // the next particle's coordinates and charge are loaded before this one's atomics
+    double xn = 0, yn = 0, zn = 0, qn = a.charge1;
+    if (m < a.np) {
+        xn = __ldg(a.x + m);
+        yn = __ldg(a.y + m);
+        zn = __ldg(a.z + m);
+        if (a.q) qn = __ldg(a.q + m);
+    }
+    for (; m < a.np; m += stride) {
+        const double xm = xn, ym = yn, zm = zn, c = qn;
+        const int64_t mn = m + stride;
+        if (mn < a.np) {
+            xn = __ldg(a.x + mn);
+            yn = __ldg(a.y + mn);
+            zn = __ldg(a.z + mn);
+            if (a.q) qn = __ldg(a.q + mn);
+        }
         bool nonfinite = false, skip = false;
         if (a.check_finite && !(isfinite(xm) && isfinite(ym) && isfinite(zm))) {
             nonfinite = true;
@@ -114,7 +131,6 @@ __global__ void __launch_bounds__(256) k_deposit_cells(DepositArgs a, float4 *__
         const double ab = ((a.xmin - xm) + fx * a.dx) * a.dxi;
         const double de = ((a.ymin - ym) + fy * a.dy) * a.dyi;
         const double gh = ((a.zmin - zm) + fz * a.dz) * a.dzi;
-        const double c = a.q ? a.q[m] : a.charge1;
         const double omab = 1. - ab, omde = 1. - de, omgh = 1. - gh;
         const double lo = gh * c, hi = omgh * c;
         const int i = (int)fx - a.nlo[0], j = (int)fy - a.nlo[1], k = (int)fz - a.nlo[2];
@@ -303,9 +319,25 @@ __device__ __forceinline__ void ldg_pair(const float4 *p, float4 &lo, float4 &hi
 __global__ void __launch_bounds__(256) k_interp_pairs(InterpArgs a, const float4 *__restrict__ g8,
                                                       double *__restrict__ E, unsigned long long *__restrict__ nclamp) {
     const int64_t plane = (int64_t)a.nx * a.ny;
-    GRID_STRIDE(m, a.np) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    // the next particle's coordinates are loaded while this particle's field is gathered
+    double xn = 0, yn = 0, zn = 0;
+    if (m < a.np) {
+        xn = __ldg(a.x + m);
+        yn = __ldg(a.y + m);
+        zn = __ldg(a.z + m);
+    }
+    for (; m < a.np; m += stride) {
+        const double xm = xn, ym = yn, zm = zn;
+        const int64_t mn = m + stride;
+        if (mn < a.np) {
+            xn = __ldg(a.x + mn);
+            yn = __ldg(a.y + mn);
+            zn = __ldg(a.z + mn);
+        }
         Cell c;
-        const bool fl = locate(a, a.x[m], a.y[m], a.z[m], c);
+        const bool fl = locate(a, xm, ym, zm, c);
         count_one(nclamp, fl);
         const int64_t n0 = c.i + (int64_t)a.nx * c.j + plane * c.k;
         const double ab = c.ab, de = c.de, gh = c.gh;
