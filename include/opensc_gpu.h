@@ -53,8 +53,9 @@ extern "C" {
                                  zero-padded FFTs, Green function rebuilt on every call */
 
 /* ---- deposition modes ------------------------------------------------------------ */
-#define OSC_DEPOSIT_ATOMIC 0 /* unsorted input, FP32/FP64 atomics, warp-aggregated */
-#define OSC_DEPOSIT_SORTED 1 /* cell-sorted, compensated, bit-reproducible run to run */
+#define OSC_DEPOSIT_ATOMIC 0        /* floating-point atomics (order-dependent last bits) */
+#define OSC_DEPOSIT_DETERMINISTIC 1 /* 64-bit fixed-point atomics: rho bit-identical for any
+                                       particle order and run to run */
 
 /* ---- context options (osc_ctx_set_option) ---------------------------------------- */
 #define OSC_OPT_PRECISION 1      /* default precision for host entry points */

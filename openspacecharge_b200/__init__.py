@@ -3,7 +3,7 @@ cathode-image / rectangular-pipe Green functions, doubled-grid FFT convolution, 
 grid and interpolation back to particles, as hand-written sm_100a CUDA kernels behind a
 C ABI (``include/opensc_gpu.h``, ``libopensc_b200.so``).
 """
-from .native import (DEPOSIT_ATOMIC, DEPOSIT_SORTED, OPT_CHECK_FINITE, OPT_DEPOSIT_MODE,
+from .native import (DEPOSIT_ATOMIC, DEPOSIT_DETERMINISTIC, OPT_CHECK_FINITE, OPT_DEPOSIT_MODE,
                      OPT_GREEN_CACHE_MB, OPT_PRECISION, OPT_PROFILE, OPT_STRICT_BOUNDS,
                      PREC_FP32, PREC_FP64, PREC_FP64_PLAIN, Context, OscError, OscMesh3D)
 from .mesh import (Mesh3D, depose_rho_scalar, deposit_particles, get_mesh_quantities,

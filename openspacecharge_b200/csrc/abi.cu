@@ -125,6 +125,65 @@ DepositArgs deposit_args(const osc_mesh3d *m, const int n[3], int64_t np, const 
     return a;
 }
 
+// Deposition of a.np particles into rho (zeroed here).  OSC_DEPOSIT_ATOMIC uses
+// floating-point atomics of the type of rho; OSC_DEPOSIT_DETERMINISTIC accumulates 64-bit
+// fixed-point integers and converts once, so rho is bit-identical for any particle order.
+// The fixed-point unit is a power of two chosen from np * max|q| (order-independent), so
+// that no node sum can exceed 2^62 units.  rho = mult * sum.
+template <typename TR> int deposit_rho(osc_ctx *ctx, DepositArgs a, TR *rho, int64_t N, double mult) {
+    if (ctx->deposit_mode != OSC_DEPOSIT_DETERMINISTIC) {
+        CK(cudaMemsetAsync(rho, 0, sizeof(TR) * N, ctx->stream), "memset rho");
+        {
+            Launch L_(ctx, sizeof(TR) == 8 ? "deposit_f64" : "deposit_f32");
+            if (launch_deposit<TR>(a, rho, ctx->d_small, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "deposit");
+        }
+        if (mult != 1.0) {
+            if constexpr (sizeof(TR) == 8) {
+                Launch L_(ctx, "scale");
+                if (launch_scale(rho, mult, N, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "scale");
+            } else {
+                return set_err(ctx, OSC_E_INVALID, "scaled FP32 deposit");
+            }
+        }
+        return OSC_OK;
+    }
+    double qmax;
+    if (a.mode == 0 && a.q) {
+        double *out;
+        TRY(ws_get(ctx, "qmax", sizeof(double), (void **)&out));
+        {
+            Launch L_(ctx, "charge_max", 2);
+            if (launch_sum(a.np, a.q, ctx->d_partials, out, ctx->stream, true))
+                return set_err(ctx, OSC_E_CUDA, "charge max");
+        }
+        TRY(d2h(ctx, &qmax, out, sizeof(double)));
+        TRY(sync(ctx));
+    } else {
+        qmax = a.mode == 0 ? std::fabs(a.charge1) : 1.0;
+    }
+    const double bound = (double)a.np * qmax;  // >= sum of |contributions| at any node
+    a.fx_scale = 1.0;
+    if (bound > 0 && std::isfinite(bound)) {
+        int e;
+        std::frexp(bound, &e);  // bound < 2^e
+        a.fx_scale = std::ldexp(1.0, 62 - e);
+    }
+    unsigned long long *acc;
+    TRY(ws_get(ctx, "rho_fixed", sizeof(unsigned long long) * N, (void **)&acc));
+    CK(cudaMemsetAsync(acc, 0, sizeof(unsigned long long) * N, ctx->stream), "memset fixed");
+    {
+        Launch L_(ctx, "deposit_fixed");
+        if (launch_deposit<unsigned long long>(a, acc, ctx->d_small, ctx->stream))
+            return set_err(ctx, OSC_E_CUDA, "deposit");
+    }
+    {
+        Launch L_(ctx, "fixed_to_real");
+        if (launch_fixed_to_real<TR>(acc, rho, a.fx_scale, mult, N, ctx->stream))
+            return set_err(ctx, OSC_E_CUDA, "fixed to real");
+    }
+    return OSC_OK;
+}
+
 InterpArgs interp_args(const osc_mesh3d *m, const int n[3], int64_t np, const double *x, const double *y,
                        const double *z) {
     InterpArgs a;
@@ -252,7 +311,7 @@ int osc_ctx_set_option(osc_ctx *ctx, int option, int64_t v) {
     switch (option) {
     case OSC_OPT_PRECISION: TRY(check_prec(ctx, (int)v)); ctx->precision = (int)v; return OSC_OK;
     case OSC_OPT_DEPOSIT_MODE:
-        if (v != OSC_DEPOSIT_ATOMIC && v != OSC_DEPOSIT_SORTED) return bad(ctx, "deposit mode");
+        if (v != OSC_DEPOSIT_ATOMIC && v != OSC_DEPOSIT_DETERMINISTIC) return bad(ctx, "deposit mode");
         ctx->deposit_mode = (int)v;
         return OSC_OK;
     case OSC_OPT_STRICT_BOUNDS: ctx->strict_bounds = v ? 1 : 0; return OSC_OK;
@@ -335,13 +394,9 @@ int osc_deposit_particles_dev(osc_ctx *ctx, int64_t np, const double *x, const d
         TRY(set_charge(ctx, np, q, total_charge, mesh, &charge1));
     }
     const int64_t N = (int64_t)n[0] * n[1] * n[2];
-    CK(cudaMemsetAsync(rho, 0, sizeof(double) * N, ctx->stream), "memset rho");
     TRY(counters_reset(ctx));
     DepositArgs a = deposit_args(mesh, n, np, x, y, z, q, charge1, ctx->check_finite);
-    {
-        Launch L_(ctx, "deposit_f64");
-        if (launch_deposit<double>(a, rho, ctx->d_small, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "deposit");
-    }
+    TRY(deposit_rho<double>(ctx, a, rho, N, 1.0));
     if (n_outside || ctx->strict_bounds || ctx->check_finite) {
         unsigned long long cnt[3];
         TRY(counters_read(ctx, cnt));
@@ -437,19 +492,11 @@ int osc_depose_rho_scalar(osc_ctx *ctx, int64_t np, const double *xa, const doub
     TRY(stage_in(ctx, "h_z", za, np, &dz));
     TRY(stage_in(ctx, "h_q", lostflag, np, &dl));
     TRY(ws_get(ctx, "h_rho", sizeof(double) * N, (void **)&drho));
-    CK(cudaMemsetAsync(drho, 0, sizeof(double) * N, ctx->stream), "memset rho");
     TRY(counters_reset(ctx));
     DepositArgs a = deposit_args(&m, n, np, dx, dy, dz, nullptr, 1.0, 0);
     a.lost = dl;
     a.mode = 1;
-    {
-        Launch L_(ctx, "deposit_f64");
-        if (launch_deposit<double>(a, drho, ctx->d_small, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "deposit");
-    }
-    {
-        Launch L_(ctx, "scale");
-        if (launch_scale(drho, chrgpermacro, N, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "scale");
-    }
+    TRY(deposit_rho<double>(ctx, a, drho, N, chrgpermacro));
     TRY(d2h(ctx, rho, drho, sizeof(double) * N));
     unsigned long long cnt[3];
     TRY(counters_read(ctx, cnt));
@@ -604,11 +651,7 @@ int osc_space_charge_step_dev(osc_ctx *ctx, osc_mesh3d *mesh, int64_t np, const 
         TRY(ws_get(ctx, "st_rho64", sizeof(double) * N, (void **)&rho));
         TRY(ws_get(ctx, "st_Eg", sizeof(double) * 3 * N, (void **)&Eg));
         if (B) TRY(ws_get(ctx, "st_Bg", sizeof(double) * 3 * N, (void **)&Bg));
-        CK(cudaMemsetAsync(rho, 0, sizeof(double) * N, ctx->stream), "memset rho");
-        {
-            Launch L_(ctx, "deposit_f64");
-            if (launch_deposit<double>(da, rho, ctx->d_small, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "deposit");
-        }
+        TRY(deposit_rho<double>(ctx, da, rho, N, 1.0));
         j.E = Eg;
         j.B = Bg;
         TRY(freespace_plain(ctx, j, rho));
@@ -623,22 +666,27 @@ int osc_space_charge_step_dev(osc_ctx *ctx, osc_mesh3d *mesh, int64_t np, const 
         return OSC_OK;
     }
     if (precision == OSC_PREC_FP32) {
-        // deposit: per-cell corner sums (two float4 atomics per particle), then a gather
-        // to nodes; field: E written as an x-pair grid; interpolation: 4 sectors/particle
-        float *rho, *acc;
+        // deposit: two float4 atomics per particle into a quad grid, then a fixed-order
+        // sum to nodes; field: E written as an x-pair grid; interpolation: 4 sectors/particle
+        float *rho, *quad;
         void *E8;
         TRY(ws_get(ctx, "st_rho32", sizeof(float) * N, (void **)&rho));
-        TRY(ws_get(ctx, "st_cells", sizeof(float) * 8 * N, (void **)&acc));
         TRY(ws_get(ctx, "st_E8", sizeof(float4) * 2 * N, &E8));
-        CK(cudaMemsetAsync(acc, 0, sizeof(float) * 8 * N, ctx->stream), "memset cells");
-        {
-            Launch L_(ctx, "deposit_f32");
-            if (launch_deposit_cells(da, acc, ctx->d_small, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "deposit");
-        }
-        {
-            Launch L_(ctx, "cells_to_nodes");
-            if (launch_cells_to_nodes(acc, rho, n[0], n[1], n[2], ctx->stream))
-                return set_err(ctx, OSC_E_CUDA, "cells to nodes");
+        if (ctx->deposit_mode == OSC_DEPOSIT_DETERMINISTIC) {
+            TRY(deposit_rho<float>(ctx, da, rho, N, 1.0));
+        } else {
+            TRY(ws_get(ctx, "st_quad", sizeof(float) * 4 * N, (void **)&quad));
+            CK(cudaMemsetAsync(quad, 0, sizeof(float) * 4 * N, ctx->stream), "memset quad");
+            {
+                Launch L_(ctx, "deposit_f32");
+                if (launch_deposit_quad(da, quad, ctx->d_small, ctx->stream))
+                    return set_err(ctx, OSC_E_CUDA, "deposit");
+            }
+            {
+                Launch L_(ctx, "quad_to_nodes");
+                if (launch_quad_to_nodes(quad, rho, n[0], n[1], n[2], ctx->stream))
+                    return set_err(ctx, OSC_E_CUDA, "quad to nodes");
+            }
         }
         j.E4 = E8;
         j.e4_pairs = 1;
@@ -665,11 +713,7 @@ int osc_space_charge_step_dev(osc_ctx *ctx, osc_mesh3d *mesh, int64_t np, const 
     void *E4;
     TRY(ws_get(ctx, "st_rho64", sizeof(double) * N, (void **)&rho));
     TRY(ws_get(ctx, "st_E4d", sizeof(double4) * N, &E4));
-    CK(cudaMemsetAsync(rho, 0, sizeof(double) * N, ctx->stream), "memset rho");
-    {
-        Launch L_(ctx, "deposit_f64");
-        if (launch_deposit<double>(da, rho, ctx->d_small, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "deposit");
-    }
+    TRY(deposit_rho<double>(ctx, da, rho, N, 1.0));
     j.E4 = E4;
     if (B) {
         double *Bg;

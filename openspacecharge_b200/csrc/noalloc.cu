@@ -99,6 +99,7 @@ int osc_deposit_particles_dev_noalloc(void *cuda_stream, const osc_mesh3d *mesh,
         return fail(errbuf, errlen, OSC_E_CUDA, "clearing the deposit scratch array failed");
     }
     osc::DepositArgs a;
+    a.fx_scale = 1.0;
     a.np = np;
     a.x = d_x;
     a.y = d_y;

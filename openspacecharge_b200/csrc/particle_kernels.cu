@@ -12,8 +12,12 @@ static inline unsigned nblocks(int64_t n, int bs, int64_t cap = (1 << 20)) {
 }
 #define GRID_STRIDE(i, n) for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (n); i += (int64_t)gridDim.x * blockDim.x)
 
-__device__ __forceinline__ void atomic_add_t(float *p, double v) { atomicAdd(p, (float)v); }
-__device__ __forceinline__ void atomic_add_t(double *p, double v) { atomicAdd(p, v); }
+__device__ __forceinline__ void atomic_add_t(float *p, double v, double) { atomicAdd(p, (float)v); }
+__device__ __forceinline__ void atomic_add_t(double *p, double v, double) { atomicAdd(p, v); }
+// Fixed point: two's-complement addition of the rounded contribution (exact, associative).
+__device__ __forceinline__ void atomic_add_t(unsigned long long *p, double v, double scale) {
+    atomicAdd(p, (unsigned long long)__double2ll_rn(v * scale));
+}
 
 // Warp-aggregated counter increment.
 __device__ __forceinline__ void count_one(unsigned long long *c, bool pred) {
@@ -70,14 +74,14 @@ __global__ void __launch_bounds__(256) k_deposit(DepositArgs a, TA *__restrict__
         const double c = a.mode == 0 ? (a.q ? a.q[m] : a.charge1) : 1.0;
         const double omab = 1. - ab, omde = 1. - de, omgh = 1. - gh;
         TA *r0 = rho + i + (int64_t)a.nx * j + plane * k;
-        atomic_add_t(r0, ab * de * gh * c);
-        atomic_add_t(r0 + a.nx, ab * omde * gh * c);
-        atomic_add_t(r0 + a.nx + plane, ab * omde * omgh * c);
-        atomic_add_t(r0 + plane, ab * de * omgh * c);
-        atomic_add_t(r0 + 1 + plane, omab * de * omgh * c);
-        atomic_add_t(r0 + 1 + a.nx + plane, omab * omde * omgh * c);
-        atomic_add_t(r0 + 1 + a.nx, omab * omde * gh * c);
-        atomic_add_t(r0 + 1, omab * de * gh * c);
+        atomic_add_t(r0, ab * de * gh * c, a.fx_scale);
+        atomic_add_t(r0 + a.nx, ab * omde * gh * c, a.fx_scale);
+        atomic_add_t(r0 + a.nx + plane, ab * omde * omgh * c, a.fx_scale);
+        atomic_add_t(r0 + plane, ab * de * omgh * c, a.fx_scale);
+        atomic_add_t(r0 + 1 + plane, omab * de * omgh * c, a.fx_scale);
+        atomic_add_t(r0 + 1 + a.nx + plane, omab * omde * omgh * c, a.fx_scale);
+        atomic_add_t(r0 + 1 + a.nx, omab * omde * gh * c, a.fx_scale);
+        atomic_add_t(r0 + 1, omab * de * gh * c, a.fx_scale);
     }
 }
 
@@ -89,13 +93,32 @@ int launch_deposit(const DepositArgs &a, TA *rho, unsigned long long *counters, 
 }
 template int launch_deposit<float>(const DepositArgs &, float *, unsigned long long *, cudaStream_t);
 template int launch_deposit<double>(const DepositArgs &, double *, unsigned long long *, cudaStream_t);
+template int launch_deposit<unsigned long long>(const DepositArgs &, unsigned long long *, unsigned long long *,
+                                                cudaStream_t);
+
+template <typename TO>
+__global__ void k_fixed_to_real(const unsigned long long *__restrict__ acc, TO *__restrict__ out, double f, int64_t n) {
+    GRID_STRIDE(i, n) out[i] = (TO)((double)(long long)acc[i] * f);
+}
+template <typename TO>
+int launch_fixed_to_real(const unsigned long long *acc, TO *out, double fx_scale, double mult, int64_t n,
+                         cudaStream_t st) {
+    k_fixed_to_real<TO><<<nblocks(n, 256), 256, 0, st>>>(acc, out, mult / fx_scale, n);
+    return ok();
+}
+template int launch_fixed_to_real<float>(const unsigned long long *, float *, double, double, int64_t, cudaStream_t);
+template int launch_fixed_to_real<double>(const unsigned long long *, double *, double, double, int64_t, cudaStream_t);
 
 // ------------------------------------------------------------------------------------
-// Corner q = a + 2b + 4c of a cell is node (i+a, j+b, k+c); its weight is
-// (a ? 1-ab : ab) * (b ? 1-de : de) * (c ? 1-gh : gh) times the charge, the factors of
-// deposit_particles (code/open_spacecharge_mod.f90:274-281).
-__global__ void __launch_bounds__(256) k_deposit_cells(DepositArgs a, float4 *__restrict__ acc,
-                                                       unsigned long long *__restrict__ counters) {
+// FP32 deposit in two passes.  Pass 1 adds each particle to a quad grid: node (i,j,k) holds
+// the contributions to the four nodes (i,j), (i+1,j), (i,j+1), (i+1,j+1) of plane k that
+// come from the cells whose lowest corner is (i,j,k) or (i,j,k-1), so a particle costs two
+// float4 atomics (planes k and k+1) on a 16-byte-per-node grid that stays in L2.  The
+// weights are the factors of deposit_particles (code/open_spacecharge_mod.f90:274-281).
+// Pass 2 sums every node's four quad slots in a fixed order.
+__global__ void __launch_bounds__(256) k_deposit_quad(DepositArgs a, float4 *__restrict__ quad,
+                                                      unsigned long long *__restrict__ counters) {
+    const int64_t plane = (int64_t)a.nx * a.ny;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     // the next particle's coordinates and charge are loaded before this one's atomics
@@ -134,59 +157,37 @@ __global__ void __launch_bounds__(256) k_deposit_cells(DepositArgs a, float4 *__
         const double omab = 1. - ab, omde = 1. - de, omgh = 1. - gh;
         const double lo = gh * c, hi = omgh * c;
         const int i = (int)fx - a.nlo[0], j = (int)fy - a.nlo[1], k = (int)fz - a.nlo[2];
-        float4 *cell = acc + 2 * ((int64_t)i + (int64_t)a.nx * (j + (int64_t)a.ny * k));
-        atomicAdd(cell, make_float4((float)(ab * de * lo), (float)(omab * de * lo), (float)(ab * omde * lo),
-                                    (float)(omab * omde * lo)));
-        atomicAdd(cell + 1, make_float4((float)(ab * de * hi), (float)(omab * de * hi), (float)(ab * omde * hi),
-                                        (float)(omab * omde * hi)));
+        float4 *q0 = quad + ((int64_t)i + (int64_t)a.nx * j + plane * k);
+        atomicAdd(q0, make_float4((float)(ab * de * lo), (float)(omab * de * lo), (float)(ab * omde * lo),
+                                  (float)(omab * omde * lo)));
+        atomicAdd(q0 + plane, make_float4((float)(ab * de * hi), (float)(omab * de * hi), (float)(ab * omde * hi),
+                                          (float)(omab * omde * hi)));
     }
 }
 
-int launch_deposit_cells(const DepositArgs &a, float *acc, unsigned long long *counters, cudaStream_t st) {
+int launch_deposit_quad(const DepositArgs &a, float *quad, unsigned long long *counters, cudaStream_t st) {
     if (a.np <= 0) return OSC_OK;
-    k_deposit_cells<<<nblocks(a.np, 256, 148 * 64), 256, 0, st>>>(a, reinterpret_cast<float4 *>(acc), counters);
+    k_deposit_quad<<<nblocks(a.np, 256, 1 << 20), 256, 0, st>>>(a, reinterpret_cast<float4 *>(quad), counters);
     return ok();
 }
 
-// rho(n) = sum over the 8 cells that have n as a corner, in a fixed order.  A CTA owns a
-// 32x4x4 tile of nodes and stages the 33x5x5 cells it needs in shared memory, one plane
-// per corner index so the reads of a warp hit consecutive words.
-constexpr int GX = 32, GY = 4, GZ = 4;
-constexpr int CX = GX + 1, CY = GY + 1, CZ = GZ + 1, NCELL = CX * CY * CZ;
-
-__global__ void __launch_bounds__(GX *GY *GZ) k_cells_to_nodes(const float4 *__restrict__ acc, float *__restrict__ rho,
-                                                               int nx, int ny, int nz) {
-    __shared__ float sm[8][NCELL];
-    const int i0 = blockIdx.x * GX, j0 = blockIdx.y * GY, k0 = blockIdx.z * GZ;
-    for (int t = threadIdx.x; t < 2 * NCELL; t += blockDim.x) {
-        const int cidx = t >> 1, half = t & 1;
-        const int cx = cidx % CX, r = cidx / CX, cy = r % CY, cz = r / CY;
-        const int i = i0 - 1 + cx, j = j0 - 1 + cy, k = k0 - 1 + cz;
-        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (i >= 0 && j >= 0 && k >= 0 && i < nx - 1 && j < ny - 1 && k < nz - 1)
-            v = __ldg(acc + 2 * ((int64_t)i + (int64_t)nx * (j + (int64_t)ny * k)) + half);
-        sm[4 * half + 0][cidx] = v.x;
-        sm[4 * half + 1][cidx] = v.y;
-        sm[4 * half + 2][cidx] = v.z;
-        sm[4 * half + 3][cidx] = v.w;
+// rho(i,j,k) = Q(i,j).x + Q(i-1,j).y + Q(i,j-1).z + Q(i-1,j-1).w of plane k, in that order.
+__global__ void __launch_bounds__(256) k_quad_to_nodes(const float4 *__restrict__ quad, float *__restrict__ rho,
+                                                       int nx, int ny, int64_t n) {
+    GRID_STRIDE(idx, n) {
+        const int i = (int)(idx % nx), j = (int)((idx / nx) % ny);
+        float s = __ldg(&quad[idx].x);
+        if (i > 0) s += __ldg(&quad[idx - 1].y);
+        if (j > 0) s += __ldg(&quad[idx - nx].z);
+        if (i > 0 && j > 0) s += __ldg(&quad[idx - nx - 1].w);
+        rho[idx] = s;
     }
-    __syncthreads();
-    const int li = threadIdx.x % GX, lj = (threadIdx.x / GX) % GY, lk = threadIdx.x / (GX * GY);
-    const int i = i0 + li, j = j0 + lj, k = k0 + lk;
-    if (i >= nx || j >= ny || k >= nz) return;
-    float s = 0.f;
-#pragma unroll
-    for (int c = 0; c < 2; ++c)
-#pragma unroll
-        for (int b = 0; b < 2; ++b)
-#pragma unroll
-            for (int a = 0; a < 2; ++a) s += sm[a + 2 * b + 4 * c][(li + 1 - a) + CX * ((lj + 1 - b) + CY * (lk + 1 - c))];
-    rho[(int64_t)i + (int64_t)nx * (j + (int64_t)ny * k)] = s;
 }
 
-int launch_cells_to_nodes(const float *acc, float *rho, int nx, int ny, int nz, cudaStream_t st) {
-    dim3 grid((unsigned)ceil_div(nx, GX), (unsigned)ceil_div(ny, GY), (unsigned)ceil_div(nz, GZ));
-    k_cells_to_nodes<<<grid, GX * GY * GZ, 0, st>>>(reinterpret_cast<const float4 *>(acc), rho, nx, ny, nz);
+int launch_quad_to_nodes(const float *quad, float *rho, int nx, int ny, int nz, cudaStream_t st) {
+    const int64_t n = (int64_t)nx * ny * nz;
+    k_quad_to_nodes<<<nblocks(n, 256, 148 * 16), 256, 0, st>>>(reinterpret_cast<const float4 *>(quad), rho, nx, ny,
+                                                               n);
     return ok();
 }
 
@@ -438,33 +439,35 @@ int launch_bbox(int64_t np, const double *x, const double *y, const double *z, u
 }
 
 // Deterministic two-pass sum: 1024 fixed partial sums in index order, then one block.
-__global__ void __launch_bounds__(256) k_sum_partial(int64_t n, const double *__restrict__ q, double *partials) {
+// Deterministic two-pass reductions of a particle array: op 0 sum, 1 maximum of |q|.
+__device__ __forceinline__ double red_op(double a, double b, int op) { return op ? fmax(a, b) : a + b; }
+__global__ void __launch_bounds__(256) k_sum_partial(int64_t n, const double *__restrict__ q, double *partials, int op) {
     __shared__ double sh[256];
     double s = 0;
     const int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
     const int64_t beg = blockIdx.x * chunk, end = min(n, beg + chunk);
-    for (int64_t m = beg + threadIdx.x; m < end; m += blockDim.x) s += q[m];
+    for (int64_t m = beg + threadIdx.x; m < end; m += blockDim.x) s = red_op(s, op ? fabs(q[m]) : q[m], op);
     sh[threadIdx.x] = s;
     __syncthreads();
     for (int w = 128; w; w >>= 1) {
-        if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+        if (threadIdx.x < w) sh[threadIdx.x] = red_op(sh[threadIdx.x], sh[threadIdx.x + w], op);
         __syncthreads();
     }
     if (threadIdx.x == 0) partials[blockIdx.x] = sh[0];
 }
-__global__ void k_sum_final(const double *partials, int np, double *out) {
+__global__ void k_sum_final(const double *partials, int np, double *out, int op) {
     __shared__ double sh[1024];
     sh[threadIdx.x] = threadIdx.x < np ? partials[threadIdx.x] : 0.0;
     __syncthreads();
     for (int w = 512; w; w >>= 1) {
-        if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+        if (threadIdx.x < w) sh[threadIdx.x] = red_op(sh[threadIdx.x], sh[threadIdx.x + w], op);
         __syncthreads();
     }
     if (threadIdx.x == 0) *out = sh[0];
 }
-int launch_sum(int64_t n, const double *q, double *partials, double *out, cudaStream_t st) {
-    k_sum_partial<<<1024, 256, 0, st>>>(n, q, partials);
-    k_sum_final<<<1, 1024, 0, st>>>(partials, 1024, out);
+int launch_sum(int64_t n, const double *q, double *partials, double *out, cudaStream_t st, bool max_abs) {
+    k_sum_partial<<<1024, 256, 0, st>>>(n, q, partials, max_abs ? 1 : 0);
+    k_sum_final<<<1, 1024, 0, st>>>(partials, 1024, out, max_abs ? 1 : 0);
     return ok();
 }
 

@@ -19,17 +19,24 @@ struct DepositArgs {
     int mode;
     double charge1;  // charge per particle when q == nullptr (mode 0)
     int check_finite;
+    double fx_scale;  // fixed-point accumulation: units per unit charge
 };
-// counters[0] += outside particles, counters[1] += non-finite particles
+// counters[0] += outside particles, counters[1] += non-finite particles.  TA = float or
+// double: floating-point atomics; TA = unsigned long long: each contribution rounded to
+// a 64-bit fixed-point integer (value * fx_scale), so the sum is exact and independent of
+// the order of the atomics (deterministic deposition).
 template <typename TA>
 int launch_deposit(const DepositArgs &a, TA *rho, unsigned long long *counters, cudaStream_t st);
+// out[n] = mult * (signed) acc[n] / fx_scale
+template <typename TO>
+int launch_fixed_to_real(const unsigned long long *acc, TO *out, double fx_scale, double mult, int64_t n,
+                         cudaStream_t st);
 
-// FP32 deposition through per-cell corner sums: each particle adds its 8 CIC weights to
-// the 8 floats of its cell (two 16-byte vector atomics instead of eight scalar ones), then
-// launch_cells_to_nodes gathers every node's 8 corner contributions in a fixed order.
-// acc is [nx*ny*nz][8] floats (cell index = its low node), zeroed by the caller.
-int launch_deposit_cells(const DepositArgs &a, float *acc, unsigned long long *counters, cudaStream_t st);
-int launch_cells_to_nodes(const float *acc, float *rho, int nx, int ny, int nz, cudaStream_t st);
+// FP32 step deposit: two float4 atomics per particle into a quad grid (N float4; node
+// (i,j,k) holds the plane-k contributions to nodes (i,j), (i+1,j), (i,j+1), (i+1,j+1)),
+// then launch_quad_to_nodes sums every node's four slots in a fixed order.
+int launch_deposit_quad(const DepositArgs &a, float *quad, unsigned long long *counters, cudaStream_t st);
+int launch_quad_to_nodes(const float *quad, float *rho, int nx, int ny, int nz, cudaStream_t st);
 
 // CIC gather (interpolate_field, code/open_spacecharge_mod.f90:311-390): clamp cells to
 // [1, nhi-1] (and the array), weights computed after clamping, 8-node sum in the
@@ -61,6 +68,8 @@ int launch_bbox(int64_t np, const double *x, const double *y, const double *z,
                 unsigned long long *keys /*6*/, double *bb /*6*/, unsigned long long *nonfinite,
                 cudaStream_t st);
 // Deterministic sum of q (two passes, fixed order) into *out.
-int launch_sum(int64_t n, const double *q, double *partials /*>= 1024*/, double *out, cudaStream_t st);
+// Sum of q (or, with max_abs, the largest |q|), reduced in a fixed order.
+int launch_sum(int64_t n, const double *q, double *partials /*>= 1024*/, double *out, cudaStream_t st,
+               bool max_abs = false);
 
 }  // namespace osc

@@ -32,7 +32,7 @@ PREC_FP64 = 1
 PREC_FP64_PLAIN = 2
 
 DEPOSIT_ATOMIC = 0
-DEPOSIT_SORTED = 1
+DEPOSIT_DETERMINISTIC = 1
 
 OPT_PRECISION = 1
 OPT_DEPOSIT_MODE = 2
