@@ -113,6 +113,26 @@ struct ZConvArgs {
     unsigned *fault;      // host-mapped fault word (bounded waits that gave up), or null
 };
 
+// Transform of real lines that are even (par = +1) or odd (par = -1) about index 0 on the
+// period L = 2n, of which only x[0..n) is stored (x[L-a] = par x[a], x[n] = 0): returns the
+// real s[k], k in [0, n], with sum_a x[a] exp(+2 pi i a k/L) = s[k] (even) or i s[k] (odd),
+// times scale.  Real lines are enumerated as (p, q), q fastest (q < nq); line (p, q)
+// starts at p*ps + q*qs and its elements are es apart, for input and output separately.
+struct SymArgs {
+    FFTPlan p;  // length L = 2n
+    int n, par;
+    int64_t nlines;
+    int nq;
+    int64_t in_ps, in_qs, in_es;
+    int64_t out_ps, out_qs, out_es;
+    double scale;
+};
+// row_load: elements of a line are contiguous in the input (load along the line);
+// k_fast_store: outputs of a line are contiguous (store along the line).
+template <typename TO>
+int launch_sym_lines(const double *in, TO *out, const SymArgs &a, const TwPair<cplx<double>> &tw, bool row_load,
+                     bool k_fast_store, cudaStream_t st);
+
 template <typename T>
 int launch_lines(const cplx<T> *in, cplx<T> *out, const LineArgs &a, int nplanes, int ncomp,
                  bool row_mode, const TwPair<cplx<T>> &tw, cudaStream_t st);

@@ -376,6 +376,55 @@ __global__ void __launch_bounds__(E::kLen * 3 * NLC / FFT_EPT) k_c2r_e8(const fl
     }
 }
 
+// Even/odd real line transforms (Green spectra): two real lines per complex line, the
+// parity extension formed in the load, the halves separated after the transform.
+template <typename TO, int NL, class E, bool LDE, bool STK>
+__global__ void __launch_bounds__(E::kMaxThreads) k_sym_lines(const double *__restrict__ in, TO *__restrict__ out,
+                                                              SymArgs a, const double2 *__restrict__ twg) {
+    typedef double2 V;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V *tw = reinterpret_cast<V *>(smem_raw);
+    const int L = E::kLen ? E::kLen : a.p.L;
+    V *buf = tw + L;
+    constexpr int lstr = NL + 1;
+    const int nthreads = blockDim.x, tid = threadIdx.x;
+    const int64_t r0 = (int64_t)blockIdx.x * (2 * NL);
+    const int n = a.n;
+    load_twiddles(tw, twg, L);
+    for (int idx = tid; idx < 2 * NL * L; idx += nthreads) {
+        int rr, e;
+        if (LDE) { rr = idx / L; e = idx - rr * L; }
+        else { e = idx / (2 * NL); rr = idx - e * (2 * NL); }
+        const int64_t r = r0 + rr;
+        double v = 0.0;
+        if (r < a.nlines && e != n) {
+            const int src = e < n ? e : L - e;
+            const int64_t pi = r / a.nq, qi = r - pi * a.nq;
+            v = in[pi * a.in_ps + qi * a.in_qs + (int64_t)src * a.in_es];
+            if (e > n && a.par < 0) v = -v;
+        }
+        double *slot = reinterpret_cast<double *>(&buf[e * lstr + (rr >> 1)]);
+        slot[rr & 1] = v;
+    }
+    __syncthreads();
+    E::template run<V, NL, false, false>(buf, a.p, tw, +1);
+    const int nk = n + 1;
+    for (int idx = tid; idx < 2 * NL * nk; idx += nthreads) {
+        int rr, k;
+        if (STK) { rr = idx / nk; k = idx - rr * nk; }
+        else { k = idx / (2 * NL); rr = idx - k * (2 * NL); }
+        const int64_t r = r0 + rr;
+        if (r >= a.nlines) continue;
+        const V Z = buf[k * lstr + (rr >> 1)];
+        const V Zm = buf[((L - k) % L) * lstr + (rr >> 1)];
+        double sv;
+        if ((rr & 1) == 0) sv = a.par > 0 ? 0.5 * (Z.x + Zm.x) : 0.5 * (Z.y - Zm.y);
+        else sv = a.par > 0 ? 0.5 * (Z.y + Zm.y) : 0.5 * (Zm.x - Z.x);
+        const int64_t pi = r / a.nq, qi = r - pi * a.nq;
+        out[pi * a.out_ps + qi * a.out_qs + (int64_t)k * a.out_es] = (TO)(sv * a.scale);
+    }
+}
+
 // ------------------------------------------------------------------------------------
 // Launchers.  Shared memory above 48 KB needs the opt-in attribute, set per kernel.
 template <typename K> inline int set_smem(K kern, size_t bytes) {
@@ -609,6 +658,33 @@ int launch_zconv(const cplx<T> *in, cplx<T> *out, const ZConvArgs &a, const TwPa
                 kern<<<nblk, nt, sm, st>>>(in, out, a, twe, tw.rt);
             }
             return launch_ok();
+        });
+    });
+}
+
+template <typename TO>
+int launch_sym_lines(const double *in, TO *out, const SymArgs &a, const TwPair<cplx<double>> &tw, bool row_load,
+                     bool k_fast_store, cudaStream_t st) {
+    const int L = a.p.L;
+    if (L != 2 * a.n) return OSC_E_INVALID;
+    return dispatch_fft_len(L, [&](auto eng) -> int {
+        using E = decltype(eng);
+        const double2 *twe = eng_tw<E>(tw);
+        return with_nl<double, E>(L, 1, 8, 0, [&](auto nlc) -> int {
+            constexpr int NL = decltype(nlc)::value;
+            const int nt = fft_threads(L, NL);
+            if (nt < 1 || nt > E::kMaxThreads || (L * NL) % FFT_EPT) return OSC_E_FFT_SIZE;
+            const size_t sm = sizeof(double2) * ((size_t)L + (size_t)L * (NL + 1));
+            const unsigned nblk = (unsigned)ceil_div(a.nlines, 2 * NL);
+            auto go = [&](auto kern) -> int {
+                int rc = set_smem(kern, sm);
+                if (rc) return rc;
+                kern<<<nblk, nt, sm, st>>>(in, out, a, twe);
+                return launch_ok();
+            };
+            if (row_load) return k_fast_store ? go(k_sym_lines<TO, NL, E, true, true>)
+                                              : go(k_sym_lines<TO, NL, E, true, false>);
+            return k_fast_store ? go(k_sym_lines<TO, NL, E, false, true>) : go(k_sym_lines<TO, NL, E, false, false>);
         });
     });
 }

@@ -104,6 +104,34 @@ int launch_green_center(const double *F, double2 *cg, const CenterArgs &a, cudaS
     return ok();
 }
 
+// Octant of the centred kernel for all-symmetric geometries: h[c][b][a] = g at displacement
+// (a, b, c) >= 0, the 8-corner difference of the cell whose corners are a, a+1 (the corner
+// block starts at index n-1 of the doubled grid, so cell a uses corners a and a+1).
+__global__ void k_green_octant(const double *__restrict__ F, double *__restrict__ h, int nx, int ny, int nz) {
+    const int cdx = nx + 1, cdy = ny + 1;
+    const int64_t n = (int64_t)nx * ny * nz;
+    GRID_STRIDE(idx, n) {
+        const int i = (int)(idx % nx);
+        const int64_t r = idx / nx;
+        const int j = (int)(r % ny);
+        const int k = (int)(r / ny);
+        auto f = [&](int p, int q, int s) { return F[p + (int64_t)cdx * (q + (int64_t)cdy * s)]; };
+        double g = +f(i + 1, j + 1, k + 1);
+        g = g - f(i, j + 1, k + 1);
+        g = g - f(i + 1, j, k + 1);
+        g = g - f(i + 1, j + 1, k);
+        g = g - f(i, j, k);
+        g = g + f(i, j, k + 1);
+        g = g + f(i, j + 1, k);
+        g = g + f(i + 1, j, k);
+        h[idx] = g;
+    }
+}
+int launch_green_octant(const double *F, double *h, int nx, int ny, int nz, cudaStream_t st) {
+    k_green_octant<<<nblocks((int64_t)nx * ny * nz, 256), 256, 0, st>>>(F, h, nx, ny, nz);
+    return ok();
+}
+
 template <typename T>
 __global__ void k_green_extract(const double2 *__restrict__ ghat, void *out, int nx, int Nx, int Ny,
                                 int dimy, int dimz, int real_valued, int imag_unit, double scale, int zpitch) {

@@ -32,6 +32,10 @@ struct CenterArgs {
 };
 int launch_green_center(const double *F, double2 *cg, const CenterArgs &a, cudaStream_t st);
 
+// All-symmetric geometries: the non-negative octant h[c][b][a] (a < nx, b < ny, c < nz) of
+// the centred kernel from corners F of extent (n+1) per axis starting at index n-1.
+int launch_green_octant(const double *F, double *h, int nx, int ny, int nz, cudaStream_t st);
+
 // Stored half-spectrum extraction: kx in [0,nx], ky in [0,dimy), kz in [0,dimz), times scale;
 // layout [kz][ky][kx], or [ky][kx][kz] with columns zpitch elements apart when zpitch > 0
 // (padding zeroed).

@@ -73,6 +73,76 @@ template int fft3d_full<float>(osc_ctx *, cplx<float> *, int, int, int, int, int
 template int fft3d_full<double>(osc_ctx *, cplx<double> *, int, int, int, int, int, int);
 
 // ------------------------------------------------------------------------------------
+// Stored spectrum of an all-symmetric kernel (offset 0 on every axis) from its corner block
+// F: octant differences, then even/odd transforms along x, y and z; the last pass applies
+// fpei/M and writes the stored layout directly.  Equals the extraction of the FP64 doubled-
+// grid FFT (osc_get_cgrn_freespace + ccfft3d, code/open_spacecharge_mod.f90:633-705,
+// code/fft_interface_mod.f90:96-143) up to FP64 rounding.
+template <typename T>
+static int green_sym_spectrum(osc_ctx *c, const double *F, int nx, int ny, int nz, const int par[3], int icomp,
+                              DevBuf &store, GSpecDev &spec) {
+    const int nxh = nx + 1, nyh = ny + 1, nzh = nz + 1;
+    double *h, *hx, *hy;
+    TRY(ws_get(c, "green_h", sizeof(double) * (size_t)nx * ny * nz, (void **)&h));
+    TRY(ws_get(c, "green_hx", sizeof(double) * (size_t)nxh * ny * nz, (void **)&hx));
+    TRY(ws_get(c, "green_hy", sizeof(double) * (size_t)nxh * nyh * nz, (void **)&hy));
+    {
+        Launch L_(c, "green_octant");
+        TRY(kerr(c, launch_green_octant(F, h, nx, ny, nz, c->stream), "green octant"));
+    }
+    FFTPlan px, py, pz;
+    if (!make_fft_plan(2 * nx, px) || !make_fft_plan(2 * ny, py) || !make_fft_plan(2 * nz, pz))
+        return set_err(c, OSC_E_FFT_SIZE, "doubled grid lengths must be 2^a 3^b 5^c");
+    TwPair<cplx<double>> twx, twy, twz;
+    TRY(twiddles<double>(c, 2 * nx, &twx));
+    TRY(twiddles<double>(c, 2 * ny, &twy));
+    TRY(twiddles<double>(c, 2 * nz, &twz));
+    spec.real_valued = 1;
+    spec.imag_unit = icomp != 0 ? 1 : 0;
+    spec.sym_y = spec.sym_z = 1;
+    spec.par_y = par[1];
+    spec.par_z = par[2];
+    spec.dimy = nyh;
+    spec.dimz = nzh;
+    spec.zinner = zconv_warp_ok(2 * nz, nz, (int)sizeof(T)) ? 1 : 0;
+    spec.zpitch = spec.zinner ? green_zpitch(nzh, sizeof(T)) : nzh;
+    const size_t bytes = sizeof(T) * (size_t)nxh * nyh * spec.zpitch;
+    cudaError_t e = cudaMalloc(&store.p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return set_err(c, OSC_E_ALLOC, "Green spectrum: cudaMalloc(%zu) failed", bytes);
+    }
+    store.bytes = bytes;
+    spec.data = store.p;
+    if (spec.zinner) TRY(cuda_check(c, cudaMemsetAsync(store.p, 0, bytes, c->stream), "memset spectrum"));
+    Launch L_(c, "green_sym_lines", 3);
+    SymArgs a;
+    // x: rows h[c][b][0..nx) -> hx[c][b][0..nx]
+    a.p = px; a.n = nx; a.par = par[0]; a.nlines = (int64_t)ny * nz; a.nq = ny;
+    a.in_ps = (int64_t)ny * nx; a.in_qs = nx; a.in_es = 1;
+    a.out_ps = (int64_t)ny * nxh; a.out_qs = nxh; a.out_es = 1;
+    a.scale = 1.0;
+    TRY(kerr(c, launch_sym_lines<double>(h, hx, a, twx, true, true, c->stream), "green x"));
+    // y: lines (c, kx) of hx -> hy[c][ky][kx]
+    a.p = py; a.n = ny; a.par = par[1]; a.nlines = (int64_t)nz * nxh; a.nq = nxh;
+    a.in_ps = (int64_t)ny * nxh; a.in_qs = 1; a.in_es = nxh;
+    a.out_ps = (int64_t)nyh * nxh; a.out_qs = 1; a.out_es = nxh;
+    TRY(kerr(c, launch_sym_lines<double>(hx, hy, a, twy, false, false, c->stream), "green y"));
+    // z: lines (ky, kx) of hy -> stored spectrum, scaled by fpei/M
+    a.p = pz; a.n = nz; a.par = par[2]; a.nlines = (int64_t)nyh * nxh; a.nq = nxh;
+    a.in_ps = nxh; a.in_qs = 1; a.in_es = (int64_t)nyh * nxh;
+    if (spec.zinner) {
+        a.out_ps = (int64_t)nxh * spec.zpitch; a.out_qs = spec.zpitch; a.out_es = 1;
+    } else {
+        a.out_ps = nxh; a.out_qs = 1; a.out_es = (int64_t)nyh * nxh;
+    }
+    a.scale = fpei_solver2() / (8.0 * nx * ny * nz);
+    TRY(kerr(c, launch_sym_lines<T>(hy, reinterpret_cast<T *>(store.p), a, twz, false, spec.zinner != 0, c->stream),
+             "green z"));
+    return OSC_OK;
+}
+
+// ------------------------------------------------------------------------------------
 // Green spectrum of one component (icomp 0 phi, 1..3 E) with the given offset.
 template <typename T>
 static int build_green_component(osc_ctx *c, int nx, int ny, int nz, const double delta[3], double gamma,
@@ -106,6 +176,14 @@ static int build_green_component(osc_ctx *c, int nx, int ny, int nz, const doubl
     {
         Launch L_(c, "green_corners");
         TRY(kerr(c, launch_igf_corners(F, ca, c->stream), "green corners"));
+    }
+    const bool all_sym = sym[0] && sym[1] && sym[2];
+    if (all_sym) {
+        // the spectrum of a kernel that is even or odd along every axis is a product of
+        // real even/odd line transforms of its non-negative octant: three passes over
+        // (n+1)^3 reals instead of an FFT of the complex doubled grid
+        TRY(green_sym_spectrum<T>(c, F, nx, ny, nz, par, icomp, store, spec));
+        return OSC_OK;
     }
     CenterArgs ce;
     ce.nx = nx; ce.ny = ny; ce.nz = nz;
