@@ -219,6 +219,33 @@ OSC_API int osc_space_charge_step_dev(osc_ctx *ctx, osc_mesh3d *mesh, int64_t np
                               const double *total_charge, int resize_mesh, int at_cathode,
                               int precision, double *d_E, double *d_B);
 
+/* ---- batched steps ---------------------------------------------------------------------
+ * Many independent bunches, each with its own mesh, in one call: the fused step above for
+ * every bunch (free space, no cathode image, E only).  The reference solves one bunch per
+ * call (space_charge_3d, code/open_spacecharge_mod.f90:431-489, called from
+ * code/test_opensc.f90:184); a tracking code with many bunches calls it in a loop, which
+ * this replaces.  Particles of all bunches are concatenated: bunch b owns entries
+ * [offset, offset + np) of x, y, z, q and of the rows of E ([total][3]).  With resize_mesh
+ * each bunch's mesh is refit to its particles as deposit_particles does; the Green
+ * spectra are rebuilt for every bunch on every call (meshes change between steps).
+ * OSC_PREC_FP32 runs all bunches through batched kernels, grouped by grid shape; the
+ * FP64 precisions solve the bunches one after another. */
+typedef struct osc_bunch {
+    osc_mesh3d mesh;      /* in: nlo, nhi, gamma (+ min, max, delta without resize);
+                             out: fitted geometry and charge */
+    int64_t offset;       /* first particle of this bunch in the concatenated arrays */
+    int64_t np;           /* particles of this bunch (>= 1) */
+    double total_charge;  /* charge of the bunch when q is NULL */
+    int64_t n_outside;    /* out: particles outside the mesh (not deposited) */
+} osc_bunch;
+
+OSC_API int osc_batch_space_charge_step(osc_ctx *ctx, int nbunch, osc_bunch *bunches, const double *x,
+                                        const double *y, const double *z, const double *q, int resize_mesh,
+                                        int precision, double *E);
+OSC_API int osc_batch_space_charge_step_dev(osc_ctx *ctx, int nbunch, osc_bunch *bunches, const double *d_x,
+                                            const double *d_y, const double *d_z, const double *d_q,
+                                            int resize_mesh, int precision, double *d_E);
+
 #ifdef __cplusplus
 }
 #endif

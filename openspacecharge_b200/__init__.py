@@ -5,8 +5,8 @@ C ABI (``include/opensc_gpu.h``, ``libopensc_b200.so``).
 """
 from .native import (DEPOSIT_ATOMIC, DEPOSIT_DETERMINISTIC, OPT_CHECK_FINITE, OPT_DEPOSIT_MODE,
                      OPT_GREEN_CACHE_MB, OPT_PRECISION, OPT_PROFILE, OPT_STRICT_BOUNDS,
-                     PREC_FP32, PREC_FP64, PREC_FP64_PLAIN, Context, OscError, OscMesh3D)
-from .mesh import (Mesh3D, depose_rho_scalar, deposit_particles, get_mesh_quantities,
+                     PREC_FP32, PREC_FP64, PREC_FP64_PLAIN, Context, OscBunch, OscError, OscMesh3D)
+from .mesh import (Mesh3D, batch_space_charge_step, batch_space_charge_step_dev, depose_rho_scalar, deposit_particles, get_mesh_quantities,
                    interpolate_field, osc_freespace_solver2, osc_read_rectpipe_grn,
                    osc_rectpipe_green, osc_write_rectpipe_grn, space_charge_3d,
                    space_charge_cathodeimages, space_charge_freespace, space_charge_rectpipe,

@@ -1,0 +1,247 @@
+// abi_util.cuh -- host helpers shared by the extern "C" entry points (abi.cu, batch.cu).
+#pragma once
+#include <cmath>
+#include <cstring>
+
+#include "../../include/opensc_gpu.h"
+#include "solver.cuh"
+
+#define TRY(...)                 \
+    do {                         \
+        int rc_ = (__VA_ARGS__); \
+        if (rc_) return rc_;     \
+    } while (0)
+#define CK(call, what) TRY(cuda_check(ctx, (call), what))
+
+namespace osc_abi {
+using namespace osc;
+
+inline int bad(osc_ctx *ctx, const char *what) { return set_err(ctx, OSC_E_INVALID, "invalid argument: %s", what); }
+
+inline int mesh_dims(osc_ctx *ctx, const osc_mesh3d *m, int n[3]) {
+    if (!m) return bad(ctx, "mesh is NULL");
+    for (int d = 0; d < 3; ++d) {
+        n[d] = m->nhi[d] - m->nlo[d] + 1;
+        if (n[d] < 2) return set_err(ctx, OSC_E_INVALID, "mesh axis %d has %d nodes (need >= 2)", d, n[d]);
+    }
+    return OSC_OK;
+}
+
+inline int check_prec(osc_ctx *ctx, int p) {
+    if (p < 0 || p > 2) return bad(ctx, "precision must be OSC_PREC_FP32, OSC_PREC_FP64 or OSC_PREC_FP64_PLAIN");
+    return OSC_OK;
+}
+
+inline int h2d(osc_ctx *ctx, void *d, const void *h, size_t bytes) {
+    return cuda_check(ctx, cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, ctx->stream), "H2D copy");
+}
+inline int d2h(osc_ctx *ctx, void *h, const void *d, size_t bytes) {
+    return cuda_check(ctx, cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, ctx->stream), "D2H copy");
+}
+inline int sync(osc_ctx *ctx) { return ctx_sync(ctx); }
+
+// Stage a host array on the device under a workspace name.
+template <typename T> inline int stage_in(osc_ctx *ctx, const char *name, const T *h, size_t n, T **d) {
+    if (!h) {
+        *d = nullptr;
+        return OSC_OK;
+    }
+    TRY(ws_get(ctx, name, sizeof(T) * n, (void **)d));
+    return h2d(ctx, *d, h, sizeof(T) * n);
+}
+
+// Mesh refit of deposit_particles (code/open_spacecharge_mod.f90:176-189) from the
+// particle bounding box: the box widened by 1e-6 cells on each side.
+inline void apply_refit(osc_mesh3d *mesh, const double bmin[3], const double bmax[3]) {
+    double mn[3] = {bmin[0], bmin[1], bmin[2]}, mx[3] = {bmax[0], bmax[1], bmax[2]}, delta[3];
+    for (int d = 0; d < 3; ++d) delta[d] = (mx[d] - mn[d]) / (double)(mesh->nhi[d] - mesh->nlo[d]);
+    for (int d = 0; d < 3; ++d) {
+        mn[d] = mn[d] - 1.0e-6 * delta[d];
+        mx[d] = mx[d] + 1.0e-6 * delta[d];
+    }
+    for (int d = 0; d < 3; ++d) delta[d] = (mx[d] - mn[d]) / (double)(mesh->nhi[d] - mesh->nlo[d]);
+    for (int d = 0; d < 3; ++d) {
+        mesh->min[d] = mn[d];
+        mesh->max[d] = mx[d];
+        mesh->delta[d] = delta[d];
+    }
+}
+
+// Reference mesh refit of deposit_particles (code/open_spacecharge_mod.f90:176-189) from
+// the particle bounding box computed on the device.
+inline int refit_mesh(osc_ctx *ctx, int64_t np, const double *x, const double *y, const double *z, osc_mesh3d *mesh) {
+    if (np <= 0) return set_err(ctx, OSC_E_INVALID, "resize_mesh needs at least one particle");
+    double *bb;
+    TRY(ws_get(ctx, "bbox", sizeof(double) * 8, (void **)&bb));
+    {
+        Launch L_(ctx, "bbox", 3);
+        TRY(launch_bbox(np, x, y, z, ctx->d_small + 8, bb, ctx->d_small + 16, ctx->stream) ? set_err(ctx, OSC_E_CUDA, "bbox") : 0);
+    }
+    double hb[6];
+    TRY(d2h(ctx, hb, bb, sizeof(hb)));
+    TRY(d2h(ctx, ctx->h_small + 16, ctx->d_small + 16, sizeof(unsigned long long)));
+    TRY(sync(ctx));
+    if (ctx->h_small[16]) return set_err(ctx, OSC_E_NAN, "%llu non-finite particle coordinates", ctx->h_small[16]);
+    const double mn[3] = {hb[0], hb[2], hb[4]}, mx[3] = {hb[1], hb[3], hb[5]};
+    apply_refit(mesh, mn, mx);
+    return OSC_OK;
+}
+
+inline int set_charge(osc_ctx *ctx, int64_t np, const double *q, const double *total_charge, osc_mesh3d *mesh,
+               double *charge1) {
+    if (q) {
+        double *out;
+        TRY(ws_get(ctx, "qsum", sizeof(double), (void **)&out));
+        {
+            Launch L_(ctx, "charge_sum", 2);
+            if (launch_sum(np, q, ctx->d_partials, out, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "charge sum");
+        }
+        double s = 0;
+        TRY(d2h(ctx, &s, out, sizeof(double)));
+        TRY(sync(ctx));
+        mesh->charge = s;
+        *charge1 = 0;
+    } else if (total_charge) {
+        mesh->charge = *total_charge;
+        *charge1 = *total_charge / (double)np;
+    } else {
+        return set_err(ctx, OSC_E_NOCHARGE, "Error, must specify qa or total_charge");
+    }
+    return OSC_OK;
+}
+
+inline DepositArgs deposit_args(const osc_mesh3d *m, const int n[3], int64_t np, const double *x, const double *y,
+                         const double *z, const double *q, double charge1, int check_finite) {
+    DepositArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.np = np;
+    a.x = x; a.y = y; a.z = z; a.q = q; a.lost = nullptr;
+    a.xmin = m->min[0]; a.ymin = m->min[1]; a.zmin = m->min[2];
+    a.dx = m->delta[0]; a.dy = m->delta[1]; a.dz = m->delta[2];
+    a.dxi = 1.0 / a.dx; a.dyi = 1.0 / a.dy; a.dzi = 1.0 / a.dz;
+    for (int d = 0; d < 3; ++d) {
+        a.nlo[d] = m->nlo[d];
+        a.nhi[d] = m->nhi[d];
+        a.nlogbl[d] = m->nlo[d];
+    }
+    a.nx = n[0]; a.ny = n[1]; a.nz = n[2];
+    a.mode = 0;
+    a.charge1 = charge1;
+    a.check_finite = check_finite;
+    return a;
+}
+
+// Deposition of a.np particles into rho (zeroed here).  OSC_DEPOSIT_ATOMIC uses
+// floating-point atomics of the type of rho; OSC_DEPOSIT_DETERMINISTIC accumulates 64-bit
+// fixed-point integers and converts once, so rho is bit-identical for any particle order.
+// The fixed-point unit is a power of two chosen from np * max|q| (order-independent), so
+// that no node sum can exceed 2^62 units.  rho = mult * sum.
+template <typename TR> inline int deposit_rho(osc_ctx *ctx, DepositArgs a, TR *rho, int64_t N, double mult) {
+    if (ctx->deposit_mode != OSC_DEPOSIT_DETERMINISTIC) {
+        CK(cudaMemsetAsync(rho, 0, sizeof(TR) * N, ctx->stream), "memset rho");
+        {
+            Launch L_(ctx, sizeof(TR) == 8 ? "deposit_f64" : "deposit_f32");
+            if (launch_deposit<TR>(a, rho, ctx->d_small, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "deposit");
+        }
+        if (mult != 1.0) {
+            if constexpr (sizeof(TR) == 8) {
+                Launch L_(ctx, "scale");
+                if (launch_scale(rho, mult, N, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "scale");
+            } else {
+                return set_err(ctx, OSC_E_INVALID, "scaled FP32 deposit");
+            }
+        }
+        return OSC_OK;
+    }
+    double qmax;
+    if (a.mode == 0 && a.q) {
+        double *out;
+        TRY(ws_get(ctx, "qmax", sizeof(double), (void **)&out));
+        {
+            Launch L_(ctx, "charge_max", 2);
+            if (launch_sum(a.np, a.q, ctx->d_partials, out, ctx->stream, true))
+                return set_err(ctx, OSC_E_CUDA, "charge max");
+        }
+        TRY(d2h(ctx, &qmax, out, sizeof(double)));
+        TRY(sync(ctx));
+    } else {
+        qmax = a.mode == 0 ? std::fabs(a.charge1) : 1.0;
+    }
+    const double bound = (double)a.np * qmax;  // >= sum of |contributions| at any node
+    a.fx_scale = 1.0;
+    if (bound > 0 && std::isfinite(bound)) {
+        int e;
+        std::frexp(bound, &e);  // bound < 2^e
+        a.fx_scale = std::ldexp(1.0, 62 - e);
+    }
+    unsigned long long *acc;
+    TRY(ws_get(ctx, "rho_fixed", sizeof(unsigned long long) * N, (void **)&acc));
+    CK(cudaMemsetAsync(acc, 0, sizeof(unsigned long long) * N, ctx->stream), "memset fixed");
+    {
+        Launch L_(ctx, "deposit_fixed");
+        if (launch_deposit<unsigned long long>(a, acc, ctx->d_small, ctx->stream))
+            return set_err(ctx, OSC_E_CUDA, "deposit");
+    }
+    {
+        Launch L_(ctx, "fixed_to_real");
+        if (launch_fixed_to_real<TR>(acc, rho, a.fx_scale, mult, N, ctx->stream))
+            return set_err(ctx, OSC_E_CUDA, "fixed to real");
+    }
+    return OSC_OK;
+}
+
+inline InterpArgs interp_args(const osc_mesh3d *m, const int n[3], int64_t np, const double *x, const double *y,
+                       const double *z) {
+    InterpArgs a;
+    a.np = np;
+    a.x = x; a.y = y; a.z = z;
+    for (int d = 0; d < 3; ++d) {
+        a.min[d] = m->min[d];
+        a.delta[d] = m->delta[d];
+        a.hinv[d] = 1.0 / m->delta[d];
+        a.nlo[d] = m->nlo[d];
+        a.nhi[d] = m->nhi[d];
+    }
+    a.nx = n[0]; a.ny = n[1]; a.nz = n[2];
+    return a;
+}
+
+inline int counters_reset(osc_ctx *ctx) {
+    return cuda_check(ctx, cudaMemsetAsync(ctx->d_small, 0, sizeof(unsigned long long) * 8, ctx->stream), "memset counters");
+}
+// counters: [0] outside, [1] non-finite, [2] clamped
+inline int counters_read(osc_ctx *ctx, unsigned long long out[3]) {
+    TRY(d2h(ctx, ctx->h_small, ctx->d_small, sizeof(unsigned long long) * 3));
+    TRY(sync(ctx));
+    for (int i = 0; i < 3; ++i) out[i] = ctx->h_small[i];
+    return OSC_OK;
+}
+
+inline FreeSpaceJob fs_job(const osc_mesh3d *mesh, const int n[3], const double *offset, int at_cathode, int calc_b) {
+    FreeSpaceJob j;
+    j.nx = n[0]; j.ny = n[1]; j.nz = n[2];
+    for (int d = 0; d < 3; ++d) {
+        j.delta[d] = mesh->delta[d];
+        j.offset[d] = offset ? offset[d] : 0.0;
+    }
+    j.gamma = mesh->gamma;
+    j.at_cathode = at_cathode ? 1 : 0;
+    // offset0(3) + 2*min(3) + (max(3)-min(3)) (code/open_spacecharge_mod.f90:472)
+    j.img_zoff = 2 * mesh->min[2] + (mesh->max[2] - mesh->min[2]);
+    j.calc_b = calc_b ? 1 : 0;
+    if (calc_b) {
+        const double beta = std::sqrt(1 - 1 / (mesh->gamma * mesh->gamma));
+        j.bcoef = beta / c_light_sc3d();
+    }
+    return j;
+}
+
+inline int run_freespace(osc_ctx *ctx, const FreeSpaceJob &j, const double *d_rho, int precision) {
+    switch (precision) {
+    case OSC_PREC_FP32: return freespace_opt<float, double>(ctx, j, d_rho);
+    case OSC_PREC_FP64: return freespace_opt<double, double>(ctx, j, d_rho);
+    default: return freespace_plain(ctx, j, d_rho);
+    }
+}
+
+}  // namespace osc_abi

@@ -76,12 +76,13 @@ struct GSpecDev {
 // Value of a stored Green spectrum at (kx, ky, kz) of the Nx/2+1 x Ny x Nz half spectrum.
 template <typename T>
 __device__ __forceinline__ cplx<T> g_lookup(const GSpecDev &g, int kx, int ky, int kz, int nxh,
-                                            int Ny, int ny, int Nz, int nz) {
+                                            int Ny, int ny, int Nz, int nz, int64_t goff = 0) {
     int yy = ky, zz = kz;
     bool neg = false;
     if (g.sym_y && ky > ny) { yy = Ny - ky; neg ^= (g.par_y < 0); }
     if (g.sym_z && kz > nz) { zz = Nz - kz; neg ^= (g.par_z < 0); }
-    const int64_t idx = g.zinner ? ((int64_t)yy * nxh + kx) * g.zpitch + zz : ((int64_t)zz * g.dimy + yy) * nxh + kx;
+    const int64_t idx =
+        goff + (g.zinner ? ((int64_t)yy * nxh + kx) * g.zpitch + zz : ((int64_t)zz * g.dimy + yy) * nxh + kx);
     if (g.real_valued) {
         T s = __ldg(reinterpret_cast<const T *>(g.data) + idx);
         if (neg) s = -s;
@@ -111,21 +112,29 @@ struct ZConvArgs {
     int ng;
     GSpecDev g[8];
     unsigned *fault;      // host-mapped fault word (bounded waits that gave up), or null
+    // batches of equal grids (blockIdx.y = member): input, output and spectrum offsets of
+    // member b are b*in_bstride, b*out_bstride and b*g_bstride (elements of the spectrum)
+    int nbatch;
+    int64_t in_bstride, out_bstride, g_bstride;
 };
 
 // Transform of real lines that are even (par = +1) or odd (par = -1) about index 0 on the
 // period L = 2n, of which only x[0..n) is stored (x[L-a] = par x[a], x[n] = 0): returns the
 // real s[k], k in [0, n], with sum_a x[a] exp(+2 pi i a k/L) = s[k] (even) or i s[k] (odd),
-// times scale.  Real lines are enumerated as (p, q), q fastest (q < nq); line (p, q)
-// starts at p*ps + q*qs and its elements are es apart, for input and output separately.
+// times scale.  Real lines are enumerated as (b, p, q), q fastest (q < nq, p*nq + q < npq);
+// line (b, p, q) starts at b*bs + p*ps + q*qs and its elements are es apart, for input and
+// output separately.
 struct SymArgs {
     FFTPlan p;  // length L = 2n
-    int n, par;
+    int n;
+    int odd_lo, odd_hi;  // members b in [odd_lo, odd_hi) are odd (par -1), the others even
     int64_t nlines;
     int nq;
     int64_t in_ps, in_qs, in_es;
     int64_t out_ps, out_qs, out_es;
     double scale;
+    // batches: lines of member b are the lines [b*npq, (b+1)*npq), offset by b*in_bs, b*out_bs
+    int64_t npq, in_bs, out_bs;
 };
 // row_load: elements of a line are contiguous in the input (load along the line);
 // k_fast_store: outputs of a line are contiguous (store along the line).

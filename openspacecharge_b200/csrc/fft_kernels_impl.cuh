@@ -277,6 +277,9 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_zconv(const cplx<T> *__restr
     constexpr int lstr = NL + 1;
     V *buf = rhat + L * lstr;
     const int col0 = blockIdx.x * NL;
+    in += blockIdx.y * a.in_bstride;
+    out += blockIdx.y * a.out_bstride;
+    const int64_t goff = blockIdx.y * a.g_bstride;
     load_twiddles(tw, twg, L);
     __syncthreads();
     auto ld_in = [&](int e, int l) -> V {
@@ -294,7 +297,8 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_zconv(const cplx<T> *__restr
             const int col = min(col0 + l, a.ncols - 1);
             const int ky = col / a.nxh, kx = col - ky * a.nxh;
             V S = mk<T>(0, 0);
-            if (gd >= 0) S = cmul(rhat[e * lstr + l], g_lookup<T>(a.g[gd], kx, ky, e, a.nxh, a.Ny, a.ny, L, a.nz));
+            if (gd >= 0)
+                S = cmul(rhat[e * lstr + l], g_lookup<T>(a.g[gd], kx, ky, e, a.nxh, a.Ny, a.ny, L, a.nz, goff));
             if (gi >= 0) {
                 // spectrum of -rho flipped in z: -w^((nz-1) kz) * rho_hat(-kz)
                 const V rm = rhat[((L - e) % L) * lstr + l];
@@ -302,7 +306,7 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_zconv(const cplx<T> *__restr
                 V ri = cmul(ph, rm);
                 ri.x = -ri.x * icoef;
                 ri.y = -ri.y * icoef;
-                S = cadd(S, cmul(ri, g_lookup<T>(a.g[gi], kx, ky, e, a.nxh, a.Ny, a.ny, L, a.nz)));
+                S = cadd(S, cmul(ri, g_lookup<T>(a.g[gi], kx, ky, e, a.nxh, a.Ny, a.ny, L, a.nz, goff)));
             }
             return S;
         };
@@ -383,6 +387,8 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_sym_lines(const double *__re
                                                               SymArgs a, const double2 *__restrict__ twg) {
     typedef double2 V;
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int64_t bin[2 * NL], bout[2 * NL];
+    __shared__ int podd[2 * NL];
     V *tw = reinterpret_cast<V *>(smem_raw);
     const int L = E::kLen ? E::kLen : a.p.L;
     V *buf = tw + L;
@@ -390,18 +396,33 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_sym_lines(const double *__re
     const int nthreads = blockDim.x, tid = threadIdx.x;
     const int64_t r0 = (int64_t)blockIdx.x * (2 * NL);
     const int n = a.n;
+    for (int t = tid; t < 2 * NL; t += nthreads) {  // line start offsets, once per line
+        const int64_t r = r0 + t;
+        int64_t oi = -1, oo = -1;
+        int odd = 0;
+        if (r < a.nlines) {
+            const int64_t bi = r / a.npq, rl = r - bi * a.npq;
+            const int64_t pi = rl / a.nq, qi = rl - pi * a.nq;
+            oi = bi * a.in_bs + pi * a.in_ps + qi * a.in_qs;
+            oo = bi * a.out_bs + pi * a.out_ps + qi * a.out_qs;
+            odd = bi >= a.odd_lo && bi < a.odd_hi;
+        }
+        bin[t] = oi;
+        bout[t] = oo;
+        podd[t] = odd;
+    }
     load_twiddles(tw, twg, L);
+    __syncthreads();
     for (int idx = tid; idx < 2 * NL * L; idx += nthreads) {
         int rr, e;
         if (LDE) { rr = idx / L; e = idx - rr * L; }
         else { e = idx / (2 * NL); rr = idx - e * (2 * NL); }
-        const int64_t r = r0 + rr;
+        const int64_t o = bin[rr];
         double v = 0.0;
-        if (r < a.nlines && e != n) {
+        if (o >= 0 && e != n) {
             const int src = e < n ? e : L - e;
-            const int64_t pi = r / a.nq, qi = r - pi * a.nq;
-            v = in[pi * a.in_ps + qi * a.in_qs + (int64_t)src * a.in_es];
-            if (e > n && a.par < 0) v = -v;
+            v = in[o + (int64_t)src * a.in_es];
+            if (e > n && podd[rr]) v = -v;
         }
         double *slot = reinterpret_cast<double *>(&buf[e * lstr + (rr >> 1)]);
         slot[rr & 1] = v;
@@ -413,15 +434,15 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_sym_lines(const double *__re
         int rr, k;
         if (STK) { rr = idx / nk; k = idx - rr * nk; }
         else { k = idx / (2 * NL); rr = idx - k * (2 * NL); }
-        const int64_t r = r0 + rr;
-        if (r >= a.nlines) continue;
+        const int64_t o = bout[rr];
+        if (o < 0) continue;
         const V Z = buf[k * lstr + (rr >> 1)];
         const V Zm = buf[((L - k) % L) * lstr + (rr >> 1)];
+        const bool odd = podd[rr];
         double sv;
-        if ((rr & 1) == 0) sv = a.par > 0 ? 0.5 * (Z.x + Zm.x) : 0.5 * (Z.y - Zm.y);
-        else sv = a.par > 0 ? 0.5 * (Z.y + Zm.y) : 0.5 * (Zm.x - Z.x);
-        const int64_t pi = r / a.nq, qi = r - pi * a.nq;
-        out[pi * a.out_ps + qi * a.out_qs + (int64_t)k * a.out_es] = (TO)(sv * a.scale);
+        if ((rr & 1) == 0) sv = !odd ? 0.5 * (Z.x + Zm.x) : 0.5 * (Z.y - Zm.y);
+        else sv = !odd ? 0.5 * (Z.y + Zm.y) : 0.5 * (Zm.x - Z.x);
+        out[o + (int64_t)k * a.out_es] = (TO)(sv * a.scale);
     }
 }
 
@@ -591,7 +612,8 @@ inline int launch_zconv_warp_k(const cplx<T> *in, cplx<T> *out, const ZConvArgs 
     auto kern = k_zconv_warp<T, W, MODE, L, Rs...>;
     int rc = set_smem(kern, sm);
     if (rc) return rc;
-    kern<<<(unsigned)ceil_div(a.ncols, W), W * 32, sm, st>>>(in, out, a, tw.wt, tw.rt);
+    const dim3 grid((unsigned)ceil_div(a.ncols, W), (unsigned)(a.nbatch > 0 ? a.nbatch : 1));
+    kern<<<grid, W * 32, sm, st>>>(in, out, a, tw.wt, tw.rt);
     return launch_ok();
 }
 template <typename T, int MODE, int L, int... Rs>
@@ -645,7 +667,7 @@ int launch_zconv(const cplx<T> *in, cplx<T> *out, const ZConvArgs &a, const TwPa
             const int nt = fft_threads(L, NL);
             if (nt < 1 || nt > E::kMaxThreads || (L * NL) % FFT_EPT) return OSC_E_FFT_SIZE;
             const size_t sm = sizeof(cplx<T>) * ((size_t)L + 2 * (size_t)L * (NL + 1));
-            const unsigned nblk = (unsigned)ceil_div(a.ncols, NL);
+            const dim3 nblk((unsigned)ceil_div(a.ncols, NL), (unsigned)(a.nbatch > 0 ? a.nbatch : 1));
             if (E::kLen > 0 && 2 * a.nz == L) {
                 auto kern = k_zconv<T, NL, E, true>;
                 int rc = set_smem(kern, sm);

@@ -109,26 +109,52 @@ int launch_green_center(const double *F, double2 *cg, const CenterArgs &a, cudaS
 // block starts at index n-1 of the doubled grid, so cell a uses corners a and a+1).
 __global__ void k_green_octant(const double *__restrict__ F, double *__restrict__ h, int nx, int ny, int nz) {
     const int cdx = nx + 1, cdy = ny + 1;
-    const int64_t n = (int64_t)nx * ny * nz;
-    GRID_STRIDE(idx, n) {
-        const int i = (int)(idx % nx);
-        const int64_t r = idx / nx;
-        const int j = (int)(r % ny);
-        const int k = (int)(r / ny);
-        auto f = [&](int p, int q, int s) { return F[p + (int64_t)cdx * (q + (int64_t)cdy * s)]; };
-        double g = +f(i + 1, j + 1, k + 1);
-        g = g - f(i, j + 1, k + 1);
-        g = g - f(i + 1, j, k + 1);
-        g = g - f(i + 1, j + 1, k);
-        g = g - f(i, j, k);
-        g = g + f(i, j, k + 1);
-        g = g + f(i, j + 1, k);
-        g = g + f(i + 1, j, k);
+    const int n = nx * ny * nz;  // one member's octant (< 2^31 nodes)
+    F += blockIdx.y * ((int64_t)cdx * cdy * (nz + 1));  // batch member
+    h += blockIdx.y * (int64_t)n;
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
+        const int i = idx % nx, r = idx / nx;
+        const int j = r % ny, k = r / ny;
+        const double *f0 = F + i + cdx * (j + cdy * k);
+        const int sy = cdx, sz = cdx * cdy;
+        double g = +f0[1 + sy + sz];
+        g = g - f0[sy + sz];
+        g = g - f0[1 + sz];
+        g = g - f0[1 + sy];
+        g = g - f0[0];
+        g = g + f0[sz];
+        g = g + f0[sy];
+        g = g + f0[1];
         h[idx] = g;
     }
 }
-int launch_green_octant(const double *F, double *h, int nx, int ny, int nz, cudaStream_t st) {
-    k_green_octant<<<nblocks((int64_t)nx * ny * nz, 256), 256, 0, st>>>(F, h, nx, ny, nz);
+int launch_green_octant(const double *F, double *h, int nx, int ny, int nz, int nbatch, cudaStream_t st) {
+    const dim3 grid(nblocks((int64_t)nx * ny * nz, 256), (unsigned)nbatch);
+    k_green_octant<<<grid, 256, 0, st>>>(F, h, nx, ny, nz);
+    return ok();
+}
+
+// Corner blocks of several geometries: member blockIdx.y uses args[blockIdx.y] and writes
+// F + blockIdx.y * fstride.
+__global__ void k_igf_corners_batch(double *__restrict__ F, const CornerArgs *__restrict__ args, int64_t fstride) {
+    const CornerArgs a = args[blockIdx.y];
+    F += blockIdx.y * fstride;
+    const int64_t n = (int64_t)a.cdx * a.cdy * a.cdz;
+    GRID_STRIDE(idx, n) {
+        const int cx = (int)(idx % a.cdx);
+        const int64_t r = idx / a.cdx;
+        const int cy = (int)(r % a.cdy);
+        const int cz = (int)(r / a.cdy);
+        const double u = (a.c0x + cx) * a.dx + a.umin;
+        const double v = (a.c0y + cy) * a.dy + a.vmin;
+        const double w = (a.c0z + cz) * a.dz + a.wmin;
+        F[idx] = igf_primitive(a.icomp, u, v, w) * a.factor;
+    }
+}
+int launch_igf_corners_batch(double *F, const CornerArgs *args_dev, int nbatch, int64_t fstride, int64_t npts,
+                             cudaStream_t st) {
+    const dim3 grid(nblocks(npts, 256), (unsigned)nbatch);
+    k_igf_corners_batch<<<grid, 256, 0, st>>>(F, args_dev, fstride);
     return ok();
 }
 

@@ -116,6 +116,30 @@ template int launch_fixed_to_real<double>(const unsigned long long *, double *, 
 // float4 atomics (planes k and k+1) on a 16-byte-per-node grid that stays in L2.  The
 // weights are the factors of deposit_particles (code/open_spacecharge_mod.f90:274-281).
 // Pass 2 sums every node's four quad slots in a fixed order.
+// One particle of the quad deposit: 0 deposited, 1 outside the mesh, 2 non-finite.
+__device__ __forceinline__ int quad_one(const DepositArgs &a, float4 *__restrict__ quad, int64_t plane, double xm,
+                                        double ym, double zm, double c) {
+    if (a.check_finite && !(isfinite(xm) && isfinite(ym) && isfinite(zm))) return 2;
+    const double fx = floor((xm - a.xmin) * a.dxi + 1);
+    const double fy = floor((ym - a.ymin) * a.dyi + 1);
+    const double fz = floor((zm - a.zmin) * a.dzi + 1);
+    if (!(fx >= a.nlo[0] && fx + 1 <= a.nhi[0] && fy >= a.nlo[1] && fy + 1 <= a.nhi[1] && fz >= a.nlo[2] &&
+          fz + 1 <= a.nhi[2]))
+        return 1;
+    const double ab = ((a.xmin - xm) + fx * a.dx) * a.dxi;
+    const double de = ((a.ymin - ym) + fy * a.dy) * a.dyi;
+    const double gh = ((a.zmin - zm) + fz * a.dz) * a.dzi;
+    const double omab = 1. - ab, omde = 1. - de, omgh = 1. - gh;
+    const double lo = gh * c, hi = omgh * c;
+    const int i = (int)fx - a.nlo[0], j = (int)fy - a.nlo[1], k = (int)fz - a.nlo[2];
+    float4 *q0 = quad + ((int64_t)i + (int64_t)a.nx * j + plane * k);
+    atomicAdd(q0, make_float4((float)(ab * de * lo), (float)(omab * de * lo), (float)(ab * omde * lo),
+                              (float)(omab * omde * lo)));
+    atomicAdd(q0 + plane, make_float4((float)(ab * de * hi), (float)(omab * de * hi), (float)(ab * omde * hi),
+                                      (float)(omab * omde * hi)));
+    return 0;
+}
+
 __global__ void __launch_bounds__(256) k_deposit_quad(DepositArgs a, float4 *__restrict__ quad,
                                                       unsigned long long *__restrict__ counters) {
     const int64_t plane = (int64_t)a.nx * a.ny;
@@ -138,30 +162,9 @@ __global__ void __launch_bounds__(256) k_deposit_quad(DepositArgs a, float4 *__r
             zn = __ldg(a.z + mn);
             if (a.q) qn = __ldg(a.q + mn);
         }
-        bool nonfinite = false, skip = false;
-        if (a.check_finite && !(isfinite(xm) && isfinite(ym) && isfinite(zm))) {
-            nonfinite = true;
-            skip = true;
-        }
-        const double fx = floor((xm - a.xmin) * a.dxi + 1);
-        const double fy = floor((ym - a.ymin) * a.dyi + 1);
-        const double fz = floor((zm - a.zmin) * a.dzi + 1);
-        const bool outside = !skip && !(fx >= a.nlo[0] && fx + 1 <= a.nhi[0] && fy >= a.nlo[1] &&
-                                        fy + 1 <= a.nhi[1] && fz >= a.nlo[2] && fz + 1 <= a.nhi[2]);
-        count_one(&counters[0], outside);
-        count_one(&counters[1], nonfinite);
-        if (skip || outside) continue;
-        const double ab = ((a.xmin - xm) + fx * a.dx) * a.dxi;
-        const double de = ((a.ymin - ym) + fy * a.dy) * a.dyi;
-        const double gh = ((a.zmin - zm) + fz * a.dz) * a.dzi;
-        const double omab = 1. - ab, omde = 1. - de, omgh = 1. - gh;
-        const double lo = gh * c, hi = omgh * c;
-        const int i = (int)fx - a.nlo[0], j = (int)fy - a.nlo[1], k = (int)fz - a.nlo[2];
-        float4 *q0 = quad + ((int64_t)i + (int64_t)a.nx * j + plane * k);
-        atomicAdd(q0, make_float4((float)(ab * de * lo), (float)(omab * de * lo), (float)(ab * omde * lo),
-                                  (float)(omab * omde * lo)));
-        atomicAdd(q0 + plane, make_float4((float)(ab * de * hi), (float)(omab * de * hi), (float)(ab * omde * hi),
-                                          (float)(omab * omde * hi)));
+        const int st = quad_one(a, quad, plane, xm, ym, zm, c);
+        count_one(&counters[0], st == 1);
+        count_one(&counters[1], st == 2);
     }
 }
 
@@ -317,6 +320,34 @@ __device__ __forceinline__ void ldg_pair(const float4 *p, float4 &lo, float4 &hi
         : "l"(p));
 }
 
+// One particle of the x-pair gather; returns true when its cell was clamped.
+__device__ __forceinline__ bool interp_pair_one(const InterpArgs &a, const float4 *__restrict__ g8, int64_t plane,
+                                                double xm, double ym, double zm, double *__restrict__ Eo) {
+    Cell c;
+    const bool fl = locate(a, xm, ym, zm, c);
+    const int64_t n0 = c.i + (int64_t)a.nx * c.j + plane * c.k;
+    const double ab = c.ab, de = c.de, gh = c.gh;
+    const double omab = 1. - ab, omde = 1. - de, omgh = 1. - gh;
+    // (j,k), (j+1,k), (j+1,k+1), (j,k+1) rows; each pair = nodes i and i+1
+    const int64_t rows[4] = {n0, n0 + a.nx, n0 + a.nx + plane, n0 + plane};
+    const double wy[4] = {de * gh, omde * gh, omde * omgh, de * omgh};
+    float4 lo[4], hi[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) ldg_pair(g8 + 2 * rows[q], lo[q], hi[q]);
+    double ex = 0, ey = 0, ez = 0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const double w0 = ab * wy[q], w1 = omab * wy[q];
+        ex += (double)lo[q].x * w0 + (double)hi[q].x * w1;
+        ey += (double)lo[q].y * w0 + (double)hi[q].y * w1;
+        ez += (double)lo[q].z * w0 + (double)hi[q].z * w1;
+    }
+    Eo[0] = ex;
+    Eo[1] = ey;
+    Eo[2] = ez;
+    return fl;
+}
+
 __global__ void __launch_bounds__(256) k_interp_pairs(InterpArgs a, const float4 *__restrict__ g8,
                                                       double *__restrict__ E, unsigned long long *__restrict__ nclamp) {
     const int64_t plane = (int64_t)a.nx * a.ny;
@@ -337,29 +368,7 @@ __global__ void __launch_bounds__(256) k_interp_pairs(InterpArgs a, const float4
             yn = __ldg(a.y + mn);
             zn = __ldg(a.z + mn);
         }
-        Cell c;
-        const bool fl = locate(a, xm, ym, zm, c);
-        count_one(nclamp, fl);
-        const int64_t n0 = c.i + (int64_t)a.nx * c.j + plane * c.k;
-        const double ab = c.ab, de = c.de, gh = c.gh;
-        const double omab = 1. - ab, omde = 1. - de, omgh = 1. - gh;
-        // (j,k), (j+1,k), (j+1,k+1), (j,k+1) rows; each pair = nodes i and i+1
-        const int64_t rows[4] = {n0, n0 + a.nx, n0 + a.nx + plane, n0 + plane};
-        const double wy[4] = {de * gh, omde * gh, omde * omgh, de * omgh};
-        float4 lo[4], hi[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) ldg_pair(g8 + 2 * rows[q], lo[q], hi[q]);
-        double ex = 0, ey = 0, ez = 0;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const double w0 = ab * wy[q], w1 = omab * wy[q];
-            ex += (double)lo[q].x * w0 + (double)hi[q].x * w1;
-            ey += (double)lo[q].y * w0 + (double)hi[q].y * w1;
-            ez += (double)lo[q].z * w0 + (double)hi[q].z * w1;
-        }
-        E[3 * m] = ex;
-        E[3 * m + 1] = ey;
-        E[3 * m + 2] = ez;
+        count_one(nclamp, interp_pair_one(a, g8, plane, xm, ym, zm, E + 3 * m));
     }
 }
 
@@ -438,7 +447,6 @@ int launch_bbox(int64_t np, const double *x, const double *y, const double *z, u
     return ok();
 }
 
-// Deterministic two-pass sum: 1024 fixed partial sums in index order, then one block.
 // Deterministic two-pass reductions of a particle array: op 0 sum, 1 maximum of |q|.
 __device__ __forceinline__ double red_op(double a, double b, int op) { return op ? fmax(a, b) : a + b; }
 __global__ void __launch_bounds__(256) k_sum_partial(int64_t n, const double *__restrict__ q, double *partials, int op) {
@@ -468,6 +476,121 @@ __global__ void k_sum_final(const double *partials, int np, double *out, int op)
 int launch_sum(int64_t n, const double *q, double *partials, double *out, cudaStream_t st, bool max_abs) {
     k_sum_partial<<<1024, 256, 0, st>>>(n, q, partials, max_abs ? 1 : 0);
     k_sum_final<<<1, 1024, 0, st>>>(partials, 1024, out, max_abs ? 1 : 0);
+    return ok();
+}
+
+// ------------------------------------------------------------------------------------
+// Batched particle passes: CTA j handles particles [jobs[j].beg, jobs[j].end) of bunch
+// jobs[j].bunch with that bunch's arguments; per-bunch counters cnt[4b + 0] outside,
+// +1 non-finite, +2 clamped.
+__global__ void __launch_bounds__(256) k_batch_deposit_quad(const BunchArgs *__restrict__ bunches,
+                                                            const BatchJob *__restrict__ jobs, float4 *quad,
+                                                            unsigned long long *cnt) {
+    const BatchJob jb = jobs[blockIdx.x];
+    const DepositArgs &a = bunches[jb.bunch].d;
+    float4 *qb = quad + bunches[jb.bunch].node_off;
+    const int64_t plane = (int64_t)a.nx * a.ny;
+    for (int64_t m = jb.beg + threadIdx.x; m < jb.end; m += blockDim.x) {
+        const double c = a.q ? a.q[m] : a.charge1;
+        const int st = quad_one(a, qb, plane, a.x[m], a.y[m], a.z[m], c);
+        count_one(&cnt[4 * jb.bunch + 0], st == 1);
+        count_one(&cnt[4 * jb.bunch + 1], st == 2);
+    }
+}
+int launch_batch_deposit_quad(const BunchArgs *bunches, const BatchJob *jobs, int njobs, float *quad,
+                              unsigned long long *cnt, cudaStream_t st) {
+    if (njobs <= 0) return OSC_OK;
+    k_batch_deposit_quad<<<njobs, 256, 0, st>>>(bunches, jobs, reinterpret_cast<float4 *>(quad), cnt);
+    return ok();
+}
+
+__global__ void __launch_bounds__(256) k_batch_interp_pairs(const BunchArgs *__restrict__ bunches,
+                                                            const BatchJob *__restrict__ jobs,
+                                                            const float4 *__restrict__ e8, unsigned long long *cnt) {
+    const BatchJob jb = jobs[blockIdx.x];
+    const InterpArgs &a = bunches[jb.bunch].in;
+    const float4 *g8 = e8 + 2 * bunches[jb.bunch].node_off;
+    double *E = bunches[jb.bunch].E;
+    const int64_t plane = (int64_t)a.nx * a.ny;
+    for (int64_t m = jb.beg + threadIdx.x; m < jb.end; m += blockDim.x)
+        count_one(&cnt[4 * jb.bunch + 2], interp_pair_one(a, g8, plane, a.x[m], a.y[m], a.z[m], E + 3 * m));
+}
+int launch_batch_interp_pairs(const BunchArgs *bunches, const BatchJob *jobs, int njobs, const float *e8,
+                              unsigned long long *cnt, cudaStream_t st) {
+    if (njobs <= 0) return OSC_OK;
+    k_batch_interp_pairs<<<njobs, 256, 0, st>>>(bunches, jobs, reinterpret_cast<const float4 *>(e8), cnt);
+    return ok();
+}
+
+// Per job: ordered min/max keys of x, y, z (6), non-finite count, and the sum of q in
+// index order within the CTA; then per bunch, its jobs combined in job order.
+__global__ void __launch_bounds__(256) k_batch_stats(const BunchArgs *__restrict__ bunches,
+                                                     const BatchJob *__restrict__ jobs, unsigned long long *keys,
+                                                     double *qsum) {
+    const BatchJob jb = jobs[blockIdx.x];
+    const DepositArgs &a = bunches[jb.bunch].d;
+    unsigned long long lo[3] = {~0ull, ~0ull, ~0ull}, hi[3] = {0, 0, 0}, bad = 0;
+    double qs = 0;
+    const double *p[3] = {a.x, a.y, a.z};
+    for (int64_t m = jb.beg + threadIdx.x; m < jb.end; m += blockDim.x) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const double v = p[d][m];
+            if (!isfinite(v)) { ++bad; continue; }
+            const unsigned long long k = ord_key(v);
+            lo[d] = k < lo[d] ? k : lo[d];
+            hi[d] = k > hi[d] ? k : hi[d];
+        }
+        if (a.q) qs += a.q[m];
+    }
+    __shared__ unsigned long long sk[7][256];
+    __shared__ double sq[256];
+    for (int d = 0; d < 3; ++d) {
+        sk[2 * d][threadIdx.x] = lo[d];
+        sk[2 * d + 1][threadIdx.x] = hi[d];
+    }
+    sk[6][threadIdx.x] = bad;
+    sq[threadIdx.x] = qs;
+    __syncthreads();
+    for (int w = 128; w; w >>= 1) {
+        if (threadIdx.x < w) {
+            const int t = threadIdx.x;
+            for (int d = 0; d < 3; ++d) {
+                sk[2 * d][t] = min(sk[2 * d][t], sk[2 * d][t + w]);
+                sk[2 * d + 1][t] = max(sk[2 * d + 1][t], sk[2 * d + 1][t + w]);
+            }
+            sk[6][t] += sk[6][t + w];
+            sq[t] += sq[t + w];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x < 7) keys[7 * (int64_t)blockIdx.x + threadIdx.x] = sk[threadIdx.x][0];
+    if (threadIdx.x == 0) qsum[blockIdx.x] = sq[0];
+}
+// out[8b .. 8b+5] = min/max of x, y, z as doubles, out[8b+6] = non-finite count,
+// out[8b+7] = sum of q
+__global__ void k_batch_stats_final(const int *__restrict__ job0, int nbunch, const unsigned long long *keys,
+                                    const double *qsum, double *out) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nbunch) return;
+    unsigned long long k[7] = {~0ull, 0, ~0ull, 0, ~0ull, 0, 0};
+    double qs = 0;
+    for (int j = job0[b]; j < job0[b + 1]; ++j) {
+        for (int d = 0; d < 3; ++d) {
+            k[2 * d] = min(k[2 * d], keys[7 * (int64_t)j + 2 * d]);
+            k[2 * d + 1] = max(k[2 * d + 1], keys[7 * (int64_t)j + 2 * d + 1]);
+        }
+        k[6] += keys[7 * (int64_t)j + 6];
+        qs += qsum[j];
+    }
+    for (int d = 0; d < 6; ++d) out[8 * b + d] = ord_val(k[d]);
+    out[8 * b + 6] = (double)k[6];
+    out[8 * b + 7] = qs;
+}
+int launch_batch_stats(const BunchArgs *bunches, const BatchJob *jobs, int njobs, const int *job0, int nbunch,
+                       unsigned long long *keys, double *qsum, double *out, cudaStream_t st) {
+    if (njobs > 0) k_batch_stats<<<njobs, 256, 0, st>>>(bunches, jobs, keys, qsum);
+    k_batch_stats_final<<<(nbunch + 127) / 128, 128, 0, st>>>(job0, nbunch, keys, qsum, out);
     return ok();
 }
 

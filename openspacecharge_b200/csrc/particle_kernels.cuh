@@ -72,4 +72,28 @@ int launch_bbox(int64_t np, const double *x, const double *y, const double *z,
 int launch_sum(int64_t n, const double *q, double *partials /*>= 1024*/, double *out, cudaStream_t st,
                bool max_abs = false);
 
+// ---- batches of bunches ---------------------------------------------------------------
+// One CTA's share of a batched particle pass: particles [beg, end) of bunch `bunch`.
+struct BatchJob {
+    int bunch;
+    int64_t beg, end;
+};
+// Per-bunch arguments of the batched passes: particle pointers already offset to the
+// bunch, its mesh, the first node of its grid in the batch arrays and its E output.
+struct BunchArgs {
+    DepositArgs d;
+    InterpArgs in;
+    int64_t node_off;
+    double *E;
+};
+// cnt[4b + 0] += outside, cnt[4b + 1] += non-finite (deposit); cnt[4b + 2] += clamped (interp)
+int launch_batch_deposit_quad(const BunchArgs *bunches, const BatchJob *jobs, int njobs, float *quad,
+                              unsigned long long *cnt, cudaStream_t st);
+int launch_batch_interp_pairs(const BunchArgs *bunches, const BatchJob *jobs, int njobs, const float *e8,
+                              unsigned long long *cnt, cudaStream_t st);
+// Per-bunch min/max of x, y, z, non-finite count and sum of q (out: [nbunch][8] doubles);
+// job0[b] .. job0[b+1] are the jobs of bunch b; keys [njobs][7], qsum [njobs] scratch.
+int launch_batch_stats(const BunchArgs *bunches, const BatchJob *jobs, int njobs, const int *job0, int nbunch,
+                       unsigned long long *keys, double *qsum, double *out, cudaStream_t st);
+
 }  // namespace osc

@@ -72,23 +72,50 @@ int fft3d_full(osc_ctx *c, cplx<T> *a, int Nx, int Ny, int Nz, int sx, int sy, i
 template int fft3d_full<float>(osc_ctx *, cplx<float> *, int, int, int, int, int, int);
 template int fft3d_full<double>(osc_ctx *, cplx<double> *, int, int, int, int, int, int);
 
+// Corner block of the IGF primitive of one component (osc_get_cgrn_freespace,
+// code/open_spacecharge_mod.f90:648-668): on symmetric axes (offset 0) only the corners
+// n-1 .. 2n-1 of the doubled grid, which the mirrored kernel needs, else all 2n.
+CornerArgs green_corner_args(const int n[3], const double delta[3], double gamma, const double off[3], int icomp) {
+    int sym[3], c0[3], cd[3], N[3];
+    for (int d = 0; d < 3; ++d) {
+        sym[d] = off[d] == 0.0 ? 1 : 0;
+        N[d] = 2 * n[d];
+        c0[d] = sym[d] ? n[d] - 1 : 0;
+        cd[d] = sym[d] ? n[d] + 1 : 2 * n[d];
+    }
+    CornerArgs ca;
+    ca.cdx = cd[0]; ca.cdy = cd[1]; ca.cdz = cd[2];
+    ca.c0x = c0[0]; ca.c0y = c0[1]; ca.c0z = c0[2];
+    ca.dx = delta[0];
+    ca.dy = delta[1];
+    ca.dz = delta[2] * gamma;
+    ca.factor = (icomp == 1 || icomp == 2) ? gamma / (ca.dx * ca.dy * ca.dz) : 1.0 / (ca.dx * ca.dy * ca.dz);
+    ca.umin = (double)(0.5f - (float)(N[0] / 2)) * ca.dx + off[0];
+    ca.vmin = (double)(0.5f - (float)(N[1] / 2)) * ca.dy + off[1];
+    ca.wmin = (double)(0.5f - (float)(N[2] / 2)) * ca.dz + off[2] * gamma;
+    ca.icomp = icomp;
+    return ca;
+}
+
 // ------------------------------------------------------------------------------------
-// Stored spectrum of an all-symmetric kernel (offset 0 on every axis) from its corner block
-// F: octant differences, then even/odd transforms along x, y and z; the last pass applies
-// fpei/M and writes the stored layout directly.  Equals the extraction of the FP64 doubled-
-// grid FFT (osc_get_cgrn_freespace + ccfft3d, code/open_spacecharge_mod.f90:633-705,
+// Stored spectra of all-symmetric kernels (offset 0 on every axis) of nb geometries with
+// equal grids, from their corner blocks F ((n+1)^3 apart): octant differences, then even/
+// odd transforms along x, y and z; the last pass applies fpei/M and writes the stored
+// layout (zinner: [ky][kx][kz] with columns zpitch apart, else [kz][ky][kx]) of member b at
+// out + b * out_bstride.  Equals the extraction of the FP64 doubled-grid FFT
+// (osc_get_cgrn_freespace + ccfft3d, code/open_spacecharge_mod.f90:633-705,
 // code/fft_interface_mod.f90:96-143) up to FP64 rounding.
 template <typename T>
-static int green_sym_spectrum(osc_ctx *c, const double *F, int nx, int ny, int nz, const int par[3], int icomp,
-                              DevBuf &store, GSpecDev &spec) {
-    const int nxh = nx + 1, nyh = ny + 1, nzh = nz + 1;
+int green_sym_lines3(osc_ctx *c, const double *F, int nb, int nx, int ny, int nz, const int odd[3][2], int zinner,
+                     int zpitch, T *out, int64_t out_bstride) {
+    const int nxh = nx + 1, nyh = ny + 1;
     double *h, *hx, *hy;
-    TRY(ws_get(c, "green_h", sizeof(double) * (size_t)nx * ny * nz, (void **)&h));
-    TRY(ws_get(c, "green_hx", sizeof(double) * (size_t)nxh * ny * nz, (void **)&hx));
-    TRY(ws_get(c, "green_hy", sizeof(double) * (size_t)nxh * nyh * nz, (void **)&hy));
+    TRY(ws_get(c, "green_h", sizeof(double) * (size_t)nb * nx * ny * nz, (void **)&h));
+    TRY(ws_get(c, "green_hx", sizeof(double) * (size_t)nb * nxh * ny * nz, (void **)&hx));
+    TRY(ws_get(c, "green_hy", sizeof(double) * (size_t)nb * nxh * nyh * nz, (void **)&hy));
     {
         Launch L_(c, "green_octant");
-        TRY(kerr(c, launch_green_octant(F, h, nx, ny, nz, c->stream), "green octant"));
+        TRY(kerr(c, launch_green_octant(F, h, nx, ny, nz, nb, c->stream), "green octant"));
     }
     FFTPlan px, py, pz;
     if (!make_fft_plan(2 * nx, px) || !make_fft_plan(2 * ny, py) || !make_fft_plan(2 * nz, pz))
@@ -97,6 +124,45 @@ static int green_sym_spectrum(osc_ctx *c, const double *F, int nx, int ny, int n
     TRY(twiddles<double>(c, 2 * nx, &twx));
     TRY(twiddles<double>(c, 2 * ny, &twy));
     TRY(twiddles<double>(c, 2 * nz, &twz));
+    Launch L_(c, "green_sym_lines", 3);
+    SymArgs a;
+    // x: rows h[c][b][0..nx) -> hx[c][b][0..nx]
+    a.p = px; a.n = nx; a.odd_lo = odd[0][0]; a.odd_hi = odd[0][1]; a.nq = ny;
+    a.npq = (int64_t)ny * nz; a.nlines = nb * a.npq;
+    a.in_ps = (int64_t)ny * nx; a.in_qs = nx; a.in_es = 1; a.in_bs = (int64_t)nx * ny * nz;
+    a.out_ps = (int64_t)ny * nxh; a.out_qs = nxh; a.out_es = 1; a.out_bs = (int64_t)nxh * ny * nz;
+    a.scale = 1.0;
+    TRY(kerr(c, launch_sym_lines<double>(h, hx, a, twx, true, true, c->stream), "green x"));
+    // y: lines (c, kx) of hx -> hy[c][ky][kx]
+    a.p = py; a.n = ny; a.odd_lo = odd[1][0]; a.odd_hi = odd[1][1]; a.nq = nxh;
+    a.npq = (int64_t)nz * nxh; a.nlines = nb * a.npq;
+    a.in_ps = (int64_t)ny * nxh; a.in_qs = 1; a.in_es = nxh; a.in_bs = (int64_t)nxh * ny * nz;
+    a.out_ps = (int64_t)nyh * nxh; a.out_qs = 1; a.out_es = nxh; a.out_bs = (int64_t)nxh * nyh * nz;
+    TRY(kerr(c, launch_sym_lines<double>(hx, hy, a, twy, false, false, c->stream), "green y"));
+    // z: lines (ky, kx) of hy -> stored spectrum, scaled by fpei/M
+    a.p = pz; a.n = nz; a.odd_lo = odd[2][0]; a.odd_hi = odd[2][1]; a.nq = nxh;
+    a.npq = (int64_t)nyh * nxh; a.nlines = nb * a.npq;
+    a.in_ps = nxh; a.in_qs = 1; a.in_es = (int64_t)nyh * nxh; a.in_bs = (int64_t)nxh * nyh * nz;
+    if (zinner) {
+        a.out_ps = (int64_t)nxh * zpitch; a.out_qs = zpitch; a.out_es = 1;
+    } else {
+        a.out_ps = nxh; a.out_qs = 1; a.out_es = (int64_t)nyh * nxh;
+    }
+    a.out_bs = out_bstride;
+    a.scale = fpei_solver2() / (8.0 * nx * ny * nz);
+    TRY(kerr(c, launch_sym_lines<T>(hy, out, a, twz, false, zinner != 0, c->stream), "green z"));
+    return OSC_OK;
+}
+template int green_sym_lines3<float>(osc_ctx *, const double *, int, int, int, int, const int (*)[2], int, int,
+                                     float *, int64_t);
+template int green_sym_lines3<double>(osc_ctx *, const double *, int, int, int, int, const int (*)[2], int, int,
+                                      double *, int64_t);
+
+// Single geometry: allocates the stored spectrum and fills its descriptor.
+template <typename T>
+static int green_sym_spectrum(osc_ctx *c, const double *F, int nx, int ny, int nz, const int par[3], int icomp,
+                              DevBuf &store, GSpecDev &spec) {
+    const int nxh = nx + 1, nyh = ny + 1, nzh = nz + 1;
     spec.real_valued = 1;
     spec.imag_unit = icomp != 0 ? 1 : 0;
     spec.sym_y = spec.sym_z = 1;
@@ -115,31 +181,12 @@ static int green_sym_spectrum(osc_ctx *c, const double *F, int nx, int ny, int n
     store.bytes = bytes;
     spec.data = store.p;
     if (spec.zinner) TRY(cuda_check(c, cudaMemsetAsync(store.p, 0, bytes, c->stream), "memset spectrum"));
-    Launch L_(c, "green_sym_lines", 3);
-    SymArgs a;
-    // x: rows h[c][b][0..nx) -> hx[c][b][0..nx]
-    a.p = px; a.n = nx; a.par = par[0]; a.nlines = (int64_t)ny * nz; a.nq = ny;
-    a.in_ps = (int64_t)ny * nx; a.in_qs = nx; a.in_es = 1;
-    a.out_ps = (int64_t)ny * nxh; a.out_qs = nxh; a.out_es = 1;
-    a.scale = 1.0;
-    TRY(kerr(c, launch_sym_lines<double>(h, hx, a, twx, true, true, c->stream), "green x"));
-    // y: lines (c, kx) of hx -> hy[c][ky][kx]
-    a.p = py; a.n = ny; a.par = par[1]; a.nlines = (int64_t)nz * nxh; a.nq = nxh;
-    a.in_ps = (int64_t)ny * nxh; a.in_qs = 1; a.in_es = nxh;
-    a.out_ps = (int64_t)nyh * nxh; a.out_qs = 1; a.out_es = nxh;
-    TRY(kerr(c, launch_sym_lines<double>(hx, hy, a, twy, false, false, c->stream), "green y"));
-    // z: lines (ky, kx) of hy -> stored spectrum, scaled by fpei/M
-    a.p = pz; a.n = nz; a.par = par[2]; a.nlines = (int64_t)nyh * nxh; a.nq = nxh;
-    a.in_ps = nxh; a.in_qs = 1; a.in_es = (int64_t)nyh * nxh;
-    if (spec.zinner) {
-        a.out_ps = (int64_t)nxh * spec.zpitch; a.out_qs = spec.zpitch; a.out_es = 1;
-    } else {
-        a.out_ps = nxh; a.out_qs = 1; a.out_es = (int64_t)nyh * nxh;
+    int odd[3][2];
+    for (int d = 0; d < 3; ++d) {
+        odd[d][0] = 0;
+        odd[d][1] = par[d] < 0 ? 1 : 0;
     }
-    a.scale = fpei_solver2() / (8.0 * nx * ny * nz);
-    TRY(kerr(c, launch_sym_lines<T>(hy, reinterpret_cast<T *>(store.p), a, twz, false, spec.zinner != 0, c->stream),
-             "green z"));
-    return OSC_OK;
+    return green_sym_lines3<T>(c, F, 1, nx, ny, nz, odd, spec.zinner, spec.zpitch, reinterpret_cast<T *>(store.p), 0);
 }
 
 // ------------------------------------------------------------------------------------
@@ -160,19 +207,7 @@ static int build_green_component(osc_ctx *c, int nx, int ny, int nz, const doubl
     double *F;
     double2 *cg;
     TRY(ws_get(c, "green_F", sizeof(double) * (size_t)cd[0] * cd[1] * cd[2], (void **)&F));
-    TRY(ws_get(c, "green_cg", sizeof(double2) * (size_t)M, (void **)&cg));
-    // osc_get_cgrn_freespace (code/open_spacecharge_mod.f90:648-668)
-    CornerArgs ca;
-    ca.cdx = cd[0]; ca.cdy = cd[1]; ca.cdz = cd[2];
-    ca.c0x = c0[0]; ca.c0y = c0[1]; ca.c0z = c0[2];
-    ca.dx = delta[0];
-    ca.dy = delta[1];
-    ca.dz = delta[2] * gamma;
-    ca.factor = (icomp == 1 || icomp == 2) ? gamma / (ca.dx * ca.dy * ca.dz) : 1.0 / (ca.dx * ca.dy * ca.dz);
-    ca.umin = (double)(0.5f - (float)(N[0] / 2)) * ca.dx + off[0];
-    ca.vmin = (double)(0.5f - (float)(N[1] / 2)) * ca.dy + off[1];
-    ca.wmin = (double)(0.5f - (float)(N[2] / 2)) * ca.dz + off[2] * gamma;
-    ca.icomp = icomp;
+    const CornerArgs ca = green_corner_args(n, delta, gamma, off, icomp);
     {
         Launch L_(c, "green_corners");
         TRY(kerr(c, launch_igf_corners(F, ca, c->stream), "green corners"));
@@ -185,6 +220,7 @@ static int build_green_component(osc_ctx *c, int nx, int ny, int nz, const doubl
         TRY(green_sym_spectrum<T>(c, F, nx, ny, nz, par, icomp, store, spec));
         return OSC_OK;
     }
+    TRY(ws_get(c, "green_cg", sizeof(double2) * (size_t)M, (void **)&cg));
     CenterArgs ce;
     ce.nx = nx; ce.ny = ny; ce.nz = nz;
     ce.symx = sym[0]; ce.symy = sym[1]; ce.symz = sym[2];
@@ -280,8 +316,18 @@ int freespace_opt(osc_ctx *c, const FreeSpaceJob &j, const TIn *rho) {
     if (j.want_e || j.calc_b)
         for (int q = 1; q <= 3; ++q) comps[ncomp++] = q;
     if (ncomp == 0) return OSC_OK;
-    GreenSet *gs;
-    TRY(green_set<T>(c, j, comps, ncomp, &gs));
+    const int B = j.nbatch > 0 ? j.nbatch : 1;
+    if (B > 1 && (j.phi || j.E || j.B || !j.E4 || !j.gbatch || j.at_cathode))
+        return set_err(c, OSC_E_INVALID, "batched solves produce the E grid only");
+    GreenSet local;
+    GreenSet *gs = &local;
+    if (j.gbatch) {
+        if (j.ngbatch != ncomp) return set_err(c, OSC_E_INVALID, "batched spectra: %d components given", j.ngbatch);
+        for (int i = 0; i < ncomp; ++i) local.spec[i] = j.gbatch[i];
+        local.nspec = ncomp;
+    } else {
+        TRY(green_set<T>(c, j, comps, ncomp, &gs));
+    }
     auto spec_index = [&](int icomp, bool img) {
         for (int i = 0; i < ncomp; ++i)
             if (comps[i] == icomp) return img ? ncomp + i : i;
@@ -335,20 +381,20 @@ int freespace_opt(osc_ctx *c, const FreeSpaceJob &j, const TIn *rho) {
     if (j.calc_b && j.B) TRY(cuda_check(c, cudaMemsetAsync(j.B + 2 * N, 0, sizeof(double) * N, c->stream), "memset B"));
 
     V *X1, *X2, *X3, *X4;
-    TRY(ws_get(c, "fs_x1", sizeof(V) * (size_t)nxh * ny * nz, (void **)&X1));
-    TRY(ws_get(c, "fs_x2", sizeof(V) * (size_t)nxh * Ny * nz, (void **)&X2));
-    TRY(ws_get(c, "fs_x3", sizeof(V) * (size_t)nout * nxh * Ny * nz, (void **)&X3));
-    TRY(ws_get(c, "fs_x4", sizeof(V) * (size_t)nout * nxh * ny * nz, (void **)&X4));
+    TRY(ws_get(c, "fs_x1", sizeof(V) * (size_t)B * nxh * ny * nz, (void **)&X1));
+    TRY(ws_get(c, "fs_x2", sizeof(V) * (size_t)B * nxh * Ny * nz, (void **)&X2));
+    TRY(ws_get(c, "fs_x3", sizeof(V) * (size_t)nout * B * nxh * Ny * nz, (void **)&X3));
+    TRY(ws_get(c, "fs_x4", sizeof(V) * (size_t)nout * B * nxh * ny * nz, (void **)&X4));
     TwPair<V> twx, twy, twz;
     TRY(twiddles<T>(c, Nx, &twx));
     TRY(twiddles<T>(c, Ny, &twy));
     TRY(twiddles<T>(c, Nz, &twz));
 
-    // x: real rows -> half spectra, [z][y][kx]
+    // x: real rows -> half spectra, [z][y][kx] (batch members stacked along z)
     R2CArgs ra;
     ra.p = px;
     ra.nin = nx;
-    ra.nrows = (int64_t)ny * nz;
+    ra.nrows = (int64_t)B * ny * nz;
     ra.in_rstride = nx;
     ra.out_rstride = nxh;
     {
@@ -375,7 +421,7 @@ int freespace_opt(osc_ctx *c, const FreeSpaceJob &j, const TIn *rho) {
     ly.flip_mask = 0;
     {
         Launch L_(c, "fft_y_fwd");
-        TRY(kerr(c, launch_lines<T>(X1, X2, ly, nz, 1, false, twy, c->stream), "y forward"));
+        TRY(kerr(c, launch_lines<T>(X1, X2, ly, B * nz, 1, false, twy, c->stream), "y forward"));
     }
     // z: forward, spectral product, inverse
     za.p = pz;
@@ -386,11 +432,14 @@ int freespace_opt(osc_ctx *c, const FreeSpaceJob &j, const TIn *rho) {
     za.ny = ny;
     za.in_estride = (int64_t)nxh * Ny;
     za.out_estride = (int64_t)nxh * Ny;
-    za.out_cstride = (int64_t)nxh * Ny * nz;
+    za.out_cstride = (int64_t)B * nxh * Ny * nz;
     za.nout = nout;
     za.img_phase_mul = nz - 1;
     za.ng = gs->nspec;
     za.fault = c->d_fault;
+    za.nbatch = B;
+    za.in_bstride = za.out_bstride = (int64_t)nxh * Ny * nz;
+    za.g_bstride = j.gbatch ? j.g_bstride : 0;
     for (int i = 0; i < gs->nspec; ++i) za.g[i] = gs->spec[i];
     {
         Launch L_(c, "fft_z_conv");
@@ -402,19 +451,19 @@ int freespace_opt(osc_ctx *c, const FreeSpaceJob &j, const TIn *rho) {
     li.in_len = Ny;
     li.out_len = ny;
     li.in_pstride = (int64_t)nxh * Ny;
-    li.in_zstride = (int64_t)nxh * Ny * nz;
+    li.in_zstride = (int64_t)B * nxh * Ny * nz;
     li.out_pstride = (int64_t)nxh * ny;
-    li.out_zstride = (int64_t)nxh * ny * nz;
+    li.out_zstride = (int64_t)B * nxh * ny * nz;
     {
         Launch L_(c, "fft_y_inv");
-        TRY(kerr(c, launch_lines<T>(X3, X4, li, nz, nout, false, twy, c->stream), "y inverse"));
+        TRY(kerr(c, launch_lines<T>(X3, X4, li, B * nz, nout, false, twy, c->stream), "y inverse"));
     }
     // x: half spectra -> real rows [0,nx), scattered to the outputs
     cr.p = px;
     cr.nout = nx;
-    cr.nrows = (int64_t)ny * nz;
+    cr.nrows = (int64_t)B * ny * nz;
     cr.in_rstride = nxh;
-    cr.in_cstride = (int64_t)nxh * ny * nz;
+    cr.in_cstride = (int64_t)B * nxh * ny * nz;
     cr.ncomp = nout;
     {
         Launch L_(c, "fft_x_c2r");

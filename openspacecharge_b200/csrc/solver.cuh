@@ -39,7 +39,22 @@ struct FreeSpaceJob {
     double *B = nullptr;    // device f64 [3][N]
     void *E4 = nullptr;     // device vec4<T> [N], or the x-pair grid vec4<T> [N][2]
     int e4_pairs = 0;       // 1: E4 is the x-pair grid read by launch_interp_pairs
+    // batch of nbatch equal grids stacked in rho and E4 (E4 output only); the spectra come
+    // from gbatch (member b at data + b*g_bstride elements) instead of the Green cache
+    int nbatch = 1;
+    const GSpecDev *gbatch = nullptr;
+    int ngbatch = 0;
+    int64_t g_bstride = 0;
 };
+
+// Corner block arguments of the IGF primitive of component icomp (0 phi, 1..3 E).
+CornerArgs green_corner_args(const int n[3], const double delta[3], double gamma, const double off[3], int icomp);
+// Stored spectra of all-symmetric kernels of nb members with equal grids from their corner
+// blocks F ((n+1)^3 each, corner index n-1 first): member b written at out + b*out_bstride.
+// Along axis d the members in [odd[d][0], odd[d][1]) are odd, the others even.
+template <typename T>
+int green_sym_lines3(osc_ctx *c, const double *F, int nb, int nx, int ny, int nz, const int odd[3][2], int zinner,
+                     int zpitch, T *out, int64_t out_bstride);
 
 // Optimised IGF convolution (cached half-spectra, pruned transforms) in precision T.
 template <typename T, typename TIn>

@@ -136,6 +136,9 @@ __global__ void __launch_bounds__(W * 32, ZW_MINB) k_zconv_warp(const cplx<T> *_
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int col0 = blockIdx.x * W;
     const int zp = a.g[0].zpitch;
+    in += blockIdx.y * a.in_bstride;
+    out += blockIdx.y * a.out_bstride;
+    const int64_t goff = blockIdx.y * a.g_bstride;
     V *wb = wbufs + warp * WB;
     if (GS) {
         if (threadIdx.x == 0) {
@@ -147,7 +150,7 @@ __global__ void __launch_bounds__(W * 32, ZW_MINB) k_zconv_warp(const cplx<T> *_
                 for (int o = 0; o < a.nout; ++o) {
                     const GSpecDev &g = a.g[a.gdir[o]];
                     const int yy = (g.sym_y && ky > a.ny) ? a.Ny - ky : ky;
-                    const T *src = reinterpret_cast<const T *>(g.data) + ((int64_t)yy * a.nxh + kx) * zp;
+                    const T *src = reinterpret_cast<const T *>(g.data) + goff + ((int64_t)yy * a.nxh + kx) * zp;
                     bulk_g2s(gst + (c * a.nout + o) * zp, src, (unsigned)(zp * sizeof(T)), &gbar);
                 }
             }
@@ -240,7 +243,7 @@ __global__ void __launch_bounds__(W * 32, ZW_MINB) k_zconv_warp(const cplx<T> *_
                         const int e = j + NB * r;
                         V S = mk<T>(0, 0);
                         if (gd >= 0)
-                            S = cmul(rh[q][r], g_lookup<T>(a.g[gd], kx, ky, e, a.nxh, a.Ny, a.ny, L, a.nz));
+                            S = cmul(rh[q][r], g_lookup<T>(a.g[gd], kx, ky, e, a.nxh, a.Ny, a.ny, L, a.nz, goff));
                         if (IMG && gi >= 0) {
                             // spectrum of -rho flipped in z: -w^((nz-1) kz) * rho_hat(-kz)
                             const V rm = rb[wpad(e == 0 ? 0 : L - e)];
@@ -248,7 +251,7 @@ __global__ void __launch_bounds__(W * 32, ZW_MINB) k_zconv_warp(const cplx<T> *_
                             V ri = cmul(ph, rm);
                             ri.x = -ri.x * icoef;
                             ri.y = -ri.y * icoef;
-                            S = cadd(S, cmul(ri, g_lookup<T>(a.g[gi], kx, ky, e, a.nxh, a.Ny, a.ny, L, a.nz)));
+                            S = cadd(S, cmul(ri, g_lookup<T>(a.g[gi], kx, ky, e, a.nxh, a.Ny, a.ny, L, a.nz, goff)));
                         }
                         v[q][r] = S;
                     }

@@ -308,3 +308,55 @@ def space_charge_step_dev(ctx, mesh3d: Mesh3D, x, y, z, E, qa=None, total_charge
     ctx.call("osc_space_charge_step_dev", ctypes.byref(m), ctypes.c_int64(x.numel()), _tp(x), _tp(y), _tp(z),
              _tp(qa), tc, int(bool(resize_mesh)), int(bool(at_cathode)), int(precision), _tp(E), _tp(B))
     mesh3d.from_c(m)
+
+
+def _bunches(meshes, counts, total_charges):
+    counts = [int(c) for c in counts]
+    if len(meshes) != len(counts):
+        raise ValueError("one mesh per bunch")
+    arr = (native.OscBunch * len(meshes))()
+    off = 0
+    for b, (m, n) in enumerate(zip(meshes, counts)):
+        arr[b].mesh = m.to_c()
+        arr[b].offset = off
+        arr[b].np = n
+        arr[b].total_charge = 0.0 if total_charges is None else float(total_charges[b])
+        off += n
+    return arr, off
+
+
+def batch_space_charge_step(ctx, meshes, x, y, z, counts, qa=None, total_charges=None, resize_mesh=True,
+                            precision=PREC_FP32):
+    """The fused step for many independent bunches in one call (osc_batch_space_charge_step).
+
+    x, y, z (and qa) hold the particles of all bunches back to back, bunch b owning the next
+    counts[b] entries; each mesh in `meshes` is refit (resize_mesh) and updated in place.
+    Returns (E (total, 3), n_outside per bunch)."""
+    ctx = _ctx(ctx)
+    if qa is None and total_charges is None:
+        raise ValueError("need qa or total_charges")
+    arr, total = _bunches(meshes, counts, total_charges)
+    x, y, z = _f64(x), _f64(y), _f64(z)
+    q = None if qa is None else _f64(qa)
+    if len(x) < total:
+        raise ValueError("particle arrays shorter than the sum of counts")
+    E = np.zeros((total, 3))
+    ctx.call("osc_batch_space_charge_step", len(meshes), arr, _p(x), _p(y), _p(z), _p(q),
+             int(bool(resize_mesh)), int(precision), _p(E))
+    for b, m in enumerate(meshes):
+        m.from_c(arr[b].mesh)
+    return E, [int(arr[b].n_outside) for b in range(len(meshes))]
+
+
+def batch_space_charge_step_dev(ctx, meshes, x, y, z, counts, E, qa=None, total_charges=None, resize_mesh=True,
+                                precision=PREC_FP32):
+    """Device-resident batched step on torch CUDA float64 tensors; E (total, 3) in place."""
+    ctx = _ctx(ctx)
+    if qa is None and total_charges is None:
+        raise ValueError("need qa or total_charges")
+    arr, total = _bunches(meshes, counts, total_charges)
+    ctx.call("osc_batch_space_charge_step_dev", len(meshes), arr, _tp(x), _tp(y), _tp(z), _tp(qa),
+             int(bool(resize_mesh)), int(precision), _tp(E))
+    for b, m in enumerate(meshes):
+        m.from_c(arr[b].mesh)
+    return [int(arr[b].n_outside) for b in range(len(meshes))]

@@ -68,6 +68,18 @@ class OscMesh3D(ctypes.Structure):
     ]
 
 
+class OscBunch(ctypes.Structure):
+    """``osc_bunch``: one bunch of a batched step (its mesh, particle range and charge)."""
+
+    _fields_ = [
+        ("mesh", OscMesh3D),
+        ("offset", ctypes.c_int64),
+        ("np", ctypes.c_int64),
+        ("total_charge", ctypes.c_double),
+        ("n_outside", ctypes.c_int64),
+    ]
+
+
 _P = ctypes.c_void_p
 _I = ctypes.c_int
 _I64 = ctypes.c_int64
@@ -110,6 +122,8 @@ SIGNATURES = {
     "osc_interpolate_field_dev": [_P, _PM, _P, _P, _I64, _P, _P, _P, _P, _P, _PI64],
     "osc_space_charge_step": [_P, _PM, _I64, _P, _P, _P, _P, _P, _I, _I, _I, _P, _P],
     "osc_space_charge_step_dev": [_P, _PM, _I64, _P, _P, _P, _P, _P, _I, _I, _I, _P, _P],
+    "osc_batch_space_charge_step": [_P, _I, ctypes.POINTER(OscBunch), _P, _P, _P, _P, _I, _I, _P],
+    "osc_batch_space_charge_step_dev": [_P, _I, ctypes.POINTER(OscBunch), _P, _P, _P, _P, _I, _I, _P],
 }
 _RESTYPES = {"osc_last_error": ctypes.c_char_p, "osc_version": ctypes.c_char_p}
 
