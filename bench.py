@@ -62,8 +62,9 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
-    ap.add_argument("--workload", default="single", choices=["single", "batch"],
-                    help="single: the headline one-bunch step; batch: 256 bunches of mixed grids per step")
+    ap.add_argument("--workload", default="single", choices=["single", "batch", "adjoint"],
+                    help="single: the headline one-bunch step; batch: 256 bunches of mixed grids per step; "
+                         "adjoint: forward + backward of sum q|E|^2 at 128^3, 4e6 particles")
     ap.add_argument("--bunches", type=int, default=BATCH_BUNCHES)
     return ap.parse_args()
 
@@ -467,6 +468,74 @@ def run_batch(args, ws, rank, local, dist):
     ctx.close()
 
 
+ADJ_GRID = (128, 128, 128)
+ADJ_NP = 4_000_000
+ADJ_METRIC = "gradient evaluations/s of sum q|E|^2 at 128^3, 4e6 ptcl (forward + adjoint)"
+
+
+def run_adjoint(args, ws, rank, local, dist):
+    """Forward step + vector-Jacobian product (the backward pass of a differentiable step)."""
+    import ctypes
+    import torch
+    import openspacecharge_b200 as osc
+    from openspacecharge_b200.bunch import gendist
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    x, y, z = gendist(ADJ_NP, sigma=(1e-3, 1e-3, 1e-3), cutoff=CUTOFF, disttype=1, seed=SEED)
+    q = np.full(ADJ_NP, QTOT / ADJ_NP)
+    ctx = osc.Context(local)
+    stream = torch.cuda.Stream(device=dev)
+    ctx.set_stream(stream.cuda_stream)
+    delta, umin = osc.get_mesh_quantities(ctx, x, y, z, (1, 1, 1), ADJ_GRID, 0)
+    mesh = osc.Mesh3D(nlo=(1, 1, 1), nhi=ADJ_GRID, min=umin, max=umin + (np.array(ADJ_GRID) - 1) * delta,
+                      delta=delta, gamma=GAMMA)
+    m = mesh.to_c()
+    tx, ty, tz, tq = (torch.from_numpy(a).to(dev) for a in (x, y, z, q))
+    E = torch.empty((ADJ_NP, 3), dtype=torch.float64, device=dev)
+    gE = torch.empty_like(E)
+    g = [torch.empty_like(tx) for _ in range(4)]
+    P = lambda t: ctypes.c_void_p(t.data_ptr())
+
+    def fwd_bwd(prec):
+        ctx.call("osc_space_charge_step_dev", ctypes.byref(m), ctypes.c_int64(ADJ_NP), P(tx), P(ty), P(tz), P(tq),
+                 None, 0, 0, prec, P(E), None)
+        with torch.cuda.stream(stream):
+            torch.mul(E, tq[:, None], out=gE)
+            gE.mul_(2.0)
+        ctx.call("osc_space_charge_step_vjp_dev", ctypes.byref(m), ctypes.c_int64(ADJ_NP), P(tx), P(ty), P(tz),
+                 P(tq), ctypes.c_double(0.0), prec, P(gE), *[P(t) for t in g])
+
+    for _ in range(max(3, args.warmup)):
+        fwd_bwd(osc.PREC_FP32)
+    ctx.synchronize()
+    torch.cuda.synchronize()
+    k = max(1, args.steps)
+    with ClockSampler(local) as clk:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k):
+            fwd_bwd(osc.PREC_FP32)
+        e1.record(stream)
+        e1.synchronize()
+    ms = e0.elapsed_time(e1) / k
+    g32 = [t.clone() for t in g]
+    fwd_bwd(osc.PREC_FP64)
+    ctx.synchronize()
+    err = max(float((a - b).abs().max() / b.abs().max()) for a, b in zip(g32, g))
+    if rank == 0:
+        print(json.dumps({
+            "metric": ADJ_METRIC, "value": ws * 1000.0 / ms, "unit": "gradients/s", "n_gpus": ws, "steps": k,
+            "warmup": max(3, args.warmup), "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "loss sum q|E|^2: FP32 step + FP32 adjoint (deposit, field, gather; deposited "
+                                   "gradients, three adjoint solves, gradient gather) on a fixed 128^3 mesh, 4e6 "
+                                   "particles, sigma = 1 mm", "grid": list(ADJ_GRID), "particles": ADJ_NP},
+            "rel_err_vs_fp64_gradients": err, "clocks": clk.summary()}))
+    ctx.close()
+
+
 def cpu_baseline(x, y, z, grid, umin, umax, delta):
     """One full step of the FP64 CPU port (oracle/) on the host cores."""
     from oracle import oracle as O
@@ -533,6 +602,8 @@ def main():
             run_reference(args, ws, rank)
         elif args.workload == "batch":
             run_batch(args, ws, rank, local, dist)
+        elif args.workload == "adjoint":
+            run_adjoint(args, ws, rank, local, dist)
         else:
             run_ours(args, ws, rank, local, dist)
     finally:

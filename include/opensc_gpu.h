@@ -86,7 +86,10 @@ typedef struct osc_mesh3d {
 OSC_API int osc_ctx_create(int device, osc_ctx **out);
 OSC_API int osc_ctx_destroy(osc_ctx *ctx);
 OSC_API const char *osc_last_error(const osc_ctx *ctx);
-OSC_API int osc_ctx_set_stream(osc_ctx *ctx, void *cuda_stream); /* NULL: the context's own stream */
+/* cuda_stream is a cudaStream_t; NULL is CUDA's default stream, as everywhere in CUDA, and
+   OSC_OWN_STREAM selects the context's own (non-blocking) stream, the initial one. */
+#define OSC_OWN_STREAM ((void *)-1)
+OSC_API int osc_ctx_set_stream(osc_ctx *ctx, void *cuda_stream);
 OSC_API int osc_ctx_set_option(osc_ctx *ctx, int option, int64_t value);
 OSC_API int osc_ctx_get_option(osc_ctx *ctx, int option, int64_t *value);
 OSC_API int osc_ctx_synchronize(osc_ctx *ctx);
@@ -218,6 +221,18 @@ OSC_API int osc_space_charge_step_dev(osc_ctx *ctx, osc_mesh3d *mesh, int64_t np
                               const double *d_y, const double *d_z, const double *d_q,
                               const double *total_charge, int resize_mesh, int at_cathode,
                               int precision, double *d_E, double *d_B);
+
+/* ---- adjoint of the step ---------------------------------------------------------------
+ * Vector-Jacobian product of the fused step with the mesh held fixed: given gE = dL/dE at
+ * every particle ([np][3]), returns dL/dx, dL/dy, dL/dz and (gq non-NULL) dL/dq per
+ * particle.  Charges are q, or total_charge/np each when q is NULL.  Device pointers.
+ * OSC_PREC_FP32 runs the field solves in FP32, the other precisions in FP64; the
+ * deposits and gathers are FP64.  The reference has no adjoint: this is the backward pass
+ * behind a differentiable (torch.autograd) step. */
+OSC_API int osc_space_charge_step_vjp_dev(osc_ctx *ctx, const osc_mesh3d *mesh, int64_t np, const double *d_x,
+                                          const double *d_y, const double *d_z, const double *d_q,
+                                          double total_charge, int precision, const double *d_gE, double *d_gx,
+                                          double *d_gy, double *d_gz, double *d_gq);
 
 /* ---- batched steps ---------------------------------------------------------------------
  * Many independent bunches, each with its own mesh, in one call: the fused step above for

@@ -71,7 +71,7 @@ const char *osc_last_error(const osc_ctx *ctx) { return ctx ? ctx->err.c_str() :
 
 int osc_ctx_set_stream(osc_ctx *ctx, void *s) {
     if (!ctx) return OSC_E_INVALID;
-    ctx->stream = s ? (cudaStream_t)s : ctx->own_stream;
+    ctx->stream = s == OSC_OWN_STREAM ? ctx->own_stream : (cudaStream_t)s;
     return OSC_OK;
 }
 

@@ -1,0 +1,66 @@
+// adjoint.cu -- vector-Jacobian product of the fused step (osc_space_charge_step_vjp_dev).
+//
+// The step maps particle positions x_m and charges q_m to E(x_m): a CIC deposit rho =
+// sum_m q_m W(x_m), the free-space solve E_c = K_c rho (space_charge_3d,
+// code/open_spacecharge_mod.f90:431-489) and the CIC gather E_c(x_m) (interpolate_field,
+// :311-390).  Given gE[m] = dL/dE(x_m), the chain rule gives
+//   dL/dx_m = sum_c gE_c[m] grad E_c(x_m) + q_m grad lambda(x_m),   dL/dq_m = lambda(x_m),
+// with the adjoint potential lambda = sum_c K_c^T a_c and a_c = sum_m gE_c[m] W(x_m).
+// Each K_c is a convolution with a kernel that is odd along axis c on the same centred
+// window, so K_c^T = -K_c: lambda is three forward solves of the deposited gradients,
+// one component each, accumulated with coefficient -1.  The mesh is held fixed.
+#include "abi_util.cuh"
+
+using namespace osc;
+using namespace osc_abi;
+
+extern "C" {
+
+int osc_space_charge_step_vjp_dev(osc_ctx *ctx, const osc_mesh3d *mesh, int64_t np, const double *x, const double *y,
+                                  const double *z, const double *q, double total_charge, int precision,
+                                  const double *gE, double *gx, double *gy, double *gz, double *gq) {
+    if (!ctx) return OSC_E_INVALID;
+    int n[3];
+    TRY(mesh_dims(ctx, mesh, n));
+    TRY(check_prec(ctx, precision));
+    if (np <= 0 || !x || !y || !z || !gE || !gx || !gy || !gz) return bad(ctx, "vjp arrays");
+    if (!(mesh->gamma >= 1.0)) return set_err(ctx, OSC_E_INVALID, "gamma must be >= 1");
+    const int64_t N = (int64_t)n[0] * n[1] * n[2];
+    const double charge1 = q ? 0.0 : total_charge / (double)np;
+    DepositArgs da = deposit_args(mesh, n, np, x, y, z, q, charge1, 0);
+    InterpArgs ia = interp_args(mesh, n, np, x, y, z);
+    double *rho, *Eg, *acc, *lam;
+    TRY(ws_get(ctx, "vjp_rho", sizeof(double) * N, (void **)&rho));
+    TRY(ws_get(ctx, "vjp_E", sizeof(double) * 3 * N, (void **)&Eg));
+    TRY(ws_get(ctx, "vjp_a", sizeof(double) * 3 * N, (void **)&acc));
+    TRY(ws_get(ctx, "vjp_lambda", sizeof(double) * N, (void **)&lam));
+    const int prec = precision == OSC_PREC_FP32 ? OSC_PREC_FP32 : OSC_PREC_FP64;
+    TRY(counters_reset(ctx));
+    // forward field on the grid (the gather term needs it)
+    TRY(deposit_rho<double>(ctx, da, rho, N, 1.0));
+    FreeSpaceJob j = fs_job(mesh, n, nullptr, 0, 0);
+    j.E = Eg;
+    TRY(run_freespace(ctx, j, rho, prec));
+    // deposited gradients a_c and the adjoint potential
+    CK(cudaMemsetAsync(acc, 0, sizeof(double) * 3 * N, ctx->stream), "memset a");
+    CK(cudaMemsetAsync(lam, 0, sizeof(double) * N, ctx->stream), "memset lambda");
+    {
+        Launch L_(ctx, "vjp_deposit");
+        if (launch_deposit_vec3(da, gE, acc, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "vjp deposit");
+    }
+    for (int c = 0; c < 3; ++c) {
+        FreeSpaceJob jc = fs_job(mesh, n, nullptr, 0, 0);
+        jc.comp_mask = 1 << c;
+        jc.Eacc = lam;
+        jc.acc_coef = -1.0;
+        TRY(run_freespace(ctx, jc, acc + c * N, prec));
+    }
+    {
+        Launch L_(ctx, "vjp_particles");
+        if (launch_vjp_particles(ia, da, Eg, lam, gE, gx, gy, gz, gq, ctx->stream))
+            return set_err(ctx, OSC_E_CUDA, "vjp gather");
+    }
+    return OSC_OK;
+}
+
+}  // extern "C"

@@ -41,7 +41,7 @@ struct OutDest {
     double coef;      // multiplier
 };
 constexpr int MAX_OUT = 6;
-constexpr int MAX_DEST = 3;
+constexpr int MAX_DEST = 4;
 
 // Inverse transform of Hermitian rows (L/2+1 stored frequencies) to real rows, keeping
 // x in [0, nout), for ncomp component arrays; each component's result goes to up to

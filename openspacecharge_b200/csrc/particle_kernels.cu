@@ -594,4 +594,126 @@ int launch_batch_stats(const BunchArgs *bunches, const BatchJob *jobs, int njobs
     return ok();
 }
 
+// ------------------------------------------------------------------------------------
+// Adjoint of the step.  Both the deposit (deposit_particles) and the gather
+// (interpolate_field) are trilinear in the particle position within a cell, with the low
+// node weighted ab = ((min - x) + f*delta)/delta, so d ab/dx = -1/delta.
+
+// a[c][n] += sum over particles of g[m][c] times the particle's deposit weight of node n.
+__global__ void __launch_bounds__(256) k_deposit_vec3(DepositArgs a, const double *__restrict__ g,
+                                                      double *__restrict__ acc) {
+    const int64_t plane = (int64_t)a.nx * a.ny, N = plane * a.nz;
+    GRID_STRIDE(m, a.np) {
+        const double xm = a.x[m], ym = a.y[m], zm = a.z[m];
+        const double fx = floor((xm - a.xmin) * a.dxi + 1);
+        const double fy = floor((ym - a.ymin) * a.dyi + 1);
+        const double fz = floor((zm - a.zmin) * a.dzi + 1);
+        if (!(fx >= a.nlo[0] && fx + 1 <= a.nhi[0] && fy >= a.nlo[1] && fy + 1 <= a.nhi[1] && fz >= a.nlo[2] &&
+              fz + 1 <= a.nhi[2]))
+            continue;
+        const double ab = ((a.xmin - xm) + fx * a.dx) * a.dxi;
+        const double de = ((a.ymin - ym) + fy * a.dy) * a.dyi;
+        const double gh = ((a.zmin - zm) + fz * a.dz) * a.dzi;
+        const int i = (int)fx - a.nlo[0], j = (int)fy - a.nlo[1], k = (int)fz - a.nlo[2];
+        const int64_t n0 = i + (int64_t)a.nx * j + plane * k;
+        double w[8];
+        int64_t off[8];
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+            const int dx = t & 1, dy = (t >> 1) & 1, dz = t >> 2;
+            w[t] = (dx ? 1. - ab : ab) * (dy ? 1. - de : de) * (dz ? 1. - gh : gh);
+            off[t] = n0 + dx + (int64_t)a.nx * dy + plane * dz;
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const double gc = g[3 * m + c];
+            if (gc == 0.0) continue;
+#pragma unroll
+            for (int t = 0; t < 8; ++t) atomicAdd(acc + c * N + off[t], w[t] * gc);
+        }
+    }
+}
+int launch_deposit_vec3(const DepositArgs &a, const double *g, double *acc, cudaStream_t st) {
+    if (a.np <= 0) return OSC_OK;
+    k_deposit_vec3<<<nblocks(a.np, 256, 148 * 64), 256, 0, st>>>(a, g, acc);
+    return ok();
+}
+
+// Value and gradient of the trilinear interpolant of F on the cell (i,j,k) with low-node
+// weights (ab, de, gh): returns F(x) and d/dx, d/dy, d/dz.
+__device__ __forceinline__ void trilinear_grad(const double *__restrict__ F, int64_t n0, int nx, int64_t plane,
+                                               double ab, double de, double gh, const double hinv[3],
+                                               double &val, double grad[3]) {
+    double f[8];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) f[t] = F[n0 + (t & 1) + (int64_t)nx * ((t >> 1) & 1) + plane * (t >> 2)];
+    const double wx[2] = {ab, 1. - ab}, wy[2] = {de, 1. - de}, wz[2] = {gh, 1. - gh};
+    double v = 0, gx = 0, gy = 0, gz = 0;
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+        const int a = t & 1, b = (t >> 1) & 1, c = t >> 2;
+        v += wx[a] * wy[b] * wz[c] * f[t];
+        gx += (a ? 1. : -1.) * wy[b] * wz[c] * f[t];
+        gy += wx[a] * (b ? 1. : -1.) * wz[c] * f[t];
+        gz += wx[a] * wy[b] * (c ? 1. : -1.) * f[t];
+    }
+    val = v;
+    grad[0] = gx * hinv[0];
+    grad[1] = gy * hinv[1];
+    grad[2] = gz * hinv[2];
+}
+
+// Per particle: g_x = sum_c gE[c] grad E_c(x) (gather at the clamped interpolation cell)
+// + q grad lambda(x) (deposit cell; particles outside the mesh deposit nothing), and
+// g_q = lambda(x), where lambda is the adjoint potential.
+__global__ void __launch_bounds__(256) k_vjp_particles(InterpArgs ia, DepositArgs da, const double *__restrict__ E,
+                                                       const double *__restrict__ lam, const double *__restrict__ gE,
+                                                       double *gx, double *gy, double *gz, double *gq) {
+    const int64_t plane = (int64_t)ia.nx * ia.ny, N = plane * ia.nz;
+    GRID_STRIDE(m, ia.np) {
+        const double xm = ia.x[m], ym = ia.y[m], zm = ia.z[m];
+        double g[3] = {0, 0, 0};
+        Cell c;
+        locate(ia, xm, ym, zm, c);
+        const int64_t n0 = c.i + (int64_t)ia.nx * c.j + plane * c.k;
+        for (int comp = 0; comp < 3; ++comp) {
+            const double w = gE[3 * m + comp];
+            if (w == 0.0) continue;
+            double v, gr[3];
+            trilinear_grad(E + comp * N, n0, ia.nx, plane, c.ab, c.de, c.gh, ia.hinv, v, gr);
+            g[0] += w * gr[0];
+            g[1] += w * gr[1];
+            g[2] += w * gr[2];
+        }
+        double lv = 0;
+        const double fx = floor((xm - da.xmin) * da.dxi + 1);
+        const double fy = floor((ym - da.ymin) * da.dyi + 1);
+        const double fz = floor((zm - da.zmin) * da.dzi + 1);
+        if (fx >= da.nlo[0] && fx + 1 <= da.nhi[0] && fy >= da.nlo[1] && fy + 1 <= da.nhi[1] && fz >= da.nlo[2] &&
+            fz + 1 <= da.nhi[2]) {
+            const double ab = ((da.xmin - xm) + fx * da.dx) * da.dxi;
+            const double de = ((da.ymin - ym) + fy * da.dy) * da.dyi;
+            const double gh = ((da.zmin - zm) + fz * da.dz) * da.dzi;
+            const int i = (int)fx - da.nlo[0], j = (int)fy - da.nlo[1], k = (int)fz - da.nlo[2];
+            const double hinv[3] = {da.dxi, da.dyi, da.dzi};
+            double gr[3];
+            trilinear_grad(lam, i + (int64_t)da.nx * j + plane * k, da.nx, plane, ab, de, gh, hinv, lv, gr);
+            const double q = da.q ? da.q[m] : da.charge1;
+            g[0] += q * gr[0];
+            g[1] += q * gr[1];
+            g[2] += q * gr[2];
+        }
+        gx[m] = g[0];
+        gy[m] = g[1];
+        gz[m] = g[2];
+        if (gq) gq[m] = lv;
+    }
+}
+int launch_vjp_particles(const InterpArgs &ia, const DepositArgs &da, const double *E, const double *lam,
+                         const double *gE, double *gx, double *gy, double *gz, double *gq, cudaStream_t st) {
+    if (ia.np <= 0) return OSC_OK;
+    k_vjp_particles<<<nblocks(ia.np, 256, 148 * 64), 256, 0, st>>>(ia, da, E, lam, gE, gx, gy, gz, gq);
+    return ok();
+}
+
 }  // namespace osc

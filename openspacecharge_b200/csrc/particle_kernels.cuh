@@ -96,4 +96,12 @@ int launch_batch_interp_pairs(const BunchArgs *bunches, const BatchJob *jobs, in
 int launch_batch_stats(const BunchArgs *bunches, const BatchJob *jobs, int njobs, const int *job0, int nbunch,
                        unsigned long long *keys, double *qsum, double *out, cudaStream_t st);
 
+// ---- adjoint of the step ---------------------------------------------------------------
+// acc[c][n] += g[m][c] * (deposit weight of particle m at node n); acc is [3][N] doubles.
+int launch_deposit_vec3(const DepositArgs &a, const double *g, double *acc, cudaStream_t st);
+// Particle gradients of sum_m gE[m] . E(x_m): the gather term through the E planes [3][N]
+// and the deposit term through the adjoint potential lam [N]; gq (nullable) = lam(x_m).
+int launch_vjp_particles(const InterpArgs &ia, const DepositArgs &da, const double *E, const double *lam,
+                         const double *gE, double *gx, double *gy, double *gz, double *gq, cudaStream_t st);
+
 }  // namespace osc

@@ -357,7 +357,9 @@ int freespace_opt(osc_ctx *c, const FreeSpaceJob &j, const TIn *rho) {
     if (j.want_phi && j.phi) add_dest(add_out(0, 1.0), j.phi, 1, 0, 1.0);
     if (j.want_e || j.calc_b) {
         for (int q = 0; q < 3; ++q) {
+            if (!((j.comp_mask >> q) & 1) && !j.calc_b) continue;
             const int o = add_out(q + 1, 1.0);
+            if (j.Eacc) add_dest(o, j.Eacc, 3, 0, j.acc_coef);
             if (j.E) add_dest(o, j.E + q * N, 1, 0, 1.0);
             if (j.E4) {
                 if (j.e4_pairs) {  // staged in the x epilogue and written as whole pairs

@@ -39,6 +39,11 @@ struct FreeSpaceJob {
     double *B = nullptr;    // device f64 [3][N]
     void *E4 = nullptr;     // device vec4<T> [N], or the x-pair grid vec4<T> [N][2]
     int e4_pairs = 0;       // 1: E4 is the x-pair grid read by launch_interp_pairs
+    // E components computed (bit c: E_c); each one is also added, times acc_coef, into
+    // the single plane Eacc when that is set (adjoint solves accumulate a potential)
+    int comp_mask = 7;
+    double *Eacc = nullptr;
+    double acc_coef = 0;
     // batch of nbatch equal grids stacked in rho and E4 (E4 output only); the spectra come
     // from gbatch (member b at data + b*g_bstride elements) instead of the Green cache
     int nbatch = 1;

@@ -122,6 +122,7 @@ SIGNATURES = {
     "osc_interpolate_field_dev": [_P, _PM, _P, _P, _I64, _P, _P, _P, _P, _P, _PI64],
     "osc_space_charge_step": [_P, _PM, _I64, _P, _P, _P, _P, _P, _I, _I, _I, _P, _P],
     "osc_space_charge_step_dev": [_P, _PM, _I64, _P, _P, _P, _P, _P, _I, _I, _I, _P, _P],
+    "osc_space_charge_step_vjp_dev": [_P, _PM, _I64, _P, _P, _P, _P, _D, _I, _P, _P, _P, _P, _P],
     "osc_batch_space_charge_step": [_P, _I, ctypes.POINTER(OscBunch), _P, _P, _P, _P, _I, _I, _P],
     "osc_batch_space_charge_step_dev": [_P, _I, ctypes.POINTER(OscBunch), _P, _P, _P, _P, _I, _I, _P],
 }
@@ -205,7 +206,9 @@ class Context:
         return int(v.value)
 
     def set_stream(self, stream_ptr: int | None) -> None:
-        self.call("osc_ctx_set_stream", ctypes.c_void_p(stream_ptr or 0))
+        """Run on the CUDA stream `stream_ptr` (0 = the default stream, e.g. torch's
+        ``cuda_stream`` of it); None returns to the context's own stream."""
+        self.call("osc_ctx_set_stream", ctypes.c_void_p(-1 if stream_ptr is None else int(stream_ptr)))
 
     def synchronize(self) -> None:
         self.call("osc_ctx_synchronize")

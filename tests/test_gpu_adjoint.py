@@ -1,0 +1,119 @@
+"""Adjoint of the fused step (osc_space_charge_step_vjp_dev) and its torch.autograd wrapper.
+
+The loss is L = sum_m q_m |E(x_m)|^2 on a fixed mesh.  Within one cell the deposit and the
+gather are trilinear in a particle's position, so central differences of L are exact up
+to round-off; components whose +-h step would cross a cell face are skipped.  The FP64
+gradients match the differences to 1e-6 (relative to the largest gradient); the FP32 path
+matches FP64 to 1e-4."""
+import numpy as np
+import pytest
+
+import openspacecharge_b200 as osc
+from openspacecharge_b200.bunch import gendist
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+N = (32, 32, 32)
+GAMMA = 9.784756683727565
+
+
+@pytest.fixture(scope="module")
+def det():
+    c = osc.Context(0)
+    c.set_option(osc.OPT_DEPOSIT_MODE, osc.DEPOSIT_DETERMINISTIC)
+    yield c
+    c.close()
+
+
+def setup(ctx, npart=20000, seed=51):
+    x, y, z = gendist(npart, sigma=(1e-3, 1e-3, 1e-3), seed=seed)
+    q = np.random.default_rng(seed).uniform(0.5, 1.5, npart) * 1e-15
+    delta, umin = osc.get_mesh_quantities(ctx, x, y, z, (1, 1, 1), N, 0)
+    umax = umin + (np.array(N) - 1) * delta
+    mesh = osc.Mesh3D(nlo=(1, 1, 1), nhi=N, min=umin, max=umax, delta=delta, gamma=GAMMA)
+    return x, y, z, q, mesh
+
+
+def loss(ctx, mesh, x, y, z, q, prec):
+    m = osc.Mesh3D(nlo=mesh.nlo, nhi=mesh.nhi, min=mesh.min.copy(), max=mesh.max.copy(), delta=mesh.delta.copy(),
+                   gamma=mesh.gamma)
+    E, _ = osc.space_charge_step(ctx, m, x, y, z, qa=q, resize_mesh=False, precision=prec)
+    return float((q[:, None] * E * E).sum()), E
+
+
+def vjp(ctx, mesh, x, y, z, q, gE, prec):
+    import ctypes
+    dev = torch.device("cuda", 0)
+    t = [torch.from_numpy(np.ascontiguousarray(a)).to(dev) for a in (x, y, z, q, gE)]
+    g = [torch.empty_like(t[0]) for _ in range(4)]
+    m = mesh.to_c()
+    ctx.call("osc_space_charge_step_vjp_dev", ctypes.byref(m), ctypes.c_int64(len(x)),
+             *[ctypes.c_void_p(a.data_ptr()) for a in t[:4]], ctypes.c_double(0.0), int(prec),
+             ctypes.c_void_p(t[4].data_ptr()), *[ctypes.c_void_p(a.data_ptr()) for a in g])
+    ctx.synchronize()
+    return [a.cpu().numpy() for a in g]
+
+
+def test_vjp_matches_central_differences(det):
+    x, y, z, q, mesh = setup(det)
+    L0, E = loss(det, mesh, x, y, z, q, osc.PREC_FP64)
+    gx, gy, gz, gq = vjp(det, mesh, x, y, z, q, 2 * q[:, None] * E, osc.PREC_FP64)
+    # the VJP's own part of dL/dq excludes the explicit q in the loss: add |E|^2
+    grads = [gx, gy, gz]
+    scale = max(np.abs(g).max() for g in grads)
+    rng = np.random.default_rng(7)
+    picks = rng.choice(len(x), 64, replace=False)
+    pos = [x, y, z]
+    checked = 0
+    for m in picks:
+        for d in range(3):
+            h = 1e-4 * 1e-3
+            u = (pos[d][m] - mesh.min[d]) / mesh.delta[d]
+            if min(u - np.floor(u), np.ceil(u) - u) * mesh.delta[d] < 3 * h:
+                continue  # the step would cross a cell face
+            p = [a.copy() for a in pos]
+            p[d][m] += h
+            Lp, _ = loss(det, mesh, *p, q, osc.PREC_FP64)
+            p[d][m] -= 2 * h
+            Lm, _ = loss(det, mesh, *p, q, osc.PREC_FP64)
+            fd = (Lp - Lm) / (2 * h)
+            assert abs(fd - grads[d][m]) <= 1e-6 * scale, (m, d, fd, grads[d][m])
+            checked += 1
+    assert checked >= 150
+    # charges: L is quadratic in q_m, so central differences are exact too
+    for m in picks[:16]:
+        hq = 1e-3 * q[m]
+        qp = q.copy()
+        qp[m] += hq
+        Lp, _ = loss(det, mesh, x, y, z, qp, osc.PREC_FP64)
+        qp[m] -= 2 * hq
+        Lm, _ = loss(det, mesh, x, y, z, qp, osc.PREC_FP64)
+        fd = (Lp - Lm) / (2 * hq)
+        full = (E[m] ** 2).sum() + gq[m]
+        assert abs(fd - full) <= 1e-6 * abs(full), (m, fd, full)
+
+
+def test_fp32_vjp_matches_fp64(ctx):
+    x, y, z, q, mesh = setup(ctx, npart=100000, seed=52)
+    _, E = loss(ctx, mesh, x, y, z, q, osc.PREC_FP64)
+    gE = 2 * q[:, None] * E
+    g64 = vjp(ctx, mesh, x, y, z, q, gE, osc.PREC_FP64)
+    g32 = vjp(ctx, mesh, x, y, z, q, gE, osc.PREC_FP32)
+    for a, b in zip(g32, g64):
+        assert np.abs(a - b).max() <= 1e-4 * np.abs(b).max()
+
+
+def test_autograd_function(ctx):
+    from openspacecharge_b200.autograd import space_charge_field
+    x, y, z, q, mesh = setup(ctx, npart=50000, seed=53)
+    dev = torch.device("cuda", 0)
+    tx, ty, tz, tq = (torch.from_numpy(a).to(dev).requires_grad_() for a in (x, y, z, q))
+    E = space_charge_field(tx, ty, tz, tq, mesh, ctx, precision=osc.PREC_FP64)
+    L = (tq[:, None] * E * E).sum()
+    L.backward()
+    Ed = E.detach().cpu().numpy()
+    gx, gy, gz, gq = vjp(ctx, mesh, x, y, z, q, 2 * q[:, None] * Ed, osc.PREC_FP64)
+    for t, ref in ((tx, gx), (ty, gy), (tz, gz)):
+        assert np.allclose(t.grad.cpu().numpy(), ref, rtol=0, atol=1e-9 * np.abs(ref).max())
+    assert np.allclose(tq.grad.cpu().numpy(), (Ed ** 2).sum(1) + gq, rtol=1e-9, atol=0)
