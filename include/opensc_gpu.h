@@ -222,6 +222,20 @@ OSC_API int osc_space_charge_step_dev(osc_ctx *ctx, osc_mesh3d *mesh, int64_t np
                               const double *total_charge, int resize_mesh, int at_cathode,
                               int precision, double *d_E, double *d_B);
 
+/* ---- line-out and plane files ---------------------------------------------------------
+ * Replace write_lines / write_plane of the reference's test program
+ * (code/test_opensc.f90:237-295): x_lineout.dat, y_lineout.dat, z_lineout.dat (x y z Ex Ey
+ * Ez, Fortran '(6(1pe14.7,1x))', points (i-1)*delta+min for i = nlo..nhi-1 along one axis
+ * through (xcent, ycent, zcent)) and x_z_Ex_Ez_By.dat (x z Ex Ez By, list-directed, plane
+ * y = 0), written into dir (NULL or "": the working directory).  efield/bfield are host
+ * grids [3][nz][ny][nx].  osc_format_1pe14_7 writes one value as Fortran 1PE14.7 (14
+ * characters and a terminating NUL into out15). */
+OSC_API int osc_write_lines(osc_ctx *ctx, const osc_mesh3d *mesh, const double *efield, double xcent,
+                            double ycent, double zcent, const char *dir);
+OSC_API int osc_write_plane(osc_ctx *ctx, const osc_mesh3d *mesh, const double *efield, const double *bfield,
+                            const char *dir);
+OSC_API int osc_format_1pe14_7(double v, char *out15);
+
 /* ---- adjoint of the step ---------------------------------------------------------------
  * Vector-Jacobian product of the fused step with the mesh held fixed: given gE = dL/dE at
  * every particle ([np][3]), returns dL/dx, dL/dy, dL/dz and (gq non-NULL) dL/dq per

@@ -360,3 +360,32 @@ def batch_space_charge_step_dev(ctx, meshes, x, y, z, counts, E, qa=None, total_
     for b, m in enumerate(meshes):
         m.from_c(arr[b].mesh)
     return [int(arr[b].n_outside) for b in range(len(meshes))]
+
+
+def write_lines(ctx, mesh3d: Mesh3D, xcent, ycent, zcent, directory=None) -> None:
+    """write_lines of the reference's test program (code/test_opensc.f90:237-274): x/y/z
+    line-outs of E through (xcent, ycent, zcent) into x_lineout.dat, y_lineout.dat and
+    z_lineout.dat in `directory` (default: the working directory)."""
+    ef = _grid(mesh3d.efield)
+    m = mesh3d.to_c()
+    d = None if directory is None else str(directory).encode()
+    _ctx(ctx).call("osc_write_lines", ctypes.byref(m), _p(ef), float(xcent), float(ycent), float(zcent), d)
+
+
+def write_plane(ctx, mesh3d: Mesh3D, directory=None) -> None:
+    """write_plane of the reference's test program (code/test_opensc.f90:278-295): x, z, Ex,
+    Ez, By on the plane y = 0 into x_z_Ex_Ez_By.dat."""
+    ef = _grid(mesh3d.efield)
+    bf = _grid(mesh3d.bfield)
+    m = mesh3d.to_c()
+    d = None if directory is None else str(directory).encode()
+    _ctx(ctx).call("osc_write_plane", ctypes.byref(m), _p(ef), _p(bf), d)
+
+
+def format_1pe14_7(v: float) -> str:
+    """One value in Fortran's 1PE14.7 edit descriptor (the line-out files' format)."""
+    buf = ctypes.create_string_buffer(16)
+    rc = native.lib().osc_format_1pe14_7(ctypes.c_double(float(v)), buf)
+    if rc:
+        raise ValueError("format")
+    return buf.value.decode()

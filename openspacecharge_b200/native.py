@@ -122,6 +122,9 @@ SIGNATURES = {
     "osc_interpolate_field_dev": [_P, _PM, _P, _P, _I64, _P, _P, _P, _P, _P, _PI64],
     "osc_space_charge_step": [_P, _PM, _I64, _P, _P, _P, _P, _P, _I, _I, _I, _P, _P],
     "osc_space_charge_step_dev": [_P, _PM, _I64, _P, _P, _P, _P, _P, _I, _I, _I, _P, _P],
+    "osc_write_lines": [_P, _PM, _P, _D, _D, _D, ctypes.c_char_p],
+    "osc_write_plane": [_P, _PM, _P, _P, ctypes.c_char_p],
+    "osc_format_1pe14_7": [_D, ctypes.c_char_p],
     "osc_space_charge_step_vjp_dev": [_P, _PM, _I64, _P, _P, _P, _P, _D, _I, _P, _P, _P, _P, _P],
     "osc_batch_space_charge_step": [_P, _I, ctypes.POINTER(OscBunch), _P, _P, _P, _P, _I, _I, _P],
     "osc_batch_space_charge_step_dev": [_P, _I, ctypes.POINTER(OscBunch), _P, _P, _P, _P, _I, _I, _P],
