@@ -62,9 +62,10 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
-    ap.add_argument("--workload", default="single", choices=["single", "batch", "adjoint"],
+    ap.add_argument("--workload", default="single", choices=["single", "batch", "adjoint", "pipe"],
                     help="single: the headline one-bunch step; batch: 256 bunches of mixed grids per step; "
-                         "adjoint: forward + backward of sum q|E|^2 at 128^3, 4e6 particles")
+                         "adjoint: forward + backward of sum q|E|^2 at 128^3, 4e6 particles; "
+                         "pipe: rectangular-pipe step at 64x64x128, 4e6 particles")
     ap.add_argument("--bunches", type=int, default=BATCH_BUNCHES)
     return ap.parse_args()
 
@@ -536,6 +537,95 @@ def run_adjoint(args, ws, rank, local, dist):
     ctx.close()
 
 
+PIPE_AB = (20e-3, 10e-3)
+PIPE_GRID = (64, 64, 128)
+PIPE_NP = 4_000_000
+PIPE_SIGMA = (2e-3, 1e-3, 1e-3)
+PIPE_METRIC = "solves/s, rectangular pipe 20x10 mm, 64x64x128 grid spanning the walls, 4e6 ptcl"
+
+
+def run_pipe(args, ws, rank, local, dist):
+    """Rectangular-pipe step: deposit, pipe potential (four cached Green spectra, FP32
+    convolution), finite-difference E and B, gather of E at the particles."""
+    import ctypes
+    import torch
+    import openspacecharge_b200 as osc
+    from openspacecharge_b200.bunch import gendist
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    a, b = PIPE_AB
+    x, y, z = gendist(PIPE_NP, sigma=PIPE_SIGMA, cutoff=CUTOFF, disttype=1, seed=SEED, pipe=(a, b),
+                      centroid=(3e-3, -1e-3, 0.0))
+    n = PIPE_GRID
+    umin = np.array([-0.5 * a, -0.5 * b, -6 * PIPE_SIGMA[2]])
+    delta = np.array([a / (n[0] - 1), b / (n[1] - 1), 12 * PIPE_SIGMA[2] / (n[2] - 1)])
+    mesh = osc.Mesh3D(nlo=(1, 1, 1), nhi=n, min=umin, max=umin + (np.array(n) - 1) * delta, delta=delta,
+                      gamma=GAMMA)
+    ctx = osc.Context(local)
+    stream = torch.cuda.Stream(device=dev)
+    ctx.set_stream(stream.cuda_stream)
+    N = n[0] * n[1] * n[2]
+    tx, ty, tz = (torch.from_numpy(v).to(dev) for v in (x, y, z))
+    rho = torch.empty(N, dtype=torch.float64, device=dev)
+    phi = torch.empty_like(rho)
+    E = torch.empty(3 * N, dtype=torch.float64, device=dev)
+    B = torch.empty_like(E)
+    Ep = torch.empty((PIPE_NP, 3), dtype=torch.float64, device=dev)
+    m = mesh.to_c()
+    tc = ctypes.c_double(QTOT)
+    P = lambda t: ctypes.c_void_p(t.data_ptr())
+    t0 = time.perf_counter()
+    osc.osc_rectpipe_green(ctx, mesh, a, b, precision=osc.PREC_FP32)
+    ctx.synchronize()
+    green_s = time.perf_counter() - t0
+
+    def step(prec, out=Ep):
+        ctx.call("osc_deposit_particles_dev", ctypes.c_int64(PIPE_NP), P(tx), P(ty), P(tz), None, ctypes.byref(tc),
+                 0, ctypes.byref(m), P(rho), None)
+        ctx.call("osc_space_charge_rectpipe_dev", ctypes.byref(m), P(rho), a, b, 0, 1, prec, P(phi), P(E), P(B))
+        ctx.call("osc_interpolate_field_dev", ctypes.byref(m), P(E), None, ctypes.c_int64(PIPE_NP), P(tx), P(ty),
+                 P(tz), P(out), None, None)
+
+    for _ in range(max(3, args.warmup)):
+        step(osc.PREC_FP32)
+    ctx.synchronize()
+    k = max(1, args.steps)
+    with ClockSampler(local) as clk:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k):
+            step(osc.PREC_FP32)
+        e1.record(stream)
+        e1.synchronize()
+    ms = e0.elapsed_time(e1) / k
+    E32 = Ep.clone()
+    osc.osc_rectpipe_green(ctx, mesh, a, b, precision=osc.PREC_FP64_PLAIN)
+    E64 = torch.empty_like(Ep)
+    step(osc.PREC_FP64_PLAIN, E64)
+    ctx.synchronize()
+    e0.record(stream)
+    step(osc.PREC_FP64_PLAIN, E64)
+    e1.record(stream)
+    e1.synchronize()
+    ms64 = e0.elapsed_time(e1)
+    d = (E32 - E64).abs()
+    err = float((d.amax(0) / E64.abs().amax(0)).max())
+    if rank == 0:
+        print(json.dumps({
+            "metric": PIPE_METRIC, "value": ws * 1000.0 / ms, "unit": "solves/s", "n_gpus": ws, "steps": k,
+            "warmup": max(3, args.warmup), "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "rectangular pipe 20x10 mm: deposit + pipe potential (FP32 convolution with the four "
+                                   "cached FP64 mode-sum Green spectra) + FD E and B + gather, 64x64x128 grid spanning "
+                                   "the walls, 4e6 particles sigma=(2,1,1) mm centred at (3,-1) mm, pipe rejection",
+                       "grid": list(n), "particles": PIPE_NP},
+            "fp64_plain": {"ms_per_step": ms64, "speedup_fp32_over_fp64": ms64 / ms},
+            "rel_err_vs_fp64": err, "green_build_s": green_s, "clocks": clk.summary()}))
+    ctx.close()
+
+
 def cpu_baseline(x, y, z, grid, umin, umax, delta):
     """One full step of the FP64 CPU port (oracle/) on the host cores."""
     from oracle import oracle as O
@@ -604,6 +694,8 @@ def main():
             run_batch(args, ws, rank, local, dist)
         elif args.workload == "adjoint":
             run_adjoint(args, ws, rank, local, dist)
+        elif args.workload == "pipe":
+            run_pipe(args, ws, rank, local, dist)
         else:
             run_ours(args, ws, rank, local, dist)
     finally:

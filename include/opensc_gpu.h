@@ -188,6 +188,11 @@ OSC_API int osc_space_charge_rectpipe(osc_ctx *ctx, const osc_mesh3d *mesh, cons
                               double apipe, double bpipe, int direct_field_calc,
                               int integrated_green_function, int precision, double *phi,
                               double *efield, double *bfield);
+/* Device pointers, asynchronous on the context stream; otherwise as above. */
+OSC_API int osc_space_charge_rectpipe_dev(osc_ctx *ctx, const osc_mesh3d *mesh, const double *d_rho,
+                                          double apipe, double bpipe, int direct_field_calc,
+                                          int integrated_green_function, int precision, double *d_phi,
+                                          double *d_efield, double *d_bfield);
 /* Replace osc_write_rectpipe_grn / osc_read_rectpipe_grn (core:825-870): a header record
  * and cgrn1..4 as complex128, Fortran unformatted sequential layout. */
 OSC_API int osc_write_rectpipe_grn(osc_ctx *ctx, const char *path, double apipe, double bpipe,

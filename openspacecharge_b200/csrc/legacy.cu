@@ -619,6 +619,31 @@ int osc_space_charge_rectpipe(osc_ctx *ctx, const osc_mesh3d *mesh, const double
     return syncc(ctx);
 }
 
+int osc_space_charge_rectpipe_dev(osc_ctx *ctx, const osc_mesh3d *mesh, const double *d_rho, double apipe,
+                                  double bpipe, int direct_field_calc, int integrated_green_function, int precision,
+                                  double *d_phi, double *d_efield, double *d_bfield) {
+    if (!ctx) return OSC_E_INVALID;
+    (void)apipe;
+    (void)bpipe;
+    (void)integrated_green_function;
+    int64_t N;
+    TRY(mesh_n(ctx, mesh, &N));
+    if (precision < 0 || precision > 2) return set_err(ctx, OSC_E_INVALID, "precision");
+    if (!d_rho || !d_phi || !d_efield || !d_bfield) return set_err(ctx, OSC_E_INVALID, "space_charge_rectpipe arrays");
+    if (direct_field_calc)
+        return set_err(ctx, OSC_E_UNSUPPORTED,
+                       "**********ERROR********* rectpipe implementation presently requires directfieldcalc=0");
+    PipeGreen &p = ctx->pipe;
+    bool same = p.valid;
+    for (int d = 0; d < 3 && same; ++d)
+        same = p.nlo[d] == mesh->nlo[d] && p.nhi[d] == mesh->nhi[d] && p.npad[d] == mesh->npad[d];
+    if (!same)
+        return set_err(ctx, OSC_E_STATE,
+                       "something wrong. rectpipe green functions should have been computed during initialization "
+                       "(call osc_rectpipe_green or osc_read_rectpipe_grn for this mesh first)");
+    return pipe_solve(ctx, precision, mesh->delta, mesh->gamma, d_rho, d_phi, d_efield, d_bfield);
+}
+
 // ---- rectpipegrn.dat (core:825-870): gfortran unformatted sequential records --------------
 namespace {
 const int64_t kMaxSub = 2147483639;  // largest gfortran subrecord payload (2^31 - 9)
