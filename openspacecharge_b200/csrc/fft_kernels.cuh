@@ -57,6 +57,10 @@ struct C2RArgs {
     int e8_comp[3];       // components giving (Ex, Ey, Ez) of the x-pair grid
     int ndest[MAX_OUT];
     OutDest dest[MAX_OUT][MAX_DEST];
+    // zin != 0: the input spectra are kz-innermost, [c][b][y][kx][z] with zin_nz planes per
+    // member and zin_ny rows y; row r = (b*ny + y)*nz + z starts at (b*ny + y)*(nx+1)*nz + z
+    // with elements nz apart and goes to grid row (b*nz + z)*ny + y ([z][y][x] per member).
+    int zin, zin_nz, zin_ny;
 };
 
 // Stored Green spectrum of one kernel component on the half-spectrum grid
@@ -102,7 +106,8 @@ struct ZConvArgs {
     int ncols;       // (nx+1)*Ny
     int nxh, Ny, ny;
     int64_t in_estride;   // complex elements between z planes of the input (= ncols)
-    int64_t out_estride;  // between z planes of the output
+    int64_t out_estride;  // between z planes of the output (1: z-innermost output)
+    int64_t out_colstride;  // between (kx,ky) columns of the output (nz when z-innermost)
     int64_t out_cstride;  // between output components
     int nout;
     int gdir[MAX_OUT];    // index into g[] of the direct term (-1 none)

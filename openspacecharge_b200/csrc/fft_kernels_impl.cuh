@@ -151,6 +151,19 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_r2c_rows(const TIn *__restri
 }
 
 // ------------------------------------------------------------------------------------
+// Input offset and output grid row of real row r of an x inverse (see C2RArgs::zin).
+__device__ __forceinline__ void row_bases(const C2RArgs &a, int64_t r, int64_t &in_off, int64_t &out_row) {
+    if (!a.zin) {
+        in_off = r * a.in_rstride;
+        out_row = r;
+        return;
+    }
+    const int64_t t = r / a.zin_nz, z = r - t * a.zin_nz;  // t = b*ny + y
+    const int64_t b = t / a.zin_ny, y = t - b * a.zin_ny;
+    in_off = t * a.in_rstride + z;
+    out_row = (b * a.zin_nz + z) * a.zin_ny + y;
+}
+
 template <typename T>
 __device__ __forceinline__ void write_dest(const OutDest &d, int64_t gidx, int x, T val) {
     // vec4 grids also write their unused 4th slot, so every 32-byte sector is written whole
@@ -196,7 +209,11 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_c2r_rows(const cplx<T> *__re
     const int64_t row0 = (int64_t)blockIdx.x * (2 * NL);
     const int half = L / 2;
     T *res = reinterpret_cast<T *>(buf + L * lstr);  // [3][2*NL][nout] when a.e8 is set
+    __shared__ int64_t rin[2 * NL], rout[2 * NL];
+    for (int t = tid; t < 2 * NL; t += nthreads) row_bases(a, row0 + t, rin[t], rout[t]);
+    const int64_t ies = a.zin ? a.zin_nz : 1;
     load_twiddles(tw, twg, L);
+    __syncthreads();
     for (int c = 0; c < a.ncomp; ++c) {
         const V *src = in + (int64_t)c * a.in_cstride;
         for (int idx = tid; idx < NL * L; idx += nthreads) {
@@ -204,8 +221,8 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_c2r_rows(const cplx<T> *__re
             const int64_t ra = row0 + 2 * line, rb = ra + 1;
             const int kk = k <= half ? k : L - k;
             V A = mk<T>(0, 0), B = mk<T>(0, 0);
-            if (ra < a.nrows) A = src[ra * a.in_rstride + kk];
-            if (rb < a.nrows) B = src[rb * a.in_rstride + kk];
+            if (ra < a.nrows) A = src[rin[2 * line] + kk * ies];
+            if (rb < a.nrows) B = src[rin[2 * line + 1] + kk * ies];
             if (k == 0 || k == half) { A.y = 0; B.y = 0; }
             if (k > half) { A.y = -A.y; B.y = -B.y; }
             buf[k * lstr + line] = mk<T>(A.x - B.y, A.y + B.x);
@@ -219,7 +236,7 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_c2r_rows(const cplx<T> *__re
             const int xs = ((a.flip_mask >> c) & 1u) ? (L - x) % L : x;
             const V z = buf[xs * lstr + (rr >> 1)];
             const T val = (rr & 1) ? z.y : z.x;
-            const int64_t gidx = row * a.nout + x;
+            const int64_t gidx = rout[rr] * a.nout + x;
             for (int d = 0; d < a.ndest[c]; ++d) write_dest<T>(a.dest[c][d], gidx, x, val);
             if (a.e8) {
 #pragma unroll
@@ -237,7 +254,7 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_c2r_rows(const cplx<T> *__re
             const int rr = idx / a.nout, x = idx - rr * a.nout;
             const int64_t row = row0 + rr;
             if (row >= a.nrows) continue;
-            const int64_t gidx = row * a.nout + x;
+            const int64_t gidx = rout[rr] * a.nout + x;
             const T *r0 = res + rr * a.nout + x;
             const int64_t cs = (int64_t)2 * NL * a.nout;
             V4 lo, hi;
@@ -313,7 +330,7 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_zconv(const cplx<T> *__restr
         V *dst = out + (int64_t)o * a.out_cstride;
         auto st_out = [&](int e, int l, const V &v) {
             const int col = col0 + l;
-            if (e < a.nz && col < a.ncols) dst[(int64_t)e * a.out_estride + col] = v;
+            if (e < a.nz && col < a.ncols) dst[(int64_t)e * a.out_estride + (int64_t)col * a.out_colstride] = v;
         };
         E::template run_io<V, NL, false, HALF>(buf, a.p, tw, -1, ld_mul, st_out);
     }
@@ -341,16 +358,30 @@ __global__ void __launch_bounds__(E::kLen * 3 * NLC / FFT_EPT) k_c2r_e8(const fl
     V *buf = tw + L;
     const int tid = threadIdx.x;
     const int64_t row0 = (int64_t)blockIdx.x * (2 * NLC);
+    __shared__ int64_t rin[2 * NLC], rout[2 * NLC];
+    for (int t = tid; t < 2 * NLC; t += nthreads) row_bases(a, row0 + t, rin[t], rout[t]);
+    const int64_t ies = a.zin ? a.zin_nz : 1;
     load_twiddles(tw, twg, L);
+    __syncthreads();
     for (int idx = tid; idx < NLT * L; idx += nthreads) {
-        const int c = idx / (NLC * L), rem = idx - c * (NLC * L);
-        const int line = rem / L, k = rem - line * L;
+        int c, line, k;
+        if (a.zin) {  // rows (adjacent z) fastest: coalesced reads of the kz-innermost spectra
+            k = idx / NLT;
+            const int rem = idx - k * NLT;
+            c = rem / NLC;
+            line = rem - c * NLC;
+        } else {
+            c = idx / (NLC * L);
+            const int rem = idx - c * (NLC * L);
+            line = rem / L;
+            k = rem - line * L;
+        }
         const V *src = in + (int64_t)a.e8_comp[c] * a.in_cstride;
         const int64_t ra = row0 + 2 * line, rb = ra + 1;
         const int kk = k <= half ? k : L - k;
         V A = mk<float>(0, 0), B = mk<float>(0, 0);
-        if (ra < a.nrows) A = src[ra * a.in_rstride + kk];
-        if (rb < a.nrows) B = src[rb * a.in_rstride + kk];
+        if (ra < a.nrows) A = src[rin[2 * line] + kk * ies];
+        if (rb < a.nrows) B = src[rin[2 * line + 1] + kk * ies];
         if (k == 0 || k == half) { A.y = 0; B.y = 0; }
         if (k > half) { A.y = -A.y; B.y = -B.y; }
         buf[k * lstr + c * NLC + line] = mk<float>(A.x - B.y, A.y + B.x);
@@ -376,7 +407,8 @@ __global__ void __launch_bounds__(E::kLen * 3 * NLC / FFT_EPT) k_c2r_e8(const fl
                 e1[c] = 0.f;
             }
         }
-        st_pair(g + 2 * (row * nout + x), make_float4(e0[0], e0[1], e0[2], 0.f), make_float4(e1[0], e1[1], e1[2], 0.f));
+        st_pair(g + 2 * (rout[rr] * nout + x), make_float4(e0[0], e0[1], e0[2], 0.f),
+                make_float4(e1[0], e1[1], e1[2], 0.f));
     }
 }
 

@@ -407,6 +407,7 @@ template <typename T> static int pipe_phi_opt(osc_ctx *c, const LGeom &g, const 
     za.ny = ny;
     za.in_estride = (int64_t)nxh * Ny;
     za.out_estride = (int64_t)nxh * Ny;
+    za.out_colstride = 1;
     za.out_cstride = (int64_t)nxh * Ny * nz;
     za.nout = nout;
     za.ng = 4;

@@ -433,7 +433,11 @@ int freespace_opt(osc_ctx *c, const FreeSpaceJob &j, const TIn *rho) {
     za.Ny = Ny;
     za.ny = ny;
     za.in_estride = (int64_t)nxh * Ny;
-    za.out_estride = (int64_t)nxh * Ny;
+    // the warp-per-column z pass writes its spectra kz-innermost ([o][b][ky][kx][z]); the
+    // inverse y and x passes then read them with adjacent z in adjacent lines
+    const bool zin = zconv_warp_ok(Nz, nz, (int)sizeof(T));
+    za.out_estride = zin ? 1 : (int64_t)nxh * Ny;
+    za.out_colstride = zin ? nz : 1;
     za.out_cstride = (int64_t)B * nxh * Ny * nz;
     za.nout = nout;
     za.img_phase_mul = nz - 1;
@@ -452,20 +456,31 @@ int freespace_opt(osc_ctx *c, const FreeSpaceJob &j, const TIn *rho) {
     li.sign = -1;
     li.in_len = Ny;
     li.out_len = ny;
-    li.in_pstride = (int64_t)nxh * Ny;
     li.in_zstride = (int64_t)B * nxh * Ny * nz;
-    li.out_pstride = (int64_t)nxh * ny;
     li.out_zstride = (int64_t)B * nxh * ny * nz;
+    if (zin) {  // lines (kx, z) with z fastest, members as planes
+        li.ncols = nxh * nz;
+        li.in_cstride = li.out_cstride = 1;
+        li.in_estride = li.out_estride = (int64_t)nxh * nz;
+        li.in_pstride = (int64_t)nxh * Ny * nz;
+        li.out_pstride = (int64_t)nxh * ny * nz;
+    } else {
+        li.in_pstride = (int64_t)nxh * Ny;
+        li.out_pstride = (int64_t)nxh * ny;
+    }
     {
         Launch L_(c, "fft_y_inv");
-        TRY(kerr(c, launch_lines<T>(X3, X4, li, B * nz, nout, false, twy, c->stream), "y inverse"));
+        TRY(kerr(c, launch_lines<T>(X3, X4, li, zin ? B : B * nz, nout, false, twy, c->stream), "y inverse"));
     }
     // x: half spectra -> real rows [0,nx), scattered to the outputs
     cr.p = px;
     cr.nout = nx;
     cr.nrows = (int64_t)B * ny * nz;
-    cr.in_rstride = nxh;
+    cr.in_rstride = zin ? (int64_t)nxh * nz : nxh;
     cr.in_cstride = (int64_t)B * nxh * ny * nz;
+    cr.zin = zin ? 1 : 0;
+    cr.zin_nz = nz;
+    cr.zin_ny = ny;
     cr.ncomp = nout;
     {
         Launch L_(c, "fft_x_c2r");

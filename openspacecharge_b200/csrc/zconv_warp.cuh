@@ -7,8 +7,9 @@
 // forward transform's last stage are exactly the inputs it owns in an inverse transform's
 // first stage: the forward spectrum stays in registers, the product with the cached Green
 // spectrum is formed in registers and fed straight into the inverse's first butterflies.
-// The inverse's last stage (window z < nz only) goes back to the warp buffer and the CTA
-// stores its W columns with coalesced writes.
+// The inverse's last stage (window z < nz only) is stored by the warp itself when the
+// output is kz-innermost (one contiguous column per warp), else it goes back to the warp
+// buffer and the CTA stores its W columns with coalesced writes.
 //
 // Warp buffers are padded by one element per sixteen (p = e + e/16) and are 2 mod 16
 // elements apart, which keeps the stride-R writes of the first stage, the unit-stride reads
@@ -266,6 +267,19 @@ __global__ void __launch_bounds__(W * 32, ZW_MINB) k_zconv_warp(const cplx<T> *_
         SL::load(wb, tw, -1, lane, v, false);
         SL::dft(v, -1);
         __syncwarp();
+        if (a.out_estride == 1) {  // kz-innermost output: this warp's column is contiguous
+            if (col0 + warp < a.ncols) {
+                V *dst = out + (int64_t)o * a.out_cstride + (int64_t)(col0 + warp) * a.out_colstride;
+#pragma unroll
+                for (int q = 0; q < Q; ++q) {
+                    const int j = lane + 32 * q;
+                    if (S0::full || j < NB)
+#pragma unroll
+                        for (int r = 0; r < RF / 2; ++r) dst[j + NB * r] = v[q][r];  // z = j + NB r < L/2
+                }
+            }
+            continue;  // wb is this warp's alone: the next output's first stage writes it
+        }
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
             const int j = lane + 32 * q;
@@ -278,7 +292,7 @@ __global__ void __launch_bounds__(W * 32, ZW_MINB) k_zconv_warp(const cplx<T> *_
         for (int idx = threadIdx.x; idx < W * a.nz; idx += W * 32) {
             const int e = idx / W, c = idx - e * W;
             const int col = col0 + c;
-            if (col < a.ncols) dst[(int64_t)e * a.out_estride + col] = wbufs[c * WB + wpad(e)];
+            if (col < a.ncols) dst[(int64_t)e * a.out_estride + (int64_t)col * a.out_colstride] = wbufs[c * WB + wpad(e)];
         }
         __syncthreads();
     }
