@@ -28,7 +28,7 @@ namespace osc {
 
 // Resident CTAs per SM the register allocation of k_zconv_warp is sized for.
 #ifndef ZW_MINB
-#define ZW_MINB 2
+#define ZW_MINB 3
 #endif
 
 
