@@ -137,6 +137,45 @@ int batch_fp32(osc_ctx *ctx, int nb, osc_bunch *bs, const double *x, const doubl
         max_g = std::max(max_g, 3 * B * (size_t)(g.n[0] + 1) * (g.n[1] + 1) * zp);
     }
     TRY(upload(ctx, "batch_args", ba.data(), sizeof(BunchArgs) * nb, (void **)&d_ba));
+    // corner-block arguments of every group's members and components, one upload
+    std::vector<CornerArgs> ca_all;
+    std::vector<size_t> ca_off;
+    for (auto &kv : groups) {
+        Group &g = kv.second;
+        const int B = (int)g.members.size();
+        const double off0[3] = {0, 0, 0};
+        ca_off.push_back(ca_all.size());
+        for (int comp = 1; comp <= 3; ++comp)
+            for (int i = 0; i < B; ++i) {
+                const osc_mesh3d &m = bs[g.members[i]].mesh;
+                ca_all.push_back(green_corner_args(g.n, m.delta, m.gamma, off0, comp));
+            }
+    }
+    CornerArgs *d_ca_all;
+    TRY(upload(ctx, "batch_corners", ca_all.data(), sizeof(CornerArgs) * ca_all.size(), (void **)&d_ca_all));
+    // grow the per-group workspaces to the largest group once (growing one synchronises)
+    {
+        size_t x1 = 0, x2 = 0, x3 = 0, x4 = 0, h = 0, hx = 0, hy = 0;
+        for (auto &kv : groups) {
+            const Group &g = kv.second;
+            const size_t B = g.members.size(), nx = g.n[0], ny = g.n[1], nz = g.n[2];
+            x1 = std::max(x1, B * (nx + 1) * ny * nz);
+            x2 = std::max(x2, B * (nx + 1) * 2 * ny * nz);
+            x3 = std::max(x3, 3 * B * (nx + 1) * 2 * ny * nz);
+            x4 = std::max(x4, 3 * B * (nx + 1) * ny * nz);
+            h = std::max(h, 3 * B * nx * ny * nz);
+            hx = std::max(hx, 3 * B * (nx + 1) * ny * nz);
+            hy = std::max(hy, 3 * B * (nx + 1) * (ny + 1) * nz);
+        }
+        void *p;
+        TRY(ws_get(ctx, "fs_x1", sizeof(float2) * x1, &p));
+        TRY(ws_get(ctx, "fs_x2", sizeof(float2) * x2, &p));
+        TRY(ws_get(ctx, "fs_x3", sizeof(float2) * x3, &p));
+        TRY(ws_get(ctx, "fs_x4", sizeof(float2) * x4, &p));
+        TRY(ws_get(ctx, "green_h", sizeof(double) * h, &p));
+        TRY(ws_get(ctx, "green_hx", sizeof(double) * hx, &p));
+        TRY(ws_get(ctx, "green_hy", sizeof(double) * hy, &p));
+    }
     // deposit every bunch into its quad grid
     float *quad, *rho, *e8, *gbuf;
     double *F;
@@ -155,6 +194,7 @@ int batch_fp32(osc_ctx *ctx, int nb, osc_bunch *bs, const double *x, const doubl
             return set_err(ctx, OSC_E_CUDA, "batch deposit");
     }
     // field of every group
+    size_t gidx = 0;
     for (auto &kv : groups) {
         Group &g = kv.second;
         const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
@@ -171,15 +211,7 @@ int batch_fp32(osc_ctx *ctx, int nb, osc_bunch *bs, const double *x, const doubl
         const int64_t fstride = (int64_t)(nx + 1) * (ny + 1) * (nz + 1);
         if (zinner) CK(cudaMemsetAsync(gbuf, 0, sizeof(float) * 3 * B * per, ctx->stream), "memset spectra");
         // Green spectra of the three E components of every member: members m = comp*B + i
-        std::vector<CornerArgs> ca(3 * B);
-        const double off0[3] = {0, 0, 0};
-        for (int comp = 1; comp <= 3; ++comp)
-            for (int i = 0; i < B; ++i) {
-                const osc_mesh3d &m = bs[g.members[i]].mesh;
-                ca[(comp - 1) * B + i] = green_corner_args(g.n, m.delta, m.gamma, off0, comp);
-            }
-        CornerArgs *d_ca;
-        TRY(upload(ctx, "batch_corners", ca.data(), sizeof(CornerArgs) * 3 * B, (void **)&d_ca));
+        const CornerArgs *d_ca = d_ca_all + ca_off[gidx++];
         {
             Launch L_(ctx, "green_corners");
             if (launch_igf_corners_batch(F, d_ca, 3 * B, fstride, fstride, ctx->stream))

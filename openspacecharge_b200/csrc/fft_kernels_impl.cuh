@@ -11,7 +11,10 @@
 // zeros (or, for the static engines, not read at all) and stores cover only the window.
 #pragma once
 #include <cstdio>
+#include <map>
+#include <mutex>
 #include <type_traits>
+#include <utility>
 
 #include "fft_kernels.cuh"
 #include "zconv_warp.cuh"
@@ -480,10 +483,26 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_sym_lines(const double *__re
 
 // ------------------------------------------------------------------------------------
 // Launchers.  Shared memory above 48 KB needs the opt-in attribute, set per kernel.
+// The attribute is set once per kernel, device and size (a lookup instead of a driver call
+// on every launch of the many small launches of a batch).
 template <typename K> inline int set_smem(K kern, size_t bytes) {
     if (bytes > 227 * 1024) return OSC_E_INVALID;
+    static std::mutex mu;
+    static std::map<std::pair<const void *, int>, size_t> done;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return OSC_E_CUDA;
+    const auto key = std::make_pair(reinterpret_cast<const void *>(kern), dev);
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = done.find(key);
+        if (it != done.end() && it->second >= bytes) return OSC_OK;
+    }
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    return e == cudaSuccess ? OSC_OK : OSC_E_CUDA;
+    if (e != cudaSuccess) return OSC_E_CUDA;
+    std::lock_guard<std::mutex> lk(mu);
+    size_t &v = done[key];
+    if (bytes > v) v = bytes;
+    return OSC_OK;
 }
 inline int launch_ok() { return cudaGetLastError() == cudaSuccess ? OSC_OK : OSC_E_CUDA; }
 
