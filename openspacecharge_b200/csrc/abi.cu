@@ -62,6 +62,8 @@ int osc_ctx_destroy(osc_ctx *ctx) {
     if (ctx->h_small) cudaFreeHost(ctx->h_small);
     if (ctx->d_partials) cudaFree(ctx->d_partials);
     if (ctx->h_fault) cudaFreeHost(ctx->h_fault);
+    for (auto s : ctx->aux) cudaStreamDestroy(s);
+    for (auto e : ctx->aux_ev) cudaEventDestroy(e);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return OSC_OK;

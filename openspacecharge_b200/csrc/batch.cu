@@ -33,6 +33,39 @@ int upload(osc_ctx *ctx, const char *name, const void *h, size_t bytes, void **d
     return h2d(ctx, *d, h, bytes);
 }
 
+constexpr int kSlots = 4;  // grid-shape groups solved concurrently on auxiliary streams
+
+// Creates the context's auxiliary streams and their events once (plus one event for the
+// main stream at index kSlots).
+int ensure_aux(osc_ctx *ctx) {
+    if ((int)ctx->aux.size() >= kSlots) return OSC_OK;
+    while ((int)ctx->aux.size() < kSlots) {
+        cudaStream_t s;
+        CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "aux stream");
+        ctx->aux.push_back(s);
+    }
+    while ((int)ctx->aux_ev.size() < kSlots + 1) {
+        cudaEvent_t e;
+        CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "aux event");
+        ctx->aux_ev.push_back(e);
+    }
+    return OSC_OK;
+}
+
+// Issues work on auxiliary slot `slot` (1-based) for its lifetime; restores the main stream.
+struct SlotGuard {
+    osc_ctx *c;
+    cudaStream_t main;
+    SlotGuard(osc_ctx *ctx, int slot) : c(ctx), main(ctx->stream) {
+        c->stream = c->aux[slot - 1];
+        c->ws_slot = slot;
+    }
+    ~SlotGuard() {
+        c->stream = main;
+        c->ws_slot = 0;
+    }
+};
+
 int check_bunches(osc_ctx *ctx, int nb, const osc_bunch *bs, const double *x, const double *y, const double *z,
                   const double *E) {
     if (nb <= 0 || !bs) return bad(ctx, "batch needs at least one bunch");
@@ -167,24 +200,27 @@ int batch_fp32(osc_ctx *ctx, int nb, osc_bunch *bs, const double *x, const doubl
             hx = std::max(hx, 3 * B * (nx + 1) * ny * nz);
             hy = std::max(hy, 3 * B * (nx + 1) * (ny + 1) * nz);
         }
-        void *p;
-        TRY(ws_get(ctx, "fs_x1", sizeof(float2) * x1, &p));
-        TRY(ws_get(ctx, "fs_x2", sizeof(float2) * x2, &p));
-        TRY(ws_get(ctx, "fs_x3", sizeof(float2) * x3, &p));
-        TRY(ws_get(ctx, "fs_x4", sizeof(float2) * x4, &p));
-        TRY(ws_get(ctx, "green_h", sizeof(double) * h, &p));
-        TRY(ws_get(ctx, "green_hx", sizeof(double) * hx, &p));
-        TRY(ws_get(ctx, "green_hy", sizeof(double) * hy, &p));
+        TRY(ensure_aux(ctx));
+        for (int slot = 1; slot <= kSlots; ++slot) {
+            SlotGuard sg(ctx, slot);
+            void *p;
+            TRY(ws_get(ctx, "fs_x1", sizeof(float2) * x1, &p));
+            TRY(ws_get(ctx, "fs_x2", sizeof(float2) * x2, &p));
+            TRY(ws_get(ctx, "fs_x3", sizeof(float2) * x3, &p));
+            TRY(ws_get(ctx, "fs_x4", sizeof(float2) * x4, &p));
+            TRY(ws_get(ctx, "green_h", sizeof(double) * h, &p));
+            TRY(ws_get(ctx, "green_hx", sizeof(double) * hx, &p));
+            TRY(ws_get(ctx, "green_hy", sizeof(double) * hy, &p));
+            TRY(ws_get(ctx, "batch_F", sizeof(double) * max_f, &p));
+            TRY(ws_get(ctx, "batch_green", sizeof(float) * max_g, &p));
+        }
     }
     // deposit every bunch into its quad grid
-    float *quad, *rho, *e8, *gbuf;
-    double *F;
+    float *quad, *rho, *e8;
     unsigned long long *cnt;
     TRY(ws_get(ctx, "batch_quad", sizeof(float) * 4 * (size_t)nodes, (void **)&quad));
     TRY(ws_get(ctx, "batch_rho", sizeof(float) * (size_t)nodes, (void **)&rho));
     TRY(ws_get(ctx, "batch_e8", sizeof(float) * 8 * (size_t)nodes, (void **)&e8));
-    TRY(ws_get(ctx, "batch_F", sizeof(double) * max_f, (void **)&F));
-    TRY(ws_get(ctx, "batch_green", sizeof(float) * max_g, (void **)&gbuf));
     TRY(ws_get(ctx, "batch_cnt", sizeof(unsigned long long) * 4 * (size_t)nb, (void **)&cnt));
     CK(cudaMemsetAsync(quad, 0, sizeof(float) * 4 * (size_t)nodes, ctx->stream), "memset quad");
     CK(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * 4 * (size_t)nb, ctx->stream), "memset counters");
@@ -193,10 +229,18 @@ int batch_fp32(osc_ctx *ctx, int nb, osc_bunch *bs, const double *x, const doubl
         if (launch_batch_deposit_quad(d_ba, d_jobs, njobs, quad, cnt, ctx->stream))
             return set_err(ctx, OSC_E_CUDA, "batch deposit");
     }
-    // field of every group
+    // field of every group: groups of different shapes are independent, so they run on
+    // kSlots auxiliary streams (each with its own workspaces) after the deposit
+    CK(cudaEventRecord(ctx->aux_ev[kSlots], ctx->stream), "record deposit");
+    for (int s2 = 0; s2 < kSlots; ++s2) CK(cudaStreamWaitEvent(ctx->aux[s2], ctx->aux_ev[kSlots], 0), "wait deposit");
     size_t gidx = 0;
     for (auto &kv : groups) {
         Group &g = kv.second;
+        SlotGuard sg(ctx, (int)(gidx % kSlots) + 1);
+        float *gbuf;
+        double *F;
+        TRY(ws_get(ctx, "batch_F", sizeof(double) * max_f, (void **)&F));
+        TRY(ws_get(ctx, "batch_green", sizeof(float) * max_g, (void **)&gbuf));
         const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
         const int B = (int)g.members.size();
         const int64_t N = (int64_t)nx * ny * nz;
@@ -246,6 +290,10 @@ int batch_fp32(osc_ctx *ctx, int nb, osc_bunch *bs, const double *x, const doubl
         j.g_bstride = per;
         TRY(freespace_opt<float, float>(ctx, j, rho + g.node0));
         (void)N;
+    }
+    for (int s2 = 0; s2 < kSlots; ++s2) {
+        CK(cudaEventRecord(ctx->aux_ev[s2], ctx->aux[s2]), "record group");
+        CK(cudaStreamWaitEvent(ctx->stream, ctx->aux_ev[s2], 0), "wait groups");
     }
     {
         Launch L_(ctx, "batch_interp");

@@ -24,7 +24,8 @@ int cuda_check(osc_ctx *c, cudaError_t e, const char *what) {
 }
 
 int ws_get(osc_ctx *c, const char *name, size_t bytes, void **out) {
-    DevBuf &b = c->ws[name];
+    // work running on an auxiliary stream slot gets its own copy of every workspace
+    DevBuf &b = c->ws_slot ? c->ws[std::string(name) + "#" + std::to_string(c->ws_slot)] : c->ws[name];
     if (bytes == 0) bytes = 16;
     if (b.bytes < bytes) {
         if (b.p) {

@@ -55,6 +55,11 @@ struct osc_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t own_stream = nullptr;
+    // auxiliary streams for independent work inside one call (batched bunches of different
+    // grid shapes); ws_slot != 0 while work is issued on aux[ws_slot - 1]
+    std::vector<cudaStream_t> aux;
+    std::vector<cudaEvent_t> aux_ev;
+    int ws_slot = 0;
     std::string err;
     // options
     int precision = 0;
