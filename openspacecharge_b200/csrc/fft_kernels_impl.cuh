@@ -34,9 +34,9 @@ bool make_fft_plan(int L, FFTPlan &p) {
     while (m % 5 == 0) { p.radix[p.nst++] = 5; m /= 5; }
     return m == 1 && p.nst <= FFT_MAX_STAGES;
 }
-// The warp-per-column z pass holds a column's spectrum in registers: FP32 only.
+// The warp-per-column z pass (FP32 and FP64) for the lengths of the warp registry.
 bool zconv_warp_ok(int L, int nz, int elem_bytes) {
-    if (elem_bytes != 4 || 2 * nz != L) return false;
+    if ((elem_bytes != 4 && elem_bytes != 8) || 2 * nz != L) return false;
     return dispatch_warp_len(L, [](auto eng) -> int { return decltype(eng)::kLen > 0 ? 1 : 0; }) != 0;
 }
 #endif
@@ -220,7 +220,14 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_c2r_rows(const cplx<T> *__re
     for (int c = 0; c < a.ncomp; ++c) {
         const V *src = in + (int64_t)c * a.in_cstride;
         for (int idx = tid; idx < NL * L; idx += nthreads) {
-            const int line = idx / L, k = idx - line * L;
+            int line, k;
+            if (a.zin) {  // adjacent lines (adjacent z) fastest for the kz-innermost spectra
+                k = idx / NL;
+                line = idx - k * NL;
+            } else {
+                line = idx / L;
+                k = idx - line * L;
+            }
             const int64_t ra = row0 + 2 * line, rb = ra + 1;
             const int kk = k <= half ? k : L - k;
             V A = mk<T>(0, 0), B = mk<T>(0, 0);
@@ -670,7 +677,7 @@ inline int launch_zconv_warp_k(const cplx<T> *in, cplx<T> *out, const ZConvArgs 
 template <typename T, int MODE, int L, int... Rs>
 inline int launch_zconv_warp(WarpFft<L, Rs...>, const cplx<T> *in, cplx<T> *out, const ZConvArgs &a,
                              const TwPair<cplx<T>> &tw, cudaStream_t st) {
-    return launch_zconv_warp_k<T, 8, MODE, L, Rs...>(in, out, a, tw, st);
+    return launch_zconv_warp_k<T, zw_warps<T>(), MODE, L, Rs...>(in, out, a, tw, st);
 }
 
 // Staged Green columns need real spectra, even/odd in z, one common 16-byte column pitch.
@@ -684,7 +691,7 @@ template <typename T> inline bool zconv_can_stage(const ZConvArgs &a) {
         if (!g.real_valued || !g.sym_z || !g.zinner || g.zpitch != zp || g.dimz > zp) return false;
         if (reinterpret_cast<uintptr_t>(g.data) % 16) return false;
     }
-    return zconv_warp_smem<T>(a.p.L, 8, ZW_STAGED, a.nout, zp) <= 100 * 1024;
+    return zconv_warp_smem<T>(a.p.L, zw_warps<T>(), ZW_STAGED, a.nout, zp) <= 100 * 1024;
 }
 
 template <typename T>
@@ -700,7 +707,7 @@ int launch_zconv(const cplx<T> *in, cplx<T> *out, const ZConvArgs &a, const TwPa
         const bool staged = !img && zconv_can_stage<T>(a);
         return dispatch_warp_len(L, [&](auto eng) -> int {
             using E = decltype(eng);
-            if constexpr (E::kLen > 0 && sizeof(T) == 4) {
+            if constexpr (E::kLen > 0) {
                 if (img) return launch_zconv_warp<T, ZW_IMAGE>(eng, in, out, a, tw, st);
                 if (staged) return launch_zconv_warp<T, ZW_STAGED>(eng, in, out, a, tw, st);
                 return launch_zconv_warp<T, ZW_DIRECT>(eng, in, out, a, tw, st);

@@ -26,10 +26,11 @@
 
 namespace osc {
 
-// Resident CTAs per SM the register allocation of k_zconv_warp is sized for.
-#ifndef ZW_MINB
-#define ZW_MINB 3
-#endif
+// Warps per CTA and resident CTAs per SM the register allocation of k_zconv_warp is sized
+// for: FP32 8 warps x 3 CTAs (<= 85 registers); FP64 holds twice the bytes per value, 4
+// warps x 2 CTAs.
+template <typename T> constexpr int zw_warps() { return sizeof(T) == 4 ? 8 : 4; }
+template <typename T> constexpr int zw_minb() { return sizeof(T) == 4 ? 3 : 2; }
 
 
 __device__ __forceinline__ int wpad(int e) { return e + (e >> 4); }
@@ -116,7 +117,7 @@ constexpr int ZW_IMAGE = 1;   // as 0, plus the mirrored-image term
 constexpr int ZW_STAGED = 2;  // real, z-symmetric spectra staged in shared memory by bulk copies
 
 template <typename T, int W, int MODE, int L, int... Rs>
-__global__ void __launch_bounds__(W * 32, ZW_MINB) k_zconv_warp(const cplx<T> *__restrict__ in, cplx<T> *__restrict__ out,
+__global__ void __launch_bounds__(W * 32, zw_minb<T>()) k_zconv_warp(const cplx<T> *__restrict__ in, cplx<T> *__restrict__ out,
                                                        ZConvArgs a, const cplx<T> *__restrict__ twg,
                                                        const cplx<T> *__restrict__ tw_rt) {
     typedef cplx<T> V;
