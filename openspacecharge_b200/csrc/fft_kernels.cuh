@@ -55,6 +55,7 @@ struct C2RArgs {
     unsigned flip_mask;   // bit c: component c is read at x -> (L-x) mod L (index flip)
     void *e8;             // optional x-pair grid vec4<T>[N][2] filled from components e8_comp
     int e8_comp[3];       // components giving (Ex, Ey, Ez) of the x-pair grid
+    int e8_node;          // 1: e8 is a plain node grid vec4<T>[N] (Ex, Ey, Ez, 0) instead
     int ndest[MAX_OUT];
     OutDest dest[MAX_OUT][MAX_DEST];
     // zin != 0: the input spectra are kz-innermost, [c][b][y][kx][z] with zin_nz planes per

@@ -280,8 +280,12 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_c2r_rows(const cplx<T> *__re
                 hi.x = hi.y = hi.z = (T)0;
             }
             hi.w = (T)0;
-            g[2 * gidx] = lo;
-            g[2 * gidx + 1] = hi;
+            if (a.e8_node) {
+                g[gidx] = lo;
+            } else {
+                g[2 * gidx] = lo;
+                g[2 * gidx + 1] = hi;
+            }
         }
     }
 }
@@ -355,12 +359,19 @@ __device__ __forceinline__ void st_pair(float4 *p, const float4 &lo, const float
                  "f"(lo.w), "f"(hi.x), "f"(hi.y), "f"(hi.z), "f"(hi.w)
                  : "memory");
 }
-template <class E> constexpr int c2r_e8_nlc() { return E::kLen <= 128 ? 16 : (E::kLen <= 256 ? 8 : 4); }
+__device__ __forceinline__ void st_node(double4 *p, double x, double y, double z) {
+    asm volatile("st.global.v4.f64 [%0], {%1,%2,%3,%4};" ::"l"(p), "d"(x), "d"(y), "d"(z), "d"(0.0) : "memory");
+}
+template <typename T, class E> constexpr int c2r_e8_nlc() {
+    return (E::kLen <= 128 ? 16 : (E::kLen <= 256 ? 8 : 4)) / (sizeof(T) == 8 ? 2 : 1);
+}
 
-template <int NLC, class E>
-__global__ void __launch_bounds__(E::kLen * 3 * NLC / FFT_EPT) k_c2r_e8(const float2 *__restrict__ in, C2RArgs a,
-                                                                      const float2 *__restrict__ twg) {
-    typedef float2 V;
+// FP32: x-pair nodes (E(x), E(x+1)) with one 256-bit store; FP64: nodes (Ex, Ey, Ez, 0)
+// with one 256-bit store.
+template <typename T, int NLC, class E>
+__global__ void __launch_bounds__(E::kLen * 3 * NLC / FFT_EPT) k_c2r_e8(const cplx<T> *__restrict__ in, C2RArgs a,
+                                                                      const cplx<T> *__restrict__ twg) {
+    typedef cplx<T> V;
     constexpr int L = E::kLen, NLT = 3 * NLC, lstr = NLT + 1, half = L / 2, nout = L / 2;
     constexpr int nthreads = L * NLT / FFT_EPT;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -389,36 +400,41 @@ __global__ void __launch_bounds__(E::kLen * 3 * NLC / FFT_EPT) k_c2r_e8(const fl
         const V *src = in + (int64_t)a.e8_comp[c] * a.in_cstride;
         const int64_t ra = row0 + 2 * line, rb = ra + 1;
         const int kk = k <= half ? k : L - k;
-        V A = mk<float>(0, 0), B = mk<float>(0, 0);
+        V A = mk<T>(0, 0), B = mk<T>(0, 0);
         if (ra < a.nrows) A = src[rin[2 * line] + kk * ies];
         if (rb < a.nrows) B = src[rin[2 * line + 1] + kk * ies];
         if (k == 0 || k == half) { A.y = 0; B.y = 0; }
         if (k > half) { A.y = -A.y; B.y = -B.y; }
-        buf[k * lstr + c * NLC + line] = mk<float>(A.x - B.y, A.y + B.x);
+        buf[k * lstr + c * NLC + line] = mk<T>(A.x - B.y, A.y + B.x);
     }
     __syncthreads();
     E::template run<V, NLT, false, true>(buf, a.p, tw, -1);
-    float4 *g = reinterpret_cast<float4 *>(a.e8);
     for (int idx = tid; idx < 2 * NLC * nout; idx += nthreads) {
         const int rr = idx / nout, x = idx - rr * nout;
         const int64_t row = row0 + rr;
         if (row >= a.nrows) continue;
         const int ln = rr >> 1;
         const bool odd = rr & 1;
-        float e0[3], e1[3];
+        T e0[3], e1[3];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             const V z0 = buf[x * lstr + c * NLC + ln];
             e0[c] = odd ? z0.y : z0.x;
-            if (x + 1 < nout) {
-                const V z1 = buf[(x + 1) * lstr + c * NLC + ln];
-                e1[c] = odd ? z1.y : z1.x;
-            } else {
-                e1[c] = 0.f;
+            if constexpr (sizeof(T) == 4) {
+                if (x + 1 < nout) {
+                    const V z1 = buf[(x + 1) * lstr + c * NLC + ln];
+                    e1[c] = odd ? z1.y : z1.x;
+                } else {
+                    e1[c] = 0;
+                }
             }
         }
-        st_pair(g + 2 * (rout[rr] * nout + x), make_float4(e0[0], e0[1], e0[2], 0.f),
-                make_float4(e1[0], e1[1], e1[2], 0.f));
+        if constexpr (sizeof(T) == 4) {
+            st_pair(reinterpret_cast<float4 *>(a.e8) + 2 * (rout[rr] * nout + x),
+                    make_float4(e0[0], e0[1], e0[2], 0.f), make_float4(e1[0], e1[1], e1[2], 0.f));
+        } else {
+            st_node(reinterpret_cast<double4 *>(a.e8) + rout[rr] * nout + x, e0[0], e0[1], e0[2]);
+        }
     }
 }
 
@@ -614,7 +630,8 @@ int launch_r2c_rows(const TIn *in, cplx<T> *out, const R2CArgs &a, const TwPair<
 template <typename T>
 int launch_c2r_rows(const cplx<T> *in, const C2RArgs &a, const TwPair<cplx<T>> &tw, cudaStream_t st) {
     const int L = a.p.L;
-    if constexpr (sizeof(T) == 4) {
+    // FP32 x-pairs or FP64 nodes: the specialised kernel; other combinations: generic
+    if (a.e8 && (a.e8_node != 0) == (sizeof(T) == 8)) {
         bool e8_only = a.e8 && a.ncomp == 3 && a.flip_mask == 0 && 2 * a.nout == L &&
                        reinterpret_cast<uintptr_t>(a.e8) % 32 == 0;
         for (int c = 0; c < a.ncomp && e8_only; ++c) e8_only = a.ndest[c] == 0;
@@ -622,14 +639,13 @@ int launch_c2r_rows(const cplx<T> *in, const C2RArgs &a, const TwPair<cplx<T>> &
             const int rc = dispatch_fft_len(L, [&](auto eng) -> int {
                 using E = decltype(eng);
                 if constexpr (E::kLen > 0) {
-                    constexpr int NLC = c2r_e8_nlc<E>();
+                    constexpr int NLC = c2r_e8_nlc<T, E>();
                     constexpr int nt = E::kLen * 3 * NLC / FFT_EPT;
-                    const size_t sm = sizeof(float2) * ((size_t)E::kLen + (size_t)E::kLen * (3 * NLC + 1));
-                    auto kern = k_c2r_e8<NLC, E>;
+                    const size_t sm = sizeof(cplx<T>) * ((size_t)E::kLen + (size_t)E::kLen * (3 * NLC + 1));
+                    auto kern = k_c2r_e8<T, NLC, E>;
                     int r = set_smem(kern, sm);
                     if (r) return r;
-                    kern<<<(unsigned)ceil_div(a.nrows, 2 * NLC), nt, sm, st>>>(
-                        reinterpret_cast<const float2 *>(in), a, reinterpret_cast<const float2 *>(tw.st));
+                    kern<<<(unsigned)ceil_div(a.nrows, 2 * NLC), nt, sm, st>>>(in, a, tw.st);
                     return launch_ok();
                 }
                 return -1;  // no static engine: generic kernel

@@ -225,10 +225,15 @@ __device__ __forceinline__ bool locate(const InterpArgs &a, double x, double y, 
 
 template <typename T>
 __device__ __forceinline__ void load_node(const vec4<T> *g, int64_t n, double &a, double &b, double &c) {
-    const vec4<T> v = g[n];
-    a = (double)v.x;
-    b = (double)v.y;
-    c = (double)v.z;
+    if constexpr (sizeof(T) == 8) {  // one 256-bit read-only load per node
+        double w;
+        asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(a), "=d"(b), "=d"(c), "=d"(w) : "l"(g + n));
+    } else {
+        const vec4<T> v = __ldg(g + n);
+        a = (double)v.x;
+        b = (double)v.y;
+        c = (double)v.z;
+    }
 }
 
 template <typename T, typename TO>

@@ -361,13 +361,10 @@ int freespace_opt(osc_ctx *c, const FreeSpaceJob &j, const TIn *rho) {
             const int o = add_out(q + 1, 1.0);
             if (j.Eacc) add_dest(o, j.Eacc, 3, 0, j.acc_coef);
             if (j.E) add_dest(o, j.E + q * N, 1, 0, 1.0);
-            if (j.E4) {
-                if (j.e4_pairs) {  // staged in the x epilogue and written as whole pairs
-                    cr.e8 = j.E4;
-                    cr.e8_comp[q] = o;
-                } else {
-                    add_dest(o, j.E4, 0, q, 1.0);
-                }
+            if (j.E4) {  // staged in the x epilogue and written as whole nodes or pairs
+                cr.e8 = j.E4;
+                cr.e8_comp[q] = o;
+                cr.e8_node = j.e4_pairs ? 0 : 1;
             }
             if (j.calc_b && j.B && !j.at_cathode) {
                 if (q == 1) add_dest(o, j.B, 1, 0, -j.bcoef);
