@@ -161,6 +161,22 @@ def kernel_bytes(nx, ny, nz, npart, at_cathode=False):
     }
 
 
+TRAFFIC_TABLE = os.path.join(ROOT, "profiles", "traffic_fp32_128x128x256.md")
+
+
+def profiled_traffic(label):
+    """DRAM bytes per launch of one kernel of the headline workload, from the committed ncu
+    table (None when the table or the kernel is missing)."""
+    try:
+        for line in open(TRAFFIC_TABLE):
+            cells = [c.strip() for c in line.strip().strip("|").split("|")]
+            if len(cells) >= 5 and cells[0] == label:
+                return int(cells[4])
+    except (OSError, ValueError):
+        pass
+    return None
+
+
 def run_ours(args, ws, rank, local, dist):
     import torch
     import openspacecharge_b200 as osc
@@ -279,9 +295,12 @@ def run_ours(args, ws, rank, local, dist):
     roof = None
     if dom:
         ach = kernels[dom]["gbs"]
+        traffic = profiled_traffic(dom) if (tuple(grid) == GRID and npart == NPART) else None
         roof = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
                 "frac": ach / hbm_peak, "peak_source": peak_src + " (MEASURED_PEAKS.json hbm_gbs)",
-                "traffic": None, "alg_bytes_per_launch": kb[dom]}
+                "traffic": traffic, "alg_bytes_per_launch": kb[dom],
+                "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of this kernel on this "
+                                   "workload, profiles/traffic_fp32_128x128x256.md") if traffic else None}
     step_bytes = sum(kb.values())
     step_gbs = step_bytes / (ms32 * 1e-3) / 1e9
 
