@@ -83,7 +83,8 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_lines(const cplx<T> *in, cpl
         E::template run_io<V, NL, MODE == 1, MODE == 2>(buf, a.p, tw, a.sign, ld, st);
         return;
     }
-    const int ld_len = (E::kLen > 0 && MODE == 1) ? a.in_len : L;  // the static first stage skips zeros
+    // the static first stage skips the zero half (MODE 1 launches only with in_len == L/2)
+    const int ld_len = (E::kLen > 0 && MODE == 1) ? E::kLen / 2 : L;
     const int nld = NL * ld_len;
     for (int idx = tid; idx < nld; idx += nthreads) {
         int e, c;
@@ -122,7 +123,7 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_r2c_rows(const TIn *__restri
     const int nthreads = blockDim.x, tid = threadIdx.x;
     const int64_t row0 = (int64_t)blockIdx.x * (2 * NL);
     load_twiddles(tw, twg, L);
-    const int ld_len = (E::kLen > 0 && HIN) ? a.nin : L;
+    const int ld_len = (E::kLen > 0 && HIN) ? E::kLen / 2 : L;  // HIN launches only with nin == L/2
     for (int idx = tid; idx < 2 * NL * ld_len; idx += nthreads) {
         const int rr = idx / ld_len, e = idx - rr * ld_len;
         const int64_t row = row0 + rr;

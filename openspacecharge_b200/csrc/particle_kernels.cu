@@ -12,11 +12,26 @@ static inline unsigned nblocks(int64_t n, int bs, int64_t cap = (1 << 20)) {
 }
 #define GRID_STRIDE(i, n) for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (n); i += (int64_t)gridDim.x * blockDim.x)
 
-__device__ __forceinline__ void atomic_add_t(float *p, double v, double) { atomicAdd(p, (float)v); }
-__device__ __forceinline__ void atomic_add_t(double *p, double v, double) { atomicAdd(p, v); }
+// Deposits add without reading the old value back: reductions (red), not atomics that
+// return a value, so a thread never waits for the L2's answer.
+__device__ __forceinline__ void red_add(float *p, float v) {
+    asm volatile("red.global.add.f32 [%0], %1;" ::"l"(p), "f"(v) : "memory");
+}
+__device__ __forceinline__ void red_add(double *p, double v) {
+    asm volatile("red.global.add.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
+}
+__device__ __forceinline__ void red_add(unsigned long long *p, unsigned long long v) {
+    asm volatile("red.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ void red_add(float4 *p, float4 v) {
+    asm volatile("red.global.add.v4.f32 [%0], {%1,%2,%3,%4};" ::"l"(p), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w)
+                 : "memory");
+}
+__device__ __forceinline__ void atomic_add_t(float *p, double v, double) { red_add(p, (float)v); }
+__device__ __forceinline__ void atomic_add_t(double *p, double v, double) { red_add(p, v); }
 // Fixed point: two's-complement addition of the rounded contribution (exact, associative).
 __device__ __forceinline__ void atomic_add_t(unsigned long long *p, double v, double scale) {
-    atomicAdd(p, (unsigned long long)__double2ll_rn(v * scale));
+    red_add(p, (unsigned long long)__double2ll_rn(v * scale));
 }
 
 // Warp-aggregated counter increment.
@@ -133,9 +148,9 @@ __device__ __forceinline__ int quad_one(const DepositArgs &a, float4 *__restrict
     const double lo = gh * c, hi = omgh * c;
     const int i = (int)fx - a.nlo[0], j = (int)fy - a.nlo[1], k = (int)fz - a.nlo[2];
     float4 *q0 = quad + ((int64_t)i + (int64_t)a.nx * j + plane * k);
-    atomicAdd(q0, make_float4((float)(ab * de * lo), (float)(omab * de * lo), (float)(ab * omde * lo),
+    red_add(q0, make_float4((float)(ab * de * lo), (float)(omab * de * lo), (float)(ab * omde * lo),
                               (float)(omab * omde * lo)));
-    atomicAdd(q0 + plane, make_float4((float)(ab * de * hi), (float)(omab * de * hi), (float)(ab * omde * hi),
+    red_add(q0 + plane, make_float4((float)(ab * de * hi), (float)(omab * de * hi), (float)(ab * omde * hi),
                                       (float)(omab * omde * hi)));
     return 0;
 }
@@ -634,7 +649,7 @@ __global__ void __launch_bounds__(256) k_deposit_vec3(DepositArgs a, const doubl
             const double gc = g[3 * m + c];
             if (gc == 0.0) continue;
 #pragma unroll
-            for (int t = 0; t < 8; ++t) atomicAdd(acc + c * N + off[t], w[t] * gc);
+            for (int t = 0; t < 8; ++t) red_add(acc + c * N + off[t], w[t] * gc);
         }
     }
 }
