@@ -614,12 +614,7 @@ def run_pipe(args, ws, rank, local, dist):
     ctx = osc.Context(local)
     stream = torch.cuda.Stream(device=dev)
     ctx.set_stream(stream.cuda_stream)
-    N = n[0] * n[1] * n[2]
     tx, ty, tz = (torch.from_numpy(v).to(dev) for v in (x, y, z))
-    rho = torch.empty(N, dtype=torch.float64, device=dev)
-    phi = torch.empty_like(rho)
-    E = torch.empty(3 * N, dtype=torch.float64, device=dev)
-    B = torch.empty_like(E)
     Ep = torch.empty((PIPE_NP, 3), dtype=torch.float64, device=dev)
     m = mesh.to_c()
     tc = ctypes.c_double(QTOT)
@@ -630,11 +625,8 @@ def run_pipe(args, ws, rank, local, dist):
     green_s = time.perf_counter() - t0
 
     def step(prec, out=Ep):
-        ctx.call("osc_deposit_particles_dev", ctypes.c_int64(PIPE_NP), P(tx), P(ty), P(tz), None, ctypes.byref(tc),
-                 0, ctypes.byref(m), P(rho), None)
-        ctx.call("osc_space_charge_rectpipe_dev", ctypes.byref(m), P(rho), a, b, 0, 1, prec, P(phi), P(E), P(B))
-        ctx.call("osc_interpolate_field_dev", ctypes.byref(m), P(E), None, ctypes.c_int64(PIPE_NP), P(tx), P(ty),
-                 P(tz), P(out), None, None)
+        ctx.call("osc_space_charge_step_rectpipe_dev", ctypes.byref(m), ctypes.c_int64(PIPE_NP), P(tx), P(ty),
+                 P(tz), None, ctypes.byref(tc), a, b, prec, P(out), None)
 
     for _ in range(max(3, args.warmup)):
         step(osc.PREC_FP32)
@@ -666,9 +658,10 @@ def run_pipe(args, ws, rank, local, dist):
             "metric": PIPE_METRIC, "value": ws * 1000.0 / ms, "unit": "solves/s", "n_gpus": ws, "steps": k,
             "warmup": max(3, args.warmup), "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "rectangular pipe 20x10 mm: deposit + pipe potential (FP32 convolution with the four "
-                                   "cached FP64 mode-sum Green spectra) + FD E and B + gather, 64x64x128 grid spanning "
-                                   "the walls, 4e6 particles sigma=(2,1,1) mm centred at (3,-1) mm, pipe rejection",
+            "config": {"workload": "rectangular pipe 20x10 mm, fused step osc_space_charge_step_rectpipe_dev: deposit + "
+                                   "pipe potential (FP32 convolution with the four cached FP64 mode-sum Green "
+                                   "spectra) + FD E and B + gather, 64x64x128 grid spanning the walls, 4e6 particles "
+                                   "sigma=(2,1,1) mm centred at (3,-1) mm, pipe rejection",
                        "grid": list(n), "particles": PIPE_NP},
             "fp64_plain": {"ms_per_step": ms64, "speedup_fp32_over_fp64": ms64 / ms},
             "rel_err_vs_fp64": err, "green_build_s": green_s, "clocks": clk.summary()}))

@@ -193,6 +193,17 @@ OSC_API int osc_space_charge_rectpipe_dev(osc_ctx *ctx, const osc_mesh3d *mesh, 
                                           double apipe, double bpipe, int direct_field_calc,
                                           int integrated_green_function, int precision, double *d_phi,
                                           double *d_efield, double *d_bfield);
+/* Fused step in the pipe (device pointers): deposit of the np particles (charges q, or
+ * total_charge/np each), pipe potential and its finite-difference E and B
+ * (space_charge_rectpipe with direct_field_calc = 0) and the gather of E (and B when B is
+ * non-NULL) at every particle, as the reference's test program does with
+ * depose_rho_scalar, space_charge_rectpipe and interpolate_field (code/test_opensc.f90:156,
+ * :203-216, :247).  The mesh is used as given (the pipe mesh spans the walls) and needs its
+ * Green spectra first (osc_rectpipe_green or osc_read_rectpipe_grn).  E, B are [np][3]. */
+OSC_API int osc_space_charge_step_rectpipe_dev(osc_ctx *ctx, const osc_mesh3d *mesh, int64_t np, const double *d_x,
+                                               const double *d_y, const double *d_z, const double *d_q,
+                                               const double *total_charge, double apipe, double bpipe,
+                                               int precision, double *d_E, double *d_B);
 /* Replace osc_write_rectpipe_grn / osc_read_rectpipe_grn (core:825-870): a header record
  * and cgrn1..4 as complex128, Fortran unformatted sequential layout. */
 OSC_API int osc_write_rectpipe_grn(osc_ctx *ctx, const char *path, double apipe, double bpipe,

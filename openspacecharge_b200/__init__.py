@@ -10,7 +10,7 @@ from .mesh import (Mesh3D, batch_space_charge_step, batch_space_charge_step_dev,
                    interpolate_field, osc_freespace_solver2, osc_read_rectpipe_grn,
                    osc_rectpipe_green, osc_write_rectpipe_grn, space_charge_3d,
                    space_charge_cathodeimages, space_charge_freespace, space_charge_rectpipe,
-                   space_charge_step, space_charge_step_dev, write_lines, write_plane,
+                   space_charge_step, space_charge_step_dev, space_charge_step_rectpipe_dev, write_lines, write_plane,
                    format_1pe14_7)
 from . import bunch
 

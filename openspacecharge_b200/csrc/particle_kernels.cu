@@ -736,4 +736,26 @@ int launch_vjp_particles(const InterpArgs &ia, const DepositArgs &da, const doub
     return ok();
 }
 
+// ------------------------------------------------------------------------------------
+// E planes [3][N] (f64) -> x-pair grid (f32): node n holds (Ex,Ey,Ez,0) at n and at n+1, the
+// last node of a row (E(n), 0); one 256-bit store per node.
+__global__ void __launch_bounds__(256) k_planes_to_pairs(const double *__restrict__ E, float4 *__restrict__ e8,
+                                                         int nx, int64_t n) {
+    GRID_STRIDE(i, n) {
+        const int x = (int)(i % nx);
+        const bool last = x == nx - 1;
+        const float4 lo = make_float4((float)E[i], (float)E[i + n], (float)E[i + 2 * n], 0.f);
+        const float4 hi = last ? make_float4(0.f, 0.f, 0.f, 0.f)
+                               : make_float4((float)E[i + 1], (float)E[i + 1 + n], (float)E[i + 1 + 2 * n], 0.f);
+        asm volatile("st.global.v8.f32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(e8 + 2 * i), "f"(lo.x), "f"(lo.y),
+                     "f"(lo.z), "f"(lo.w), "f"(hi.x), "f"(hi.y), "f"(hi.z), "f"(hi.w)
+                     : "memory");
+    }
+}
+int launch_planes_to_pairs(const double *E, float *e8, int nx, int64_t n, cudaStream_t st) {
+    if (reinterpret_cast<uintptr_t>(e8) % 32) return OSC_E_INVALID;
+    k_planes_to_pairs<<<nblocks(n, 256), 256, 0, st>>>(E, reinterpret_cast<float4 *>(e8), nx, n);
+    return ok();
+}
+
 }  // namespace osc

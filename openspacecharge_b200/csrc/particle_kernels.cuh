@@ -104,4 +104,7 @@ int launch_deposit_vec3(const DepositArgs &a, const double *g, double *acc, cuda
 int launch_vjp_particles(const InterpArgs &ia, const DepositArgs &da, const double *E, const double *lam,
                          const double *gE, double *gx, double *gy, double *gz, double *gq, cudaStream_t st);
 
+// E planes [3][N] (f64) to the x-pair grid read by launch_interp_pairs (e8 32-byte aligned).
+int launch_planes_to_pairs(const double *E, float *e8, int nx, int64_t n, cudaStream_t st);
+
 }  // namespace osc

@@ -389,3 +389,14 @@ def format_1pe14_7(v: float) -> str:
     if rc:
         raise ValueError("format")
     return buf.value.decode()
+
+
+def space_charge_step_rectpipe_dev(ctx, mesh3d: Mesh3D, x, y, z, E, apipe, bpipe, qa=None, total_charge=None,
+                                   precision=PREC_FP32, B=None) -> None:
+    """Fused step in the rectangular pipe on torch CUDA float64 tensors (mesh as given; its
+    pipe Green spectra must exist, osc_rectpipe_green): E (np, 3) (and B) in place."""
+    ctx = _ctx(ctx)
+    m = mesh3d.to_c()
+    tc = None if total_charge is None else ctypes.byref(ctypes.c_double(float(total_charge)))
+    ctx.call("osc_space_charge_step_rectpipe_dev", ctypes.byref(m), ctypes.c_int64(x.numel()), _tp(x), _tp(y),
+             _tp(z), _tp(qa), tc, ctypes.c_double(apipe), ctypes.c_double(bpipe), int(precision), _tp(E), _tp(B))

@@ -117,6 +117,7 @@ SIGNATURES = {
     "osc_rectpipe_green": [_P, _PM, _D, _D, _I],
     "osc_space_charge_rectpipe": [_P, _PM, _P, _D, _D, _I, _I, _I, _P, _P, _P],
     "osc_space_charge_rectpipe_dev": [_P, _PM, _P, _D, _D, _I, _I, _I, _P, _P, _P],
+    "osc_space_charge_step_rectpipe_dev": [_P, _PM, _I64, _P, _P, _P, _P, _P, _D, _D, _I, _P, _P],
     "osc_write_rectpipe_grn": [_P, ctypes.c_char_p, _D, _D, _PM],
     "osc_read_rectpipe_grn": [_P, ctypes.c_char_p, _PM, _PD, _PD],
     "osc_interpolate_field": [_P, _PM, _P, _P, _I64, _P, _P, _P, _P, _P, _PI64],

@@ -80,7 +80,8 @@ def pipe_case(oracle):
     gam = 5e6 / 0.510998910e6
     grn = oracle.getgrnpipe(gam, a, b, delta, umin, (1, 1, 1), n)
     phi0, e0, b0 = oracle.rectpipe_solver(rho, grn, gam, delta, (1, 1, 1), n)
-    return dict(a=a, b=b, n=n, umin=umin, umax=umax, delta=delta, rho=rho, gam=gam, phi=phi0, e=e0, bf=b0)
+    return dict(a=a, b=b, n=n, umin=umin, umax=umax, delta=delta, rho=rho, gam=gam, phi=phi0, e=e0, bf=b0,
+                x=x, y=y, z=z)
 
 
 @pytest.mark.parametrize("prec", [osc.PREC_FP64_PLAIN, osc.PREC_FP64, osc.PREC_FP32])
@@ -131,3 +132,26 @@ def test_rectpipe_green_file_roundtrip(ctx, pipe_case, tmp_path):
     osc.space_charge_rectpipe(ctx2, m, c["a"], c["b"], direct_field_calc=False, precision=osc.PREC_FP64_PLAIN)
     assert np.array_equal(m.phi, phi_a)
     ctx2.close()
+
+
+@pytest.mark.parametrize("prec", [osc.PREC_FP64_PLAIN, osc.PREC_FP64, osc.PREC_FP32])
+def test_fused_pipe_step_matches_oracle(ctx, oracle, pipe_case, prec):
+    """deposit + space_charge_rectpipe + interpolate_field in one device call against the
+    oracle's chain (depose_rho_scalar, osc_rectpipe_solver, interpolate_field)."""
+    torch = pytest.importorskip("torch")
+    c = pipe_case
+    m = osc.Mesh3D(nlo=(1, 1, 1), nhi=c["n"], min=c["umin"], max=c["umax"], delta=c["delta"], gamma=c["gam"])
+    osc.osc_rectpipe_green(ctx, m, c["a"], c["b"], precision=prec)
+    dev = torch.device("cuda", 0)
+    tx, ty, tz = (torch.from_numpy(v).to(dev) for v in (c["x"], c["y"], c["z"]))
+    E = torch.empty((len(c["x"]), 3), dtype=torch.float64, device=dev)
+    B = torch.empty_like(E)
+    osc.space_charge_step_rectpipe_dev(ctx, m, tx, ty, tz, E, c["a"], c["b"], total_charge=1e-9, precision=prec,
+                                       B=B)
+    ctx.synchronize()
+    om = oracle.make_mesh((1, 1, 1), c["n"], (1, 1, 1), c["umin"], c["umax"], c["delta"], c["gam"])
+    E0, B0, _ = oracle.interpolate_field(om, c["e"], c["x"], c["y"], c["z"], bfield=c["bf"])
+    mx, _ = field_err(E.cpu().numpy(), E0)
+    assert mx <= 10 * TOL[prec], mx
+    bm = np.abs(B.cpu().numpy()[:, :2] - B0[:, :2]).max() / np.abs(B0[:, :2]).max()
+    assert bm <= 10 * TOL[prec], bm
