@@ -437,13 +437,14 @@ int osc_space_charge_step_dev(osc_ctx *ctx, osc_mesh3d *mesh, int64_t np, const 
         return OSC_OK;
     }
     if (precision == OSC_PREC_FP32) {
-        // deposit: two float4 atomics per particle into a quad grid, then a fixed-order
-        // sum to nodes; field: E written as an x-pair grid; interpolation: 4 sectors/particle
-        float *rho, *quad;
+        // deposit: two float4 atomics per particle into a quad grid, summed to nodes in a
+        // fixed order by the x transform's loads; field: E written as an x-pair grid;
+        // interpolation: 4 sectors/particle
+        float *rho = nullptr, *quad;
         void *E8;
-        TRY(ws_get(ctx, "st_rho32", sizeof(float) * N, (void **)&rho));
         TRY(ws_get(ctx, "st_E8", sizeof(float4) * 2 * N, &E8));
         if (ctx->deposit_mode == OSC_DEPOSIT_DETERMINISTIC) {
+            TRY(ws_get(ctx, "st_rho32", sizeof(float) * N, (void **)&rho));
             TRY(deposit_rho<float>(ctx, da, rho, N, 1.0));
         } else {
             TRY(ws_get(ctx, "st_quad", sizeof(float) * 4 * N, (void **)&quad));
@@ -453,11 +454,7 @@ int osc_space_charge_step_dev(osc_ctx *ctx, osc_mesh3d *mesh, int64_t np, const 
                 if (launch_deposit_quad(da, quad, ctx->d_small, ctx->stream))
                     return set_err(ctx, OSC_E_CUDA, "deposit");
             }
-            {
-                Launch L_(ctx, "quad_to_nodes");
-                if (launch_quad_to_nodes(quad, rho, n[0], n[1], n[2], ctx->stream))
-                    return set_err(ctx, OSC_E_CUDA, "quad to nodes");
-            }
+            j.quad = reinterpret_cast<const float4 *>(quad);
         }
         j.E4 = E8;
         j.e4_pairs = 1;

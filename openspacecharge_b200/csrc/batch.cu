@@ -216,10 +216,9 @@ int batch_fp32(osc_ctx *ctx, int nb, osc_bunch *bs, const double *x, const doubl
         }
     }
     // deposit every bunch into its quad grid
-    float *quad, *rho, *e8;
+    float *quad, *e8;
     unsigned long long *cnt;
     TRY(ws_get(ctx, "batch_quad", sizeof(float) * 4 * (size_t)nodes, (void **)&quad));
-    TRY(ws_get(ctx, "batch_rho", sizeof(float) * (size_t)nodes, (void **)&rho));
     TRY(ws_get(ctx, "batch_e8", sizeof(float) * 8 * (size_t)nodes, (void **)&e8));
     TRY(ws_get(ctx, "batch_cnt", sizeof(unsigned long long) * 4 * (size_t)nb, (void **)&cnt));
     CK(cudaMemsetAsync(quad, 0, sizeof(float) * 4 * (size_t)nodes, ctx->stream), "memset quad");
@@ -244,11 +243,6 @@ int batch_fp32(osc_ctx *ctx, int nb, osc_bunch *bs, const double *x, const doubl
         const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
         const int B = (int)g.members.size();
         const int64_t N = (int64_t)nx * ny * nz;
-        {
-            Launch L_(ctx, "quad_to_nodes");
-            if (launch_quad_to_nodes(quad + 4 * g.node0, rho + g.node0, nx, ny, nz * B, ctx->stream))
-                return set_err(ctx, OSC_E_CUDA, "quad to nodes");
-        }
         const int zinner = zconv_warp_ok(2 * nz, nz, 4) ? 1 : 0;
         const int zp = zinner ? green_zpitch(nz + 1, sizeof(float)) : nz + 1;
         const int64_t per = (int64_t)(nx + 1) * (ny + 1) * zp;
@@ -288,7 +282,8 @@ int batch_fp32(osc_ctx *ctx, int nb, osc_bunch *bs, const double *x, const doubl
         j.gbatch = spec;
         j.ngbatch = 3;
         j.g_bstride = per;
-        TRY(freespace_opt<float, float>(ctx, j, rho + g.node0));
+        j.quad = reinterpret_cast<const float4 *>(quad) + g.node0;  // the x transform sums the nodes
+        TRY(freespace_opt<float, float>(ctx, j, nullptr));
         (void)N;
     }
     for (int s2 = 0; s2 < kSlots; ++s2) {

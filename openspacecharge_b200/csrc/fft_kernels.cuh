@@ -29,6 +29,7 @@ struct R2CArgs {
     int64_t nrows;
     int64_t in_rstride;   // elements between rows of the real input
     int64_t out_rstride;  // complex elements between output rows
+    int qny = 0;          // quad-grid input (float4): rows per plane, for the node sum's y neighbour
 };
 
 // Where the real result of one inverse component goes.

@@ -7,6 +7,8 @@ template int launch_lines<float>(const cplx<float> *, cplx<float> *, const LineA
                                  const TwPair<cplx<float>> &, cudaStream_t);
 template int launch_r2c_rows<float, float>(const float *, cplx<float> *, const R2CArgs &, const TwPair<cplx<float>> &,
                                            cudaStream_t);
+template int launch_r2c_rows<float, float4>(const float4 *, cplx<float> *, const R2CArgs &,
+                                            const TwPair<cplx<float>> &, cudaStream_t);
 template int launch_r2c_rows<float, double>(const double *, cplx<float> *, const R2CArgs &,
                                             const TwPair<cplx<float>> &, cudaStream_t);
 template int launch_c2r_rows<float>(const cplx<float> *, const C2RArgs &, const TwPair<cplx<float>> &, cudaStream_t);

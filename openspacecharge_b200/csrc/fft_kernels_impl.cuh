@@ -111,6 +111,24 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_lines(const cplx<T> *in, cpl
 }
 
 // ------------------------------------------------------------------------------------
+// Element e of real input row `row` (row < nrows, e < nin).
+template <typename TIn>
+__device__ __forceinline__ TIn r2c_in(const TIn *__restrict__ in, const R2CArgs &a, int64_t row, int e) {
+    return in[row * a.in_rstride + e];
+}
+// Quad-grid input of the FP32 deposit: node (i,j) of a plane is the sum of the four
+// contributions held at (i,j).x, (i-1,j).y, (i,j-1).z and (i-1,j-1).w, added in that
+// fixed order (the order of k_quad_to_nodes, so rho is the same to the bit).
+__device__ __forceinline__ float r2c_in(const float4 *__restrict__ in, const R2CArgs &a, int64_t row, int e) {
+    const float4 *q = in + row * a.in_rstride + e;
+    const bool jn = (row % a.qny) > 0;
+    float s = __ldg(&q->x);
+    if (e > 0) s += __ldg(&q[-1].y);
+    if (jn) s += __ldg(&q[-a.in_rstride].z);
+    if (e > 0 && jn) s += __ldg(&q[-a.in_rstride - 1].w);
+    return s;
+}
+
 template <typename T, typename TIn, int NL, class E, bool HIN>
 __global__ void __launch_bounds__(E::kMaxThreads) k_r2c_rows(const TIn *__restrict__ in, cplx<T> *__restrict__ out,
                                                              R2CArgs a, const cplx<T> *__restrict__ twg) {
@@ -120,7 +138,8 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_r2c_rows(const TIn *__restri
     const int L = E::kLen ? E::kLen : a.p.L;
     V *buf = tw + L;
     constexpr int lstr = NL + 1;
-    const int nthreads = blockDim.x, tid = threadIdx.x;
+    // static engines launch with L*NL/FFT_EPT threads: compile-time trip counts below
+    const int nthreads = E::kLen ? E::kLen * NL / FFT_EPT : (int)blockDim.x, tid = threadIdx.x;
     const int64_t row0 = (int64_t)blockIdx.x * (2 * NL);
     load_twiddles(tw, twg, L);
     const int ld_len = (E::kLen > 0 && HIN) ? E::kLen / 2 : L;  // HIN launches only with nin == L/2
@@ -128,7 +147,7 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_r2c_rows(const TIn *__restri
         const int rr = idx / ld_len, e = idx - rr * ld_len;
         const int64_t row = row0 + rr;
         T v = 0;
-        if (row < a.nrows && e < a.nin) v = (T)in[row * a.in_rstride + e];
+        if (row < a.nrows && e < a.nin) v = (T)r2c_in(in, a, row, e);
         T *slot = reinterpret_cast<T *>(&buf[e * lstr + (rr >> 1)]);
         slot[rr & 1] = v;
     }
@@ -385,7 +404,10 @@ __global__ void __launch_bounds__(E::kLen * 3 * NLC / FFT_EPT) k_c2r_e8(const cp
     const int64_t ies = a.zin ? a.zin_nz : 1;
     load_twiddles(tw, twg, L);
     __syncthreads();
-    for (int idx = tid; idx < NLT * L; idx += nthreads) {
+    // line = two real rows A + iB; each stored value k <= L/2 is read once and also gives
+    // the line's value at L-k (from the conjugates)
+    constexpr int nk = half + 1;
+    for (int idx = tid; idx < NLT * nk; idx += nthreads) {
         int c, line, k;
         if (a.zin) {  // rows (adjacent z) fastest: coalesced reads of the kz-innermost spectra
             k = idx / NLT;
@@ -393,20 +415,19 @@ __global__ void __launch_bounds__(E::kLen * 3 * NLC / FFT_EPT) k_c2r_e8(const cp
             c = rem / NLC;
             line = rem - c * NLC;
         } else {
-            c = idx / (NLC * L);
-            const int rem = idx - c * (NLC * L);
-            line = rem / L;
-            k = rem - line * L;
+            c = idx / (NLC * nk);
+            const int rem = idx - c * (NLC * nk);
+            line = rem / nk;
+            k = rem - line * nk;
         }
         const V *src = in + (int64_t)a.e8_comp[c] * a.in_cstride;
         const int64_t ra = row0 + 2 * line, rb = ra + 1;
-        const int kk = k <= half ? k : L - k;
         V A = mk<T>(0, 0), B = mk<T>(0, 0);
-        if (ra < a.nrows) A = src[rin[2 * line] + kk * ies];
-        if (rb < a.nrows) B = src[rin[2 * line + 1] + kk * ies];
+        if (ra < a.nrows) A = src[rin[2 * line] + k * ies];
+        if (rb < a.nrows) B = src[rin[2 * line + 1] + k * ies];
         if (k == 0 || k == half) { A.y = 0; B.y = 0; }
-        if (k > half) { A.y = -A.y; B.y = -B.y; }
         buf[k * lstr + c * NLC + line] = mk<T>(A.x - B.y, A.y + B.x);
+        if (k > 0 && k < half) buf[(L - k) * lstr + c * NLC + line] = mk<T>(A.x + B.y, B.x - A.y);
     }
     __syncthreads();
     E::template run<V, NLT, false, true>(buf, a.p, tw, -1);

@@ -10,6 +10,7 @@
 // spectral product, so the image costs one more spectrum read, not one more solve.
 #include <cstring>
 #include <sstream>
+#include <type_traits>
 
 #include "solver.cuh"
 
@@ -398,7 +399,16 @@ int freespace_opt(osc_ctx *c, const FreeSpaceJob &j, const TIn *rho) {
     ra.out_rstride = nxh;
     {
         Launch L_(c, "fft_x_r2c");
-        TRY(kerr(c, launch_r2c_rows<T, TIn>(rho, X1, ra, twx, c->stream), "x r2c"));
+        if constexpr (std::is_same<T, float>::value) {
+            if (j.quad) {
+                ra.qny = ny;
+                TRY(kerr(c, launch_r2c_rows<float, float4>(j.quad, X1, ra, twx, c->stream), "x r2c"));
+            } else {
+                TRY(kerr(c, launch_r2c_rows<T, TIn>(rho, X1, ra, twx, c->stream), "x r2c"));
+            }
+        } else {
+            TRY(kerr(c, launch_r2c_rows<T, TIn>(rho, X1, ra, twx, c->stream), "x r2c"));
+        }
     }
     // y forward: [z][y][kx] -> [z][ky][kx]
     LineArgs ly;

@@ -39,6 +39,9 @@ struct FreeSpaceJob {
     double *B = nullptr;    // device f64 [3][N]
     void *E4 = nullptr;     // device vec4<T> [N], or the x-pair grid vec4<T> [N][2]
     int e4_pairs = 0;       // 1: E4 is the x-pair grid read by launch_interp_pairs
+    // FP32 only: the deposit's quad grid (float4 [N]); when set, the x transform sums each
+    // node from it and the rho argument is not read
+    const float4 *quad = nullptr;
     // E components computed (bit c: E_c); each one is also added, times acc_coef, into
     // the single plane Eacc when that is set (adjoint solves accumulate a potential)
     int comp_mask = 7;
