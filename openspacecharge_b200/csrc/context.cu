@@ -137,7 +137,7 @@ template <typename T> int twiddles(osc_ctx *c, int L, TwPair<cplx<T>> *out) {
             if constexpr (E::kLen > 0) h = stage_table<T>(L, E::kRad, E::kNst);
             return 0;
         };
-        if (which == 0) dispatch_fft_len(L, make);
+        if (which == 0) dispatch_fft_len<T>(L, make);
         else dispatch_warp_len(L, make);
         DevBuf b{nullptr, 0};
         if (!h.empty()) {

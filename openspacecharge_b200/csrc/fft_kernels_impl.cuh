@@ -604,7 +604,7 @@ template <typename T>
 int launch_lines(const cplx<T> *in, cplx<T> *out, const LineArgs &a, int nplanes, int ncomp, bool row_mode,
                  const TwPair<cplx<T>> &tw, cudaStream_t st) {
     const int L = a.p.L;
-    return dispatch_fft_len(L, [&](auto eng) -> int {
+    return dispatch_fft_len<T>(L, [&](auto eng) -> int {
         using E = decltype(eng);
         const cplx<T> *twe = eng_tw<E>(tw);
         return with_nl<T, E>(L, 1, sizeof(T) == 4 ? 16 : 8, 0, [&](auto nlc) -> int {
@@ -624,7 +624,7 @@ int launch_lines(const cplx<T> *in, cplx<T> *out, const LineArgs &a, int nplanes
 template <typename T, typename TIn>
 int launch_r2c_rows(const TIn *in, cplx<T> *out, const R2CArgs &a, const TwPair<cplx<T>> &tw, cudaStream_t st) {
     const int L = a.p.L;
-    return dispatch_fft_len(L, [&](auto eng) -> int {
+    return dispatch_fft_len<T>(L, [&](auto eng) -> int {
         using E = decltype(eng);
         const cplx<T> *twe = eng_tw<E>(tw);
         return with_nl<T, E>(L, 1, sizeof(T) == 4 ? 16 : 8, 0, [&](auto nlc) -> int {
@@ -658,7 +658,7 @@ int launch_c2r_rows(const cplx<T> *in, const C2RArgs &a, const TwPair<cplx<T>> &
                        reinterpret_cast<uintptr_t>(a.e8) % 32 == 0;
         for (int c = 0; c < a.ncomp && e8_only; ++c) e8_only = a.ndest[c] == 0;
         if (e8_only) {
-            const int rc = dispatch_fft_len(L, [&](auto eng) -> int {
+            const int rc = dispatch_fft_len<T>(L, [&](auto eng) -> int {
                 using E = decltype(eng);
                 if constexpr (E::kLen > 0) {
                     constexpr int NLC = c2r_e8_nlc<T, E>();
@@ -675,7 +675,7 @@ int launch_c2r_rows(const cplx<T> *in, const C2RArgs &a, const TwPair<cplx<T>> &
             if (rc != -1) return rc;
         }
     }
-    return dispatch_fft_len(L, [&](auto eng) -> int {
+    return dispatch_fft_len<T>(L, [&](auto eng) -> int {
         using E = decltype(eng);
         const cplx<T> *twe = eng_tw<E>(tw);
         return with_nl<T, E>(L, 1, sizeof(T) == 4 ? 16 : 8, 0, [&](auto nlc) -> int {
@@ -755,7 +755,7 @@ int launch_zconv(const cplx<T> *in, cplx<T> *out, const ZConvArgs &a, const TwPa
     }
     for (int i = 0; i < a.ng; ++i)
         if (a.g[i].zinner) return OSC_E_INVALID;
-    return dispatch_fft_len(L, [&](auto eng) -> int {
+    return dispatch_fft_len<T>(L, [&](auto eng) -> int {
         using E = decltype(eng);
         const cplx<T> *twe = eng_tw<E>(tw);
         return with_nl<T, E>(L, 2, sizeof(T) == 4 ? 8 : 4, nl, [&](auto nlc) -> int {
@@ -785,7 +785,7 @@ int launch_sym_lines(const double *in, TO *out, const SymArgs &a, const TwPair<c
                      bool k_fast_store, cudaStream_t st) {
     const int L = a.p.L;
     if (L != 2 * a.n) return OSC_E_INVALID;
-    return dispatch_fft_len(L, [&](auto eng) -> int {
+    return dispatch_fft_len<double>(L, [&](auto eng) -> int {
         using E = decltype(eng);
         const double2 *twe = eng_tw<E>(tw);
         return with_nl<double, E>(L, 1, 8, 0, [&](auto nlc) -> int {

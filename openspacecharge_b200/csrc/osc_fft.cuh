@@ -104,6 +104,44 @@ template <> struct Dft<8> {
     }
 };
 
+// Radix 16 by decimation in frequency: X[2q] is the 8-point DFT of a_r = v_r + v_{r+8},
+// X[2q+1] the 8-point DFT of b_r = (v_r - v_{r+8}) w16^r, w16 = exp(s i pi/8).
+template <> struct Dft<16> {
+    template <typename V> __device__ __forceinline__ static void run(V *v, int s) {
+        typedef decltype(v[0].x) T;
+        const T c1 = (T)0.92387953251128675612818318939679;  // cos(pi/8)
+        const T s1 = (T)0.38268343236508977172845998403040;  // sin(pi/8)
+        const T h = (T)0.70710678118654752440084436210485;   // cos(pi/4)
+        const T sg = (T)s;
+        V a[8], b[8];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            a[r] = cadd(v[r], v[r + 8]);
+            b[r] = csub(v[r], v[r + 8]);
+        }
+        // b_r *= cos(r pi/8) + s i sin(r pi/8)
+        auto rot = [&](V &t, T cr, T sr) {
+            const V u = t;
+            t.x = cr * u.x - sg * sr * u.y;
+            t.y = cr * u.y + sg * sr * u.x;
+        };
+        rot(b[1], c1, s1);
+        rot(b[2], h, h);
+        rot(b[3], s1, c1);
+        b[4] = cmul_si(b[4], s);
+        rot(b[5], -s1, c1);
+        rot(b[6], -h, h);
+        rot(b[7], -c1, s1);
+        Dft<8>::run(a, s);
+        Dft<8>::run(b, s);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            v[2 * q] = a[q];
+            v[2 * q + 1] = b[q];
+        }
+    }
+};
+
 template <> struct Dft<3> {
     template <typename V> __device__ __forceinline__ static void run(V *v, int s) {
         typedef decltype(v[0].x) T;
@@ -393,15 +431,19 @@ constexpr int nl_static(int L, int nl_max, int elem_bytes, int nbuf, int budget 
     return nl;
 }
 
-// Calls f(engine) with the static engine for L when there is one, else FftRuntime.
-template <class F> inline int dispatch_fft_len(int L, F &&f) {
+// Calls f(engine) with the static engine for L when there is one, else FftRuntime.  T is
+// the real type of the transform: at L = 256 the FP64 transforms take two radix-16 stages,
+// the FP32 ones (whose y passes measured faster so) radix 8-8-4.
+template <typename T, class F> inline int dispatch_fft_len(int L, F &&f) {
     switch (L) {
     case 32: return f(FftStatic<32, 8, 4>{});
     case 64: return f(FftStatic<64, 8, 8>{});
     case 96: return f(FftStatic<96, 8, 4, 3>{});
-    case 128: return f(FftStatic<128, 8, 4, 4>{});
+    case 128: return f(FftStatic<128, 16, 8>{});
     case 192: return f(FftStatic<192, 8, 8, 3>{});
-    case 256: return f(FftStatic<256, 8, 8, 4>{});
+    case 256:
+        if constexpr (sizeof(T) == 8) return f(FftStatic<256, 16, 16>{});
+        else return f(FftStatic<256, 8, 8, 4>{});
     case 384: return f(FftStatic<384, 8, 8, 2, 3>{});
     case 512: return f(FftStatic<512, 8, 8, 8>{});
     default: return f(FftRuntime{});
