@@ -148,10 +148,10 @@ def kernel_bytes(nx, ny, nz, npart, at_cathode=False):
     nout = 3
     g_bytes = 3 * 4 * nxh * (ny + 1) * (nz + 1)
     return {
-        # CIC weights into a quad grid (4 floats per node), then summed to nodes
+        # CIC weights into a quad grid (4 floats per node); the x transform sums each node
+        # from the quad grid as it loads it
         "deposit_f32": 24 * npart + 16 * N,
-        "quad_to_nodes": 16 * N + 4 * N,
-        "fft_x_r2c": 4 * N + c8 * nxh * ny * nz,
+        "fft_x_r2c": 16 * N + c8 * nxh * ny * nz,
         "fft_y_fwd": c8 * nxh * ny * nz + c8 * nxh * Ny * nz,
         "fft_z_conv": c8 * nxh * Ny * nz + g_bytes + nout * c8 * nxh * Ny * nz,
         "fft_y_inv": nout * c8 * nxh * Ny * nz + nout * c8 * nxh * ny * nz,
