@@ -143,13 +143,32 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_r2c_rows(const TIn *__restri
     const int64_t row0 = (int64_t)blockIdx.x * (2 * NL);
     load_twiddles(tw, twg, L);
     const int ld_len = (E::kLen > 0 && HIN) ? E::kLen / 2 : L;  // HIN launches only with nin == L/2
-    for (int idx = tid; idx < 2 * NL * ld_len; idx += nthreads) {
-        const int rr = idx / ld_len, e = idx - rr * ld_len;
-        const int64_t row = row0 + rr;
-        T v = 0;
-        if (row < a.nrows && e < a.nin) v = (T)r2c_in(in, a, row, e);
-        T *slot = reinterpret_cast<T *>(&buf[e * lstr + (rr >> 1)]);
-        slot[rr & 1] = v;
+    if constexpr (E::kLen > 0) {
+        // all of a thread's loads are issued before any is stored to shared memory
+        constexpr int LDL = HIN ? E::kLen / 2 : E::kLen, NT = E::kLen * NL / FFT_EPT;
+        constexpr int IT = (2 * NL * LDL + NT - 1) / NT;
+        T v[IT];
+#pragma unroll
+        for (int it = 0; it < IT; ++it) {
+            const int idx = tid + it * NT, rr = idx / LDL, e = idx - rr * LDL;
+            const int64_t row = row0 + rr;
+            v[it] = 0;
+            if (idx < 2 * NL * LDL && row < a.nrows && e < a.nin) v[it] = (T)r2c_in(in, a, row, e);
+        }
+#pragma unroll
+        for (int it = 0; it < IT; ++it) {
+            const int idx = tid + it * NT, rr = idx / LDL, e = idx - rr * LDL;
+            if (idx < 2 * NL * LDL) reinterpret_cast<T *>(&buf[e * lstr + (rr >> 1)])[rr & 1] = v[it];
+        }
+    } else {
+        for (int idx = tid; idx < 2 * NL * ld_len; idx += nthreads) {
+            const int rr = idx / ld_len, e = idx - rr * ld_len;
+            const int64_t row = row0 + rr;
+            T v = 0;
+            if (row < a.nrows && e < a.nin) v = (T)r2c_in(in, a, row, e);
+            T *slot = reinterpret_cast<T *>(&buf[e * lstr + (rr >> 1)]);
+            slot[rr & 1] = v;
+        }
     }
     __syncthreads();
     E::template run<V, NL, HIN, false>(buf, a.p, tw, +1);
@@ -389,7 +408,7 @@ template <typename T, class E> constexpr int c2r_e8_nlc() {
 // FP32: x-pair nodes (E(x), E(x+1)) with one 256-bit store; FP64: nodes (Ex, Ey, Ez, 0)
 // with one 256-bit store.
 template <typename T, int NLC, class E>
-__global__ void __launch_bounds__(E::kLen * 3 * NLC / FFT_EPT) k_c2r_e8(const cplx<T> *__restrict__ in, C2RArgs a,
+__global__ void __launch_bounds__(E::kLen * 3 * NLC / FFT_EPT, sizeof(T) == 4 ? 3 : 1) k_c2r_e8(const cplx<T> *__restrict__ in, C2RArgs a,
                                                                       const cplx<T> *__restrict__ twg) {
     typedef cplx<T> V;
     constexpr int L = E::kLen, NLT = 3 * NLC, lstr = NLT + 1, half = L / 2, nout = L / 2;
@@ -406,9 +425,8 @@ __global__ void __launch_bounds__(E::kLen * 3 * NLC / FFT_EPT) k_c2r_e8(const cp
     __syncthreads();
     // line = two real rows A + iB; each stored value k <= L/2 is read once and also gives
     // the line's value at L-k (from the conjugates)
-    constexpr int nk = half + 1;
-    for (int idx = tid; idx < NLT * nk; idx += nthreads) {
-        int c, line, k;
+    constexpr int nk = half + 1, IT = (NLT * nk + nthreads - 1) / nthreads;
+    auto slot_of = [&](int idx, int &c, int &line, int &k) {
         if (a.zin) {  // rows (adjacent z) fastest: coalesced reads of the kz-innermost spectra
             k = idx / NLT;
             const int rem = idx - k * NLT;
@@ -420,14 +438,34 @@ __global__ void __launch_bounds__(E::kLen * 3 * NLC / FFT_EPT) k_c2r_e8(const cp
             line = rem / nk;
             k = rem - line * nk;
         }
-        const V *src = in + (int64_t)a.e8_comp[c] * a.in_cstride;
-        const int64_t ra = row0 + 2 * line, rb = ra + 1;
-        V A = mk<T>(0, 0), B = mk<T>(0, 0);
-        if (ra < a.nrows) A = src[rin[2 * line] + k * ies];
-        if (rb < a.nrows) B = src[rin[2 * line + 1] + k * ies];
-        if (k == 0 || k == half) { A.y = 0; B.y = 0; }
-        buf[k * lstr + c * NLC + line] = mk<T>(A.x - B.y, A.y + B.x);
-        if (k > 0 && k < half) buf[(L - k) * lstr + c * NLC + line] = mk<T>(A.x + B.y, B.x - A.y);
+    };
+    // all of a thread's loads are issued before any is stored to shared memory
+    V A[IT], B[IT];
+#pragma unroll
+    for (int it = 0; it < IT; ++it) {
+        const int idx = tid + it * nthreads;
+        A[it] = mk<T>(0, 0);
+        B[it] = mk<T>(0, 0);
+        if (idx < NLT * nk) {
+            int c, line, k;
+            slot_of(idx, c, line, k);
+            const V *src = in + (int64_t)a.e8_comp[c] * a.in_cstride;
+            const int64_t ra = row0 + 2 * line, rb = ra + 1;
+            if (ra < a.nrows) A[it] = src[rin[2 * line] + k * ies];
+            if (rb < a.nrows) B[it] = src[rin[2 * line + 1] + k * ies];
+        }
+    }
+#pragma unroll
+    for (int it = 0; it < IT; ++it) {
+        const int idx = tid + it * nthreads;
+        if (idx < NLT * nk) {
+            int c, line, k;
+            slot_of(idx, c, line, k);
+            V a0 = A[it], b0 = B[it];
+            if (k == 0 || k == half) { a0.y = 0; b0.y = 0; }
+            buf[k * lstr + c * NLC + line] = mk<T>(a0.x - b0.y, a0.y + b0.x);
+            if (k > 0 && k < half) buf[(L - k) * lstr + c * NLC + line] = mk<T>(a0.x + b0.y, b0.x - a0.y);
+        }
     }
     __syncthreads();
     E::template run<V, NLT, false, true>(buf, a.p, tw, -1);
@@ -493,19 +531,53 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_sym_lines(const double *__re
     }
     load_twiddles(tw, twg, L);
     __syncthreads();
-    for (int idx = tid; idx < 2 * NL * L; idx += nthreads) {
-        int rr, e;
-        if (LDE) { rr = idx / L; e = idx - rr * L; }
-        else { e = idx / (2 * NL); rr = idx - e * (2 * NL); }
-        const int64_t o = bin[rr];
-        double v = 0.0;
-        if (o >= 0 && e != n) {
-            const int src = e < n ? e : L - e;
-            v = in[o + (int64_t)src * a.in_es];
-            if (e > n && podd[rr]) v = -v;
+    if constexpr (E::kLen > 0) {
+        // static engine (L = 2n known, L*NL/FFT_EPT threads): each thread first loads its
+        // share of the n+1 distinct values of every line into registers (all loads in
+        // flight), then writes each value at e and its parity image at L-e
+        constexpr int nh = E::kLen / 2, NK = nh + 1, TOT = 2 * NL * NK;
+        constexpr int NT = E::kLen * NL / FFT_EPT, IT = (TOT + NT - 1) / NT;
+        double v[IT];
+#pragma unroll
+        for (int it = 0; it < IT; ++it) {
+            const int idx = tid + it * NT;
+            v[it] = 0.0;
+            if (idx < TOT) {
+                int rr, e;
+                if (LDE) { rr = idx / NK; e = idx - rr * NK; }
+                else { e = idx / (2 * NL); rr = idx - e * (2 * NL); }
+                const int64_t o = bin[rr];
+                if (o >= 0 && e != nh) v[it] = in[o + (int64_t)e * a.in_es];
+            }
         }
-        double *slot = reinterpret_cast<double *>(&buf[e * lstr + (rr >> 1)]);
-        slot[rr & 1] = v;
+#pragma unroll
+        for (int it = 0; it < IT; ++it) {
+            const int idx = tid + it * NT;
+            if (idx < TOT) {
+                int rr, e;
+                if (LDE) { rr = idx / NK; e = idx - rr * NK; }
+                else { e = idx / (2 * NL); rr = idx - e * (2 * NL); }
+                reinterpret_cast<double *>(&buf[e * lstr + (rr >> 1)])[rr & 1] = v[it];
+                if (e > 0 && e < nh)
+                    reinterpret_cast<double *>(&buf[(E::kLen - e) * lstr + (rr >> 1)])[rr & 1] =
+                        podd[rr] ? -v[it] : v[it];
+            }
+        }
+    } else {
+        for (int idx = tid; idx < 2 * NL * L; idx += nthreads) {
+            int rr, e;
+            if (LDE) { rr = idx / L; e = idx - rr * L; }
+            else { e = idx / (2 * NL); rr = idx - e * (2 * NL); }
+            const int64_t o = bin[rr];
+            double v = 0.0;
+            if (o >= 0 && e != n) {
+                const int src = e < n ? e : L - e;
+                v = in[o + (int64_t)src * a.in_es];
+                if (e > n && podd[rr]) v = -v;
+            }
+            double *slot = reinterpret_cast<double *>(&buf[e * lstr + (rr >> 1)]);
+            slot[rr & 1] = v;
+        }
     }
     __syncthreads();
     E::template run<V, NL, false, false>(buf, a.p, tw, +1);
