@@ -8,6 +8,7 @@
 // line transforms; the stacked FFT passes with the members as extra rows, planes and
 // columns), and one pass interpolates E for every particle.  The reference solves one
 // bunch per call (space_charge_3d, code/open_spacecharge_mod.f90:431-489).
+#include <algorithm>
 #include <map>
 #include <tuple>
 #include <vector>
@@ -232,10 +233,25 @@ int batch_fp32(osc_ctx *ctx, int nb, osc_bunch *bs, const double *x, const doubl
     // kSlots auxiliary streams (each with its own workspaces) after the deposit
     CK(cudaEventRecord(ctx->aux_ev[kSlots], ctx->stream), "record deposit");
     for (int s2 = 0; s2 < kSlots; ++s2) CK(cudaStreamWaitEvent(ctx->aux[s2], ctx->aux_ev[kSlots], 0), "wait deposit");
-    size_t gidx = 0;
-    for (auto &kv : groups) {
-        Group &g = kv.second;
-        SlotGuard sg(ctx, (int)(gidx % kSlots) + 1);
+    // largest groups first, each on the stream with the least work queued so far, so the
+    // streams finish together (cost ~ members x corner-block nodes)
+    std::vector<std::pair<Group *, size_t>> order;  // (group, index in map order)
+    for (auto &kv : groups) order.push_back({&kv.second, order.size()});
+    auto gcost = [](const Group *g) {
+        return (double)g->members.size() * (g->n[0] + 1) * (double)(g->n[1] + 1) * (double)(g->n[2] + 1);
+    };
+    std::stable_sort(order.begin(), order.end(),
+                     [&](const std::pair<Group *, size_t> &u, const std::pair<Group *, size_t> &v) {
+                         return gcost(u.first) > gcost(v.first);
+                     });
+    double queued[kSlots] = {};
+    for (auto &og : order) {
+        Group &g = *og.first;
+        int slot = 0;
+        for (int s2 = 1; s2 < kSlots; ++s2)
+            if (queued[s2] < queued[slot]) slot = s2;
+        queued[slot] += gcost(&g);
+        SlotGuard sg(ctx, slot + 1);
         float *gbuf;
         double *F;
         TRY(ws_get(ctx, "batch_F", sizeof(double) * max_f, (void **)&F));
@@ -249,7 +265,7 @@ int batch_fp32(osc_ctx *ctx, int nb, osc_bunch *bs, const double *x, const doubl
         const int64_t fstride = (int64_t)(nx + 1) * (ny + 1) * (nz + 1);
         if (zinner) CK(cudaMemsetAsync(gbuf, 0, sizeof(float) * 3 * B * per, ctx->stream), "memset spectra");
         // Green spectra of the three E components of every member: members m = comp*B + i
-        const CornerArgs *d_ca = d_ca_all + ca_off[gidx++];
+        const CornerArgs *d_ca = d_ca_all + ca_off[og.second];
         {
             Launch L_(ctx, "green_corners");
             if (launch_igf_corners_batch(F, d_ca, 3 * B, fstride, fstride, ctx->stream))

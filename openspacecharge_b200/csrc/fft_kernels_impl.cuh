@@ -860,7 +860,15 @@ int launch_sym_lines(const double *in, TO *out, const SymArgs &a, const TwPair<c
     return dispatch_fft_len<double>(L, [&](auto eng) -> int {
         using E = decltype(eng);
         const double2 *twe = eng_tw<E>(tw);
-        return with_nl<double, E>(L, 1, 8, 0, [&](auto nlc) -> int {
+        // static engines: up to 16 line pairs per CTA, so the short lines of small batch
+        // groups still give CTAs of several warps
+        auto with_sym_nl = [&](auto &&f) -> int {
+            if constexpr (E::kLen > 0)
+                return f(std::integral_constant<int, nl_static(E::kLen, 16, (int)sizeof(double2), 1)>{});
+            else
+                return with_nl<double, E>(L, 1, 8, 0, f);
+        };
+        return with_sym_nl([&](auto nlc) -> int {
             constexpr int NL = decltype(nlc)::value;
             const int nt = fft_threads(L, NL);
             if (nt < 1 || nt > E::kMaxThreads || (L * NL) % FFT_EPT) return OSC_E_FFT_SIZE;
