@@ -164,6 +164,19 @@ def kernel_bytes(nx, ny, nz, npart, at_cathode=False):
 TRAFFIC_TABLE = os.path.join(ROOT, "profiles", "traffic_fp32_128x128x256.md")
 
 
+def kernel_profile(ctx, osc, run, n):
+    """Per-kernel CUDA-event times (OSC_OPT_PROFILE) over n untimed calls of run()."""
+    ctx.set_option(osc.OPT_PROFILE, 1)
+    ctx.profile_reset()
+    for _ in range(n):
+        run()
+    prof = ctx.profile()
+    ctx.set_option(osc.OPT_PROFILE, 0)
+    tot = sum(t for _, t in prof.values())
+    return {name: {"launches_per_call": cnt / n, "ms_per_call": t / n, "share": t / max(tot, 1e-12)}
+            for name, (cnt, t) in sorted(prof.items(), key=lambda kv: -kv[1][1])}
+
+
 def profiled_traffic(label):
     """DRAM bytes per launch of one kernel of the headline workload, from the committed ncu
     table (None when the table or the kernel is missing)."""
@@ -570,6 +583,7 @@ def run_adjoint(args, ws, rank, local, dist):
         e1.record(stream)
         e1.synchronize()
     ms = e0.elapsed_time(e1) / k
+    kern = kernel_profile(ctx, osc, lambda: fwd_bwd(osc.PREC_FP32), 3)
     g32 = [t.clone() for t in g]
     fwd_bwd(osc.PREC_FP64)
     ctx.synchronize()
@@ -582,7 +596,7 @@ def run_adjoint(args, ws, rank, local, dist):
             "config": {"workload": "loss sum q|E|^2: FP32 step + FP32 adjoint (deposit, field, gather; deposited "
                                    "gradients, three adjoint solves, gradient gather) on a fixed 128^3 mesh, 4e6 "
                                    "particles, sigma = 1 mm", "grid": list(ADJ_GRID), "particles": ADJ_NP},
-            "rel_err_vs_fp64_gradients": err, "clocks": clk.summary()}))
+            "rel_err_vs_fp64_gradients": err, "kernels": kern, "clocks": clk.summary()}))
     ctx.close()
 
 
@@ -641,6 +655,7 @@ def run_pipe(args, ws, rank, local, dist):
         e1.record(stream)
         e1.synchronize()
     ms = e0.elapsed_time(e1) / k
+    kern = kernel_profile(ctx, osc, lambda: step(osc.PREC_FP32), 3)
     E32 = Ep.clone()
     osc.osc_rectpipe_green(ctx, mesh, a, b, precision=osc.PREC_FP64_PLAIN)
     E64 = torch.empty_like(Ep)
@@ -664,7 +679,7 @@ def run_pipe(args, ws, rank, local, dist):
                                    "sigma=(2,1,1) mm centred at (3,-1) mm, pipe rejection",
                        "grid": list(n), "particles": PIPE_NP},
             "fp64_plain": {"ms_per_step": ms64, "speedup_fp32_over_fp64": ms64 / ms},
-            "rel_err_vs_fp64": err, "green_build_s": green_s, "clocks": clk.summary()}))
+            "rel_err_vs_fp64": err, "green_build_s": green_s, "kernels": kern, "clocks": clk.summary()}))
     ctx.close()
 
 

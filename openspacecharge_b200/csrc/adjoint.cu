@@ -8,7 +8,9 @@
 // with the adjoint potential lambda = sum_c K_c^T a_c and a_c = sum_m gE_c[m] W(x_m).
 // Each K_c is a convolution with a kernel that is odd along axis c on the same centred
 // window, so K_c^T = -K_c: lambda is three forward solves of the deposited gradients,
-// one component each, accumulated with coefficient -1.  The mesh is held fixed.
+// one component each, accumulated with coefficient -1.  The mesh is held fixed.  The FP32
+// path deposits into quad grids and gathers E and lambda from one x-pair grid, as the FP32
+// step does; the FP64 path (and the deterministic deposit mode) uses FP64 planes.
 #include "abi_util.cuh"
 
 using namespace osc;
@@ -29,6 +31,49 @@ int osc_space_charge_step_vjp_dev(osc_ctx *ctx, const osc_mesh3d *mesh, int64_t 
     const double charge1 = q ? 0.0 : total_charge / (double)np;
     DepositArgs da = deposit_args(mesh, n, np, x, y, z, q, charge1, 0);
     InterpArgs ia = interp_args(mesh, n, np, x, y, z);
+    if (precision == OSC_PREC_FP32 && ctx->deposit_mode != OSC_DEPOSIT_DETERMINISTIC) {
+        // FP32: quad-grid deposits (the x transform sums the nodes as it loads them), E and
+        // lambda in one x-pair grid, one gather of four 256-bit loads per particle
+        float *quad, *quad3, *e8;
+        double *lam;
+        TRY(ws_get(ctx, "vjp_quad", sizeof(float4) * N, (void **)&quad));
+        TRY(ws_get(ctx, "vjp_quad3", sizeof(float4) * 3 * N, (void **)&quad3));
+        TRY(ws_get(ctx, "vjp_e8", sizeof(float4) * 2 * N, (void **)&e8));
+        TRY(ws_get(ctx, "vjp_lambda", sizeof(double) * N, (void **)&lam));
+        TRY(counters_reset(ctx));
+        CK(cudaMemsetAsync(quad, 0, sizeof(float4) * N, ctx->stream), "memset quad");
+        CK(cudaMemsetAsync(quad3, 0, sizeof(float4) * 3 * N, ctx->stream), "memset quad3");
+        CK(cudaMemsetAsync(lam, 0, sizeof(double) * N, ctx->stream), "memset lambda");
+        {
+            Launch L_(ctx, "deposit_f32");
+            if (launch_deposit_quad(da, quad, ctx->d_small, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "deposit");
+        }
+        FreeSpaceJob j = fs_job(mesh, n, nullptr, 0, 0);
+        j.quad = reinterpret_cast<const float4 *>(quad);
+        j.E4 = e8;
+        j.e4_pairs = 1;
+        TRY(freespace_opt<float, float>(ctx, j, nullptr));
+        {
+            Launch L_(ctx, "vjp_deposit");
+            if (launch_deposit_quad3(da, gE, quad3, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "vjp deposit");
+        }
+        for (int c = 0; c < 3; ++c) {
+            FreeSpaceJob jc = fs_job(mesh, n, nullptr, 0, 0);
+            jc.quad = reinterpret_cast<const float4 *>(quad3) + c * N;
+            jc.comp_mask = 1 << c;
+            jc.Eacc = lam;
+            jc.acc_coef = -1.0;
+            TRY(freespace_opt<float, float>(ctx, jc, nullptr));
+        }
+        {
+            Launch L_(ctx, "vjp_pack");
+            if (launch_pack_lambda(e8, lam, n[0], N, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "pack lambda");
+        }
+        Launch L_(ctx, "vjp_particles");
+        if (launch_vjp_pairs(ia, da, e8, gE, gx, gy, gz, gq, ctx->stream))
+            return set_err(ctx, OSC_E_CUDA, "vjp gather");
+        return OSC_OK;
+    }
     double *rho, *Eg, *acc, *lam;
     TRY(ws_get(ctx, "vjp_rho", sizeof(double) * N, (void **)&rho));
     TRY(ws_get(ctx, "vjp_E", sizeof(double) * 3 * N, (void **)&Eg));

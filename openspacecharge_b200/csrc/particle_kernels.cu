@@ -659,6 +659,56 @@ int launch_deposit_vec3(const DepositArgs &a, const double *g, double *acc, cuda
     return ok();
 }
 
+// Three quad grids at once: the CIC weights of a particle are computed once and each of
+// the three gradient components adds two float4 reductions (planes k and k+1), the slots
+// of quad_one in the same order.
+__global__ void __launch_bounds__(256) k_deposit_quad3(DepositArgs a, const double *__restrict__ g,
+                                                       float4 *__restrict__ quad3) {
+    const int64_t plane = (int64_t)a.nx * a.ny, N = plane * a.nz;
+    GRID_STRIDE(m, a.np) {
+        const double xm = a.x[m], ym = a.y[m], zm = a.z[m];
+        const double fx = floor((xm - a.xmin) * a.dxi + 1);
+        const double fy = floor((ym - a.ymin) * a.dyi + 1);
+        const double fz = floor((zm - a.zmin) * a.dzi + 1);
+        if (!(fx >= a.nlo[0] && fx + 1 <= a.nhi[0] && fy >= a.nlo[1] && fy + 1 <= a.nhi[1] && fz >= a.nlo[2] &&
+              fz + 1 <= a.nhi[2]))
+            continue;
+        const double ab = ((a.xmin - xm) + fx * a.dx) * a.dxi;
+        const double de = ((a.ymin - ym) + fy * a.dy) * a.dyi;
+        const double gh = ((a.zmin - zm) + fz * a.dz) * a.dzi;
+        const double omab = 1. - ab, omde = 1. - de, omgh = 1. - gh;
+        const int i = (int)fx - a.nlo[0], j = (int)fy - a.nlo[1], k = (int)fz - a.nlo[2];
+        float4 *q0 = quad3 + ((int64_t)i + (int64_t)a.nx * j + plane * k);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const double gc = g[3 * m + c];
+            if (gc == 0.0) continue;
+            const double lo = gh * gc, hi = omgh * gc;
+            red_add(q0 + c * N, make_float4((float)(ab * de * lo), (float)(omab * de * lo), (float)(ab * omde * lo),
+                                            (float)(omab * omde * lo)));
+            red_add(q0 + c * N + plane, make_float4((float)(ab * de * hi), (float)(omab * de * hi),
+                                                    (float)(ab * omde * hi), (float)(omab * omde * hi)));
+        }
+    }
+}
+int launch_deposit_quad3(const DepositArgs &a, const double *g, float *quad3, cudaStream_t st) {
+    if (a.np <= 0) return OSC_OK;
+    k_deposit_quad3<<<nblocks(a.np, 256, 148 * 64), 256, 0, st>>>(a, g, reinterpret_cast<float4 *>(quad3));
+    return ok();
+}
+
+__global__ void k_pack_lambda(float *__restrict__ e8, const double *__restrict__ lam, int nx, int64_t n) {
+    GRID_STRIDE(idx, n) {
+        const bool last = (idx % nx) == nx - 1;
+        e8[8 * idx + 3] = (float)lam[idx];
+        e8[8 * idx + 7] = last ? 0.f : (float)lam[idx + 1];
+    }
+}
+int launch_pack_lambda(float *e8, const double *lam, int nx, int64_t n, cudaStream_t st) {
+    k_pack_lambda<<<nblocks(n, 256), 256, 0, st>>>(e8, lam, nx, n);
+    return ok();
+}
+
 // Value and gradient of the trilinear interpolant of F on the cell (i,j,k) with low-node
 // weights (ab, de, gh): returns F(x) and d/dx, d/dy, d/dz.
 __device__ __forceinline__ void trilinear_grad(const double *__restrict__ F, int64_t n0, int nx, int64_t plane,
@@ -729,6 +779,76 @@ __global__ void __launch_bounds__(256) k_vjp_particles(InterpArgs ia, DepositArg
         if (gq) gq[m] = lv;
     }
 }
+// k_vjp_particles on the x-pair grid: one cell, four 256-bit loads give the 8 nodes' (Ex,
+// Ey, Ez, lam).  A particle whose deposit cell is valid has that cell as its interpolation
+// cell (same formula, same range), so the lam term uses the same nodes; other particles
+// deposit nothing and get no lam term.
+__global__ void __launch_bounds__(256) k_vjp_pairs(InterpArgs ia, DepositArgs da, const float4 *__restrict__ g8,
+                                                   const double *__restrict__ gE, double *gx, double *gy, double *gz,
+                                                   double *gq) {
+    const int64_t plane = (int64_t)ia.nx * ia.ny;
+    GRID_STRIDE(m, ia.np) {
+        const double xm = ia.x[m], ym = ia.y[m], zm = ia.z[m];
+        Cell c;
+        locate(ia, xm, ym, zm, c);
+        const int64_t n0 = c.i + (int64_t)ia.nx * c.j + plane * c.k;
+        // t = dx + 2 dy + 4 dz: rows (dy, dz) hold nodes i (lo) and i+1 (hi)
+        const int64_t rows[4] = {n0, n0 + ia.nx, n0 + plane, n0 + ia.nx + plane};
+        float4 lo[4], hi[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) ldg_pair(g8 + 2 * rows[r], lo[r], hi[r]);
+        const double wx[2] = {c.ab, 1. - c.ab}, wy[2] = {c.de, 1. - c.de}, wz[2] = {c.gh, 1. - c.gh};
+        double val[4] = {0, 0, 0, 0}, d[4][3] = {};
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+            const int a = t & 1, b = (t >> 1) & 1, cz = t >> 2;
+            const float4 f = a ? hi[b + 2 * cz] : lo[b + 2 * cz];
+            const double fv[4] = {f.x, f.y, f.z, f.w};
+            const double w = wx[a] * wy[b] * wz[cz];
+            const double sx = (a ? 1. : -1.) * wy[b] * wz[cz], sy = wx[a] * (b ? 1. : -1.) * wz[cz],
+                         sz = wx[a] * wy[b] * (cz ? 1. : -1.);
+#pragma unroll
+            for (int f4 = 0; f4 < 4; ++f4) {
+                val[f4] += w * fv[f4];
+                d[f4][0] += sx * fv[f4];
+                d[f4][1] += sy * fv[f4];
+                d[f4][2] += sz * fv[f4];
+            }
+        }
+        double g[3] = {0, 0, 0};
+#pragma unroll
+        for (int comp = 0; comp < 3; ++comp) {
+            const double w = gE[3 * m + comp];
+#pragma unroll
+            for (int ax = 0; ax < 3; ++ax) g[ax] += w * d[comp][ax] * ia.hinv[ax];
+        }
+        double lv = 0;
+        const double fx = floor((xm - da.xmin) * da.dxi + 1);
+        const double fy = floor((ym - da.ymin) * da.dyi + 1);
+        const double fz = floor((zm - da.zmin) * da.dzi + 1);
+        if (fx >= da.nlo[0] && fx + 1 <= da.nhi[0] && fy >= da.nlo[1] && fy + 1 <= da.nhi[1] && fz >= da.nlo[2] &&
+            fz + 1 <= da.nhi[2]) {
+            const double q = da.q ? da.q[m] : da.charge1;
+            lv = val[3];
+            g[0] += q * d[3][0] * ia.hinv[0];
+            g[1] += q * d[3][1] * ia.hinv[1];
+            g[2] += q * d[3][2] * ia.hinv[2];
+        }
+        gx[m] = g[0];
+        gy[m] = g[1];
+        gz[m] = g[2];
+        if (gq) gq[m] = lv;
+    }
+}
+int launch_vjp_pairs(const InterpArgs &ia, const DepositArgs &da, const float *e8, const double *gE, double *gx,
+                     double *gy, double *gz, double *gq, cudaStream_t st) {
+    if (ia.np <= 0) return OSC_OK;
+    if (reinterpret_cast<uintptr_t>(e8) % 32) return OSC_E_INVALID;
+    k_vjp_pairs<<<nblocks(ia.np, 256, 148 * 64), 256, 0, st>>>(ia, da, reinterpret_cast<const float4 *>(e8), gE, gx,
+                                                               gy, gz, gq);
+    return ok();
+}
+
 int launch_vjp_particles(const InterpArgs &ia, const DepositArgs &da, const double *E, const double *lam,
                          const double *gE, double *gx, double *gy, double *gz, double *gq, cudaStream_t st) {
     if (ia.np <= 0) return OSC_OK;

@@ -104,6 +104,16 @@ int launch_deposit_vec3(const DepositArgs &a, const double *g, double *acc, cuda
 int launch_vjp_particles(const InterpArgs &ia, const DepositArgs &da, const double *E, const double *lam,
                          const double *gE, double *gx, double *gy, double *gz, double *gq, cudaStream_t st);
 
+// FP32 adjoint: the three gradient components deposited into three quad grids (quad3 =
+// [3][N] float4, the layout of launch_deposit_quad; weights times g[m][c] instead of q).
+int launch_deposit_quad3(const DepositArgs &a, const double *g, float *quad3, cudaStream_t st);
+// Slot 3 of every x-pair node of e8 (the grid launch_interp_pairs reads) set to lam:
+// node n holds lam(n) and lam(n+1) (0 past the row end).
+int launch_pack_lambda(float *e8, const double *lam, int nx, int64_t n, cudaStream_t st);
+// launch_vjp_particles with E and lam read from one x-pair grid (Ex, Ey, Ez, lam per node).
+int launch_vjp_pairs(const InterpArgs &ia, const DepositArgs &da, const float *e8, const double *gE, double *gx,
+                     double *gy, double *gz, double *gq, cudaStream_t st);
+
 // E planes [3][N] (f64) to the x-pair grid read by launch_interp_pairs (e8 32-byte aligned).
 int launch_planes_to_pairs(const double *E, float *e8, int nx, int64_t n, cudaStream_t st);
 

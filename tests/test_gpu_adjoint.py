@@ -104,6 +104,34 @@ def test_fp32_vjp_matches_fp64(ctx):
         assert np.abs(a - b).max() <= 1e-4 * np.abs(b).max()
 
 
+def test_fp32_vjp_outside_particles_and_total_charge(ctx):
+    """FP32 path (quad deposits, x-pair gather) against FP64 with the mesh shifted by three
+    cells, so some particles lie outside it (clamped gather cell, no adjoint-potential term),
+    and with the charge given as a total (q null)."""
+    import ctypes
+    x, y, z, q, mesh = setup(ctx, npart=60000, seed=54)
+    mesh.min = mesh.min + 3 * mesh.delta
+    mesh.max = mesh.max + 3 * mesh.delta
+    rng = np.random.default_rng(7)
+    gE = rng.normal(size=(len(x), 3)) * 1e-3
+    dev = torch.device("cuda", 0)
+    t = [torch.from_numpy(np.ascontiguousarray(a)).to(dev) for a in (x, y, z, gE)]
+    m = mesh.to_c()
+    out = {}
+    for prec in (osc.PREC_FP64, osc.PREC_FP32):
+        g = [torch.empty_like(t[0]) for _ in range(4)]
+        ctx.call("osc_space_charge_step_vjp_dev", ctypes.byref(m), ctypes.c_int64(len(x)),
+                 *[ctypes.c_void_p(a.data_ptr()) for a in t[:3]], None, ctypes.c_double(1e-9), int(prec),
+                 ctypes.c_void_p(t[3].data_ptr()), *[ctypes.c_void_p(a.data_ptr()) for a in g])
+        ctx.synchronize()
+        out[prec] = [a.cpu().numpy() for a in g]
+    lam64 = out[osc.PREC_FP64][3]
+    assert (lam64 == 0).sum() > 0 and (lam64 != 0).sum() > 0  # some particles outside, some inside
+    for a, b in zip(out[osc.PREC_FP32], out[osc.PREC_FP64]):
+        assert np.abs(a - b).max() <= 1e-4 * np.abs(b).max()
+    assert np.array_equal(out[osc.PREC_FP32][3] == 0, lam64 == 0)
+
+
 def test_autograd_function(ctx):
     from openspacecharge_b200.autograd import space_charge_field
     x, y, z, q, mesh = setup(ctx, npart=50000, seed=53)
