@@ -90,28 +90,61 @@ def make_bunch(npart):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    """SM clock, its maximum and the throttle reasons of one GPU, read during the timed region:
+    through NVML every 5 ms (read-only queries), or from nvidia-smi every 200 ms when NVML
+    cannot be loaded."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, gpu_index):
         self.gpu = gpu_index
-        self.samples = []
+        self.samples = []  # (sm_mhz, sm_max_mhz, set of reason names)
+        self.source = None
         self._stop = threading.Event()
         self._t = None
+        self._nvml = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(gpu_index)
+            bits = (pynvml.nvmlClocksEventReasonHwSlowdown, pynvml.nvmlClocksEventReasonHwThermalSlowdown,
+                    pynvml.nvmlClocksEventReasonSwThermalSlowdown, pynvml.nvmlClocksEventReasonSwPowerCap)
+            self._nvml = (pynvml, h, bits)
+        except Exception:
+            self._nvml = None
+
+    def _sample_nvml(self):
+        nv, h, bits = self._nvml
+        sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        self.samples.append((float(sm), float(mx), {n for n, b in zip(self.NAMES, bits) if r & b}))
+
+    def _sample_smi(self):
+        out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                              "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+        if out.returncode == 0 and out.stdout.strip():
+            f = [v.strip() for v in out.stdout.strip().split(",")]
+            num = lambda v: float(v) if v.replace(".", "").isdigit() else None
+            self.samples.append((num(f[1]), num(f[2]),
+                                 {n for i, n in enumerate(self.NAMES) if len(f) > 5 + i and
+                                  f[5 + i].lower().startswith("active")}))
 
     def _run(self):
         while not self._stop.is_set():
             try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
-                if out.returncode == 0 and out.stdout.strip():
-                    self.samples.append([s.strip() for s in out.stdout.strip().split(",")])
+                if self._nvml:
+                    self._sample_nvml()
+                    self.source = "nvml"
+                else:
+                    self._sample_smi()
+                    self.source = "nvidia-smi"
             except Exception:
                 pass
-            self._stop.wait(0.2)
+            self._stop.wait(0.005 if self._nvml else 0.2)
 
     def __enter__(self):
         self._t = threading.Thread(target=self._run, daemon=True)
@@ -121,20 +154,21 @@ class ClockSampler:
     def __exit__(self, *a):
         self._stop.set()
         self._t.join(timeout=10)
+        if not self.samples:  # the region ended before the first poll: one sample right after it
+            try:
+                self._sample_nvml() if self._nvml else self._sample_smi()
+                self.source = "nvml" if self._nvml else "nvidia-smi"
+            except Exception:
+                pass
 
     def summary(self):
         if not self.samples:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
-        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = set()
-        for s in self.samples:
-            for i, nm in enumerate(names):
-                if len(s) > 5 + i and s[5 + i].lower().startswith("active"):
-                    reasons.add(nm)
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock query unavailable"], "samples": 0}
+        sm = [s[0] for s in self.samples if s[0] is not None]
+        mx = [s[1] for s in self.samples if s[1] is not None]
+        reasons = set().union(*(s[2] for s in self.samples))
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(self.samples)}
+                "reasons": sorted(reasons), "samples": len(self.samples), "source": self.source}
 
 
 # ---------------------------------------------------------------------------------------
