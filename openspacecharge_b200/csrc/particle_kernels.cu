@@ -56,9 +56,9 @@ __global__ void __launch_bounds__(256) k_deposit(DepositArgs a, TA *__restrict__
         int i = 0, j = 0, k = 0;
         if (!skip) {
             if (a.mode == 0) {
-                fx = floor((xm - a.xmin) * a.dxi + 1);
-                fy = floor((ym - a.ymin) * a.dyi + 1);
-                fz = floor((zm - a.zmin) * a.dzi + 1);
+                fx = floor(__dmul_rn(xm - a.xmin, a.dxi) + 1);
+                fy = floor(__dmul_rn(ym - a.ymin, a.dyi) + 1);
+                fz = floor(__dmul_rn(zm - a.zmin, a.dzi) + 1);
                 ab = ((a.xmin - xm) + fx * a.dx) * a.dxi;
                 de = ((a.ymin - ym) + fy * a.dy) * a.dyi;
                 gh = ((a.zmin - zm) + fz * a.dz) * a.dzi;
@@ -66,9 +66,9 @@ __global__ void __launch_bounds__(256) k_deposit(DepositArgs a, TA *__restrict__
                 outside = !(fx >= a.nlo[0] && fx + 1 <= a.nhi[0] && fy >= a.nlo[1] && fy + 1 <= a.nhi[1] &&
                             fz >= a.nlo[2] && fz + 1 <= a.nhi[2]);
             } else {
-                fx = floor((xm - a.xmin) * a.dxi + a.nlogbl[0]);
-                fy = floor((ym - a.ymin) * a.dyi + a.nlogbl[1]);
-                fz = floor((zm - a.zmin) * a.dzi + a.nlogbl[2]);
+                fx = floor(__dmul_rn(xm - a.xmin, a.dxi) + a.nlogbl[0]);
+                fy = floor(__dmul_rn(ym - a.ymin, a.dyi) + a.nlogbl[1]);
+                fz = floor(__dmul_rn(zm - a.zmin, a.dzi) + a.nlogbl[2]);
                 ab = ((a.xmin - xm) + (fx - a.nlogbl[0] + 1) * a.dx) * a.dxi;
                 de = ((a.ymin - ym) + (fy - a.nlogbl[1] + 1) * a.dy) * a.dyi;
                 gh = ((a.zmin - zm) + (fz - a.nlogbl[2] + 1) * a.dz) * a.dzi;
@@ -135,9 +135,9 @@ template int launch_fixed_to_real<double>(const unsigned long long *, double *, 
 __device__ __forceinline__ int quad_one(const DepositArgs &a, float4 *__restrict__ quad, int64_t plane, double xm,
                                         double ym, double zm, double c) {
     if (a.check_finite && !(isfinite(xm) && isfinite(ym) && isfinite(zm))) return 2;
-    const double fx = floor((xm - a.xmin) * a.dxi + 1);
-    const double fy = floor((ym - a.ymin) * a.dyi + 1);
-    const double fz = floor((zm - a.zmin) * a.dzi + 1);
+    const double fx = floor(__dmul_rn(xm - a.xmin, a.dxi) + 1);
+    const double fy = floor(__dmul_rn(ym - a.ymin, a.dyi) + 1);
+    const double fz = floor(__dmul_rn(zm - a.zmin, a.dzi) + 1);
     if (!(fx >= a.nlo[0] && fx + 1 <= a.nhi[0] && fy >= a.nlo[1] && fy + 1 <= a.nhi[1] && fz >= a.nlo[2] &&
           fz + 1 <= a.nhi[2]))
         return 1;
@@ -222,7 +222,7 @@ __device__ __forceinline__ bool locate(const InterpArgs &a, double x, double y, 
     bool flag = false;
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-        double f = floor((pos[d] - a.min[d]) * a.hinv[d] + 1);
+        double f = floor(__dmul_rn(pos[d] - a.min[d], a.hinv[d]) + 1);
         const double hi = (double)(a.nhi[d] - 1);
         if (!(f >= 1.0 && f <= hi)) {  // NaN lands here too
             flag = true;
@@ -625,9 +625,9 @@ __global__ void __launch_bounds__(256) k_deposit_vec3(DepositArgs a, const doubl
     const int64_t plane = (int64_t)a.nx * a.ny, N = plane * a.nz;
     GRID_STRIDE(m, a.np) {
         const double xm = a.x[m], ym = a.y[m], zm = a.z[m];
-        const double fx = floor((xm - a.xmin) * a.dxi + 1);
-        const double fy = floor((ym - a.ymin) * a.dyi + 1);
-        const double fz = floor((zm - a.zmin) * a.dzi + 1);
+        const double fx = floor(__dmul_rn(xm - a.xmin, a.dxi) + 1);
+        const double fy = floor(__dmul_rn(ym - a.ymin, a.dyi) + 1);
+        const double fz = floor(__dmul_rn(zm - a.zmin, a.dzi) + 1);
         if (!(fx >= a.nlo[0] && fx + 1 <= a.nhi[0] && fy >= a.nlo[1] && fy + 1 <= a.nhi[1] && fz >= a.nlo[2] &&
               fz + 1 <= a.nhi[2]))
             continue;
@@ -667,9 +667,9 @@ __global__ void __launch_bounds__(256) k_deposit_quad3(DepositArgs a, const doub
     const int64_t plane = (int64_t)a.nx * a.ny, N = plane * a.nz;
     GRID_STRIDE(m, a.np) {
         const double xm = a.x[m], ym = a.y[m], zm = a.z[m];
-        const double fx = floor((xm - a.xmin) * a.dxi + 1);
-        const double fy = floor((ym - a.ymin) * a.dyi + 1);
-        const double fz = floor((zm - a.zmin) * a.dzi + 1);
+        const double fx = floor(__dmul_rn(xm - a.xmin, a.dxi) + 1);
+        const double fy = floor(__dmul_rn(ym - a.ymin, a.dyi) + 1);
+        const double fz = floor(__dmul_rn(zm - a.zmin, a.dzi) + 1);
         if (!(fx >= a.nlo[0] && fx + 1 <= a.nhi[0] && fy >= a.nlo[1] && fy + 1 <= a.nhi[1] && fz >= a.nlo[2] &&
               fz + 1 <= a.nhi[2]))
             continue;
@@ -756,9 +756,9 @@ __global__ void __launch_bounds__(256) k_vjp_particles(InterpArgs ia, DepositArg
             g[2] += w * gr[2];
         }
         double lv = 0;
-        const double fx = floor((xm - da.xmin) * da.dxi + 1);
-        const double fy = floor((ym - da.ymin) * da.dyi + 1);
-        const double fz = floor((zm - da.zmin) * da.dzi + 1);
+        const double fx = floor(__dmul_rn(xm - da.xmin, da.dxi) + 1);
+        const double fy = floor(__dmul_rn(ym - da.ymin, da.dyi) + 1);
+        const double fz = floor(__dmul_rn(zm - da.zmin, da.dzi) + 1);
         if (fx >= da.nlo[0] && fx + 1 <= da.nhi[0] && fy >= da.nlo[1] && fy + 1 <= da.nhi[1] && fz >= da.nlo[2] &&
             fz + 1 <= da.nhi[2]) {
             const double ab = ((da.xmin - xm) + fx * da.dx) * da.dxi;
@@ -823,9 +823,9 @@ __global__ void __launch_bounds__(256) k_vjp_pairs(InterpArgs ia, DepositArgs da
             for (int ax = 0; ax < 3; ++ax) g[ax] += w * d[comp][ax] * ia.hinv[ax];
         }
         double lv = 0;
-        const double fx = floor((xm - da.xmin) * da.dxi + 1);
-        const double fy = floor((ym - da.ymin) * da.dyi + 1);
-        const double fz = floor((zm - da.zmin) * da.dzi + 1);
+        const double fx = floor(__dmul_rn(xm - da.xmin, da.dxi) + 1);
+        const double fy = floor(__dmul_rn(ym - da.ymin, da.dyi) + 1);
+        const double fz = floor(__dmul_rn(zm - da.zmin, da.dzi) + 1);
         if (fx >= da.nlo[0] && fx + 1 <= da.nhi[0] && fy >= da.nlo[1] && fy + 1 <= da.nhi[1] && fz >= da.nlo[2] &&
             fz + 1 <= da.nhi[2]) {
             const double q = da.q ? da.q[m] : da.charge1;

@@ -6,7 +6,9 @@
 namespace osc {
 
 // CIC deposition.  mode 0 follows deposit_particles (code/open_spacecharge_mod.f90:257-283):
-// ip = floor((x-xmin)/dx + 1), low-node weight ab = ((xmin-x) + ip*dx)/dx, charge per
+// ip = floor((x-xmin)*dxi + 1) with the product rounded before the add (no fused multiply-
+// add, as the reference evaluates it, so a particle on a cell plane gets the reference's
+// cell), low-node weight ab = ((xmin-x) + ip*dx)*dxi, charge per
 // particle.  mode 1 follows depose_rho_scalar (code/test_mod.f90:442-470): ip uses the
 // global lower index nlogbl, lost particles are skipped, weights carry no charge (the grid
 // is scaled afterwards).  Particles whose stencil leaves the array are counted, not written.
