@@ -40,6 +40,23 @@ inline int d2h(osc_ctx *ctx, void *h, const void *d, size_t bytes) {
 }
 inline int sync(osc_ctx *ctx) { return ctx_sync(ctx); }
 
+// Auxiliary streams of a context: kAuxSlots streams and kAuxSlots + 1 events, created once
+// (the last event belongs to the main stream).
+constexpr int kAuxSlots = 4;
+inline int ensure_aux(osc_ctx *ctx) {
+    while ((int)ctx->aux.size() < kAuxSlots) {
+        cudaStream_t s;
+        CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "aux stream");
+        ctx->aux.push_back(s);
+    }
+    while ((int)ctx->aux_ev.size() < kAuxSlots + 1) {
+        cudaEvent_t e;
+        CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "aux event");
+        ctx->aux_ev.push_back(e);
+    }
+    return OSC_OK;
+}
+
 // Stage a host array on the device under a workspace name.
 template <typename T> inline int stage_in(osc_ctx *ctx, const char *name, const T *h, size_t n, T **d) {
     if (!h) {

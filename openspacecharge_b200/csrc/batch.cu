@@ -34,24 +34,7 @@ int upload(osc_ctx *ctx, const char *name, const void *h, size_t bytes, void **d
     return h2d(ctx, *d, h, bytes);
 }
 
-constexpr int kSlots = 4;  // grid-shape groups solved concurrently on auxiliary streams
-
-// Creates the context's auxiliary streams and their events once (plus one event for the
-// main stream at index kSlots).
-int ensure_aux(osc_ctx *ctx) {
-    if ((int)ctx->aux.size() >= kSlots) return OSC_OK;
-    while ((int)ctx->aux.size() < kSlots) {
-        cudaStream_t s;
-        CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "aux stream");
-        ctx->aux.push_back(s);
-    }
-    while ((int)ctx->aux_ev.size() < kSlots + 1) {
-        cudaEvent_t e;
-        CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "aux event");
-        ctx->aux_ev.push_back(e);
-    }
-    return OSC_OK;
-}
+constexpr int kSlots = kAuxSlots;  // grid-shape groups solved concurrently on auxiliary streams
 
 // Issues work on auxiliary slot `slot` (1-based) for its lifetime; restores the main stream.
 struct SlotGuard {
