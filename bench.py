@@ -319,7 +319,8 @@ def run_ours(args, ws, rank, local, dist):
         ctx.synchronize()
         d = (E64o - E64).abs()
         fp64["fp64_optimised"] = {"value": ws * 1000.0 / ms64o, "ms_per_step": ms64o,
-                                  "max_rel_err_vs_plain": float((d.amax(0) / E64.abs().amax(0)).max())}
+                                  "max_rel_err_vs_plain": float((d.amax(0) / E64.abs().amax(0)).max()),
+                                  "kernels": kernel_profile(ctx, osc, lambda: step(osc.PREC_FP64, E64o), 3)}
 
     # per-kernel profile of the FP32 step: CUDA events around each launch on the stream
     ctx.set_option(osc.OPT_PROFILE, 1)
