@@ -43,7 +43,7 @@ int osc_space_charge_step_vjp_dev(osc_ctx *ctx, const osc_mesh3d *mesh, int64_t 
         TRY(counters_reset(ctx));
         CK(cudaMemsetAsync(quad, 0, sizeof(float4) * N, ctx->stream), "memset quad");
         CK(cudaMemsetAsync(quad3, 0, sizeof(float4) * 3 * N, ctx->stream), "memset quad3");
-        CK(cudaMemsetAsync(lam, 0, sizeof(double) * N, ctx->stream), "memset lambda");
+        CK(cudaMemsetAsync(lam, 0, sizeof(double) * N, ctx->stream), "memset lambda");  // three-solve path
         {
             Launch L_(ctx, "deposit_f32");
             if (launch_deposit_quad(da, quad, ctx->d_small, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "deposit");
@@ -57,15 +57,26 @@ int osc_space_charge_step_vjp_dev(osc_ctx *ctx, const osc_mesh3d *mesh, int64_t 
             Launch L_(ctx, "vjp_deposit");
             if (launch_deposit_quad3(da, gE, quad3, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "vjp deposit");
         }
-        for (int c = 0; c < 3; ++c) {
-            FreeSpaceJob jc = fs_job(mesh, n, nullptr, 0, 0);
-            jc.quad = reinterpret_cast<const float4 *>(quad3) + c * N;
-            jc.comp_mask = 1 << c;
-            jc.Eacc = lam;
-            jc.acc_coef = -1.0;
-            TRY(freespace_opt<float, float>(ctx, jc, nullptr));
-        }
-        {
+        if (zconv_warp_ok(2 * n[2], n[2], (int)sizeof(float))) {
+            // one solve: the three gradient grids are transformed, multiplied by their
+            // kernels' spectra and summed before a single inverse, which writes lambda
+            // straight into slot 3 of the x-pair grid
+            FreeSpaceJob js = fs_job(mesh, n, nullptr, 0, 0);
+            js.quad = reinterpret_cast<const float4 *>(quad3);
+            js.sum3 = 1;
+            js.E4 = e8;
+            js.e4_pairs = 1;
+            js.acc_coef = -1.0;
+            TRY(freespace_opt<float, float>(ctx, js, nullptr));
+        } else {
+            for (int c = 0; c < 3; ++c) {
+                FreeSpaceJob jc = fs_job(mesh, n, nullptr, 0, 0);
+                jc.quad = reinterpret_cast<const float4 *>(quad3) + c * N;
+                jc.comp_mask = 1 << c;
+                jc.Eacc = lam;
+                jc.acc_coef = -1.0;
+                TRY(freespace_opt<float, float>(ctx, jc, nullptr));
+            }
             Launch L_(ctx, "vjp_pack");
             if (launch_pack_lambda(e8, lam, n[0], N, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "pack lambda");
         }

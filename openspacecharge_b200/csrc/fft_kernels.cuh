@@ -123,6 +123,9 @@ struct ZConvArgs {
     // member b are b*in_bstride, b*out_bstride and b*g_bstride (elements of the spectrum)
     int nbatch;
     int64_t in_bstride, out_bstride, g_bstride;
+    // > 0: the nsum members are the inputs of the single output (warp engine, staged real
+    // spectra): out = inverse of sum_s spectrum[gdir[s]] x forward(input s)
+    int nsum;
 };
 
 // Transform of real lines that are even (par = +1) or odd (par = -1) about index 0 on the

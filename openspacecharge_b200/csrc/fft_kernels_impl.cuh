@@ -776,11 +776,13 @@ int launch_c2r_rows(const cplx<T> *in, const C2RArgs &a, const TwPair<cplx<T>> &
 template <typename T, int W, int MODE, int L, int... Rs>
 inline int launch_zconv_warp_k(const cplx<T> *in, cplx<T> *out, const ZConvArgs &a, const TwPair<cplx<T>> &tw,
                                cudaStream_t st) {
-    const size_t sm = zconv_warp_smem<T>(L, W, MODE, a.nout, a.g[0].zpitch);
+    const size_t sm = zconv_warp_smem<T>(L, W, MODE, MODE == ZW_SUM ? a.nsum : a.nout, a.g[0].zpitch);
     auto kern = k_zconv_warp<T, W, MODE, L, Rs...>;
     int rc = set_smem(kern, sm);
     if (rc) return rc;
-    const dim3 grid((unsigned)ceil_div(a.ncols, W), (unsigned)(a.nbatch > 0 ? a.nbatch : 1));
+    // summed inputs: the members are the inputs of one output, read by every CTA
+    const unsigned gy = MODE == ZW_SUM ? 1u : (unsigned)(a.nbatch > 0 ? a.nbatch : 1);
+    const dim3 grid((unsigned)ceil_div(a.ncols, W), gy);
     kern<<<grid, W * 32, sm, st>>>(in, out, a, tw.wt, tw.rt);
     return launch_ok();
 }
@@ -790,18 +792,20 @@ inline int launch_zconv_warp(WarpFft<L, Rs...>, const cplx<T> *in, cplx<T> *out,
     return launch_zconv_warp_k<T, zw_warps<T>(), MODE, L, Rs...>(in, out, a, tw, st);
 }
 
-// Staged Green columns need real spectra, even/odd in z, one common 16-byte column pitch.
+// Staged Green columns need real spectra, even/odd in z, one common 16-byte column pitch
+// (one column per output, or per input when the inputs are summed).
 template <typename T> inline bool zconv_can_stage(const ZConvArgs &a) {
     const int zp = a.g[0].zpitch;
     if (zp <= 0 || (zp * sizeof(T)) % 16) return false;
-    for (int o = 0; o < a.nout; ++o) {
+    const int ns = a.nsum > 0 ? a.nsum : a.nout;
+    for (int o = 0; o < ns; ++o) {
         const int gd = a.gdir[o];
         if (gd < 0 || a.gimg[o] >= 0) return false;
         const GSpecDev &g = a.g[gd];
         if (!g.real_valued || !g.sym_z || !g.zinner || g.zpitch != zp || g.dimz > zp) return false;
         if (reinterpret_cast<uintptr_t>(g.data) % 16) return false;
     }
-    return zconv_warp_smem<T>(a.p.L, zw_warps<T>(), ZW_STAGED, a.nout, zp) <= 100 * 1024;
+    return zconv_warp_smem<T>(a.p.L, zw_warps<T>(), ZW_STAGED, ns, zp) <= 100 * 1024;
 }
 
 template <typename T>
@@ -815,9 +819,11 @@ int launch_zconv(const cplx<T> *in, cplx<T> *out, const ZConvArgs &a, const TwPa
         for (int o = 0; o < a.nout; ++o) img |= a.gimg[o] >= 0;
         if (tw.wt == tw.rt) return OSC_E_INVALID;
         const bool staged = !img && zconv_can_stage<T>(a);
+        if (a.nsum > 0 && (img || !staged || a.nout != 1)) return OSC_E_UNSUPPORTED;
         return dispatch_warp_len(L, [&](auto eng) -> int {
             using E = decltype(eng);
             if constexpr (E::kLen > 0) {
+                if (a.nsum > 0) return launch_zconv_warp<T, ZW_SUM>(eng, in, out, a, tw, st);
                 if (img) return launch_zconv_warp<T, ZW_IMAGE>(eng, in, out, a, tw, st);
                 if (staged) return launch_zconv_warp<T, ZW_STAGED>(eng, in, out, a, tw, st);
                 return launch_zconv_warp<T, ZW_DIRECT>(eng, in, out, a, tw, st);
@@ -825,6 +831,7 @@ int launch_zconv(const cplx<T> *in, cplx<T> *out, const ZConvArgs &a, const TwPa
             return OSC_E_INVALID;
         });
     }
+    if (a.nsum > 0) return OSC_E_UNSUPPORTED;  // summed inputs: warp engine lengths only
     for (int i = 0; i < a.ng; ++i)
         if (a.g[i].zinner) return OSC_E_INVALID;
     return dispatch_fft_len<T>(L, [&](auto eng) -> int {

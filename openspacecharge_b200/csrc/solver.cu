@@ -320,6 +320,11 @@ int freespace_opt(osc_ctx *c, const FreeSpaceJob &j, const TIn *rho) {
     const int B = j.nbatch > 0 ? j.nbatch : 1;
     if (B > 1 && (j.phi || j.E || j.B || !j.E4 || !j.gbatch || j.at_cathode))
         return set_err(c, OSC_E_INVALID, "batched solves produce the E grid only");
+    if (j.sum3 && (B > 1 || !j.quad || !j.E4 || !j.e4_pairs || j.phi || j.E || j.B || j.at_cathode || j.want_phi ||
+                   j.calc_b || !std::is_same<T, float>::value))
+        return set_err(c, OSC_E_INVALID, "summed solve: FP32 quad inputs to the x-pair grid only");
+    // input and output members: the summed solve reads three grids and writes one
+    const int Bin = j.sum3 ? 3 : B, Bout = j.sum3 ? 1 : B;
     GreenSet local;
     GreenSet *gs = &local;
     if (j.gbatch) {
@@ -355,6 +360,16 @@ int freespace_opt(osc_ctx *c, const FreeSpaceJob &j, const TIn *rho) {
         d.coef = coef;
         d.last_x = nx - 1;
     };
+    if (j.sum3) {
+        za.nsum = 3;
+        for (int q = 0; q < 3; ++q) {
+            za.gdir[q] = spec_index(q + 1, false);
+            za.gimg[q] = -1;
+        }
+        cr.ndest[0] = 0;
+        nout = 1;
+        add_dest(0, j.E4, 4, 3, j.acc_coef);
+    } else {
     if (j.want_phi && j.phi) add_dest(add_out(0, 1.0), j.phi, 1, 0, 1.0);
     if (j.want_e || j.calc_b) {
         for (int q = 0; q < 3; ++q) {
@@ -378,13 +393,14 @@ int freespace_opt(osc_ctx *c, const FreeSpaceJob &j, const TIn *rho) {
             add_dest(add_out(2, -1.0), j.B, 1, 0, -j.bcoef);
         }
     }
+    }  // summed solve or per-output destinations
     if (j.calc_b && j.B) TRY(cuda_check(c, cudaMemsetAsync(j.B + 2 * N, 0, sizeof(double) * N, c->stream), "memset B"));
 
     V *X1, *X2, *X3, *X4;
-    TRY(ws_get(c, "fs_x1", sizeof(V) * (size_t)B * nxh * ny * nz, (void **)&X1));
-    TRY(ws_get(c, "fs_x2", sizeof(V) * (size_t)B * nxh * Ny * nz, (void **)&X2));
-    TRY(ws_get(c, "fs_x3", sizeof(V) * (size_t)nout * B * nxh * Ny * nz, (void **)&X3));
-    TRY(ws_get(c, "fs_x4", sizeof(V) * (size_t)nout * B * nxh * ny * nz, (void **)&X4));
+    TRY(ws_get(c, "fs_x1", sizeof(V) * (size_t)Bin * nxh * ny * nz, (void **)&X1));
+    TRY(ws_get(c, "fs_x2", sizeof(V) * (size_t)Bin * nxh * Ny * nz, (void **)&X2));
+    TRY(ws_get(c, "fs_x3", sizeof(V) * (size_t)nout * Bout * nxh * Ny * nz, (void **)&X3));
+    TRY(ws_get(c, "fs_x4", sizeof(V) * (size_t)nout * Bout * nxh * ny * nz, (void **)&X4));
     TwPair<V> twx, twy, twz;
     TRY(twiddles<T>(c, Nx, &twx));
     TRY(twiddles<T>(c, Ny, &twy));
@@ -394,7 +410,7 @@ int freespace_opt(osc_ctx *c, const FreeSpaceJob &j, const TIn *rho) {
     R2CArgs ra;
     ra.p = px;
     ra.nin = nx;
-    ra.nrows = (int64_t)B * ny * nz;
+    ra.nrows = (int64_t)Bin * ny * nz;
     ra.in_rstride = nx;
     ra.out_rstride = nxh;
     {
@@ -430,7 +446,7 @@ int freespace_opt(osc_ctx *c, const FreeSpaceJob &j, const TIn *rho) {
     ly.flip_mask = 0;
     {
         Launch L_(c, "fft_y_fwd");
-        TRY(kerr(c, launch_lines<T>(X1, X2, ly, B * nz, 1, false, twy, c->stream), "y forward"));
+        TRY(kerr(c, launch_lines<T>(X1, X2, ly, Bin * nz, 1, false, twy, c->stream), "y forward"));
     }
     // z: forward, spectral product, inverse
     za.p = pz;
@@ -445,12 +461,12 @@ int freespace_opt(osc_ctx *c, const FreeSpaceJob &j, const TIn *rho) {
     const bool zin = zconv_warp_ok(Nz, nz, (int)sizeof(T));
     za.out_estride = zin ? 1 : (int64_t)nxh * Ny;
     za.out_colstride = zin ? nz : 1;
-    za.out_cstride = (int64_t)B * nxh * Ny * nz;
+    za.out_cstride = (int64_t)Bout * nxh * Ny * nz;
     za.nout = nout;
     za.img_phase_mul = nz - 1;
     za.ng = gs->nspec;
     za.fault = c->d_fault;
-    za.nbatch = B;
+    za.nbatch = j.sum3 ? 1 : B;
     za.in_bstride = za.out_bstride = (int64_t)nxh * Ny * nz;
     za.g_bstride = j.gbatch ? j.g_bstride : 0;
     for (int i = 0; i < gs->nspec; ++i) za.g[i] = gs->spec[i];
@@ -463,8 +479,8 @@ int freespace_opt(osc_ctx *c, const FreeSpaceJob &j, const TIn *rho) {
     li.sign = -1;
     li.in_len = Ny;
     li.out_len = ny;
-    li.in_zstride = (int64_t)B * nxh * Ny * nz;
-    li.out_zstride = (int64_t)B * nxh * ny * nz;
+    li.in_zstride = (int64_t)Bout * nxh * Ny * nz;
+    li.out_zstride = (int64_t)Bout * nxh * ny * nz;
     if (zin) {  // lines (kx, z) with z fastest, members as planes
         li.ncols = nxh * nz;
         li.in_cstride = li.out_cstride = 1;
@@ -477,14 +493,14 @@ int freespace_opt(osc_ctx *c, const FreeSpaceJob &j, const TIn *rho) {
     }
     {
         Launch L_(c, "fft_y_inv");
-        TRY(kerr(c, launch_lines<T>(X3, X4, li, zin ? B : B * nz, nout, false, twy, c->stream), "y inverse"));
+        TRY(kerr(c, launch_lines<T>(X3, X4, li, zin ? Bout : Bout * nz, nout, false, twy, c->stream), "y inverse"));
     }
     // x: half spectra -> real rows [0,nx), scattered to the outputs
     cr.p = px;
     cr.nout = nx;
-    cr.nrows = (int64_t)B * ny * nz;
+    cr.nrows = (int64_t)Bout * ny * nz;
     cr.in_rstride = zin ? (int64_t)nxh * nz : nxh;
-    cr.in_cstride = (int64_t)B * nxh * ny * nz;
+    cr.in_cstride = (int64_t)Bout * nxh * ny * nz;
     cr.zin = zin ? 1 : 0;
     cr.zin_nz = nz;
     cr.zin_ny = ny;

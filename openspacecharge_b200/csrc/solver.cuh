@@ -42,6 +42,10 @@ struct FreeSpaceJob {
     // FP32 only: the deposit's quad grid (float4 [N]); when set, the x transform sums each
     // node from it and the rho argument is not read
     const float4 *quad = nullptr;
+    // FP32, warp-engine z lengths only: sum3 = 1 makes the three quad grids stacked in quad
+    // ([3][N]) the inputs of one output, sum_c K_c a_c (K_c the E_c kernel), written times
+    // acc_coef into slot 3 of the x-pair grid E4 (the adjoint potential of the step)
+    int sum3 = 0;
     // E components computed (bit c: E_c); each one is also added, times acc_coef, into
     // the single plane Eacc when that is set (adjoint solves accumulate a potential)
     int comp_mask = 7;

@@ -115,13 +115,15 @@ __device__ __forceinline__ void wfft_mid_of(Radices<R0, Rest...>, V *wb, const V
 constexpr int ZW_DIRECT = 0;  // spectra read from global memory
 constexpr int ZW_IMAGE = 1;   // as 0, plus the mirrored-image term
 constexpr int ZW_STAGED = 2;  // real, z-symmetric spectra staged in shared memory by bulk copies
+constexpr int ZW_SUM = 3;     // as 2, for a.nsum inputs (members) and one output: the sum over
+                              // members s of (spectrum gdir[s]) x (transform of input s)
 
 template <typename T, int W, int MODE, int L, int... Rs>
 __global__ void __launch_bounds__(W * 32, zw_minb<T>()) k_zconv_warp(const cplx<T> *__restrict__ in, cplx<T> *__restrict__ out,
                                                        ZConvArgs a, const cplx<T> *__restrict__ twg,
                                                        const cplx<T> *__restrict__ tw_rt) {
     typedef cplx<T> V;
-    constexpr bool IMG = MODE == ZW_IMAGE, GS = MODE == ZW_STAGED;
+    constexpr bool IMG = MODE == ZW_IMAGE, SUM = MODE == ZW_SUM, GS = MODE == ZW_STAGED || SUM;
     constexpr int RF = WarpFft<L, Rs...>::kRad[0];
     static_assert(RF == WarpFft<L, Rs...>::kRad[sizeof...(Rs) - 1], "first and last radix must match");
     static_assert(RF % 2 == 0, "first radix must be even");
@@ -134,10 +136,11 @@ __global__ void __launch_bounds__(W * 32, zw_minb<T>()) k_zconv_warp(const cplx<
     V *tw = reinterpret_cast<V *>(smem_raw);
     V *wbufs = tw + L;
     V *rbufs = wbufs + W * WB;                          // IMG: forward spectra, read at mirrored kz
-    T *gst = reinterpret_cast<T *>(wbufs + W * WB);     // GS: Green columns [W][nout][zpitch]
+    T *gst = reinterpret_cast<T *>(wbufs + W * WB);     // GS: Green columns [W][nst][zpitch]
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int col0 = blockIdx.x * W;
     const int zp = a.g[0].zpitch;
+    const int nst = SUM ? a.nsum : a.nout;  // staged Green columns per (kx,ky) column
     in += blockIdx.y * a.in_bstride;
     out += blockIdx.y * a.out_bstride;
     const int64_t goff = blockIdx.y * a.g_bstride;
@@ -146,30 +149,32 @@ __global__ void __launch_bounds__(W * 32, zw_minb<T>()) k_zconv_warp(const cplx<
         if (threadIdx.x == 0) {
             mbar_init(&gbar, 1);
             const int ncv = min(W, a.ncols - col0);
-            mbar_arrive_expect_tx(&gbar, (unsigned)(ncv * a.nout * zp * (int)sizeof(T)));
+            mbar_arrive_expect_tx(&gbar, (unsigned)(ncv * nst * zp * (int)sizeof(T)));
             for (int c = 0; c < ncv; ++c) {
                 const int col = col0 + c, ky = col / a.nxh, kx = col - ky * a.nxh;
-                for (int o = 0; o < a.nout; ++o) {
+                for (int o = 0; o < nst; ++o) {
                     const GSpecDev &g = a.g[a.gdir[o]];
                     const int yy = (g.sym_y && ky > a.ny) ? a.Ny - ky : ky;
                     const T *src = reinterpret_cast<const T *>(g.data) + goff + ((int64_t)yy * a.nxh + kx) * zp;
-                    bulk_g2s(gst + (c * a.nout + o) * zp, src, (unsigned)(zp * sizeof(T)), &gbar);
+                    bulk_g2s(gst + (c * nst + o) * zp, src, (unsigned)(zp * sizeof(T)), &gbar);
                 }
             }
         }
     }
     load_twiddles(tw, twg, L);
-    for (int idx = threadIdx.x; idx < W * a.nz; idx += W * 32) {
-        const int e = idx / W, c = idx - e * W;
-        const int col = col0 + c;
-        V v = mk<T>(0, 0);
-        if (col < a.ncols) v = in[(int64_t)e * a.in_estride + col];
-        wbufs[c * WB + wpad(e)] = v;
-    }
-    __syncthreads();
-    // forward transform (sign +1) of the column; the upper half of its input is zero
-    V rh[Q][RF];
-    {
+    // the non-zero half (z < nz) of this CTA's W columns of input `src`, into the warp buffers
+    auto load_columns = [&](const cplx<T> *__restrict__ src) {
+        for (int idx = threadIdx.x; idx < W * a.nz; idx += W * 32) {
+            const int e = idx / W, c = idx - e * W;
+            const int col = col0 + c;
+            V v = mk<T>(0, 0);
+            if (col < a.ncols) v = src[(int64_t)e * a.in_estride + col];
+            wbufs[c * WB + wpad(e)] = v;
+        }
+    };
+    // forward transform (sign +1) of this warp's column; the upper half of its input is zero.
+    // rh[q][r] is the spectrum at kz = lane + 32q + NB r
+    auto forward = [&](V (&rh)[Q][RF]) {
         V v[Q][RF];
         S0::load(wb, tw, +1, lane, v, true);
         S0::dft(v, +1);
@@ -179,8 +184,115 @@ __global__ void __launch_bounds__(W * 32, zw_minb<T>()) k_zconv_warp(const cplx<
         wfft_mid_of<V, L>(Radices<Rs...>{}, wb, tw, +1, lane);
         SL::load(wb, tw, +1, lane, rh, false);
         SL::dft(rh, +1);
+    };
+    // CTA-wide wait for the staged Green columns; false when the copies did not complete
+    auto wait_green = [&]() -> bool {
+        if (threadIdx.x == 0) {
+            const bool ok = mbar_wait_bounded(&gbar, 0);
+            if (!ok) {
+                report_fault(a.fault, FAULT_BULK_WAIT);
+                mbar_wait_bounded(&gbar, 0);  // let copies in flight land before leaving
+            }
+            gfail = ok ? 0 : 1;
+        }
+        __syncthreads();
+        return !gfail;  // CTA-uniform
+    };
+    const int colc = min(col0 + warp, a.ncols - 1);
+    const int ky = colc / a.nxh, kx = colc - ky * a.nxh;
+    // v = rh times the staged Green column `slot` of spectrum g (real, even/odd in z)
+    auto staged_product = [&](const V (&rh)[Q][RF], int gd, int slot, V (&v)[Q][RF]) {
+        const GSpecDev &g = a.g[gd];
+        const T *gc = gst + (warp * nst + slot) * zp;
+        const bool yneg = g.sym_y && ky > a.ny && g.par_y < 0;
+        const bool zodd = g.par_z < 0, iu = g.imag_unit;
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const int j = lane + 32 * q;
+            if (S0::full || j < NB) {
+#pragma unroll
+                for (int r = 0; r < RF; ++r) {
+                    const int e = j + NB * r;
+                    T sv;
+                    if (r < RF / 2) {
+                        sv = gc[e];
+                    } else {  // kz >= nz: the value at Nz - kz, odd spectra change sign
+                        sv = gc[L - e];
+                        if (zodd && e != a.nz) sv = -sv;
+                    }
+                    if (yneg) sv = -sv;
+                    const V x = rh[q][r];
+                    v[q][r] = iu ? mk<T>(-x.y * sv, x.x * sv) : mk<T>(x.x * sv, x.y * sv);
+                }
+            }
+        }
+    };
+    // inverse transform of v (first stage from registers) and the store of output o's
+    // window z < nz; false when the store went through the CTA (all warps must follow)
+    auto inverse_store = [&](V (&v)[Q][RF], int o) {
+        S0::dft(v, -1);
+        S0::store(wb, lane, v);
+        __syncwarp();
+        wfft_mid_of<V, L>(Radices<Rs...>{}, wb, tw, -1, lane);
+        SL::load(wb, tw, -1, lane, v, false);
+        SL::dft(v, -1);
+        __syncwarp();
+        if (a.out_estride == 1) {  // kz-innermost output: this warp's column is contiguous
+            if (col0 + warp < a.ncols) {
+                V *dst = out + (int64_t)o * a.out_cstride + (int64_t)(col0 + warp) * a.out_colstride;
+#pragma unroll
+                for (int q = 0; q < Q; ++q) {
+                    const int j = lane + 32 * q;
+                    if (S0::full || j < NB)
+#pragma unroll
+                        for (int r = 0; r < RF / 2; ++r) dst[j + NB * r] = v[q][r];  // z = j + NB r < L/2
+                }
+            }
+            return;  // wb is this warp's alone: the next output's first stage writes it
+        }
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const int j = lane + 32 * q;
+            if (S0::full || j < NB)
+#pragma unroll
+                for (int r = 0; r < RF / 2; ++r) wb[wpad(j + NB * r)] = v[q][r];  // z = j + NB r < L/2
+        }
+        __syncthreads();
+        V *dst = out + (int64_t)o * a.out_cstride;
+        for (int idx = threadIdx.x; idx < W * a.nz; idx += W * 32) {
+            const int e = idx / W, c = idx - e * W;
+            const int col = col0 + c;
+            if (col < a.ncols) dst[(int64_t)e * a.out_estride + (int64_t)col * a.out_colstride] = wbufs[c * WB + wpad(e)];
+        }
+        __syncthreads();
+    };
+
+    if constexpr (SUM) {
+        // one output: sum over the inputs of (Green spectrum s) x (transform of input s)
+        V acc[Q][RF];
+        for (int sidx = 0; sidx < a.nsum; ++sidx) {
+            if (sidx) __syncthreads();  // every warp is done with the previous input's columns
+            load_columns(in + sidx * a.in_bstride);
+            __syncthreads();
+            V rh[Q][RF];
+            forward(rh);
+            if (sidx == 0 && !wait_green()) return;
+            __syncwarp();
+            V v[Q][RF];
+            staged_product(rh, a.gdir[sidx], sidx, v);
+#pragma unroll
+            for (int q = 0; q < Q; ++q)
+#pragma unroll
+                for (int r = 0; r < RF; ++r) acc[q][r] = sidx ? cadd(acc[q][r], v[q][r]) : v[q][r];
+        }
+        inverse_store(acc, 0);
+        return;
     }
-    // rh[q][r] holds the spectrum at kz = lane + 32q + NB r
+
+    load_columns(in);
+    __syncthreads();
+    V rh[Q][RF];
+    forward(rh);
     V *rb = rbufs + warp * WB;
     if (IMG) {
 #pragma unroll
@@ -191,49 +303,13 @@ __global__ void __launch_bounds__(W * 32, zw_minb<T>()) k_zconv_warp(const cplx<
                 for (int r = 0; r < RF; ++r) rb[wpad(j + NB * r)] = rh[q][r];
         }
     }
-    if (GS) {
-        if (threadIdx.x == 0) {
-            const bool ok = mbar_wait_bounded(&gbar, 0);
-            if (!ok) {
-                report_fault(a.fault, FAULT_BULK_WAIT);
-                mbar_wait_bounded(&gbar, 0);  // let copies in flight land before leaving
-            }
-            gfail = ok ? 0 : 1;
-        }
-        __syncthreads();
-        if (gfail) return;  // CTA-uniform
-    }
+    if (GS && !wait_green()) return;
     __syncwarp();
-    const int colc = min(col0 + warp, a.ncols - 1);
-    const int ky = colc / a.nxh, kx = colc - ky * a.nxh;
     for (int o = 0; o < a.nout; ++o) {
         const int gd = a.gdir[o], gi = a.gimg[o];
         V v[Q][RF];
         if (GS) {
-            const GSpecDev &g = a.g[gd];
-            const T *gc = gst + (warp * a.nout + o) * zp;
-            const bool yneg = g.sym_y && ky > a.ny && g.par_y < 0;
-            const bool zodd = g.par_z < 0, iu = g.imag_unit;
-#pragma unroll
-            for (int q = 0; q < Q; ++q) {
-                const int j = lane + 32 * q;
-                if (S0::full || j < NB) {
-#pragma unroll
-                    for (int r = 0; r < RF; ++r) {
-                        const int e = j + NB * r;
-                        T s;
-                        if (r < RF / 2) {
-                            s = gc[e];
-                        } else {  // kz >= nz: the value at Nz - kz, odd spectra change sign
-                            s = gc[L - e];
-                            if (zodd && e != a.nz) s = -s;
-                        }
-                        if (yneg) s = -s;
-                        const V x = rh[q][r];
-                        v[q][r] = iu ? mk<T>(-x.y * s, x.x * s) : mk<T>(x.x * s, x.y * s);
-                    }
-                }
-            }
+            staged_product(rh, gd, o, v);
         } else {
             const T icoef = (T)a.img_coef[o];
 #pragma unroll
@@ -260,42 +336,7 @@ __global__ void __launch_bounds__(W * 32, zw_minb<T>()) k_zconv_warp(const cplx<
                 }
             }
         }
-        // inverse transform: first stage from registers, last stage back to the buffer
-        S0::dft(v, -1);
-        S0::store(wb, lane, v);
-        __syncwarp();
-        wfft_mid_of<V, L>(Radices<Rs...>{}, wb, tw, -1, lane);
-        SL::load(wb, tw, -1, lane, v, false);
-        SL::dft(v, -1);
-        __syncwarp();
-        if (a.out_estride == 1) {  // kz-innermost output: this warp's column is contiguous
-            if (col0 + warp < a.ncols) {
-                V *dst = out + (int64_t)o * a.out_cstride + (int64_t)(col0 + warp) * a.out_colstride;
-#pragma unroll
-                for (int q = 0; q < Q; ++q) {
-                    const int j = lane + 32 * q;
-                    if (S0::full || j < NB)
-#pragma unroll
-                        for (int r = 0; r < RF / 2; ++r) dst[j + NB * r] = v[q][r];  // z = j + NB r < L/2
-                }
-            }
-            continue;  // wb is this warp's alone: the next output's first stage writes it
-        }
-#pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            const int j = lane + 32 * q;
-            if (S0::full || j < NB)
-#pragma unroll
-                for (int r = 0; r < RF / 2; ++r) wb[wpad(j + NB * r)] = v[q][r];  // z = j + NB r < L/2
-        }
-        __syncthreads();
-        V *dst = out + (int64_t)o * a.out_cstride;
-        for (int idx = threadIdx.x; idx < W * a.nz; idx += W * 32) {
-            const int e = idx / W, c = idx - e * W;
-            const int col = col0 + c;
-            if (col < a.ncols) dst[(int64_t)e * a.out_estride + (int64_t)col * a.out_colstride] = wbufs[c * WB + wpad(e)];
-        }
-        __syncthreads();
+        inverse_store(v, o);
     }
 }
 
@@ -304,7 +345,7 @@ __global__ void __launch_bounds__(W * 32, zw_minb<T>()) k_zconv_warp(const cplx<
 template <typename T> inline size_t zconv_warp_smem(int L, int W, int mode, int nout, int zp) {
     size_t b = sizeof(cplx<T>) * ((size_t)L + (size_t)W * wbuf_len(L));
     if (mode == ZW_IMAGE) b += sizeof(cplx<T>) * (size_t)W * wbuf_len(L);
-    if (mode == ZW_STAGED) b += sizeof(T) * (size_t)W * nout * zp;
+    if (mode == ZW_STAGED || mode == ZW_SUM) b += sizeof(T) * (size_t)W * nout * zp;
     return b;
 }
 

@@ -26,12 +26,17 @@ def det():
     c.close()
 
 
-def setup(ctx, npart=20000, seed=51):
+# z length 2*32 = 64 has no warp z engine: the FP32 adjoint potential takes three one-
+# component solves; 2*48 = 96 has one: the three are summed in one solve
+N_SUMMED = (32, 32, 48)
+
+
+def setup(ctx, npart=20000, seed=51, n=N):
     x, y, z = gendist(npart, sigma=(1e-3, 1e-3, 1e-3), seed=seed)
     q = np.random.default_rng(seed).uniform(0.5, 1.5, npart) * 1e-15
-    delta, umin = osc.get_mesh_quantities(ctx, x, y, z, (1, 1, 1), N, 0)
-    umax = umin + (np.array(N) - 1) * delta
-    mesh = osc.Mesh3D(nlo=(1, 1, 1), nhi=N, min=umin, max=umax, delta=delta, gamma=GAMMA)
+    delta, umin = osc.get_mesh_quantities(ctx, x, y, z, (1, 1, 1), n, 0)
+    umax = umin + (np.array(n) - 1) * delta
+    mesh = osc.Mesh3D(nlo=(1, 1, 1), nhi=n, min=umin, max=umax, delta=delta, gamma=GAMMA)
     return x, y, z, q, mesh
 
 
@@ -94,8 +99,9 @@ def test_vjp_matches_central_differences(det):
         assert abs(fd - full) <= 1e-6 * abs(full), (m, fd, full)
 
 
-def test_fp32_vjp_matches_fp64(ctx):
-    x, y, z, q, mesh = setup(ctx, npart=100000, seed=52)
+@pytest.mark.parametrize("n", [N, N_SUMMED])
+def test_fp32_vjp_matches_fp64(ctx, n):
+    x, y, z, q, mesh = setup(ctx, npart=100000, seed=52, n=n)
     _, E = loss(ctx, mesh, x, y, z, q, osc.PREC_FP64)
     gE = 2 * q[:, None] * E
     g64 = vjp(ctx, mesh, x, y, z, q, gE, osc.PREC_FP64)
@@ -104,12 +110,13 @@ def test_fp32_vjp_matches_fp64(ctx):
         assert np.abs(a - b).max() <= 1e-4 * np.abs(b).max()
 
 
-def test_fp32_vjp_outside_particles_and_total_charge(ctx):
+@pytest.mark.parametrize("n", [N, N_SUMMED])
+def test_fp32_vjp_outside_particles_and_total_charge(ctx, n):
     """FP32 path (quad deposits, x-pair gather) against FP64 with the mesh shifted by three
     cells, so some particles lie outside it (clamped gather cell, no adjoint-potential term),
     and with the charge given as a total (q null)."""
     import ctypes
-    x, y, z, q, mesh = setup(ctx, npart=60000, seed=54)
+    x, y, z, q, mesh = setup(ctx, npart=60000, seed=54, n=n)
     mesh.min = mesh.min + 3 * mesh.delta
     mesh.max = mesh.max + 3 * mesh.delta
     rng = np.random.default_rng(7)
