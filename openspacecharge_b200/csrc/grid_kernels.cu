@@ -311,6 +311,43 @@ int launch_fd_efield(const double *phi, double *E, int nx, int ny, int nz, doubl
     return ok();
 }
 
+// The same finite differences written as the x-pair grid read by the FP32 gather: node m
+// holds (Ex,Ey,Ez,0) of m and of m+1 (0 past the row end), each value the FP32 rounding of
+// the FP64 difference, as the planes and their repacking into pairs give.
+__global__ void k_fd_efield_pairs(const double *__restrict__ phi, float4 *__restrict__ e8, int nx, int ny, int nz,
+                                  double dx, double dy, double dz, double gam0) {
+    const int64_t N = (int64_t)nx * ny * nz;
+    GRID_STRIDE(m, N) {
+        const int i = (int)(m % nx);
+        const int64_t r = m / nx;
+        const int j = (int)(r % ny);
+        const int k = (int)(r / ny);
+        int km1 = k - 1; if (km1 < 0) km1 = k;
+        int kp1 = k + 1; if (kp1 > nz - 1) kp1 = k;
+        const double zfac = (km1 == k || kp1 == k) ? 2.0 : 1.0;
+        int jm1 = j - 1; if (jm1 < 0) jm1 = j;
+        int jp1 = j + 1; if (jp1 > ny - 1) jp1 = j;
+        const double yfac = (jm1 == j || jp1 == j) ? 2.0 : 1.0;
+        int im1 = i - 1; if (im1 < 0) im1 = i;
+        int ip1 = i + 1; if (ip1 > nx - 1) ip1 = i;
+        const double xfac = (im1 == i || ip1 == i) ? 2.0 : 1.0;
+        auto P = [&](int a, int b, int c) { return phi[a + (int64_t)nx * (b + (int64_t)ny * c)]; };
+        const double ex = -(P(ip1, j, k) - P(im1, j, k)) / (2.0 * dx) * gam0 * xfac;
+        const double ey = -(P(i, jp1, k) - P(i, jm1, k)) / (2.0 * dy) * gam0 * yfac;
+        const double ez = -(P(i, j, kp1) - P(i, j, km1)) / (2.0 * dz) / gam0 * zfac;
+        const float4 v = make_float4((float)ex, (float)ey, (float)ez, 0.f);
+        e8[2 * m] = v;
+        if (i > 0) e8[2 * (m - 1) + 1] = v;
+        if (i == nx - 1) e8[2 * m + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+}
+int launch_fd_efield_pairs(const double *phi, float *e8, int nx, int ny, int nz, double dx, double dy, double dz,
+                           double gam0, cudaStream_t st) {
+    k_fd_efield_pairs<<<nblocks((int64_t)nx * ny * nz, 256), 256, 0, st>>>(phi, reinterpret_cast<float4 *>(e8), nx, ny,
+                                                                           nz, dx, dy, dz, gam0);
+    return ok();
+}
+
 __global__ void k_flip_z(double *a, int nx, int ny, int nz) {
     const int64_t plane = (int64_t)nx * ny;
     const int64_t n = plane * (nz / 2);

@@ -69,6 +69,9 @@ int launch_scale(double *y, double a, int64_t n, cudaStream_t st);
 // Centred differences with first-order one-sided edges (core:87-104).
 int launch_fd_efield(const double *phi, double *E, int nx, int ny, int nz, double dx, double dy,
                      double dz, double gam0, cudaStream_t st);
+// As launch_fd_efield, written as the x-pair grid (float4 [N][2]) of launch_interp_pairs.
+int launch_fd_efield_pairs(const double *phi, float *e8, int nx, int ny, int nz, double dx, double dy, double dz,
+                           double gam0, cudaStream_t st);
 // In-place flip of a [nz][ny][nx] grid along z.
 int launch_flip_z(double *a, int nx, int ny, int nz, cudaStream_t st);
 // vec4<T> interleaved grid -> three double planes [3][N] (and optional B from E).

@@ -13,6 +13,8 @@
 #include <cstring>
 #include <vector>
 
+#include <type_traits>
+
 #include "../../include/opensc_gpu.h"
 #include "solver.cuh"
 
@@ -350,7 +352,8 @@ template <typename T> static int pipe_comb(osc_ctx *c, const LGeom &g) {
 }
 
 // Optimised pipe potential: phi = sum_t sign_t * fpei/M * IFFT_{inv_t}(rho_hat * G_t).
-template <typename T> static int pipe_phi_opt(osc_ctx *c, const LGeom &g, const double *rho, double *phi) {
+template <typename T>
+static int pipe_phi_opt(osc_ctx *c, const LGeom &g, const double *rho, double *phi, const float4 *quad = nullptr) {
     typedef cplx<T> V;
     TRY(pipe_comb<T>(c, g));
     const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
@@ -377,7 +380,16 @@ template <typename T> static int pipe_phi_opt(osc_ctx *c, const LGeom &g, const 
     ra.out_rstride = nxh;
     {
         Launch L_(c, "fft_x_r2c");
-        TRY(kchk(c, launch_r2c_rows<T, double>(rho, X1, ra, twx, c->stream), "x r2c"));
+        if constexpr (std::is_same<T, float>::value) {
+            if (quad) {  // the deposit's quad grid, summed to nodes as it is loaded
+                ra.qny = ny;
+                TRY(kchk(c, launch_r2c_rows<float, float4>(quad, X1, ra, twx, c->stream), "x r2c"));
+            } else {
+                TRY(kchk(c, launch_r2c_rows<T, double>(rho, X1, ra, twx, c->stream), "x r2c"));
+            }
+        } else {
+            TRY(kchk(c, launch_r2c_rows<T, double>(rho, X1, ra, twx, c->stream), "x r2c"));
+        }
     }
     LineArgs ly;
     std::memset(&ly, 0, sizeof(ly));
@@ -468,12 +480,15 @@ template <typename T> static int pipe_phi_opt(osc_ctx *c, const LGeom &g, const 
 }
 
 int pipe_solve(osc_ctx *c, int precision, const double delta[3], double gam0, const double *rho, double *phi,
-               double *E, double *B) {
+               double *E, double *B, const float4 *quad, float *e8) {
     PipeGreen &p = c->pipe;
     LGeom g;
     TRY(lgeom(c, p.nlo, p.nhi, p.npad, g));
-    if (precision != OSC_PREC_FP64_PLAIN && p.npad[0] == 1 && p.npad[1] == 1 && p.npad[2] == 1) {
-        if (precision == OSC_PREC_FP32) TRY(pipe_phi_opt<float>(c, g, rho, phi));
+    const bool opt = precision != OSC_PREC_FP64_PLAIN && p.npad[0] == 1 && p.npad[1] == 1 && p.npad[2] == 1;
+    if (quad && !(opt && precision == OSC_PREC_FP32))
+        return set_err(c, OSC_E_INVALID, "pipe solve: quad-grid input needs the FP32 path and npad = 1");
+    if (opt) {
+        if (precision == OSC_PREC_FP32) TRY(pipe_phi_opt<float>(c, g, rho, phi, quad));
         else TRY(pipe_phi_opt<double>(c, g, rho, phi));
     } else {
         // fftconvcorr3d (core:763-818), term by term into phi
@@ -488,14 +503,41 @@ int pipe_solve(osc_ctx *c, int precision, const double delta[3], double gam0, co
             TRY(conv_extract(c, g, crho, ct, PIPE_INV[t], PIPE_SIGN[t] * factr, phi, t > 0));
         }
     }
+    if (e8 && !E && !B) {  // E only as the x-pair grid of the FP32 gather
+        Launch L_(c, "fd_efield");
+        return kchk(c, launch_fd_efield_pairs(phi, e8, g.n[0], g.n[1], g.n[2], delta[0], delta[1], delta[2], gam0,
+                                              c->stream),
+                    "fd pairs");
+    }
+    if (!E) return set_err(c, OSC_E_INVALID, "pipe solve: E planes needed");
     {
         Launch L_(c, "fd_efield");
         TRY(kchk(c, launch_fd_efield(phi, E, g.n[0], g.n[1], g.n[2], delta[0], delta[1], delta[2], gam0, c->stream),
                  "fd"));
     }
+    if (e8) {
+        Launch L_(c, "planes_to_pairs");
+        TRY(kchk(c, launch_planes_to_pairs(E, e8, g.n[0], g.N, c->stream), "E pairs"));
+    }
+    if (!B) return OSC_OK;
     const double beta0 = std::sqrt(1 - 1 / (gam0 * gam0));
     Launch L_(c, "plain_bfield");
     return kchk(c, launch_bfield(E, B, g.N, beta0 / CLIGHT_CORE, 0, c->stream), "bfield");
+}
+
+// The checks of osc_space_charge_rectpipe_dev (Green set computed for this mesh), then the
+// solve; the fused pipe step's entry to pipe_solve.
+int pipe_solve_checked(osc_ctx *ctx, const osc_mesh3d *mesh, int precision, const double *rho, double *phi,
+                       double *E, double *B, const float4 *quad, float *e8) {
+    PipeGreen &p = ctx->pipe;
+    bool same = p.valid;
+    for (int d = 0; d < 3 && same; ++d)
+        same = p.nlo[d] == mesh->nlo[d] && p.nhi[d] == mesh->nhi[d] && p.npad[d] == mesh->npad[d];
+    if (!same)
+        return set_err(ctx, OSC_E_STATE,
+                       "something wrong. rectpipe green functions should have been computed during initialization "
+                       "(call osc_rectpipe_green or osc_read_rectpipe_grn for this mesh first)");
+    return pipe_solve(ctx, precision, mesh->delta, mesh->gamma, rho, phi, E, B, quad, e8);
 }
 
 }  // namespace osc

@@ -37,6 +37,30 @@ int osc_space_charge_step_rectpipe_dev(osc_ctx *ctx, const osc_mesh3d *mesh, int
     DepositArgs da = deposit_args(&m, n, np, x, y, z, q, charge1, ctx->check_finite);
     InterpArgs ia = interp_args(&m, n, np, x, y, z);
     const bool fp32 = precision == OSC_PREC_FP32 && ctx->deposit_mode != OSC_DEPOSIT_DETERMINISTIC;
+    if (fp32 && m.npad[0] == 1 && m.npad[1] == 1 && m.npad[2] == 1) {
+        // the x transform reads the quad grid; E goes straight from phi to the x-pair grid
+        // (and to FP64 planes only when B is wanted)
+        float *quad, *e8;
+        TRY(ws_get(ctx, "ps_quad", sizeof(float) * 4 * N, (void **)&quad));
+        TRY(ws_get(ctx, "ps_E8", sizeof(float) * 8 * N, (void **)&e8));
+        CK(cudaMemsetAsync(quad, 0, sizeof(float) * 4 * N, ctx->stream), "memset quad");
+        {
+            Launch L_(ctx, "deposit_f32");
+            if (launch_deposit_quad(da, quad, ctx->d_small, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "deposit");
+        }
+        TRY(pipe_solve_checked(ctx, &m, precision, nullptr, phi, B ? Eg : nullptr, B ? Bg : nullptr,
+                               reinterpret_cast<const float4 *>(quad), e8));
+        {
+            Launch L_(ctx, "interp_f32");
+            if (launch_interp_pairs(ia, reinterpret_cast<const float4 *>(e8), E, ctx->d_small + 2, ctx->stream))
+                return set_err(ctx, OSC_E_CUDA, "interp");
+        }
+        if (B) {
+            Launch L_(ctx, "interp_f64");
+            if (launch_interp_planes(ia, Bg, B, ctx->d_small + 3, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "interp");
+        }
+        return OSC_OK;
+    }
     if (fp32) {
         float *quad, *rho32;
         TRY(ws_get(ctx, "ps_quad", sizeof(float) * 4 * N, (void **)&quad));

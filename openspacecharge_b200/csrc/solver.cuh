@@ -1,6 +1,7 @@
 // solver.cuh -- field-solve pipelines on one context.
 #pragma once
 
+#include "../../include/opensc_gpu.h"
 #include "context.cuh"
 #include "grid_kernels.cuh"
 #include "particle_kernels.cuh"
@@ -87,7 +88,13 @@ int legacy_cathode(osc_ctx *c, const int nlo[3], const int nhi[3], const int npa
                    int direct, int igf, int imethod, double *phi, double *E, double *B);
 int pipe_green_build(osc_ctx *c, const int nlo[3], const int nhi[3], const int npad[3],
                      const double delta[3], const double umin[3], double gam, double a, double b);
+// Pipe potential phi from rho (or, FP32 with npad 1, from the deposit's quad grid), then
+// E = -grad phi as FP64 planes E and/or the FP32 x-pair grid e8 (E null: e8 only, written
+// straight from phi), and B from the planes when B is given.
 int pipe_solve(osc_ctx *c, int precision, const double delta[3], double gam0, const double *rho,
-               double *phi, double *E, double *B);
+               double *phi, double *E, double *B, const float4 *quad = nullptr, float *e8 = nullptr);
+// pipe_solve after checking that the pipe Green set was built for this mesh.
+int pipe_solve_checked(osc_ctx *ctx, const osc_mesh3d *mesh, int precision, const double *rho, double *phi,
+                       double *E, double *B, const float4 *quad, float *e8);
 
 }  // namespace osc

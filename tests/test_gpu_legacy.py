@@ -155,3 +155,29 @@ def test_fused_pipe_step_matches_oracle(ctx, oracle, pipe_case, prec):
     assert mx <= 10 * TOL[prec], mx
     bm = np.abs(B.cpu().numpy()[:, :2] - B0[:, :2]).max() / np.abs(B0[:, :2]).max()
     assert bm <= 10 * TOL[prec], bm
+
+
+def test_fused_pipe_step_without_b(ctx, oracle, pipe_case):
+    """FP32 fused pipe step with no B requested: E goes from phi straight to the x-pair grid.
+    Same fields as the call that also computes B (float atomics reorder: 2e-6) and as the
+    oracle's chain."""
+    torch = pytest.importorskip("torch")
+    c = pipe_case
+    m = osc.Mesh3D(nlo=(1, 1, 1), nhi=c["n"], min=c["umin"], max=c["umax"], delta=c["delta"], gamma=c["gam"])
+    osc.osc_rectpipe_green(ctx, m, c["a"], c["b"], precision=osc.PREC_FP32)
+    dev = torch.device("cuda", 0)
+    tx, ty, tz = (torch.from_numpy(v).to(dev) for v in (c["x"], c["y"], c["z"]))
+    E1 = torch.empty((len(c["x"]), 3), dtype=torch.float64, device=dev)
+    E2, B2 = torch.empty_like(E1), torch.empty_like(E1)
+    osc.space_charge_step_rectpipe_dev(ctx, m, tx, ty, tz, E1, c["a"], c["b"], total_charge=1e-9,
+                                       precision=osc.PREC_FP32)
+    osc.space_charge_step_rectpipe_dev(ctx, m, tx, ty, tz, E2, c["a"], c["b"], total_charge=1e-9,
+                                       precision=osc.PREC_FP32, B=B2)
+    ctx.synchronize()
+    E1, E2 = E1.cpu().numpy(), E2.cpu().numpy()
+    mx, _ = field_err(E1, E2)
+    assert mx <= 2e-6, mx
+    om = oracle.make_mesh((1, 1, 1), c["n"], (1, 1, 1), c["umin"], c["umax"], c["delta"], c["gam"])
+    E0, _, _ = oracle.interpolate_field(om, c["e"], c["x"], c["y"], c["z"])
+    mx, _ = field_err(E1, E0)
+    assert mx <= 10 * TOL[osc.PREC_FP32], mx
