@@ -138,14 +138,14 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_r2c_rows(const TIn *__restri
     const int L = E::kLen ? E::kLen : a.p.L;
     V *buf = tw + L;
     constexpr int lstr = NL + 1;
-    // static engines launch with L*NL/FFT_EPT threads: compile-time trip counts below
-    const int nthreads = E::kLen ? E::kLen * NL / FFT_EPT : (int)blockDim.x, tid = threadIdx.x;
+    // static engines launch with L*NL/E::kEPT threads: compile-time trip counts below
+    const int nthreads = E::kLen ? E::kLen * NL / E::kEPT : (int)blockDim.x, tid = threadIdx.x;
     const int64_t row0 = (int64_t)blockIdx.x * (2 * NL);
     load_twiddles(tw, twg, L);
     const int ld_len = (E::kLen > 0 && HIN) ? E::kLen / 2 : L;  // HIN launches only with nin == L/2
     if constexpr (E::kLen > 0) {
         // all of a thread's loads are issued before any is stored to shared memory
-        constexpr int LDL = HIN ? E::kLen / 2 : E::kLen, NT = E::kLen * NL / FFT_EPT;
+        constexpr int LDL = HIN ? E::kLen / 2 : E::kLen, NT = E::kLen * NL / E::kEPT;
         constexpr int IT = (2 * NL * LDL + NT - 1) / NT;
         T v[IT];
 #pragma unroll
@@ -408,11 +408,11 @@ template <typename T, class E> constexpr int c2r_e8_nlc() {
 // FP32: x-pair nodes (E(x), E(x+1)) with one 256-bit store; FP64: nodes (Ex, Ey, Ez, 0)
 // with one 256-bit store.
 template <typename T, int NLC, class E>
-__global__ void __launch_bounds__(E::kLen * 3 * NLC / FFT_EPT, sizeof(T) == 4 ? 3 : 1) k_c2r_e8(const cplx<T> *__restrict__ in, C2RArgs a,
+__global__ void __launch_bounds__(E::kLen * 3 * NLC / E::kEPT, sizeof(T) == 4 ? 3 : 1) k_c2r_e8(const cplx<T> *__restrict__ in, C2RArgs a,
                                                                       const cplx<T> *__restrict__ twg) {
     typedef cplx<T> V;
     constexpr int L = E::kLen, NLT = 3 * NLC, lstr = NLT + 1, half = L / 2, nout = L / 2;
-    constexpr int nthreads = L * NLT / FFT_EPT;
+    constexpr int nthreads = L * NLT / E::kEPT;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V *tw = reinterpret_cast<V *>(smem_raw);
     V *buf = tw + L;
@@ -532,11 +532,11 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_sym_lines(const double *__re
     load_twiddles(tw, twg, L);
     __syncthreads();
     if constexpr (E::kLen > 0) {
-        // static engine (L = 2n known, L*NL/FFT_EPT threads): each thread first loads its
+        // static engine (L = 2n known, L*NL/E::kEPT threads): each thread first loads its
         // share of the n+1 distinct values of every line into registers (all loads in
         // flight), then writes each value at e and its parity image at L-e
         constexpr int nh = E::kLen / 2, NK = nh + 1, TOT = 2 * NL * NK;
-        constexpr int NT = E::kLen * NL / FFT_EPT, IT = (TOT + NT - 1) / NT;
+        constexpr int NT = E::kLen * NL / E::kEPT, IT = (TOT + NT - 1) / NT;
         double v[IT];
 #pragma unroll
         for (int it = 0; it < IT; ++it) {
@@ -641,8 +641,8 @@ template <typename T, class E, class F> inline int with_nl(int L, int nbuf, int 
         (void)L;
         (void)nl_req;
         (void)nl_max;
-        constexpr int NL1 = nl_static(E::kLen, sizeof(T) == 4 ? 16 : 8, (int)sizeof(cplx<T>), 1);
-        constexpr int NL2 = nl_static(E::kLen, 4, (int)sizeof(cplx<T>), 2, 64 * 1024);
+        constexpr int NL1 = nl_static(E::kLen, sizeof(T) == 4 ? 16 : 8, (int)sizeof(cplx<T>), 1, 100 * 1024, E::kEPT);
+        constexpr int NL2 = nl_static(E::kLen, 4, (int)sizeof(cplx<T>), 2, 64 * 1024, E::kEPT);
         if (nbuf >= 2) return f(std::integral_constant<int, NL2>{});
         return f(std::integral_constant<int, NL1>{});
     } else {
@@ -661,8 +661,8 @@ template <typename T, int NL, bool ROW, class E, int MODE>
 inline int launch_lines_k(const cplx<T> *in, cplx<T> *out, const LineArgs &a, int nplanes, int ncomp, const cplx<T> *tw,
                           cudaStream_t st) {
     const int L = a.p.L;
-    const int nt = fft_threads(L, NL);
-    if (nt < 1 || nt > E::kMaxThreads || (L * NL) % FFT_EPT) return OSC_E_FFT_SIZE;
+    const int nt = fft_threads(L, NL, E::kEPT);
+    if (nt < 1 || nt > E::kMaxThreads || (L * NL) % E::kEPT) return OSC_E_FFT_SIZE;
     const size_t sm = sizeof(cplx<T>) * ((size_t)L + (size_t)L * (NL + 1));
     auto kern = k_lines<T, NL, ROW, E, MODE>;
     int rc = set_smem(kern, sm);
@@ -701,8 +701,8 @@ int launch_r2c_rows(const TIn *in, cplx<T> *out, const R2CArgs &a, const TwPair<
         const cplx<T> *twe = eng_tw<E>(tw);
         return with_nl<T, E>(L, 1, sizeof(T) == 4 ? 16 : 8, 0, [&](auto nlc) -> int {
             constexpr int NL = decltype(nlc)::value;
-            const int nt = fft_threads(L, NL);
-            if (nt < 1 || nt > E::kMaxThreads || (L * NL) % FFT_EPT) return OSC_E_FFT_SIZE;
+            const int nt = fft_threads(L, NL, E::kEPT);
+            if (nt < 1 || nt > E::kMaxThreads || (L * NL) % E::kEPT) return OSC_E_FFT_SIZE;
             const size_t sm = sizeof(cplx<T>) * ((size_t)L + (size_t)L * (NL + 1));
             const unsigned nblk = (unsigned)ceil_div(a.nrows, 2 * NL);
             if (E::kLen > 0 && 2 * a.nin == L) {
@@ -734,7 +734,7 @@ int launch_c2r_rows(const cplx<T> *in, const C2RArgs &a, const TwPair<cplx<T>> &
                 using E = decltype(eng);
                 if constexpr (E::kLen > 0) {
                     constexpr int NLC = c2r_e8_nlc<T, E>();
-                    constexpr int nt = E::kLen * 3 * NLC / FFT_EPT;
+                    constexpr int nt = E::kLen * 3 * NLC / E::kEPT;
                     const size_t sm = sizeof(cplx<T>) * ((size_t)E::kLen + (size_t)E::kLen * (3 * NLC + 1));
                     auto kern = k_c2r_e8<T, NLC, E>;
                     int r = set_smem(kern, sm);
@@ -752,8 +752,8 @@ int launch_c2r_rows(const cplx<T> *in, const C2RArgs &a, const TwPair<cplx<T>> &
         const cplx<T> *twe = eng_tw<E>(tw);
         return with_nl<T, E>(L, 1, sizeof(T) == 4 ? 16 : 8, 0, [&](auto nlc) -> int {
             constexpr int NL = decltype(nlc)::value;
-            const int nt = fft_threads(L, NL);
-            if (nt < 1 || nt > E::kMaxThreads || (L * NL) % FFT_EPT) return OSC_E_FFT_SIZE;
+            const int nt = fft_threads(L, NL, E::kEPT);
+            if (nt < 1 || nt > E::kMaxThreads || (L * NL) % E::kEPT) return OSC_E_FFT_SIZE;
             const size_t sm = sizeof(cplx<T>) * ((size_t)L + (size_t)L * (NL + 1)) +
                               (a.e8 ? sizeof(T) * 3 * 2 * NL * (size_t)a.nout : 0);
             const unsigned nblk = (unsigned)ceil_div(a.nrows, 2 * NL);
@@ -839,8 +839,8 @@ int launch_zconv(const cplx<T> *in, cplx<T> *out, const ZConvArgs &a, const TwPa
         const cplx<T> *twe = eng_tw<E>(tw);
         return with_nl<T, E>(L, 2, sizeof(T) == 4 ? 8 : 4, nl, [&](auto nlc) -> int {
             constexpr int NL = decltype(nlc)::value;
-            const int nt = fft_threads(L, NL);
-            if (nt < 1 || nt > E::kMaxThreads || (L * NL) % FFT_EPT) return OSC_E_FFT_SIZE;
+            const int nt = fft_threads(L, NL, E::kEPT);
+            if (nt < 1 || nt > E::kMaxThreads || (L * NL) % E::kEPT) return OSC_E_FFT_SIZE;
             const size_t sm = sizeof(cplx<T>) * ((size_t)L + 2 * (size_t)L * (NL + 1));
             const dim3 nblk((unsigned)ceil_div(a.ncols, NL), (unsigned)(a.nbatch > 0 ? a.nbatch : 1));
             if (E::kLen > 0 && 2 * a.nz == L) {
@@ -871,14 +871,15 @@ int launch_sym_lines(const double *in, TO *out, const SymArgs &a, const TwPair<c
         // groups still give CTAs of several warps
         auto with_sym_nl = [&](auto &&f) -> int {
             if constexpr (E::kLen > 0)
-                return f(std::integral_constant<int, nl_static(E::kLen, 16, (int)sizeof(double2), 1)>{});
+                return f(std::integral_constant<int, nl_static(E::kLen, 16, (int)sizeof(double2), 1, 100 * 1024,
+                                                               E::kEPT)>{});
             else
                 return with_nl<double, E>(L, 1, 8, 0, f);
         };
         return with_sym_nl([&](auto nlc) -> int {
             constexpr int NL = decltype(nlc)::value;
-            const int nt = fft_threads(L, NL);
-            if (nt < 1 || nt > E::kMaxThreads || (L * NL) % FFT_EPT) return OSC_E_FFT_SIZE;
+            const int nt = fft_threads(L, NL, E::kEPT);
+            if (nt < 1 || nt > E::kMaxThreads || (L * NL) % E::kEPT) return OSC_E_FFT_SIZE;
             const size_t sm = sizeof(double2) * ((size_t)L + (size_t)L * (NL + 1));
             const unsigned nblk = (unsigned)ceil_div(a.nlines, 2 * NL);
             auto go = [&](auto kern) -> int {

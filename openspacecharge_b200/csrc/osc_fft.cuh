@@ -40,7 +40,7 @@ struct FFTPlan {
 // for other lengths, odd lengths or L > FFT_MAX_LEN.
 bool make_fft_plan(int L, FFTPlan &p);
 // Threads of a CTA that transforms NL lines of length L.
-inline int fft_threads(int L, int NL) { return (L * NL) / FFT_EPT; }
+inline int fft_threads(int L, int NL, int ept = FFT_EPT) { return (L * NL) / ept; }
 
 template <typename V> __device__ __forceinline__ V tw_get(const V *tw, int m, int sign) {
     V w = tw[m];
@@ -250,13 +250,13 @@ __device__ __forceinline__ void fft_smem(V *buf, int lstr, const FFTPlan &p, con
 // ---- compile-time engine ------------------------------------------------------------------
 // MODE 0: full stage; 1: first stage whose upper input half is zero (not read);
 // 2: last stage whose upper output half is not needed (not written).
-template <typename V, int R, int NL, int L, int Ns, int MODE>
+template <typename V, int R, int NL, int L, int Ns, int MODE, int EPT>
 __device__ __forceinline__ void stage_ct(V *buf, const V *tw, int sign) {
     constexpr int lstr = NL + 1;
-    constexpr int MAXB = (FFT_EPT + R - 1) / R;
+    constexpr int MAXB = (EPT + R - 1) / R;
     constexpr int nb = L / R;
     constexpr int total = nb * NL;
-    constexpr int nthreads = L * NL / FFT_EPT;
+    constexpr int nthreads = L * NL / EPT;
     constexpr int toff = Ns - 1;  // this stage's block of the per-stage twiddle table
     constexpr bool half_in = MODE == 1 && (R % 2 == 0);
     constexpr bool half_out = MODE == 2 && (R % 2 == 0);
@@ -297,24 +297,24 @@ __device__ __forceinline__ void stage_ct(V *buf, const V *tw, int sign) {
     __syncthreads();
 }
 
-template <typename V, int NL, int L, int Ns, bool HIN, bool HOUT, int R, int... Rest>
+template <typename V, int NL, int L, int Ns, bool HIN, bool HOUT, int EPT, int R, int... Rest>
 __device__ __forceinline__ void fft_ct(V *buf, const V *tw, int sign) {
     constexpr bool last = sizeof...(Rest) == 0;
     constexpr int mode = (Ns == 1 && HIN) ? 1 : ((last && HOUT) ? 2 : 0);
-    stage_ct<V, R, NL, L, Ns, mode>(buf, tw, sign);
-    if constexpr (!last) fft_ct<V, NL, L, Ns * R, false, HOUT, Rest...>(buf, tw, sign);
+    stage_ct<V, R, NL, L, Ns, mode, EPT>(buf, tw, sign);
+    if constexpr (!last) fft_ct<V, NL, L, Ns * R, false, HOUT, EPT, Rest...>(buf, tw, sign);
 }
 
 // Stage with explicit input and output functors: ld(e, line) -> V and st(e, line, V).
 // The first stage of a transform can read straight from global memory (or compute its
 // input, e.g. a spectral product) and the last stage can write straight to global memory,
 // which saves two shared-memory passes per transform.
-template <typename V, int R, int NL, int L, int Ns, bool HALF_IN, bool HALF_OUT, class LD, class ST>
+template <typename V, int R, int NL, int L, int Ns, bool HALF_IN, bool HALF_OUT, int EPT, class LD, class ST>
 __device__ __forceinline__ void stage_io(const LD &ld, const ST &st, const V *tw, int sign) {
-    constexpr int MAXB = (FFT_EPT + R - 1) / R;
+    constexpr int MAXB = (EPT + R - 1) / R;
     constexpr int nb = L / R;
     constexpr int total = nb * NL;
-    constexpr int nthreads = L * NL / FFT_EPT;
+    constexpr int nthreads = L * NL / EPT;
     constexpr int toff = Ns - 1;
     constexpr bool half_in = HALF_IN && (R % 2 == 0);
     constexpr bool half_out = HALF_OUT && (R % 2 == 0);
@@ -357,18 +357,18 @@ __device__ __forceinline__ void stage_io(const LD &ld, const ST &st, const V *tw
 
 template <int... Rs> struct Radices {};
 
-template <typename V, int NL, int L, int Ns, bool HIN, bool HOUT, int R, int... Rest, class LD, class ST>
+template <typename V, int NL, int L, int Ns, bool HIN, bool HOUT, int EPT, int R, int... Rest, class LD, class ST>
 __device__ __forceinline__ void fft_io_rec(Radices<R, Rest...>, V *buf, const V *tw, int sign, const LD &ld,
                                            const ST &st) {
     constexpr bool first = Ns == 1, last = sizeof...(Rest) == 0;
     constexpr int lstr = NL + 1;
     auto sld = [buf](int e, int l) -> V { return buf[e * lstr + l]; };
     auto sst = [buf](int e, int l, const V &x) { buf[e * lstr + l] = x; };
-    if constexpr (first && last) stage_io<V, R, NL, L, Ns, HIN, HOUT>(ld, st, tw, sign);
-    else if constexpr (first) stage_io<V, R, NL, L, Ns, HIN, false>(ld, sst, tw, sign);
-    else if constexpr (last) stage_io<V, R, NL, L, Ns, false, HOUT>(sld, st, tw, sign);
-    else stage_io<V, R, NL, L, Ns, false, false>(sld, sst, tw, sign);
-    if constexpr (!last) fft_io_rec<V, NL, L, Ns * R, HIN, HOUT>(Radices<Rest...>{}, buf, tw, sign, ld, st);
+    if constexpr (first && last) stage_io<V, R, NL, L, Ns, HIN, HOUT, EPT>(ld, st, tw, sign);
+    else if constexpr (first) stage_io<V, R, NL, L, Ns, HIN, false, EPT>(ld, sst, tw, sign);
+    else if constexpr (last) stage_io<V, R, NL, L, Ns, false, HOUT, EPT>(sld, st, tw, sign);
+    else stage_io<V, R, NL, L, Ns, false, false, EPT>(sld, sst, tw, sign);
+    if constexpr (!last) fft_io_rec<V, NL, L, Ns * R, HIN, HOUT, EPT>(Radices<Rest...>{}, buf, tw, sign, ld, st);
 }
 
 // FFT engines.  FftRuntime CTAs are capped at 256 threads so the generic stage code keeps
@@ -380,6 +380,7 @@ __device__ __forceinline__ void fft_io_rec(Radices<R, Rest...>, V *buf, const V 
 // read another shared buffer.
 struct FftRuntime {
     static constexpr int kLen = 0;
+    static constexpr int kEPT = FFT_EPT;
     static constexpr int kMaxThreads = 256;
     static constexpr int kNst = 0;
     static constexpr int kRad[1] = {0};
@@ -405,48 +406,66 @@ struct FftRuntime {
         __syncthreads();
     }
 };
-template <int L_, int... Rs> struct FftStatic {
+// Static engine with EPT_ complex values per thread and stage (L*NL/EPT_ threads per CTA).
+template <int EPT_, int L_, int... Rs> struct FftStaticT {
     static constexpr int kLen = L_;
+    static constexpr int kEPT = EPT_;
     static constexpr int kMaxThreads = 512;
     static constexpr int kNst = sizeof...(Rs);
     static constexpr int kRad[sizeof...(Rs)] = {Rs...};
     template <typename V, int NL, bool HIN, bool HOUT>
     __device__ __forceinline__ static void run(V *buf, const FFTPlan &, const V *tw, int sign) {
-        fft_ct<V, NL, L_, 1, HIN, HOUT, Rs...>(buf, tw, sign);
+        fft_ct<V, NL, L_, 1, HIN, HOUT, EPT_, Rs...>(buf, tw, sign);
     }
     template <typename V, int NL, bool HIN, bool HOUT, class LD, class ST>
     __device__ __forceinline__ static void run_io(V *buf, const FFTPlan &, const V *tw, int sign, const LD &ld,
                                                   const ST &st) {
-        fft_io_rec<V, NL, L_, 1, HIN, HOUT>(Radices<Rs...>{}, buf, tw, sign, ld, st);
+        fft_io_rec<V, NL, L_, 1, HIN, HOUT, EPT_>(Radices<Rs...>{}, buf, tw, sign, ld, st);
     }
 };
+// FP32 transforms: 16 values per thread.  FP64: 8 (half the registers of the same bytes),
+// with radices of at most 8 so that every thread owns a butterfly in every stage.
+template <int L_, int... Rs> using FftStatic = FftStaticT<FFT_EPT, L_, Rs...>;
+template <int L_, int... Rs> using FftStatic8 = FftStaticT<8, L_, Rs...>;
 
 // Lines per CTA for a static engine: the largest NL <= nl_max with a whole number of
 // threads, at most 512 threads, and nbuf line buffers within budget bytes of shared memory.
-constexpr int nl_static(int L, int nl_max, int elem_bytes, int nbuf, int budget = 100 * 1024) {
+constexpr int nl_static(int L, int nl_max, int elem_bytes, int nbuf, int budget = 100 * 1024, int ept = FFT_EPT) {
     int nl = nl_max;
-    while (nl > 2 && ((L * nl) % FFT_EPT != 0 || (L * nl) / FFT_EPT > 512 ||
+    while (nl > 2 && ((L * nl) % ept != 0 || (L * nl) / ept > 512 ||
                       nbuf * L * (nl + 1) * elem_bytes + L * elem_bytes > budget))
         nl /= 2;
     return nl;
 }
 
 // Calls f(engine) with the static engine for L when there is one, else FftRuntime.  T is
-// the real type of the transform: at L = 256 the FP64 transforms take two radix-16 stages,
-// the FP32 ones (whose y passes measured faster so) radix 8-8-4.
+// the real type of the transform: FP64 transforms use 8 values per thread and radices up to
+// 8; FP32 transforms 16 values per thread, radix 16-8 at L = 128.
 template <typename T, class F> inline int dispatch_fft_len(int L, F &&f) {
-    switch (L) {
-    case 32: return f(FftStatic<32, 8, 4>{});
-    case 64: return f(FftStatic<64, 8, 8>{});
-    case 96: return f(FftStatic<96, 8, 4, 3>{});
-    case 128: return f(FftStatic<128, 16, 8>{});
-    case 192: return f(FftStatic<192, 8, 8, 3>{});
-    case 256:
-        if constexpr (sizeof(T) == 8) return f(FftStatic<256, 16, 16>{});
-        else return f(FftStatic<256, 8, 8, 4>{});
-    case 384: return f(FftStatic<384, 8, 8, 2, 3>{});
-    case 512: return f(FftStatic<512, 8, 8, 8>{});
-    default: return f(FftRuntime{});
+    if constexpr (sizeof(T) == 8) {
+        switch (L) {
+        case 32: return f(FftStatic8<32, 8, 4>{});
+        case 64: return f(FftStatic8<64, 8, 8>{});
+        case 96: return f(FftStatic8<96, 8, 4, 3>{});
+        case 128: return f(FftStatic8<128, 8, 4, 4>{});
+        case 192: return f(FftStatic8<192, 8, 8, 3>{});
+        case 256: return f(FftStatic8<256, 8, 8, 4>{});
+        case 384: return f(FftStatic8<384, 8, 8, 2, 3>{});
+        case 512: return f(FftStatic8<512, 8, 8, 8>{});
+        default: return f(FftRuntime{});
+        }
+    } else {
+        switch (L) {
+        case 32: return f(FftStatic<32, 8, 4>{});
+        case 64: return f(FftStatic<64, 8, 8>{});
+        case 96: return f(FftStatic<96, 8, 4, 3>{});
+        case 128: return f(FftStatic<128, 16, 8>{});
+        case 192: return f(FftStatic<192, 8, 8, 3>{});
+        case 256: return f(FftStatic<256, 8, 8, 4>{});
+        case 384: return f(FftStatic<384, 8, 8, 2, 3>{});
+        case 512: return f(FftStatic<512, 8, 8, 8>{});
+        default: return f(FftRuntime{});
+        }
     }
 }
 
