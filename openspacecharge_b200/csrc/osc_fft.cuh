@@ -440,7 +440,8 @@ constexpr int nl_static(int L, int nl_max, int elem_bytes, int nbuf, int budget 
 
 // Calls f(engine) with the static engine for L when there is one, else FftRuntime.  T is
 // the real type of the transform: FP64 transforms use 8 values per thread and radices up to
-// 8; FP32 transforms 16 values per thread, radix 16-8 at L = 128.
+// 8; FP32 transforms 8 values per thread up to L = 192 (the many short lines of batched
+// small grids) and 16 from L = 256 (where the 8-value engines measured slower).
 template <typename T, class F> inline int dispatch_fft_len(int L, F &&f) {
     if constexpr (sizeof(T) == 8) {
         switch (L) {
@@ -456,11 +457,11 @@ template <typename T, class F> inline int dispatch_fft_len(int L, F &&f) {
         }
     } else {
         switch (L) {
-        case 32: return f(FftStatic<32, 8, 4>{});
-        case 64: return f(FftStatic<64, 8, 8>{});
-        case 96: return f(FftStatic<96, 8, 4, 3>{});
-        case 128: return f(FftStatic<128, 16, 8>{});
-        case 192: return f(FftStatic<192, 8, 8, 3>{});
+        case 32: return f(FftStatic8<32, 8, 4>{});
+        case 64: return f(FftStatic8<64, 8, 8>{});
+        case 96: return f(FftStatic8<96, 8, 4, 3>{});
+        case 128: return f(FftStatic8<128, 8, 4, 4>{});
+        case 192: return f(FftStatic8<192, 8, 8, 3>{});
         case 256: return f(FftStatic<256, 8, 8, 4>{});
         case 384: return f(FftStatic<384, 8, 8, 2, 3>{});
         case 512: return f(FftStatic<512, 8, 8, 8>{});
