@@ -27,10 +27,11 @@
 namespace osc {
 
 // Warps per CTA and resident CTAs per SM the register allocation of k_zconv_warp is sized
-// for: FP32 8 warps x 3 CTAs (<= 85 registers); FP64 holds twice the bytes per value, 4
-// warps x 2 CTAs.
-template <typename T> constexpr int zw_warps() { return sizeof(T) == 4 ? 8 : 4; }
-template <typename T> constexpr int zw_minb() { return sizeof(T) == 4 ? 3 : 2; }
+// for: FP32 4 warps x 6 CTAs (<= 85 registers; 8 warps x 3 CTAs measured 171 us against 153
+// for the 128x128x256 step, the CTA-wide waits for the loads and Green copies being shorter
+// with fewer warps); FP64 holds twice the bytes per value, 4 warps x 2 CTAs.
+template <typename T> constexpr int zw_warps() { return 4; }
+template <typename T> constexpr int zw_minb() { return sizeof(T) == 4 ? 6 : 2; }
 
 
 __device__ __forceinline__ int wpad(int e) { return e + (e >> 4); }
