@@ -254,30 +254,47 @@ __device__ __forceinline__ void load_node(const vec4<T> *g, int64_t n, double &a
 template <typename T, typename TO>
 __global__ void __launch_bounds__(256) k_interp_vec4(InterpArgs a, const vec4<T> *__restrict__ g, TO *__restrict__ E,
                                                      unsigned long long *__restrict__ nclamp) {
+    // E goes through a per-warp shared-memory stage and is stored as contiguous rows (as in
+    // k_interp_pairs); the loop runs while the warp's first particle exists
+    __shared__ TO stage[256 * 3];
+    const int lane = threadIdx.x & 31;
+    TO *ws = stage + (threadIdx.x - lane) * 3;
     const int64_t plane = (int64_t)a.nx * a.ny;
-    GRID_STRIDE(m, a.np) {
-        Cell c;
-        const bool fl = locate(a, a.x[m], a.y[m], a.z[m], c);
-        count_one(nclamp, fl);
-        const int64_t n0 = c.i + (int64_t)a.nx * c.j + plane * c.k;
-        const double ab = c.ab, de = c.de, gh = c.gh;
-        const double omab = 1. - ab, omde = 1. - de, omgh = 1. - gh;
-        const int64_t nodes[8] = {n0, n0 + a.nx, n0 + a.nx + plane, n0 + plane,
-                                  n0 + 1 + plane, n0 + 1 + a.nx + plane, n0 + 1 + a.nx, n0 + 1};
-        const double wts[8] = {ab * de * gh, ab * omde * gh, ab * omde * omgh, ab * de * omgh,
-                               omab * de * omgh, omab * omde * omgh, omab * omde * gh, omab * de * gh};
-        double ex = 0, ey = 0, ez = 0;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; m - lane < a.np; m += stride) {
+        bool fl = false;
+        if (m < a.np) {
+            Cell c;
+            fl = locate(a, a.x[m], a.y[m], a.z[m], c);
+            const int64_t n0 = c.i + (int64_t)a.nx * c.j + plane * c.k;
+            const double ab = c.ab, de = c.de, gh = c.gh;
+            const double omab = 1. - ab, omde = 1. - de, omgh = 1. - gh;
+            const int64_t nodes[8] = {n0, n0 + a.nx, n0 + a.nx + plane, n0 + plane,
+                                      n0 + 1 + plane, n0 + 1 + a.nx + plane, n0 + 1 + a.nx, n0 + 1};
+            const double wts[8] = {ab * de * gh, ab * omde * gh, ab * omde * omgh, ab * de * omgh,
+                                   omab * de * omgh, omab * omde * omgh, omab * omde * gh, omab * de * gh};
+            double ex = 0, ey = 0, ez = 0;
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            double vx, vy, vz;
-            load_node<T>(g, nodes[q], vx, vy, vz);
-            ex = ex + vx * wts[q];
-            ey = ey + vy * wts[q];
-            ez = ez + vz * wts[q];
+            for (int q = 0; q < 8; ++q) {
+                double vx, vy, vz;
+                load_node<T>(g, nodes[q], vx, vy, vz);
+                ex = ex + vx * wts[q];
+                ey = ey + vy * wts[q];
+                ez = ez + vz * wts[q];
+            }
+            ws[3 * lane] = (TO)ex;
+            ws[3 * lane + 1] = (TO)ey;
+            ws[3 * lane + 2] = (TO)ez;
         }
-        E[3 * m] = (TO)ex;
-        E[3 * m + 1] = (TO)ey;
-        E[3 * m + 2] = (TO)ez;
+        count_one(nclamp, fl);
+        __syncwarp();
+        const int64_t o0 = 3 * (m - lane), n3 = 3 * a.np;
+#pragma unroll
+        for (int t = 0; t < 3; ++t) {
+            const int e = 32 * t + lane;
+            if (o0 + e < n3) E[o0 + e] = ws[e];
+        }
+        __syncwarp();
     }
 }
 
@@ -551,8 +568,23 @@ __global__ void __launch_bounds__(256) k_batch_interp_pairs(const BunchArgs *__r
     const float4 *g8 = e8 + 2 * bunches[jb.bunch].node_off;
     double *E = bunches[jb.bunch].E;
     const int64_t plane = (int64_t)a.nx * a.ny;
-    for (int64_t m = jb.beg + threadIdx.x; m < jb.end; m += blockDim.x)
-        count_one(&cnt[4 * jb.bunch + 2], interp_pair_one(a, g8, plane, a.x[m], a.y[m], a.z[m], E + 3 * m));
+    // E staged per warp and stored as contiguous rows, as in k_interp_pairs
+    __shared__ double stage[256 * 3];
+    const int lane = threadIdx.x & 31;
+    double *ws = stage + (threadIdx.x - lane) * 3;
+    for (int64_t m = jb.beg + threadIdx.x; m - lane < jb.end; m += blockDim.x) {
+        bool fl = false;
+        if (m < jb.end) fl = interp_pair_one(a, g8, plane, a.x[m], a.y[m], a.z[m], ws + 3 * lane);
+        count_one(&cnt[4 * jb.bunch + 2], fl);
+        __syncwarp();
+        const int64_t o0 = 3 * (m - lane), n3 = 3 * jb.end;
+#pragma unroll
+        for (int t = 0; t < 3; ++t) {
+            const int e = 32 * t + lane;
+            if (o0 + e < n3) E[o0 + e] = ws[e];
+        }
+        __syncwarp();
+    }
 }
 int launch_batch_interp_pairs(const BunchArgs *bunches, const BatchJob *jobs, int njobs, const float *e8,
                               unsigned long long *cnt, cudaStream_t st) {
@@ -806,8 +838,32 @@ __global__ void __launch_bounds__(256) k_vjp_pairs(InterpArgs ia, DepositArgs da
                                                    const double *__restrict__ gE, double *gx, double *gy, double *gz,
                                                    double *gq) {
     const int64_t plane = (int64_t)ia.nx * ia.ny;
-    GRID_STRIDE(m, ia.np) {
-        const double xm = ia.x[m], ym = ia.y[m], zm = ia.z[m];
+    // the warp's 32 particles' dL/dE (96 doubles) are read as three contiguous 256-byte rows
+    // into shared memory; the loop runs while the warp's first particle exists
+    __shared__ double stage[256 * 3];
+    const int lane = threadIdx.x & 31;
+    double *ws = stage + (threadIdx.x - lane) * 3;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; m - lane < ia.np; m += stride) {
+        // coordinates first, so that their loads are in flight with the dL/dE rows
+        double xm = 0, ym = 0, zm = 0;
+        if (m < ia.np) {
+            xm = ia.x[m];
+            ym = ia.y[m];
+            zm = ia.z[m];
+        }
+        {
+            const int64_t o0 = 3 * (m - lane), n3 = 3 * ia.np;
+#pragma unroll
+            for (int t = 0; t < 3; ++t) {
+                const int e = 32 * t + lane;
+                if (o0 + e < n3) ws[e] = gE[o0 + e];
+            }
+        }
+        __syncwarp();
+        const double gEm[3] = {ws[3 * lane], ws[3 * lane + 1], ws[3 * lane + 2]};
+        __syncwarp();
+        if (m >= ia.np) continue;
         Cell c;
         locate(ia, xm, ym, zm, c);
         const int64_t n0 = c.i + (int64_t)ia.nx * c.j + plane * c.k;
@@ -837,7 +893,7 @@ __global__ void __launch_bounds__(256) k_vjp_pairs(InterpArgs ia, DepositArgs da
         double g[3] = {0, 0, 0};
 #pragma unroll
         for (int comp = 0; comp < 3; ++comp) {
-            const double w = gE[3 * m + comp];
+            const double w = gEm[comp];
 #pragma unroll
             for (int ax = 0; ax < 3; ++ax) g[ax] += w * d[comp][ax] * ia.hinv[ax];
         }

@@ -11,10 +11,15 @@
 // output is kz-innermost (one contiguous column per warp), else it goes back to the warp
 // buffer and the CTA stores its W columns with coalesced writes.
 //
-// Warp buffers are padded by one element per sixteen (p = e + e/16) and are 2 mod 16
-// elements apart, which keeps the stride-R writes of the first stage, the unit-stride reads
-// of the others and the column-interleaved CTA loads and stores (nearly) free of
-// shared-memory bank conflicts.  The Green spectra of this kernel are stored with kz
+// Warp buffers are padded by one element per sixteen (p = e + e/16) for 8-byte complex
+// values and one per eight (p = e + e/8) for 16-byte ones, and are 4 mod 16 (8-byte) or
+// 2 mod 8 (16-byte) elements apart.  A shared-memory access of 8-byte values is served a
+// half warp at a time, of 16-byte values a quarter warp at a time; under these paddings the
+// stride-R writes of the first stage, the unit-stride reads of the others and the
+// column-interleaved CTA loads of 4 warps fall on distinct banks.  For 16-byte values the
+// writes of the middle stages are conflict-free too; for 8-byte values the middle-stage
+// writes of a half warp that spans two output groups are 2-way conflicted (no additive
+// padding serves both these writes and the 16-element unit-stride reads).  The Green spectra of this kernel are stored with kz
 // innermost (GSpecDev::zinner), so the 32 lanes of a warp read 32 consecutive kz.  When
 // all spectra are real and even/odd in z (free space without images), each CTA fetches the
 // Green columns of its W columns into shared memory with bulk copies at launch, which
@@ -34,8 +39,15 @@ template <typename T> constexpr int zw_warps() { return 4; }
 template <typename T> constexpr int zw_minb() { return sizeof(T) == 4 ? 6 : 2; }
 
 
-__device__ __forceinline__ int wpad(int e) { return e + (e >> 4); }
-constexpr int wbuf_len(int L) { return L + L / 16 + 2; }
+// padding shift of a complex type: 4 (one element in 16) for 8-byte, 3 (one in 8) for 16-byte
+template <typename V> constexpr int wpad_shift() { return sizeof(V) >= 16 ? 3 : 4; }
+template <typename V> __device__ __forceinline__ int wpad(int e) { return e + (e >> wpad_shift<V>()); }
+// elements per warp buffer of real type T: the padded length, rounded up to 4 mod 16 (FP32)
+// or 2 mod 8 (FP64) so that the 4 warp buffers start on different banks
+template <typename T> constexpr int wbuf_len(int L) {
+    return sizeof(T) == 4 ? (L + L / 16) + ((4 - (L + L / 16)) % 16 + 16) % 16
+                          : (L + L / 8) + ((2 - (L + L / 8)) % 8 + 8) % 8;
+}
 
 // One stage of one warp's transform: butterflies j = lane + 32q (j < L/R), input elements
 // j + (L/R) r, outputs (j/Ns) Ns R + j%Ns + Ns r; per-stage twiddles at (Ns-1) + k(R-1) + r-1.
@@ -45,12 +57,13 @@ template <typename V, int R, int L, int Ns> struct WStage {
     static constexpr int nb = L / R;
     static constexpr int Q = (nb + 31) / 32;
     static constexpr bool full = nb % 32 == 0;
-    static constexpr bool ld_lin = nb % 16 == 0;  // wpad(j + r nb) = wpad(j) + r (nb + nb/16)
-    // store: 1 = Ns multiple of 16, 2 = Ns | 16 and 16 | Ns R, 3 = Ns R | 16, 0 = per element
+    static constexpr int PS = wpad_shift<V>(), PB = 1 << PS;  // one pad element per PB
+    static constexpr bool ld_lin = nb % PB == 0;  // wpad(j + r nb) = wpad(j) + r (nb + nb/PB)
+    // store: 1 = Ns multiple of PB, 2 = Ns | PB and PB | Ns R, 3 = Ns R | PB, 0 = per element
     static constexpr int st_kind =
-        Ns % 16 == 0 ? 1 : (16 % Ns == 0 && (Ns * R) % 16 == 0) ? 2 : (16 % (Ns * R) == 0) ? 3 : 0;
+        Ns % PB == 0 ? 1 : (PB % Ns == 0 && (Ns * R) % PB == 0) ? 2 : (PB % (Ns * R) == 0) ? 3 : 0;
     __device__ __forceinline__ static constexpr int st_off(int r) {
-        return st_kind == 1 ? r * (Ns + Ns / 16) : st_kind == 2 ? r * Ns + ((r * Ns) >> 4) : r * Ns;
+        return st_kind == 1 ? r * (Ns + Ns / PB) : st_kind == 2 ? r * Ns + ((r * Ns) >> PS) : r * Ns;
     }
 
     __device__ __forceinline__ static void load(const V *wb, const V *tw, int sign, int lane, V (&v)[Q][R],
@@ -58,7 +71,7 @@ template <typename V, int R, int L, int Ns> struct WStage {
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
             const int j = lane + 32 * q, k = j % Ns;
-            const int pb = wpad(j);
+            const int pb = wpad<V>(j);
             if (full || j < nb) {
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
@@ -67,7 +80,7 @@ template <typename V, int R, int L, int Ns> struct WStage {
                         x.x = 0;
                         x.y = 0;
                     } else {
-                        x = wb[ld_lin ? pb + r * (nb + nb / 16) : wpad(j + r * nb)];
+                        x = wb[ld_lin ? pb + r * (nb + nb / PB) : wpad<V>(j + r * nb)];
                         if (r && Ns > 1) x = cmul(x, tw_get(tw, (Ns - 1) + k * (R - 1) + (r - 1), sign));
                     }
                     v[q][r] = x;
@@ -85,9 +98,9 @@ template <typename V, int R, int L, int Ns> struct WStage {
             const int j = lane + 32 * q, k = j % Ns;
             if (full || j < nb) {
                 const int idxD = (j / Ns) * Ns * R + k;
-                const int pb = wpad(idxD);
+                const int pb = wpad<V>(idxD);
 #pragma unroll
-                for (int r = 0; r < R; ++r) wb[st_kind ? pb + st_off(r) : wpad(idxD + r * Ns)] = v[q][r];
+                for (int r = 0; r < R; ++r) wb[st_kind ? pb + st_off(r) : wpad<V>(idxD + r * Ns)] = v[q][r];
             }
         }
     }
@@ -130,7 +143,7 @@ __global__ void __launch_bounds__(W * 32, zw_minb<T>()) k_zconv_warp(const cplx<
     static_assert(RF % 2 == 0, "first radix must be even");
     typedef WStage<V, RF, L, 1> S0;       // first stage
     typedef WStage<V, RF, L, L / RF> SL;  // last stage
-    constexpr int NB = L / RF, Q = S0::Q, WB = wbuf_len(L);
+    constexpr int NB = L / RF, Q = S0::Q, WB = wbuf_len<T>(L);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ uint64_t gbar;
     __shared__ int gfail;
@@ -170,7 +183,7 @@ __global__ void __launch_bounds__(W * 32, zw_minb<T>()) k_zconv_warp(const cplx<
             const int col = col0 + c;
             V v = mk<T>(0, 0);
             if (col < a.ncols) v = src[(int64_t)e * a.in_estride + col];
-            wbufs[c * WB + wpad(e)] = v;
+            wbufs[c * WB + wpad<V>(e)] = v;
         }
     };
     // forward transform (sign +1) of this warp's column; the upper half of its input is zero.
@@ -256,14 +269,14 @@ __global__ void __launch_bounds__(W * 32, zw_minb<T>()) k_zconv_warp(const cplx<
             const int j = lane + 32 * q;
             if (S0::full || j < NB)
 #pragma unroll
-                for (int r = 0; r < RF / 2; ++r) wb[wpad(j + NB * r)] = v[q][r];  // z = j + NB r < L/2
+                for (int r = 0; r < RF / 2; ++r) wb[wpad<V>(j + NB * r)] = v[q][r];  // z = j + NB r < L/2
         }
         __syncthreads();
         V *dst = out + (int64_t)o * a.out_cstride;
         for (int idx = threadIdx.x; idx < W * a.nz; idx += W * 32) {
             const int e = idx / W, c = idx - e * W;
             const int col = col0 + c;
-            if (col < a.ncols) dst[(int64_t)e * a.out_estride + (int64_t)col * a.out_colstride] = wbufs[c * WB + wpad(e)];
+            if (col < a.ncols) dst[(int64_t)e * a.out_estride + (int64_t)col * a.out_colstride] = wbufs[c * WB + wpad<V>(e)];
         }
         __syncthreads();
     };
@@ -301,7 +314,7 @@ __global__ void __launch_bounds__(W * 32, zw_minb<T>()) k_zconv_warp(const cplx<
             const int j = lane + 32 * q;
             if (S0::full || j < NB)
 #pragma unroll
-                for (int r = 0; r < RF; ++r) rb[wpad(j + NB * r)] = rh[q][r];
+                for (int r = 0; r < RF; ++r) rb[wpad<V>(j + NB * r)] = rh[q][r];
         }
     }
     if (GS && !wait_green()) return;
@@ -325,7 +338,7 @@ __global__ void __launch_bounds__(W * 32, zw_minb<T>()) k_zconv_warp(const cplx<
                             S = cmul(rh[q][r], g_lookup<T>(a.g[gd], kx, ky, e, a.nxh, a.Ny, a.ny, L, a.nz, goff));
                         if (IMG && gi >= 0) {
                             // spectrum of -rho flipped in z: -w^((nz-1) kz) * rho_hat(-kz)
-                            const V rm = rb[wpad(e == 0 ? 0 : L - e)];
+                            const V rm = rb[wpad<V>(e == 0 ? 0 : L - e)];
                             const V ph = __ldg(tw_rt + (int)(((int64_t)a.img_phase_mul * e) % L));
                             V ri = cmul(ph, rm);
                             ri.x = -ri.x * icoef;
@@ -344,8 +357,8 @@ __global__ void __launch_bounds__(W * 32, zw_minb<T>()) k_zconv_warp(const cplx<
 // Shared memory bytes of k_zconv_warp for length L, W warps; zp = Green column pitch
 // (elements) of the staged mode.
 template <typename T> inline size_t zconv_warp_smem(int L, int W, int mode, int nout, int zp) {
-    size_t b = sizeof(cplx<T>) * ((size_t)L + (size_t)W * wbuf_len(L));
-    if (mode == ZW_IMAGE) b += sizeof(cplx<T>) * (size_t)W * wbuf_len(L);
+    size_t b = sizeof(cplx<T>) * ((size_t)L + (size_t)W * wbuf_len<T>(L));
+    if (mode == ZW_IMAGE) b += sizeof(cplx<T>) * (size_t)W * wbuf_len<T>(L);
     if (mode == ZW_STAGED || mode == ZW_SUM) b += sizeof(T) * (size_t)W * nout * zp;
     return b;
 }
