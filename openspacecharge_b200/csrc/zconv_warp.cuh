@@ -17,9 +17,11 @@
 // half warp at a time, of 16-byte values a quarter warp at a time; under these paddings the
 // stride-R writes of the first stage, the unit-stride reads of the others and the
 // column-interleaved CTA loads of 4 warps fall on distinct banks.  For 16-byte values the
-// writes of the middle stages are conflict-free too; for 8-byte values the middle-stage
-// writes of a half warp that spans two output groups are 2-way conflicted (no additive
-// padding serves both these writes and the 16-element unit-stride reads).  The Green spectra of this kernel are stored with kz
+// writes of the middle stages are conflict-free too.  For 8-byte values a radix-8 middle
+// stage with Ns = 8 writes two output groups 64 elements apart per half warp, which the
+// one-in-sixteen padding puts on overlapping banks; the buffer between that stage and the
+// next takes layout 1 (wpadl), under which those writes and the next stage's reads are both
+// conflict-free.  The Green spectra of this kernel are stored with kz
 // innermost (GSpecDev::zinner), so the 32 lanes of a warp read 32 consecutive kz.  When
 // all spectra are real and even/odd in z (free space without images), each CTA fetches the
 // Green columns of its W columns into shared memory with bulk copies at launch, which
@@ -42,28 +44,44 @@ template <typename T> constexpr int zw_minb() { return sizeof(T) == 4 ? 6 : 2; }
 // padding shift of a complex type: 4 (one element in 16) for 8-byte, 3 (one in 8) for 16-byte
 template <typename V> constexpr int wpad_shift() { return sizeof(V) >= 16 ? 3 : 4; }
 template <typename V> __device__ __forceinline__ int wpad(int e) { return e + (e >> wpad_shift<V>()); }
-// elements per warp buffer of real type T: the padded length, rounded up to 4 mod 16 (FP32)
-// or 2 mod 8 (FP64) so that the 4 warp buffers start on different banks
+// Layout 1, for 8-byte values between a radix-8 stage with Ns = 8 and the next stage: one
+// pad element in 16 plus four in 64.  That stage writes, per half warp, two output groups 64
+// elements apart (x = 64g + k + 8r, k < 8); the extra four per 64 puts them 8 banks pairs
+// apart, while 16 consecutive elements (the next stage's reads) keep distinct banks.
+template <typename V, int LAY> __device__ __forceinline__ int wpadl(int e) {
+    return LAY ? e + (e >> 4) + 4 * (e >> 6) : wpad<V>(e);
+}
+constexpr int zw_lay_of(int vbytes, int Ns, int R) { return vbytes == 8 && Ns == 8 && R == 8 ? 1 : 0; }
+// elements per warp buffer of real type T: the largest padded index of either layout plus
+// one, rounded up to 4 mod 16 (FP32) or 2 mod 8 (FP64) so that the 4 warp buffers start on
+// different banks
 template <typename T> constexpr int wbuf_len(int L) {
-    return sizeof(T) == 4 ? (L + L / 16) + ((4 - (L + L / 16)) % 16 + 16) % 16
-                          : (L + L / 8) + ((2 - (L + L / 8)) % 8 + 8) % 8;
+    return sizeof(T) == 4
+               ? (L + (L - 1) / 16 + 4 * ((L - 1) / 64) + 1) + ((4 - (L + (L - 1) / 16 + 4 * ((L - 1) / 64) + 1)) % 16 + 16) % 16
+               : (L + L / 8) + ((2 - (L + L / 8)) % 8 + 8) % 8;
 }
 
 // One stage of one warp's transform: butterflies j = lane + 32q (j < L/R), input elements
 // j + (L/R) r, outputs (j/Ns) Ns R + j%Ns + Ns r; per-stage twiddles at (Ns-1) + k(R-1) + r-1.
 // Padded positions of a butterfly's R elements are a per-lane base plus compile-time
 // offsets wherever the padding allows it.
-template <typename V, int R, int L, int Ns> struct WStage {
+// LDL / STL: layouts (0 = wpad, 1 = wpadl<V, 1>) of the buffer this stage reads and writes.
+template <typename V, int R, int L, int Ns, int LDL = 0, int STL = 0> struct WStage {
     static constexpr int nb = L / R;
     static constexpr int Q = (nb + 31) / 32;
     static constexpr bool full = nb % 32 == 0;
     static constexpr int PS = wpad_shift<V>(), PB = 1 << PS;  // one pad element per PB
-    static constexpr bool ld_lin = nb % PB == 0;  // wpad(j + r nb) = wpad(j) + r (nb + nb/PB)
-    // store: 1 = Ns multiple of PB, 2 = Ns | PB and PB | Ns R, 3 = Ns R | PB, 0 = per element
+    // wpadl(j + r nb) = wpadl(j) + r ld_step: layout 0 when PB | nb; layout 1 when 64 | nb
+    static constexpr bool ld_lin = LDL ? nb % 64 == 0 : nb % PB == 0;
+    static constexpr int ld_step = LDL ? nb + nb / 16 + nb / 16 : nb + nb / PB;
+    // store: 1 = Ns multiple of PB, 2 = Ns | PB and PB | Ns R, 3 = Ns R | PB, 0 = per element;
+    // layout 1 takes form 2 when Ns | 16, 16 | Ns R and Ns R | 64 (one 64-block per butterfly)
     static constexpr int st_kind =
-        Ns % PB == 0 ? 1 : (PB % Ns == 0 && (Ns * R) % PB == 0) ? 2 : (PB % (Ns * R) == 0) ? 3 : 0;
+        STL ? ((16 % Ns == 0 && (Ns * R) % 16 == 0 && 64 % (Ns * R) == 0) ? 2 : 0)
+            : Ns % PB == 0 ? 1 : (PB % Ns == 0 && (Ns * R) % PB == 0) ? 2 : (PB % (Ns * R) == 0) ? 3 : 0;
     __device__ __forceinline__ static constexpr int st_off(int r) {
-        return st_kind == 1 ? r * (Ns + Ns / PB) : st_kind == 2 ? r * Ns + ((r * Ns) >> PS) : r * Ns;
+        return STL ? r * Ns + ((r * Ns) >> 4)
+                   : st_kind == 1 ? r * (Ns + Ns / PB) : st_kind == 2 ? r * Ns + ((r * Ns) >> PS) : r * Ns;
     }
 
     __device__ __forceinline__ static void load(const V *wb, const V *tw, int sign, int lane, V (&v)[Q][R],
@@ -71,7 +89,7 @@ template <typename V, int R, int L, int Ns> struct WStage {
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
             const int j = lane + 32 * q, k = j % Ns;
-            const int pb = wpad<V>(j);
+            const int pb = wpadl<V, LDL>(j);
             if (full || j < nb) {
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
@@ -80,7 +98,7 @@ template <typename V, int R, int L, int Ns> struct WStage {
                         x.x = 0;
                         x.y = 0;
                     } else {
-                        x = wb[ld_lin ? pb + r * (nb + nb / PB) : wpad<V>(j + r * nb)];
+                        x = wb[ld_lin ? pb + r * ld_step : wpadl<V, LDL>(j + r * nb)];
                         if (r && Ns > 1) x = cmul(x, tw_get(tw, (Ns - 1) + k * (R - 1) + (r - 1), sign));
                     }
                     v[q][r] = x;
@@ -98,31 +116,41 @@ template <typename V, int R, int L, int Ns> struct WStage {
             const int j = lane + 32 * q, k = j % Ns;
             if (full || j < nb) {
                 const int idxD = (j / Ns) * Ns * R + k;
-                const int pb = wpad<V>(idxD);
+                const int pb = wpadl<V, STL>(idxD);
 #pragma unroll
-                for (int r = 0; r < R; ++r) wb[st_kind ? pb + st_off(r) : wpad<V>(idxD + r * Ns)] = v[q][r];
+                for (int r = 0; r < R; ++r) wb[st_kind ? pb + st_off(r) : wpadl<V, STL>(idxD + r * Ns)] = v[q][r];
             }
         }
     }
 };
 
-// Stages strictly between the first and the last, in place in the warp buffer.
-template <typename V, int L, int Ns, int R, int... Rest>
+// Stages strictly between the first and the last, in place in the warp buffer; LIN is the
+// layout of the buffer the stage reads (the first stage writes layout 0).
+template <typename V, int L, int LIN, int Ns, int R, int... Rest>
 __device__ __forceinline__ void wfft_mid(V *wb, const V *tw, int sign, int lane) {
     if constexpr (sizeof...(Rest) > 0) {
-        typedef WStage<V, R, L, Ns> S;
+        constexpr int LOUT = zw_lay_of((int)sizeof(V), Ns, R);
+        typedef WStage<V, R, L, Ns, LIN, LOUT> S;
         V v[S::Q][R];
         S::load(wb, tw, sign, lane, v, false);
         S::dft(v, sign);
         __syncwarp();
         S::store(wb, lane, v);
         __syncwarp();
-        wfft_mid<V, L, Ns * R, Rest...>(wb, tw, sign, lane);
+        wfft_mid<V, L, LOUT, Ns * R, Rest...>(wb, tw, sign, lane);
     }
 }
 template <typename V, int L, int R0, int... Rest>
 __device__ __forceinline__ void wfft_mid_of(Radices<R0, Rest...>, V *wb, const V *tw, int sign, int lane) {
-    wfft_mid<V, L, R0, Rest...>(wb, tw, sign, lane);
+    wfft_mid<V, L, 0, R0, Rest...>(wb, tw, sign, lane);
+}
+// layout of the buffer the last stage reads: written by the second-to-last stage
+template <typename V, int... Rs> constexpr int zw_last_lay() {
+    constexpr int n = sizeof...(Rs);
+    constexpr int r[n] = {Rs...};
+    int ns = 1;
+    for (int i = 0; i + 2 < n; ++i) ns *= r[i];
+    return n >= 3 ? zw_lay_of((int)sizeof(V), ns, r[n - 2]) : 0;
 }
 
 // Green term modes of the kernel.
@@ -142,7 +170,7 @@ __global__ void __launch_bounds__(W * 32, zw_minb<T>()) k_zconv_warp(const cplx<
     static_assert(RF == WarpFft<L, Rs...>::kRad[sizeof...(Rs) - 1], "first and last radix must match");
     static_assert(RF % 2 == 0, "first radix must be even");
     typedef WStage<V, RF, L, 1> S0;       // first stage
-    typedef WStage<V, RF, L, L / RF> SL;  // last stage
+    typedef WStage<V, RF, L, L / RF, zw_last_lay<V, Rs...>()> SL;  // last stage
     constexpr int NB = L / RF, Q = S0::Q, WB = wbuf_len<T>(L);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ uint64_t gbar;
