@@ -195,7 +195,7 @@ def kernel_bytes(nx, ny, nz, npart, at_cathode=False):
     }
 
 
-TRAFFIC_TABLE = os.path.join(ROOT, "profiles", "traffic_fp32_128x128x256.md")
+TRAFFIC_DATA = os.path.join(ROOT, "profiles", "dram_traffic_fp32_128x128x256.json")
 
 
 def kernel_profile(ctx, osc, run, n):
@@ -211,17 +211,17 @@ def kernel_profile(ctx, osc, run, n):
             for name, (cnt, t) in sorted(prof.items(), key=lambda kv: -kv[1][1])}
 
 
-def profiled_traffic(label):
-    """DRAM bytes per launch of one kernel of the headline workload, from the committed ncu
-    table (None when the table or the kernel is missing)."""
+def profiled_traffic(label, grid, npart, order):
+    """DRAM bytes per launch of one kernel, from the committed ncu data file, when the file
+    was captured on this exact workload (None otherwise)."""
     try:
-        for line in open(TRAFFIC_TABLE):
-            cells = [c.strip() for c in line.strip().strip("|").split("|")]
-            if len(cells) >= 5 and cells[0] == label:
-                return int(cells[4])
-    except (OSError, ValueError):
-        pass
-    return None
+        d = json.load(open(TRAFFIC_DATA))
+        w = d["workload"]
+        if tuple(w["grid"]) != tuple(grid) or int(w["particles"]) != npart or w.get("order") != order:
+            return None
+        return int(d["kernels"][label]["traffic_bytes"])
+    except (OSError, ValueError, KeyError, TypeError):
+        return None
 
 
 def run_ours(args, ws, rank, local, dist):
@@ -343,12 +343,12 @@ def run_ours(args, ws, rank, local, dist):
     roof = None
     if dom:
         ach = kernels[dom]["gbs"]
-        traffic = profiled_traffic(dom) if (tuple(grid) == GRID and npart == NPART) else None
+        traffic = profiled_traffic(dom, grid, npart, "random")
         roof = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
                 "frac": ach / hbm_peak, "peak_source": peak_src + " (MEASURED_PEAKS.json hbm_gbs)",
                 "traffic": traffic, "alg_bytes_per_launch": kb[dom],
                 "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of this kernel on this "
-                                   "workload, profiles/traffic_fp32_128x128x256.md") if traffic else None}
+                                   "workload, " + os.path.relpath(TRAFFIC_DATA, ROOT)) if traffic else None}
     step_bytes = sum(kb.values())
     step_gbs = step_bytes / (ms32 * 1e-3) / 1e9
 

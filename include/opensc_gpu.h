@@ -64,6 +64,10 @@ extern "C" {
 #define OSC_OPT_GREEN_CACHE_MB 4 /* byte budget of the Green-spectrum cache (default 4096) */
 #define OSC_OPT_PROFILE 5        /* 1: time every kernel with CUDA events (osc_profile_*) */
 #define OSC_OPT_CHECK_FINITE 6   /* 1: deposit rejects non-finite coordinates (OSC_E_NAN) */
+#define OSC_OPT_TEST_WAIT_TIMEOUT 7 /* test only, 1: the z pass arms its Green-column barrier
+                                       but issues no bulk copy and polls 64 times, so its
+                                       bounded wait gives up; the call returns OSC_E_TIMEOUT
+                                       and the context stays usable */
 
 typedef struct osc_ctx osc_ctx;
 
@@ -124,10 +128,16 @@ OSC_API int osc_deposit_particles_dev(osc_ctx *ctx, int64_t np, const double *d_
  * mesh and device buffers; the deposit accumulates in FP32 in a fixed array compiled into
  * the library (OSC_NOALLOC_MAX_NODES floats, 16 MiB, held on every GPU that loads the
  * library until the process exits) and writes REAL64 rho.  Meshes with more nodes are
- * rejected with OSC_E_INVALID.  Charges are d_q per particle, or total_charge/np when d_q
- * is NULL; the mesh is not refitted and mesh->charge is not touched.  The first call on a
- * device looks up the array's device address once (make that first call before any stream
- * capture).  All calls share the one array, so calls whose work overlaps on the GPU race.
+ * rejected with OSC_E_INVALID (the node count is formed in 64-bit arithmetic and checked
+ * after every factor, so no mesh can wrap it).  Charges are d_q per particle, or
+ * total_charge/np when d_q is NULL: total_charge is used as given (zero deposits zeros, a
+ * non-finite value is OSC_E_INVALID), since this signature has no "absent" value for the
+ * reference's missing-charge case.  The mesh is not refitted and mesh->charge is not
+ * touched.  *n_outside counts particles outside the mesh plus particles with a non-finite
+ * coordinate, the count osc_deposit_particles_dev reports with its default options.  The
+ * first call in a CUDA context (normally once per device) looks up the array's device
+ * address (make that first call before any stream capture); cudaDeviceReset invalidates
+ * it.  All calls share the one array, so calls whose work overlaps on the GPU race.
  * errbuf (optional, errlen bytes) receives a message. */
 #define OSC_NOALLOC_MAX_NODES 4194304
 OSC_API int osc_deposit_particles_dev_noalloc(void *cuda_stream, const osc_mesh3d *mesh, int64_t np,

@@ -89,6 +89,7 @@ int osc_ctx_set_option(osc_ctx *ctx, int option, int64_t v) {
     case OSC_OPT_GREEN_CACHE_MB: ctx->gcache_budget = (size_t)(v < 0 ? 0 : v) << 20; return OSC_OK;
     case OSC_OPT_PROFILE: ctx->profile = v ? 1 : 0; return OSC_OK;
     case OSC_OPT_CHECK_FINITE: ctx->check_finite = v ? 1 : 0; return OSC_OK;
+    case OSC_OPT_TEST_WAIT_TIMEOUT: ctx->test_wait_timeout = v ? 1 : 0; return OSC_OK;
     default: return bad(ctx, "unknown option");
     }
 }
@@ -102,6 +103,7 @@ int osc_ctx_get_option(osc_ctx *ctx, int option, int64_t *v) {
     case OSC_OPT_GREEN_CACHE_MB: *v = (int64_t)(ctx->gcache_budget >> 20); return OSC_OK;
     case OSC_OPT_PROFILE: *v = ctx->profile; return OSC_OK;
     case OSC_OPT_CHECK_FINITE: *v = ctx->check_finite; return OSC_OK;
+    case OSC_OPT_TEST_WAIT_TIMEOUT: *v = ctx->test_wait_timeout; return OSC_OK;
     default: return bad(ctx, "unknown option");
     }
 }

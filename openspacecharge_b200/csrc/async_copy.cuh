@@ -52,9 +52,10 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
     return done != 0;
 }
 
-// Polls phase `parity` of the barrier at most MBAR_POLL_LIMIT times.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity) {
-    for (unsigned it = 0; it < MBAR_POLL_LIMIT; ++it)
+// Polls phase `parity` of the barrier at most `limit` times (0: MBAR_POLL_LIMIT).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity, unsigned limit = 0) {
+    if (limit == 0) limit = MBAR_POLL_LIMIT;
+    for (unsigned it = 0; it < limit; ++it)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }

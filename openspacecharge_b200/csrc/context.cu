@@ -54,7 +54,7 @@ int ctx_sync(osc_ctx *c) {
     if (c->h_fault && *reinterpret_cast<volatile unsigned *>(c->h_fault)) {
         const unsigned f = *c->h_fault;
         *reinterpret_cast<volatile unsigned *>(c->h_fault) = 0;
-        return set_err(c, OSC_E_CUDA, "device wait gave up (fault code %u): a bulk copy did not complete", f);
+        return set_err(c, OSC_E_TIMEOUT, "device wait gave up (fault code %u): a bulk copy did not complete", f);
     }
     return OSC_OK;
 }

@@ -67,6 +67,7 @@ struct osc_ctx {
     int strict_bounds = 0;
     int profile = 0;
     int check_finite = 0;
+    int test_wait_timeout = 0;  // OSC_OPT_TEST_WAIT_TIMEOUT
     size_t gcache_budget = (size_t)4096 << 20;
     // workspaces by name
     std::map<std::string, osc::DevBuf> ws;

@@ -119,6 +119,9 @@ struct ZConvArgs {
     int ng;
     GSpecDev g[8];
     unsigned *fault;      // host-mapped fault word (bounded waits that gave up), or null
+    unsigned poll_limit;  // polls of a bounded mbarrier wait (0: MBAR_POLL_LIMIT)
+    int skip_copies;      // test only: arm the Green-column barrier but issue no bulk copy,
+                          // so the bounded wait runs out and the fault path is exercised
     // batches of equal grids (blockIdx.y = member): input, output and spectrum offsets of
     // member b are b*in_bstride, b*out_bstride and b*g_bstride (elements of the spectrum)
     int nbatch;

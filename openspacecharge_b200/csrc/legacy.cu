@@ -424,6 +424,10 @@ static int pipe_phi_opt(osc_ctx *c, const LGeom &g, const double *rho, double *p
     za.nout = nout;
     za.ng = 4;
     za.fault = c->d_fault;
+    if (c->test_wait_timeout) {  // test only: waits that must run out quickly
+        za.poll_limit = 64;
+        za.skip_copies = 1;
+    }
     const size_t each = (size_t)nxh * Ny * Nz;
     for (int t = 0; t < 4; ++t) {
         za.gdir[t] = t;

@@ -11,6 +11,9 @@
 //
 // Cost of that array: OSC_NOALLOC_MAX_NODES floats (16 MiB) plus a few counters, held on
 // every GPU that loads this library until the process exits.
+#include <cuda.h>
+
+#include <cmath>
 #include <mutex>
 
 #include "../../include/opensc_gpu.h"
@@ -26,9 +29,21 @@ constexpr int kCounterWords = 32;  // 256 bytes of counters after the grid
 // On the host this name is only a handle for cudaGetSymbolAddress, never a device address.
 __device__ __align__(256) unsigned char g_noalloc_scratch[kMaxNodes * sizeof(float) + kCounterWords * 8];
 
-constexpr int kMaxDevices = 64;
-void *g_scratch_addr[kMaxDevices] = {nullptr};
+// The array's device address belongs to one CUDA context.  It is looked up once per
+// context (normally once per device: the primary context) and cached under the context
+// handle, so a caller that makes another driver context current gets that context's
+// address.  cudaDeviceReset destroys the primary context and with it this address: a
+// process that resets a device must not call the entry point on that device afterwards.
+constexpr int kMaxContexts = 64;
+struct ScratchSlot {
+    void *cuctx;
+    void *addr;
+};
+ScratchSlot g_slots[kMaxContexts] = {};
+int g_nslots = 0;
 std::mutex g_scratch_mu;
+
+typedef CUresult (*CtxGetCurrentFn)(CUcontext *);
 
 int fail(char *errbuf, size_t errlen, int code, const char *msg) {
     if (errbuf && errlen > 0) {
@@ -42,24 +57,48 @@ int fail(char *errbuf, size_t errlen, int code, const char *msg) {
     return code;
 }
 
-// Device address of the scratch array on the current device, looked up once per device.
+// Device address of the scratch array in the current context (set-up on first use).
 int scratch_address(void **out, char *errbuf, size_t errlen) {
     int dev = -1;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) {
         cudaGetLastError();
         return fail(errbuf, errlen, OSC_E_CUDA, "no current CUDA device");
     }
     std::lock_guard<std::mutex> lock(g_scratch_mu);
-    if (!g_scratch_addr[dev]) {
-        void *p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p) {
+    static CtxGetCurrentFn get_current = nullptr;
+    if (!get_current) {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult qr;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &qr) != cudaSuccess ||
+            qr != cudaDriverEntryPointSuccess || !fn) {
             cudaGetLastError();
-            return fail(errbuf, errlen, OSC_E_CUDA, "cudaGetSymbolAddress of the deposit scratch array failed");
+            return fail(errbuf, errlen, OSC_E_CUDA, "cuCtxGetCurrent is not available");
         }
-        g_scratch_addr[dev] = p;
+        get_current = reinterpret_cast<CtxGetCurrentFn>(fn);
     }
-    *out = g_scratch_addr[dev];
+    CUcontext cur = nullptr;
+    if (get_current(&cur) != CUDA_SUCCESS) return fail(errbuf, errlen, OSC_E_CUDA, "cuCtxGetCurrent failed");
+    if (!cur) {
+        // nothing current yet: cudaSetDevice initialises the device's primary context
+        if (cudaSetDevice(dev) != cudaSuccess || get_current(&cur) != CUDA_SUCCESS || !cur) {
+            cudaGetLastError();
+            return fail(errbuf, errlen, OSC_E_CUDA, "no current CUDA context");
+        }
+    }
+    for (int i = 0; i < g_nslots; ++i)
+        if (g_slots[i].cuctx == (void *)cur) {
+            *out = g_slots[i].addr;
+            return OSC_OK;
+        }
+    if (g_nslots == kMaxContexts) return fail(errbuf, errlen, OSC_E_CUDA, "too many CUDA contexts");
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+        cudaGetLastError();
+        return fail(errbuf, errlen, OSC_E_CUDA, "cudaGetSymbolAddress of the deposit scratch array failed");
+    }
+    g_slots[g_nslots++] = ScratchSlot{(void *)cur, p};
+    *out = p;
     return OSC_OK;
 }
 
@@ -73,16 +112,20 @@ int osc_deposit_particles_dev_noalloc(void *cuda_stream, const osc_mesh3d *mesh,
                                       size_t errlen) {
     if (!mesh || np < 0 || (np > 0 && (!d_x || !d_y || !d_z)) || !d_rho)
         return fail(errbuf, errlen, OSC_E_INVALID, "invalid argument: mesh, particle arrays or rho is NULL");
+    // node count in 64-bit arithmetic, checked after every factor: no product can wrap
     int n[3];
     int64_t nodes = 1;
     for (int d = 0; d < 3; ++d) {
-        n[d] = mesh->nhi[d] - mesh->nlo[d] + 1;
-        if (n[d] < 2) return fail(errbuf, errlen, OSC_E_INVALID, "mesh axis with fewer than 2 nodes");
-        nodes *= n[d];
+        const int64_t nd = (int64_t)mesh->nhi[d] - (int64_t)mesh->nlo[d] + 1;
+        if (nd < 2) return fail(errbuf, errlen, OSC_E_INVALID, "mesh axis with fewer than 2 nodes");
+        if (nd > kMaxNodes || nodes * nd > kMaxNodes)
+            return fail(errbuf, errlen, OSC_E_INVALID,
+                        "mesh has more nodes than the no-allocation deposit holds (OSC_NOALLOC_MAX_NODES = 4194304)");
+        n[d] = (int)nd;
+        nodes *= nd;
     }
-    if (nodes > kMaxNodes)
-        return fail(errbuf, errlen, OSC_E_INVALID,
-                    "mesh has more nodes than the no-allocation deposit holds (OSC_NOALLOC_MAX_NODES = 4194304)");
+    if (!std::isfinite(total_charge))
+        return fail(errbuf, errlen, OSC_E_INVALID, "total_charge must be finite");
     if (!(mesh->delta[0] > 0 && mesh->delta[1] > 0 && mesh->delta[2] > 0))
         return fail(errbuf, errlen, OSC_E_INVALID, "mesh delta must be positive");
     void *base = nullptr;
@@ -125,17 +168,18 @@ int osc_deposit_particles_dev_noalloc(void *cuda_stream, const osc_mesh3d *mesh,
     a.nz = n[2];
     a.mode = 0;
     a.charge1 = np > 0 ? total_charge / (double)np : 0.0;
-    a.check_finite = 0;
+    a.check_finite = 1;
     if (osc::launch_deposit<float>(a, grid, counters, st) || osc::launch_f32_to_f64(grid, d_rho, nodes, st))
         return fail(errbuf, errlen, OSC_E_CUDA, "deposit kernel launch failed");
     if (n_outside) {
-        unsigned long long h = 0;
-        if (cudaMemcpyAsync(&h, counters, sizeof(h), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        // out-of-mesh and non-finite particles, the count the context entry point reports
+        unsigned long long h[2] = {0, 0};
+        if (cudaMemcpyAsync(h, counters, sizeof(h), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
             cudaStreamSynchronize(st) != cudaSuccess) {
             cudaGetLastError();
             return fail(errbuf, errlen, OSC_E_CUDA, "reading the out-of-mesh count failed");
         }
-        *n_outside = (int64_t)h;
+        *n_outside = (int64_t)(h[0] + h[1]);
     }
     return fail(errbuf, errlen, OSC_OK, "");
 }

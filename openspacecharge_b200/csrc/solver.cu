@@ -466,6 +466,10 @@ int freespace_opt(osc_ctx *c, const FreeSpaceJob &j, const TIn *rho) {
     za.img_phase_mul = nz - 1;
     za.ng = gs->nspec;
     za.fault = c->d_fault;
+    if (c->test_wait_timeout) {  // test only: waits that must run out quickly
+        za.poll_limit = 64;
+        za.skip_copies = 1;
+    }
     za.nbatch = j.sum3 ? 1 : B;
     za.in_bstride = za.out_bstride = (int64_t)nxh * Ny * nz;
     za.g_bstride = j.gbatch ? j.g_bstride : 0;

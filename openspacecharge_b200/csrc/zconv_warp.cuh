@@ -198,7 +198,7 @@ __global__ void __launch_bounds__(W * 32, zw_minb<T>()) k_zconv_warp(const cplx<
                     const GSpecDev &g = a.g[a.gdir[o]];
                     const int yy = (g.sym_y && ky > a.ny) ? a.Ny - ky : ky;
                     const T *src = reinterpret_cast<const T *>(g.data) + goff + ((int64_t)yy * a.nxh + kx) * zp;
-                    bulk_g2s(gst + (c * nst + o) * zp, src, (unsigned)(zp * sizeof(T)), &gbar);
+                    if (!a.skip_copies) bulk_g2s(gst + (c * nst + o) * zp, src, (unsigned)(zp * sizeof(T)), &gbar);
                 }
             }
         }
@@ -230,10 +230,13 @@ __global__ void __launch_bounds__(W * 32, zw_minb<T>()) k_zconv_warp(const cplx<
     // CTA-wide wait for the staged Green columns; false when the copies did not complete
     auto wait_green = [&]() -> bool {
         if (threadIdx.x == 0) {
-            const bool ok = mbar_wait_bounded(&gbar, 0);
+            const bool ok = mbar_wait_bounded(&gbar, 0, a.poll_limit);
             if (!ok) {
                 report_fault(a.fault, FAULT_BULK_WAIT);
-                mbar_wait_bounded(&gbar, 0);  // let copies in flight land before leaving
+                // let copies in flight land before leaving.  If this wait runs out too, the
+                // CTA leaves with copies that may still be in flight into its shared memory;
+                // the CTA reads none of it, and the host reports the call as timed out
+                mbar_wait_bounded(&gbar, 0, a.poll_limit);
             }
             gfail = ok ? 0 : 1;
         }

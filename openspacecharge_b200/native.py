@@ -40,6 +40,7 @@ OPT_STRICT_BOUNDS = 3
 OPT_GREEN_CACHE_MB = 4
 OPT_PROFILE = 5
 OPT_CHECK_FINITE = 6
+OPT_TEST_WAIT_TIMEOUT = 7
 
 _ERRNAMES = {v: k for k, v in globals().items() if k.startswith("OSC_E_") or k == "OSC_OK"}
 

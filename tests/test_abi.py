@@ -65,3 +65,33 @@ def test_bunch_generator_shapes():
     assert np.array_equal(x, x2)
     xp, yp, _ = gendist(5000, sigma=(2e-3, 1e-3, 1e-3), seed=3, pipe=(20e-3, 10e-3), centroid=(3e-3, -1e-3, 0))
     assert (((xp - 3e-3) / 10e-3) ** 2 + ((yp + 1e-3) / 5e-3) ** 2).max() <= 0.81 * 1.05
+
+
+def _noalloc_status(nlo, nhi, total_charge=1e-9):
+    """Status of the no-allocation deposit for a mesh whose checks fail before any CUDA
+    call; the particle and rho pointers are dummies that are never dereferenced."""
+    m = native.OscMesh3D()
+    for d in range(3):
+        m.nlo[d], m.nhi[d], m.delta[d] = nlo[d], nhi[d], 1e-3
+    dummy = ctypes.c_void_p(16)
+    err = ctypes.create_string_buffer(256)
+    rc = native.lib().osc_deposit_particles_dev_noalloc(None, ctypes.byref(m), 4, dummy, dummy, dummy, None,
+                                                        ctypes.c_double(total_charge), dummy, None, err,
+                                                        ctypes.sizeof(err))
+    return rc, err.value.decode()
+
+
+@pytest.mark.parametrize("nhi", [(2 ** 21, 2 ** 21, 2 ** 22),      # product 2^64 wraps to 0 in int64
+                                 (2 ** 31 - 1, 2 ** 31 - 1, 8),    # each factor overflows int32 products
+                                 (256, 256, 128)])                 # plainly above the limit
+def test_noalloc_rejects_oversized_and_wrapping_meshes_before_any_launch(nhi):
+    rc, msg = _noalloc_status((1, 1, 1), nhi)
+    assert rc == native.OSC_E_INVALID
+    assert "OSC_NOALLOC_MAX_NODES" in msg
+
+
+def test_noalloc_rejects_a_negative_extent_and_a_non_finite_charge():
+    rc, msg = _noalloc_status((1, 1, 1), (-(2 ** 31) + 1, 8, 8))
+    assert rc == native.OSC_E_INVALID and "fewer than 2 nodes" in msg
+    rc, msg = _noalloc_status((1, 1, 1), (8, 8, 8), total_charge=float("nan"))
+    assert rc == native.OSC_E_INVALID and "total_charge" in msg

@@ -4,7 +4,9 @@ It serves callers that may not allocate device memory when they deposit charge: 
 running inside another framework's memory pool, loops that cannot take the device
 synchronisation of cudaMalloc/cudaFree, and programs that do not create a library context.
 Its FP32 accumulation grid is a fixed array inside the library, shared by every call, so
-each call must clear it; two calls in a row must both reproduce the ordinary entry point.
+each call must clear the part it uses: two calls in a row, a smaller mesh after a larger
+one and a call without particles must all reproduce the ordinary entry point, including
+its count of particles outside the mesh or with non-finite coordinates.
 This file is collected last and also runs on its own in a fresh process.
 """
 import ctypes
@@ -80,3 +82,67 @@ def test_noalloc_rejects_meshes_above_its_limit(ctx):
     rc, _, msg = _noalloc(mesh.to_c(), t, t, t, None, 1e-9, rho)
     assert rc == native.OSC_E_INVALID
     assert "OSC_NOALLOC_MAX_NODES" in msg
+
+
+def _ordinary(ctx, mesh_c, tx, ty, tz, total_charge, n):
+    """rho and the outside count from the ordinary entry point (context workspaces)."""
+    import torch
+    ref = torch.zeros(n[::-1], dtype=torch.float64, device=tx.device)
+    tc = ctypes.c_double(total_charge)
+    nref = ctypes.c_int64()
+    torch.cuda.synchronize()
+    ctx.call("osc_deposit_particles_dev", ctypes.c_int64(tx.numel()), ctypes.c_void_p(tx.data_ptr()),
+             ctypes.c_void_p(ty.data_ptr()), ctypes.c_void_p(tz.data_ptr()), None, ctypes.byref(tc), 0,
+             ctypes.byref(mesh_c), ctypes.c_void_p(ref.data_ptr()), ctypes.byref(nref))
+    ctx.synchronize()
+    return ref.cpu().numpy(), int(nref.value)
+
+
+def test_noalloc_counts_outside_and_non_finite_like_the_entry_point(ctx):
+    torch = pytest.importorskip("torch")
+    dev = torch.device("cuda", 0)
+    x, y, z = gendist(200_000, sigma=(0.5e-3, 0.5e-3, 2e-3), seed=78)
+    n = (32, 32, 48)
+    delta, umin = osc.get_mesh_quantities(ctx, x, y, z, (1, 1, 1), n, 0)
+    # shrink the mesh so the tails fall outside, and plant non-finite coordinates
+    delta = delta * 0.8
+    x[:50] = np.nan
+    y[50:60] = np.inf
+    z[60:70] = -np.inf
+    mesh = osc.Mesh3D(nlo=(1, 1, 1), nhi=n, min=umin, max=umin + (np.array(n) - 1) * delta, delta=delta)
+    tx, ty, tz = (torch.from_numpy(a).to(dev) for a in (x, y, z))
+    r, nref = _ordinary(ctx, mesh.to_c(), tx, ty, tz, 1e-9, n)
+    assert nref > 70
+    out = torch.full(n[::-1], -1.0, dtype=torch.float64, device=dev)
+    rc, nout, msg = _noalloc(mesh.to_c(), tx, ty, tz, None, 1e-9, out)
+    torch.cuda.synchronize()
+    assert rc == native.OSC_OK, msg
+    assert nout == nref
+    o = out.cpu().numpy()
+    assert np.abs(o - r).max() / np.abs(r).max() <= FP32_TOL
+
+
+def test_noalloc_smaller_mesh_after_larger_and_empty_call(ctx):
+    torch = pytest.importorskip("torch")
+    dev = torch.device("cuda", 0)
+    x, y, z = gendist(300_000, sigma=(0.5e-3, 0.5e-3, 2e-3), seed=79)
+    tx, ty, tz = (torch.from_numpy(a).to(dev) for a in (x, y, z))
+    for n in [(64, 64, 96), (20, 24, 28)]:  # the second call uses a prefix of what the first filled
+        delta, umin = osc.get_mesh_quantities(ctx, x, y, z, (1, 1, 1), n, 0)
+        mesh = osc.Mesh3D(nlo=(1, 1, 1), nhi=n, min=umin, max=umin + (np.array(n) - 1) * delta, delta=delta)
+        r, nref = _ordinary(ctx, mesh.to_c(), tx, ty, tz, 1e-9, n)
+        out = torch.full(n[::-1], -1.0, dtype=torch.float64, device=dev)
+        rc, nout, msg = _noalloc(mesh.to_c(), tx, ty, tz, None, 1e-9, out)
+        torch.cuda.synchronize()
+        assert rc == native.OSC_OK, msg
+        assert nout == nref == 0
+        o = out.cpu().numpy()
+        assert np.abs(o - r).max() / np.abs(r).max() <= FP32_TOL
+    # no particles: rho comes back all zero although the array holds the last call's sums
+    empty = torch.zeros(0, dtype=torch.float64, device=dev)
+    out = torch.full(n[::-1], -1.0, dtype=torch.float64, device=dev)
+    rc, nout, msg = _noalloc(mesh.to_c(), empty, empty, empty, None, 1e-9, out)
+    torch.cuda.synchronize()
+    assert rc == native.OSC_OK, msg
+    assert nout == 0
+    assert not out.any().item()
