@@ -62,6 +62,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-refit", action="store_true", help="skip the refit + Green rebuild leg")
     ap.add_argument("--workload", default="single", choices=["single", "batch", "adjoint", "pipe"],
                     help="single: the headline one-bunch step; batch: 256 bunches of mixed grids per step; "
                          "adjoint: forward + backward of sum q|E|^2 at 128^3, 4e6 particles; "
@@ -310,6 +311,7 @@ def run_ours(args, ws, rank, local, dist):
                "definition": "per component max|E-E_ref|/max|E_ref| and RMS ratio, at all particles"}
         fp64 = {"value": ws * 1000.0 / ms64, "ms_per_step": ms64, "steps": k64,
                 "speedup_fp32_over_fp64": ms64 / ms32}
+        E64_plain = E64
         # the optimised pipeline in FP64 (the precision the Fortran drop-in uses by default)
         E64o = torch.empty_like(E)
         step(osc.PREC_FP64, E64o)
@@ -318,6 +320,8 @@ def run_ours(args, ws, rank, local, dist):
         step(osc.PREC_FP64, E64o)
         ctx.synchronize()
         d = (E64o - E64).abs()
+        E64_opt = E64o
+        fp64["speedup_fp32_over_fp64_optimised"] = ms64o / ms32
         fp64["fp64_optimised"] = {"value": ws * 1000.0 / ms64o, "ms_per_step": ms64o,
                                   "max_rel_err_vs_plain": float((d.amax(0) / E64.abs().amax(0)).max()),
                                   "kernels": kernel_profile(ctx, osc, lambda: step(osc.PREC_FP64, E64o), 3)}
@@ -385,9 +389,49 @@ def run_ours(args, ws, rank, local, dist):
                "d2h_bytes_per_step": 3 * 8 * npart, "ms_per_step": te * 1e3,
                "api": "osc_space_charge_step (C ABI, pinned host buffers)"}
 
+    # the reference's default path: mesh refitted to the bunch and Green spectra rebuilt on
+    # every call (code/open_spacecharge_mod.f90:169-174, 570-573)
+    refit = None
+    if not args.no_refit:
+        mesh_r = osc.Mesh3D(nlo=(1, 1, 1), nhi=grid, min=umin.copy(), max=umax.copy(), delta=delta.copy(),
+                            gamma=GAMMA)
+        ctx.set_option(osc.OPT_GREEN_CACHE_MB, 0)
+
+        def step_refit():
+            osc.space_charge_step_dev(ctx, mesh_r, tx, ty, tz, E, total_charge=QTOT, resize_mesh=True,
+                                      precision=osc.PREC_FP32)
+        for _ in range(3):
+            step_refit()
+        ctx.synchronize()
+        kr = max(3, min(args.steps, 10))
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(kr):
+            step_refit()
+        e1.record(stream)
+        e1.synchronize()
+        msr = max_over_ranks(e0.elapsed_time(e1) / kr, dist)
+        prof_r = kernel_profile(ctx, osc, step_refit, 3)
+        ctx.set_option(osc.OPT_GREEN_CACHE_MB, 4096)
+        green_ms = sum(v["ms_per_call"] for k, v in prof_r.items() if k.startswith("green"))
+        refit = {"value": ws * 1000.0 / msr, "unit": "solves/s", "ms_per_step": msr, "steps": kr,
+                 "green_build_ms": green_ms, "green_build_share": green_ms / msr,
+                 "how": "resize_mesh=1 and the Green cache off (OSC_OPT_GREEN_CACHE_MB=0): bounding box, mesh "
+                        "refit, Green spectra rebuilt (FP64 IGF corners, octant differences, three even/odd "
+                        "line-transform passes), deposit, field, interpolation on every call",
+                 "kernels": prof_r}
+
     cpu = None
+    err_oracle = None
     if rank == 0 and ws == 1 and not args.no_cpu:
-        cpu = cpu_baseline(x, y, z, grid, umin, umax, delta)
+        cpu, E_orc = cpu_baseline(x, y, z, grid, umin, umax, delta)
+        # every GPU path against the FP64 oracle on the same arrays, at every particle
+        err_oracle = {"definition": "per component max|E-E_oracle|/max|E_oracle| and RMS ratio, all particles",
+                      "fp32": field_errors(E32.cpu().numpy(), E_orc)}
+        if fp64 is not None:
+            err_oracle["fp64_plain"] = field_errors(E64_plain.cpu().numpy(), E_orc)
+            err_oracle["fp64_optimised"] = field_errors(E64_opt.cpu().numpy(), E_orc)
 
     if rank == 0:
         line = {
@@ -398,7 +442,8 @@ def run_ours(args, ws, rank, local, dist):
                        "particle_dtype": "f64 coordinates in, f64 E out",
                        "l2": "inputs larger than L2 (240 MB of particle coordinates per step)",
                        "parallelism": f"{ws} independent replica(s)"},
-            "fp64_plain": fp64, "rel_err_vs_fp64": err,
+            "fp64_plain": fp64, "rel_err_vs_fp64": err, "rel_err_vs_oracle": err_oracle,
+            "refit_rebuild": refit,
             "step_alg_bytes": step_bytes, "step_alg_gbs": step_gbs,
             "kernels": kernels, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches, "clocks": clk.summary(),
@@ -718,19 +763,27 @@ def run_pipe(args, ws, rank, local, dist):
     ctx.close()
 
 
+def field_errors(E, ref):
+    """Per component max|E-ref|/max|ref| and RMS ratio of (np, 3) fields, with their maxima."""
+    mx = [float(np.abs(E[:, c] - ref[:, c]).max() / np.abs(ref[:, c]).max()) for c in range(3)]
+    rms = [float(np.sqrt(np.mean((E[:, c] - ref[:, c]) ** 2)) / np.sqrt(np.mean(ref[:, c] ** 2))) for c in range(3)]
+    return {"max": max(mx), "rms": max(rms), "max_per_component": mx, "rms_per_component": rms}
+
+
 def cpu_baseline(x, y, z, grid, umin, umax, delta):
-    """One full step of the FP64 CPU port (oracle/) on the host cores."""
+    """One full step of the FP64 CPU port (oracle/) on the host cores; returns the baseline
+    entry and the oracle's E at the particles."""
     from oracle import oracle as O
     O.build()
     m = O.make_mesh((1, 1, 1), grid, (1, 1, 1), umin, umax, delta, GAMMA)
     t0 = time.perf_counter()
     rho, _ = O.deposit_particles(x, y, z, m, total_charge=QTOT, resize_mesh=False)
     ef, _ = O.space_charge_3d(m, rho)
-    O.interpolate_field(m, ef, x, y, z)
+    E_orc, _, _ = O.interpolate_field(m, ef, x, y, z)
     dt = time.perf_counter() - t0
-    return {"value": 1.0 / dt, "unit": "solves/s", "cores": O.num_threads(), "kind": "port",
-            "sample": "1 full step (deposit + solve + interpolation, 1e7 particles, 128x128x256) of the FP64 C++ "
-                      "restatement of the reference algorithm (7 full complex FFTs, G rebuilt), OpenMP"}
+    return ({"value": 1.0 / dt, "unit": "solves/s", "cores": O.num_threads(), "kind": "port",
+             "sample": "1 full step (deposit + solve + interpolation, 1e7 particles, 128x128x256) of the FP64 C++ "
+                       "restatement of the reference algorithm (7 full complex FFTs, G rebuilt), OpenMP"}, E_orc)
 
 
 def run_reference(args, ws, rank):

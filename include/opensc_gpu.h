@@ -61,7 +61,8 @@ extern "C" {
 #define OSC_OPT_PRECISION 1      /* default precision for host entry points */
 #define OSC_OPT_DEPOSIT_MODE 2   /* OSC_DEPOSIT_* */
 #define OSC_OPT_STRICT_BOUNDS 3  /* 1: out-of-mesh particles make deposit return OSC_E_BOUNDS */
-#define OSC_OPT_GREEN_CACHE_MB 4 /* byte budget of the Green-spectrum cache (default 4096) */
+#define OSC_OPT_GREEN_CACHE_MB 4 /* byte budget of the Green-spectrum cache (default 4096); 0
+                                    rebuilds the spectra on every solve, as the reference does */
 #define OSC_OPT_PROFILE 5        /* 1: time every kernel with CUDA events (osc_profile_*) */
 #define OSC_OPT_CHECK_FINITE 6   /* 1: deposit rejects non-finite coordinates (OSC_E_NAN) */
 #define OSC_OPT_TEST_WAIT_TIMEOUT 7 /* test only, 1: the z pass arms its Green-column barrier
@@ -91,7 +92,8 @@ OSC_API int osc_ctx_create(int device, osc_ctx **out);
 OSC_API int osc_ctx_destroy(osc_ctx *ctx);
 OSC_API const char *osc_last_error(const osc_ctx *ctx);
 /* cuda_stream is a cudaStream_t; NULL is CUDA's default stream, as everywhere in CUDA, and
-   OSC_OWN_STREAM selects the context's own (non-blocking) stream, the initial one. */
+   OSC_OWN_STREAM selects the context's own (non-blocking) stream, the initial one.  Work
+   issued on the new stream waits (on the device) for all work issued on the previous one. */
 #define OSC_OWN_STREAM ((void *)-1)
 OSC_API int osc_ctx_set_stream(osc_ctx *ctx, void *cuda_stream);
 OSC_API int osc_ctx_set_option(osc_ctx *ctx, int option, int64_t value);

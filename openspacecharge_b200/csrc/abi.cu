@@ -49,8 +49,7 @@ int osc_ctx_destroy(osc_ctx *ctx) {
     for (auto &kv : ctx->ws) cudaFree(kv.second.p);
     for (auto &kv : ctx->tw32) cudaFree(kv.second.p);
     for (auto &kv : ctx->tw64) cudaFree(kv.second.p);
-    for (auto &g : ctx->gcache)
-        for (int i = 0; i < g.nspec; ++i) cudaFree(g.buf[i].p);
+    gcache_free_all(ctx);
     for (int t = 0; t < 4; ++t) cudaFree(ctx->pipe.g[t].p);
     cudaFree(ctx->pipe.comb.p);
     for (auto &r : ctx->prof_pending) {
@@ -64,6 +63,7 @@ int osc_ctx_destroy(osc_ctx *ctx) {
     if (ctx->h_fault) cudaFreeHost(ctx->h_fault);
     for (auto s : ctx->aux) cudaStreamDestroy(s);
     for (auto e : ctx->aux_ev) cudaEventDestroy(e);
+    if (ctx->switch_ev) cudaEventDestroy(ctx->switch_ev);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return OSC_OK;
@@ -73,7 +73,22 @@ const char *osc_last_error(const osc_ctx *ctx) { return ctx ? ctx->err.c_str() :
 
 int osc_ctx_set_stream(osc_ctx *ctx, void *s) {
     if (!ctx) return OSC_E_INVALID;
-    ctx->stream = s == OSC_OWN_STREAM ? ctx->own_stream : (cudaStream_t)s;
+    cudaStream_t ns = s == OSC_OWN_STREAM ? ctx->own_stream : (cudaStream_t)s;
+    if (ns != ctx->stream) {
+        // work on the new stream starts after everything issued on the old one: the context's
+        // workspaces and Green buffers are reused without further synchronisation
+        if (!ctx->switch_ev && cudaEventCreateWithFlags(&ctx->switch_ev, cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            ctx->switch_ev = nullptr;
+            return set_err(ctx, OSC_E_CUDA, "set_stream: event creation failed");
+        }
+        if (cudaEventRecord(ctx->switch_ev, ctx->stream) != cudaSuccess ||
+            cudaStreamWaitEvent(ns, ctx->switch_ev, 0) != cudaSuccess) {
+            cudaGetLastError();
+            return set_err(ctx, OSC_E_CUDA, "set_stream: ordering the new stream after the old one failed");
+        }
+    }
+    ctx->stream = ns;
     return OSC_OK;
 }
 
@@ -116,9 +131,7 @@ int osc_ctx_synchronize(osc_ctx *ctx) {
 int osc_clear_green_cache(osc_ctx *ctx) {
     if (!ctx) return OSC_E_INVALID;
     TRY(sync(ctx));
-    for (auto &g : ctx->gcache)
-        for (int i = 0; i < g.nspec; ++i) cudaFree(g.buf[i].p);
-    ctx->gcache.clear();
+    gcache_free_all(ctx);
     return OSC_OK;
 }
 

@@ -199,6 +199,7 @@ int prof_flush(osc_ctx *c) {
 }
 
 GreenSet *gcache_find(osc_ctx *c, const std::string &key) {
+    if (c->gcache_budget == 0) return nullptr;  // cache disabled: rebuild on every solve
     for (auto it = c->gcache.begin(); it != c->gcache.end(); ++it) {
         if (it->key == key) {
             it->stamp = ++c->stamp;
@@ -208,22 +209,80 @@ GreenSet *gcache_find(osc_ctx *c, const std::string &key) {
     return nullptr;
 }
 
-GreenSet *gcache_insert(osc_ctx *c, GreenSet &&g) {
-    // evict least recently used sets until the new one fits the budget
-    size_t total = g.bytes;
-    for (auto &s : c->gcache) total += s.bytes;
-    while (total > c->gcache_budget && !c->gcache.empty()) {
-        auto victim = c->gcache.begin();
-        for (auto it = c->gcache.begin(); it != c->gcache.end(); ++it)
-            if (it->stamp < victim->stamp) victim = it;
-        cudaStreamSynchronize(c->stream);
-        for (int i = 0; i < victim->nspec; ++i) cudaFree(victim->buf[i].p);
-        total -= victim->bytes;
-        c->gcache.erase(victim);
+static size_t gcache_bytes(const osc_ctx *c) {
+    size_t t = 0;
+    for (auto &s : c->gcache) t += s.bytes;
+    return t;
+}
+
+// Moves the least recently used set's buffers into the pool; false when the cache is empty.
+static bool gcache_evict_one(osc_ctx *c) {
+    if (c->gcache.empty()) return false;
+    auto victim = c->gcache.begin();
+    for (auto it = c->gcache.begin(); it != c->gcache.end(); ++it)
+        if (it->stamp < victim->stamp) victim = it;
+    for (int i = 0; i < victim->nspec; ++i) c->gpool.push_back(victim->buf[i]);
+    c->gcache.erase(victim);
+    return true;
+}
+
+// Frees pooled buffers beyond the most recent 16.
+static void gpool_trim(osc_ctx *c) {
+    if (c->gpool.size() <= 16) return;
+    cudaStreamSynchronize(c->stream);
+    while (c->gpool.size() > 16) {
+        cudaFree(c->gpool.front().p);
+        c->gpool.erase(c->gpool.begin());
     }
+}
+
+int green_alloc(osc_ctx *c, size_t bytes, DevBuf &out) {
+    for (;;) {
+        for (size_t i = 0; i < c->gpool.size(); ++i)
+            if (c->gpool[i].bytes == bytes) {
+                out = c->gpool[i];
+                c->gpool.erase(c->gpool.begin() + i);
+                return OSC_OK;
+            }
+        if (gcache_bytes(c) + bytes <= c->gcache_budget || !gcache_evict_one(c)) break;
+    }
+    gpool_trim(c);
+    out.p = nullptr;
+    out.bytes = 0;
+    cudaError_t e = cudaMalloc(&out.p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        out.p = nullptr;
+        return set_err(c, OSC_E_ALLOC, "Green spectrum: cudaMalloc(%zu) failed", bytes);
+    }
+    out.bytes = bytes;
+    return OSC_OK;
+}
+
+void green_release(osc_ctx *c, DevBuf &b) {
+    if (b.p) c->gpool.push_back(b);
+    b.p = nullptr;
+    b.bytes = 0;
+}
+
+GreenSet *gcache_insert(osc_ctx *c, GreenSet &&g) {
+    // evict least recently used sets (into the pool) until the new one fits the budget; with
+    // the cache disabled the new set is still kept, as the one the current solve uses
+    while (gcache_bytes(c) + g.bytes > c->gcache_budget && gcache_evict_one(c)) {
+    }
+    gpool_trim(c);
     g.stamp = ++c->stamp;
     c->gcache.push_back(std::move(g));
     return &c->gcache.back();
+}
+
+void gcache_free_all(osc_ctx *c) {
+    cudaStreamSynchronize(c->stream);
+    for (auto &g : c->gcache)
+        for (int i = 0; i < g.nspec; ++i) cudaFree(g.buf[i].p);
+    c->gcache.clear();
+    for (auto &b : c->gpool) cudaFree(b.p);
+    c->gpool.clear();
 }
 
 }  // namespace osc

@@ -59,6 +59,7 @@ struct osc_ctx {
     // grid shapes); ws_slot != 0 while work is issued on aux[ws_slot - 1]
     std::vector<cudaStream_t> aux;
     std::vector<cudaEvent_t> aux_ev;
+    cudaEvent_t switch_ev = nullptr;  // orders a newly set stream after the previous one
     int ws_slot = 0;
     std::string err;
     // options
@@ -73,6 +74,9 @@ struct osc_ctx {
     std::map<std::string, osc::DevBuf> ws;
     std::map<int, osc::DevBuf> tw32, tw64;
     std::list<osc::GreenSet> gcache;
+    // spectrum buffers of evicted sets, reused (same byte size) by the next builds; all
+    // cache users run on the context stream, so reuse is stream-ordered
+    std::vector<osc::DevBuf> gpool;
     uint64_t stamp = 0;
     // small device/pinned scratch for counters and reductions
     unsigned long long *d_small = nullptr;  // 64 words
@@ -112,8 +116,17 @@ struct Launch {
 };
 int prof_flush(osc_ctx *c);
 
-// Green-spectrum cache.
+// Green-spectrum cache.  A budget of 0 disables it: every solve rebuilds its spectra (the
+// reference's behaviour, code/open_spacecharge_mod.f90:570-573) into reused buffers.
 GreenSet *gcache_find(osc_ctx *c, const std::string &key);
 GreenSet *gcache_insert(osc_ctx *c, GreenSet &&g);
+// Device buffer of exactly `bytes` for a new spectrum: a pooled buffer of that size, else
+// least recently used sets are evicted into the pool while the cache is over budget, else
+// cudaMalloc.
+int green_alloc(osc_ctx *c, size_t bytes, DevBuf &out);
+// Returns an unused spectrum buffer to the pool.
+void green_release(osc_ctx *c, DevBuf &b);
+// Frees every cached set and pooled buffer (after synchronising the stream).
+void gcache_free_all(osc_ctx *c);
 
 }  // namespace osc

@@ -174,12 +174,7 @@ static int green_sym_spectrum(osc_ctx *c, const double *F, int nx, int ny, int n
     spec.zinner = zconv_warp_ok(2 * nz, nz, (int)sizeof(T)) ? 1 : 0;
     spec.zpitch = spec.zinner ? green_zpitch(nzh, sizeof(T)) : nzh;
     const size_t bytes = sizeof(T) * (size_t)nxh * nyh * spec.zpitch;
-    cudaError_t e = cudaMalloc(&store.p, bytes);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        return set_err(c, OSC_E_ALLOC, "Green spectrum: cudaMalloc(%zu) failed", bytes);
-    }
-    store.bytes = bytes;
+    TRY(green_alloc(c, bytes, store));
     spec.data = store.p;
     if (spec.zinner) TRY(cuda_check(c, cudaMemsetAsync(store.p, 0, bytes, c->stream), "memset spectrum"));
     int odd[3][2];
@@ -245,12 +240,7 @@ static int build_green_component(osc_ctx *c, int nx, int ny, int nz, const doubl
     spec.zpitch = spec.zinner ? green_zpitch(spec.dimz, spec.real_valued ? sizeof(T) : sizeof(cplx<T>)) : spec.dimz;
     const size_t elems = (size_t)(nx + 1) * spec.dimy * spec.zpitch;
     const size_t bytes = elems * (spec.real_valued ? sizeof(T) : sizeof(cplx<T>));
-    cudaError_t e = cudaMalloc(&store.p, bytes);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        return set_err(c, OSC_E_ALLOC, "Green spectrum: cudaMalloc(%zu) failed", bytes);
-    }
-    store.bytes = bytes;
+    TRY(green_alloc(c, bytes, store));
     const double scale = fpei_solver2() / (double)M;
     {
         Launch L_(c, "green_extract");
@@ -290,8 +280,7 @@ static int green_set(osc_ctx *c, const FreeSpaceJob &j, const int *comps, int nc
             const int k = gs.nspec;
             int rc = build_green_component<T>(c, j.nx, j.ny, j.nz, j.delta, j.gamma, off, comps[i], gs.buf[k], gs.spec[k]);
             if (rc) {
-                for (int q = 0; q <= k; ++q)
-                    if (gs.buf[q].p) cudaFree(gs.buf[q].p);
+                for (int q = 0; q <= k; ++q) green_release(c, gs.buf[q]);
                 return rc;
             }
             gs.bytes += gs.buf[k].bytes;
