@@ -57,18 +57,49 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--np", type=int, default=NPART, help="particles (default: the headline 1e7)")
+    ap.add_argument("--particles", "--np", dest="np", type=int, default=NPART,
+                    help="particles (default: the headline 1e7)")
     ap.add_argument("--grid", type=str, default="", help="nx,ny,nz (default 128,128,256)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-refit", action="store_true", help="skip the refit + Green rebuild leg")
+    ap.add_argument("--no-order", action="store_true", help="skip the cell-sorted particle-order legs")
     ap.add_argument("--workload", default="single", choices=["single", "batch", "adjoint", "pipe"],
                     help="single: the headline one-bunch step; batch: 256 bunches of mixed grids per step; "
                          "adjoint: forward + backward of sum q|E|^2 at 128^3, 4e6 particles; "
                          "pipe: rectangular-pipe step at 64x64x128, 4e6 particles")
     ap.add_argument("--bunches", type=int, default=BATCH_BUNCHES)
     return ap.parse_args()
+
+
+def plan_launch(gpus, env):
+    """How to run `--gpus N`: "run" in this process (one rank, or a rank of an external
+    launcher with WORLD_SIZE == N), "spawn" N ranks through torch.distributed.run (N > 1 and
+    no launcher), or "error" (a launcher whose WORLD_SIZE differs from N).  Never times one
+    GPU for a request of several."""
+    ws = env.get("WORLD_SIZE")
+    if gpus < 1:
+        return "error", f"--gpus must be >= 1 (got {gpus})"
+    if ws is None:
+        return ("run", "") if gpus == 1 else ("spawn", "")
+    if int(ws) != gpus:
+        return "error", f"--gpus {gpus} but WORLD_SIZE={ws}: launch one rank per GPU"
+    return "run", ""
+
+
+def spawn_ranks(gpus, argv):
+    """Re-run this command as `gpus` ranks on this node (127.0.0.1 rendezvous); returns the
+    launcher's exit status.  Rank 0 prints the JSON line."""
+    import socket
+    with socket.socket() as s_:
+        s_.bind(("127.0.0.1", 0))
+        port = s_.getsockname()[1]
+    # the launcher would read "--np" as an abbreviation of its own --nproc-per-node
+    argv = ["--particles" if a == "--np" else a for a in argv]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={gpus}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + argv
+    return subprocess.run(cmd).returncode
 
 
 def dist_init():
@@ -389,6 +420,58 @@ def run_ours(args, ws, rank, local, dist):
                "d2h_bytes_per_step": 3 * 8 * npart, "ms_per_step": te * 1e3,
                "api": "osc_space_charge_step (C ABI, pinned host buffers)"}
 
+    # particle order: the same step with the particles sorted by cell inside the call (sort
+    # cost included), and on particles already in cell order (the tracking steady state,
+    # where particles move about a cell per step and a periodic osc_sort_particles_dev keeps
+    # them sorted; E is compared after undoing the permutation)
+    orders = None
+    E_sorted_mode = E_presorted = None
+    if not args.no_order:
+        orders = {}
+        xs, ys, zs, _, perm, _ = osc.sort_particles_dev(ctx, mesh, tx, ty, tz)
+        torch.cuda.synchronize()
+        for label, mode, px_ in (("sort_in_step", osc.ORDER_SORT, (tx, ty, tz)),
+                                 ("presorted", osc.ORDER_CELL_SORTED, (xs, ys, zs))):
+            ctx.set_option(osc.OPT_PARTICLE_ORDER, mode)
+
+            def step_o(out=E, p=px_):
+                osc.space_charge_step_dev(ctx, mesh, p[0], p[1], p[2], out, total_charge=QTOT, resize_mesh=False,
+                                          precision=osc.PREC_FP32)
+            for _ in range(3):
+                step_o()
+            ctx.synchronize()
+            ko = max(3, min(args.steps, 20))
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(ko):
+                step_o()
+            e1.record(stream)
+            e1.synchronize()
+            mso = max_over_ranks(e0.elapsed_time(e1) / ko, dist)
+            prof_o = kernel_profile(ctx, osc, step_o, 3)
+            kbo = kernel_bytes(*grid, npart)
+            kbo["deposit_f32_runs"] = kbo["deposit_f32"]
+            for name, ent in prof_o.items():
+                if name in kbo:
+                    ent["alg_bytes"] = kbo[name]
+                    ent["gbs"] = kbo[name] / (ent["ms_per_call"] / ent["launches_per_call"] * 1e-3) / 1e9
+                    ent["frac_of_hbm"] = ent["gbs"] / hbm_peak
+            Eo = E.clone()
+            if mode == osc.ORDER_CELL_SORTED:
+                Eu = torch.empty_like(Eo)
+                Eu[perm] = Eo
+                Eo = Eu
+                E_presorted = Eo
+            else:
+                E_sorted_mode = Eo
+            orders[label] = {"value": ws * 1000.0 / mso, "ms_per_step": mso, "steps": ko,
+                             "speedup_vs_random_order": ms32 / mso, "kernels": prof_o,
+                             "max_rel_err_vs_random_order": float(((Eo - E32).abs().amax(0) / E32.abs().amax(0)).max())}
+        ctx.set_option(osc.OPT_PARTICLE_ORDER, osc.ORDER_ANY)
+        orders["random_order"] = {"value": value, "ms_per_step": ms32, "how": "the headline: any order, no sort"}
+        del xs, ys, zs
+
     # the reference's default path: mesh refitted to the bunch and Green spectra rebuilt on
     # every call (code/open_spacecharge_mod.f90:169-174, 570-573)
     refit = None
@@ -429,6 +512,9 @@ def run_ours(args, ws, rank, local, dist):
         # every GPU path against the FP64 oracle on the same arrays, at every particle
         err_oracle = {"definition": "per component max|E-E_oracle|/max|E_oracle| and RMS ratio, all particles",
                       "fp32": field_errors(E32.cpu().numpy(), E_orc)}
+        if E_sorted_mode is not None:
+            err_oracle["fp32_sort_in_step"] = field_errors(E_sorted_mode.cpu().numpy(), E_orc)
+            err_oracle["fp32_presorted"] = field_errors(E_presorted.cpu().numpy(), E_orc)
         if fp64 is not None:
             err_oracle["fp64_plain"] = field_errors(E64_plain.cpu().numpy(), E_orc)
             err_oracle["fp64_optimised"] = field_errors(E64_opt.cpu().numpy(), E_orc)
@@ -443,7 +529,7 @@ def run_ours(args, ws, rank, local, dist):
                        "l2": "inputs larger than L2 (240 MB of particle coordinates per step)",
                        "parallelism": f"{ws} independent replica(s)"},
             "fp64_plain": fp64, "rel_err_vs_fp64": err, "rel_err_vs_oracle": err_oracle,
-            "refit_rebuild": refit,
+            "refit_rebuild": refit, "particle_order": orders,
             "step_alg_bytes": step_bytes, "step_alg_gbs": step_gbs,
             "kernels": kernels, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches, "clocks": clk.summary(),
@@ -452,28 +538,10 @@ def run_ours(args, ws, rank, local, dist):
     ctx.close()
 
 
-def shard_bunches(grids, counts, rank, ws):
-    """Bunches of this rank: longest-processing-time assignment by estimated cost (grid nodes
-    plus 0.35 per particle, the measured ratio of field to particle time per unit), the same
-    on every rank, no communication."""
-    cost = [g[0] * g[1] * g[2] + 0.35 * n for g, n in zip(grids, counts)]
-    load = [0.0] * ws
-    owner = [0] * len(cost)
-    for b in sorted(range(len(cost)), key=lambda i: (-cost[i], i)):
-        r = min(range(ws), key=lambda k: (load[k], k))
-        owner[b] = r
-        load[r] += cost[b]
-    return [b for b in range(len(cost)) if owner[b] == rank]
-
-
 def max_over_ranks(v, dist):
     """The largest of the ranks' values (the job's time is its slowest rank's)."""
-    if dist is None:
-        return v
-    import torch
-    t = torch.tensor([float(v)], dtype=torch.float64)
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from openspacecharge_b200.multirank import max_over_ranks as mor
+    return mor(v) if dist is not None else float(v)
 
 
 def make_batch(nb, seed=SEED):
@@ -498,23 +566,23 @@ def run_batch(args, ws, rank, local, dist):
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    from openspacecharge_b200.multirank import ShardedBatch
     grids, counts, charges, x, y, z = make_batch(args.bunches)
-    offs = np.concatenate([[0], np.cumsum(counts)])
-    mine = shard_bunches(grids, counts, rank, ws)
-    sel = np.concatenate([np.arange(offs[b], offs[b + 1]) for b in mine])
-    x, y, z = x[sel], y[sel], z[sel]
-    counts_m = [counts[b] for b in mine]
-    charges_m = [charges[b] for b in mine]
+    sb = ShardedBatch([osc.Mesh3D(nlo=(1, 1, 1), nhi=g, gamma=GAMMA) for g in grids], counts, charges,
+                      rank=rank, world_size=ws)
+    mine = sb.mine
+    x, y, z = sb.select(x), sb.select(y), sb.select(z)
+    counts_m = sb.counts
+    charges_m = sb.charges
     ctx = osc.Context(local)
     stream = torch.cuda.Stream(device=dev)
     ctx.set_stream(stream.cuda_stream)
     tx, ty, tz = (torch.from_numpy(a).to(dev) for a in (x, y, z))
     E = torch.empty((len(x), 3), dtype=torch.float64, device=dev)
-    meshes = [osc.Mesh3D(nlo=(1, 1, 1), nhi=grids[b], gamma=GAMMA) for b in mine]
+    meshes = sb.meshes
 
     def step():
-        osc.batch_space_charge_step_dev(ctx, meshes, tx, ty, tz, counts_m, E, total_charges=charges_m,
-                                        resize_mesh=True, precision=osc.PREC_FP32)
+        sb.step_dev(ctx, tx, ty, tz, E, resize_mesh=True, precision=osc.PREC_FP32)
 
     def barrier():
         if dist is not None:
@@ -831,6 +899,12 @@ def run_reference(args, ws, rank):
 
 def main():
     args = parse()
+    action, msg = plan_launch(args.gpus, os.environ)
+    if action == "error":
+        print(json.dumps({"error": msg}), file=sys.stderr)
+        sys.exit(2)
+    if action == "spawn":
+        sys.exit(spawn_ranks(args.gpus, sys.argv[1:]))
     ws, rank, local, dist = dist_init()
     try:
         if args.impl == "reference":

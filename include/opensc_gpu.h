@@ -56,6 +56,25 @@ extern "C" {
 #define OSC_DEPOSIT_ATOMIC 0        /* floating-point atomics (order-dependent last bits) */
 #define OSC_DEPOSIT_DETERMINISTIC 1 /* 64-bit fixed-point atomics: rho bit-identical for any
                                        particle order and run to run */
+#define OSC_DEPOSIT_SORTED_SEGMENT 2 /* the same bits as OSC_DEPOSIT_DETERMINISTIC from particles
+                                        in cell order (sorted by the call unless
+                                        OSC_OPT_PARTICLE_ORDER says they already are): each
+                                        run of particles in one cell is summed exactly in
+                                        64-bit integers before its eight reductions */
+
+/* ---- particle order (OSC_OPT_PARTICLE_ORDER) ------------------------------------------
+ * The reference deposits and gathers in the caller's particle order.  On the GPU, particles
+ * in cell order (sorted by the cell osc_sort_particles_dev uses) share their CIC stencils'
+ * memory transactions.  Results are the same for every setting up to FP32 rounding (and
+ * bit-identical in the fixed-point deposit modes). */
+#define OSC_ORDER_ANY 0         /* any order: one set of reductions and gathers per particle */
+#define OSC_ORDER_CELL_SORTED 1 /* the caller's particles are in cell order (e.g. kept sorted
+                                   by osc_sort_particles_dev between tracking steps): deposits
+                                   sum runs of equal cells before reducing; still correct if
+                                   the order is not sorted, only slower */
+#define OSC_ORDER_SORT 2        /* the FP32 step sorts a copy of the particles by cell,
+                                   deposits and gathers in that order, and returns E (and B)
+                                   in the caller's order */
 
 /* ---- context options (osc_ctx_set_option) ---------------------------------------- */
 #define OSC_OPT_PRECISION 1      /* default precision for host entry points */
@@ -65,6 +84,7 @@ extern "C" {
                                     rebuilds the spectra on every solve, as the reference does */
 #define OSC_OPT_PROFILE 5        /* 1: time every kernel with CUDA events (osc_profile_*) */
 #define OSC_OPT_CHECK_FINITE 6   /* 1: deposit rejects non-finite coordinates (OSC_E_NAN) */
+#define OSC_OPT_PARTICLE_ORDER 8 /* OSC_ORDER_* (default OSC_ORDER_ANY) */
 #define OSC_OPT_TEST_WAIT_TIMEOUT 7 /* test only, 1: the z pass arms its Green-column barrier
                                        but issues no bulk copy and polls 64 times, so its
                                        bounded wait gives up; the call returns OSC_E_TIMEOUT
@@ -146,6 +166,20 @@ OSC_API int osc_deposit_particles_dev_noalloc(void *cuda_stream, const osc_mesh3
                                               const double *d_x, const double *d_y, const double *d_z,
                                               const double *d_q, double total_charge, double *d_rho,
                                               int64_t *n_outside, char *errbuf, size_t errlen);
+
+/* No counterpart in the reference (it deposits in the caller's order,
+ * code/open_spacecharge_mod.f90:257-283).  Counting sort of the particles by deposit cell:
+ * the key of a particle is the linear index i + nx*(j + ny*k) of its cell's lowest corner
+ * under deposit_particles' formula (the cell osc_deposit_particles uses); particles whose
+ * stencil leaves the mesh or with a non-finite coordinate go last.  Within a cell the order
+ * is unspecified.  Writes the sorted copies xs, ys, zs (and qs when q is given; q and qs
+ * are both NULL or both set; no output may alias an input) and, when perm is non-NULL,
+ * perm[s] = the original index of sorted particle s, so a tracking code can apply the same
+ * permutation to its other particle arrays.  *n_outside (optional) counts the particles
+ * sorted last.  Device pointers; np < 2^32 - 1. */
+OSC_API int osc_sort_particles_dev(osc_ctx *ctx, const osc_mesh3d *mesh, int64_t np, const double *d_x,
+                                   const double *d_y, const double *d_z, const double *d_q, double *d_xs,
+                                   double *d_ys, double *d_zs, double *d_qs, int64_t *d_perm, int64_t *n_outside);
 
 /* Replaces get_mesh_quantities (code/test_mod.f90:288-358), the test-path mesh rule:
  * delta=(max-min)/(n-3), min=bunch_min-delta; isetzmin=1 pins zmin=1e-9 for cathodes. */

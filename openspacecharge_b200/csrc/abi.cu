@@ -97,8 +97,13 @@ int osc_ctx_set_option(osc_ctx *ctx, int option, int64_t v) {
     switch (option) {
     case OSC_OPT_PRECISION: TRY(check_prec(ctx, (int)v)); ctx->precision = (int)v; return OSC_OK;
     case OSC_OPT_DEPOSIT_MODE:
-        if (v != OSC_DEPOSIT_ATOMIC && v != OSC_DEPOSIT_DETERMINISTIC) return bad(ctx, "deposit mode");
+        if (v != OSC_DEPOSIT_ATOMIC && v != OSC_DEPOSIT_DETERMINISTIC && v != OSC_DEPOSIT_SORTED_SEGMENT)
+            return bad(ctx, "deposit mode");
         ctx->deposit_mode = (int)v;
+        return OSC_OK;
+    case OSC_OPT_PARTICLE_ORDER:
+        if (v != OSC_ORDER_ANY && v != OSC_ORDER_CELL_SORTED && v != OSC_ORDER_SORT) return bad(ctx, "particle order");
+        ctx->particle_order = (int)v;
         return OSC_OK;
     case OSC_OPT_STRICT_BOUNDS: ctx->strict_bounds = v ? 1 : 0; return OSC_OK;
     case OSC_OPT_GREEN_CACHE_MB: ctx->gcache_budget = (size_t)(v < 0 ? 0 : v) << 20; return OSC_OK;
@@ -114,6 +119,7 @@ int osc_ctx_get_option(osc_ctx *ctx, int option, int64_t *v) {
     switch (option) {
     case OSC_OPT_PRECISION: *v = ctx->precision; return OSC_OK;
     case OSC_OPT_DEPOSIT_MODE: *v = ctx->deposit_mode; return OSC_OK;
+    case OSC_OPT_PARTICLE_ORDER: *v = ctx->particle_order; return OSC_OK;
     case OSC_OPT_STRICT_BOUNDS: *v = ctx->strict_bounds; return OSC_OK;
     case OSC_OPT_GREEN_CACHE_MB: *v = (int64_t)(ctx->gcache_budget >> 20); return OSC_OK;
     case OSC_OPT_PROFILE: *v = ctx->profile; return OSC_OK;
@@ -165,6 +171,31 @@ int osc_launch_count(osc_ctx *ctx, int64_t *n) {
 }
 
 // ---------------------------------------------------------------------------------------
+int osc_sort_particles_dev(osc_ctx *ctx, const osc_mesh3d *mesh, int64_t np, const double *x, const double *y,
+                           const double *z, const double *q, double *xs, double *ys, double *zs, double *qs,
+                           int64_t *perm, int64_t *n_outside) {
+    if (!ctx) return OSC_E_INVALID;
+    int n[3];
+    TRY(mesh_dims(ctx, mesh, n));
+    if (np < 0 || (np > 0 && (!x || !y || !z || !xs || !ys || !zs))) return bad(ctx, "sort arrays");
+    if ((q == nullptr) != (qs == nullptr)) return bad(ctx, "q and qs must both be given or both be NULL");
+    if (np > 0 && (xs == x || ys == y || zs == z || (q && qs == q)))
+        return bad(ctx, "sorted copies must not alias the input arrays");
+    if (!(mesh->delta[0] > 0 && mesh->delta[1] > 0 && mesh->delta[2] > 0)) return bad(ctx, "mesh delta must be positive");
+    if (n_outside) *n_outside = 0;
+    if (np == 0) return OSC_OK;
+    DepositArgs a = deposit_args(mesh, n, np, x, y, z, q, 0.0, 1);
+    TRY(cell_sort(ctx, a, xs, ys, zs, qs, perm, nullptr));
+    if (n_outside) {
+        unsigned long long h[2];
+        TRY(d2h(ctx, h, ctx->d_small + 24, sizeof(h)));
+        TRY(sync(ctx));
+        *n_outside = (int64_t)(h[0] + h[1]);
+    }
+    return OSC_OK;
+}
+
+// ---------------------------------------------------------------------------------------
 int osc_deposit_particles_dev(osc_ctx *ctx, int64_t np, const double *x, const double *y, const double *z,
                               const double *q, const double *total_charge, int resize_mesh, osc_mesh3d *mesh,
                               double *rho, int64_t *n_outside) {
@@ -182,7 +213,7 @@ int osc_deposit_particles_dev(osc_ctx *ctx, int64_t np, const double *x, const d
     const int64_t N = (int64_t)n[0] * n[1] * n[2];
     TRY(counters_reset(ctx));
     DepositArgs a = deposit_args(mesh, n, np, x, y, z, q, charge1, ctx->check_finite);
-    TRY(deposit_rho<double>(ctx, a, rho, N, 1.0));
+    TRY(deposit_rho<double>(ctx, a, rho, N, 1.0, ctx->particle_order == OSC_ORDER_CELL_SORTED));
     if (n_outside || ctx->strict_bounds || ctx->check_finite) {
         unsigned long long cnt[3];
         TRY(counters_read(ctx, cnt));
@@ -437,7 +468,7 @@ int osc_space_charge_step_dev(osc_ctx *ctx, osc_mesh3d *mesh, int64_t np, const 
         TRY(ws_get(ctx, "st_rho64", sizeof(double) * N, (void **)&rho));
         TRY(ws_get(ctx, "st_Eg", sizeof(double) * 3 * N, (void **)&Eg));
         if (B) TRY(ws_get(ctx, "st_Bg", sizeof(double) * 3 * N, (void **)&Bg));
-        TRY(deposit_rho<double>(ctx, da, rho, N, 1.0));
+        TRY(deposit_rho<double>(ctx, da, rho, N, 1.0, ctx->particle_order == OSC_ORDER_CELL_SORTED));
         j.E = Eg;
         j.B = Bg;
         TRY(freespace_plain(ctx, j, rho));
@@ -454,19 +485,29 @@ int osc_space_charge_step_dev(osc_ctx *ctx, osc_mesh3d *mesh, int64_t np, const 
     if (precision == OSC_PREC_FP32) {
         // deposit: two float4 atomics per particle into a quad grid, summed to nodes in a
         // fixed order by the x transform's loads; field: E written as an x-pair grid;
-        // interpolation: 4 sectors/particle
+        // interpolation: 4 sectors/particle.  Particles in cell order (the caller's, or
+        // sorted here) deposit per run of equal cells and gather from shared sectors.
+        const int order = ctx->particle_order;
+        uint32_t *inv = nullptr;
+        if (order == OSC_ORDER_SORT) {
+            TRY(cell_sort_ws(ctx, da, "st_s", &inv));
+            ia.x = da.x;
+            ia.y = da.y;
+            ia.z = da.z;
+        }
         float *rho = nullptr, *quad;
         void *E8;
         TRY(ws_get(ctx, "st_E8", sizeof(float4) * 2 * N, &E8));
-        if (ctx->deposit_mode == OSC_DEPOSIT_DETERMINISTIC) {
+        if (ctx->deposit_mode != OSC_DEPOSIT_ATOMIC) {
             TRY(ws_get(ctx, "st_rho32", sizeof(float) * N, (void **)&rho));
-            TRY(deposit_rho<float>(ctx, da, rho, N, 1.0));
+            TRY(deposit_rho<float>(ctx, da, rho, N, 1.0, order != OSC_ORDER_ANY));
         } else {
             TRY(ws_get(ctx, "st_quad", sizeof(float) * 4 * N, (void **)&quad));
             CK(cudaMemsetAsync(quad, 0, sizeof(float) * 4 * N, ctx->stream), "memset quad");
             {
-                Launch L_(ctx, "deposit_f32");
-                if (launch_deposit_quad(da, quad, ctx->d_small, ctx->stream))
+                Launch L_(ctx, order == OSC_ORDER_ANY ? "deposit_f32" : "deposit_f32_runs");
+                if ((order == OSC_ORDER_ANY ? launch_deposit_quad(da, quad, ctx->d_small, ctx->stream)
+                                            : launch_deposit_quad_runs(da, quad, ctx->d_small, ctx->stream)))
                     return set_err(ctx, OSC_E_CUDA, "deposit");
             }
             j.quad = reinterpret_cast<const float4 *>(quad);
@@ -480,14 +521,27 @@ int osc_space_charge_step_dev(osc_ctx *ctx, osc_mesh3d *mesh, int64_t np, const 
             j.B = Bg;
         }
         TRY(freespace_opt<float, float>(ctx, j, rho));
+        // with the particles sorted here, E and B are gathered in sorted order and then
+        // permuted back to the caller's order
+        double *Eo = E, *Bo = B;
+        if (inv) {
+            TRY(ws_get(ctx, "st_sE", sizeof(double) * 3 * (size_t)np, (void **)&Eo));
+            if (B) TRY(ws_get(ctx, "st_sB", sizeof(double) * 3 * (size_t)np, (void **)&Bo));
+        }
         {
             Launch L_(ctx, "interp_f32");
-            if (launch_interp_pairs(ia, reinterpret_cast<const float4 *>(E8), E, ctx->d_small + 2, ctx->stream))
+            if (launch_interp_pairs(ia, reinterpret_cast<const float4 *>(E8), Eo, ctx->d_small + 2, ctx->stream))
                 return set_err(ctx, OSC_E_CUDA, "interp");
         }
         if (B) {
             Launch L_(ctx, "interp_f64");
-            if (launch_interp_planes(ia, j.B, B, ctx->d_small + 3, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "interp");
+            if (launch_interp_planes(ia, j.B, Bo, ctx->d_small + 3, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "interp");
+        }
+        if (inv) {
+            Launch L_(ctx, "unpermute", B ? 2 : 1);
+            if (launch_unpermute_rows3(np, inv, Eo, E, ctx->stream) ||
+                (B && launch_unpermute_rows3(np, inv, Bo, B, ctx->stream)))
+                return set_err(ctx, OSC_E_CUDA, "unpermute");
         }
         return OSC_OK;
     }
@@ -496,7 +550,7 @@ int osc_space_charge_step_dev(osc_ctx *ctx, osc_mesh3d *mesh, int64_t np, const 
     void *E4;
     TRY(ws_get(ctx, "st_rho64", sizeof(double) * N, (void **)&rho));
     TRY(ws_get(ctx, "st_E4d", sizeof(double4) * N, &E4));
-    TRY(deposit_rho<double>(ctx, da, rho, N, 1.0));
+    TRY(deposit_rho<double>(ctx, da, rho, N, 1.0, ctx->particle_order == OSC_ORDER_CELL_SORTED));
     j.E4 = E4;
     if (B) {
         double *Bg;

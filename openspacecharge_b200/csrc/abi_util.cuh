@@ -4,6 +4,7 @@
 #include <cstring>
 
 #include "../../include/opensc_gpu.h"
+#include "cell_sort.cuh"
 #include "solver.cuh"
 
 #define TRY(...)                 \
@@ -148,13 +149,62 @@ inline DepositArgs deposit_args(const osc_mesh3d *m, const int n[3], int64_t np,
     return a;
 }
 
+// Counting sort of a's particles by deposit cell (cell_sort.cuh) into xs, ys, zs, qs (qs
+// when a.q is set); perm64[pos] = original index and inv[m] = sorted position, each when
+// non-null.  Five kernels: keys, three scan passes, scatter.
+inline int cell_sort(osc_ctx *ctx, const DepositArgs &a, double *xs, double *ys, double *zs, double *qs,
+                     int64_t *perm64, uint32_t *inv) {
+    if (a.np >= (int64_t)0xffffffff) return set_err(ctx, OSC_E_UNSUPPORTED, "cell sort: at most 2^32 - 2 particles");
+    if (a.mode != 0 || a.lost) return set_err(ctx, OSC_E_INVALID, "cell sort: deposit_particles cells only");
+    const int64_t N = (int64_t)a.nx * a.ny * a.nz;
+    uint32_t *keys, *ranks, *counts, *parts;
+    TRY(ws_get(ctx, "cs_keys", sizeof(uint32_t) * (size_t)a.np, (void **)&keys));
+    TRY(ws_get(ctx, "cs_ranks", sizeof(uint32_t) * (size_t)a.np, (void **)&ranks));
+    TRY(ws_get(ctx, "cs_counts", sizeof(uint32_t) * (size_t)(N + 2), (void **)&counts));
+    TRY(ws_get(ctx, "cs_parts", sizeof(uint32_t) * (size_t)cell_scan_partials(N + 2), (void **)&parts));
+    CK(cudaMemsetAsync(counts, 0, sizeof(uint32_t) * (size_t)(N + 2), ctx->stream), "memset cell counts");
+    // the sort's own outside/non-finite counts go to scratch words 24-25 (the deposit counts)
+    CK(cudaMemsetAsync(ctx->d_small + 24, 0, 2 * sizeof(unsigned long long), ctx->stream), "memset sort counters");
+    Launch L_(ctx, "cell_sort", 5);
+    if (launch_cell_keys(a, keys, ranks, counts, ctx->d_small + 24, ctx->stream) ||
+        launch_cell_scan(counts, N + 2, parts, ctx->stream) ||
+        launch_cell_scatter(a.np, keys, ranks, counts, a.x, a.y, a.z, a.q, xs, ys, zs, qs, perm64, inv, ctx->stream))
+        return set_err(ctx, OSC_E_CUDA, "cell sort");
+    return OSC_OK;
+}
+
+// a's particles sorted by cell into the named workspaces "<prefix>x" ...; a then points at
+// the copies.  inv (nullable) receives the original-to-sorted map.
+inline int cell_sort_ws(osc_ctx *ctx, DepositArgs &a, const char *prefix, uint32_t **inv) {
+    double *xs, *ys, *zs, *qs = nullptr;
+    const std::string p(prefix);
+    const size_t b = sizeof(double) * (size_t)a.np;
+    TRY(ws_get(ctx, (p + "x").c_str(), b, (void **)&xs));
+    TRY(ws_get(ctx, (p + "y").c_str(), b, (void **)&ys));
+    TRY(ws_get(ctx, (p + "z").c_str(), b, (void **)&zs));
+    if (a.q) TRY(ws_get(ctx, (p + "q").c_str(), b, (void **)&qs));
+    uint32_t *iv = nullptr;
+    if (inv) TRY(ws_get(ctx, (p + "inv").c_str(), sizeof(uint32_t) * (size_t)a.np, (void **)&iv));
+    TRY(cell_sort(ctx, a, xs, ys, zs, qs, nullptr, iv));
+    a.x = xs;
+    a.y = ys;
+    a.z = zs;
+    a.q = qs;
+    if (inv) *inv = iv;
+    return OSC_OK;
+}
+
 // Deposition of a.np particles into rho (zeroed here).  OSC_DEPOSIT_ATOMIC uses
 // floating-point atomics of the type of rho; OSC_DEPOSIT_DETERMINISTIC accumulates 64-bit
-// fixed-point integers and converts once, so rho is bit-identical for any particle order.
-// The fixed-point unit is a power of two chosen from np * max|q| (order-independent), so
-// that no node sum can exceed 2^62 units.  rho = mult * sum.
-template <typename TR> inline int deposit_rho(osc_ctx *ctx, DepositArgs a, TR *rho, int64_t N, double mult) {
-    if (ctx->deposit_mode != OSC_DEPOSIT_DETERMINISTIC) {
+// fixed-point integers and converts once, so rho is bit-identical for any particle order;
+// OSC_DEPOSIT_SORTED_SEGMENT gives the same bits from particles in cell order (sorted here
+// unless cell_ordered says the caller's order already is), each run of equal cells summed
+// exactly in registers before its reductions.  The fixed-point unit is a power of two
+// chosen from np * max|q| (order-independent), so that no node sum can exceed 2^62 units.
+// rho = mult * sum.
+template <typename TR>
+inline int deposit_rho(osc_ctx *ctx, DepositArgs a, TR *rho, int64_t N, double mult, bool cell_ordered = false) {
+    if (ctx->deposit_mode == OSC_DEPOSIT_ATOMIC) {
         CK(cudaMemsetAsync(rho, 0, sizeof(TR) * N, ctx->stream), "memset rho");
         {
             Launch L_(ctx, sizeof(TR) == 8 ? "deposit_f64" : "deposit_f32");
@@ -194,7 +244,11 @@ template <typename TR> inline int deposit_rho(osc_ctx *ctx, DepositArgs a, TR *r
     unsigned long long *acc;
     TRY(ws_get(ctx, "rho_fixed", sizeof(unsigned long long) * N, (void **)&acc));
     CK(cudaMemsetAsync(acc, 0, sizeof(unsigned long long) * N, ctx->stream), "memset fixed");
-    {
+    if (ctx->deposit_mode == OSC_DEPOSIT_SORTED_SEGMENT && a.mode == 0 && !a.lost) {
+        if (!cell_ordered) TRY(cell_sort_ws(ctx, a, "dsort_", nullptr));
+        Launch L_(ctx, "deposit_fixed_runs");
+        if (launch_deposit_fixed_runs(a, acc, ctx->d_small, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "deposit");
+    } else {
         Launch L_(ctx, "deposit_fixed");
         if (launch_deposit<unsigned long long>(a, acc, ctx->d_small, ctx->stream))
             return set_err(ctx, OSC_E_CUDA, "deposit");

@@ -31,7 +31,7 @@ int osc_space_charge_step_vjp_dev(osc_ctx *ctx, const osc_mesh3d *mesh, int64_t 
     const double charge1 = q ? 0.0 : total_charge / (double)np;
     DepositArgs da = deposit_args(mesh, n, np, x, y, z, q, charge1, 0);
     InterpArgs ia = interp_args(mesh, n, np, x, y, z);
-    if (precision == OSC_PREC_FP32 && ctx->deposit_mode != OSC_DEPOSIT_DETERMINISTIC) {
+    if (precision == OSC_PREC_FP32 && ctx->deposit_mode == OSC_DEPOSIT_ATOMIC) {
         // FP32: quad-grid deposits (the x transform sums the nodes as it loads them), E and
         // lambda in one x-pair grid, one gather of four 256-bit loads per particle
         float *quad, *quad3, *e8;

@@ -65,6 +65,7 @@ struct osc_ctx {
     // options
     int precision = 0;
     int deposit_mode = 0;
+    int particle_order = 0;  // OSC_ORDER_*
     int strict_bounds = 0;
     int profile = 0;
     int check_finite = 0;

@@ -56,15 +56,15 @@ __global__ void __launch_bounds__(256) k_deposit(DepositArgs a, TA *__restrict__
         int i = 0, j = 0, k = 0;
         if (!skip) {
             if (a.mode == 0) {
-                fx = floor(__dmul_rn(xm - a.xmin, a.dxi) + 1);
-                fy = floor(__dmul_rn(ym - a.ymin, a.dyi) + 1);
-                fz = floor(__dmul_rn(zm - a.zmin, a.dzi) + 1);
-                ab = ((a.xmin - xm) + fx * a.dx) * a.dxi;
-                de = ((a.ymin - ym) + fy * a.dy) * a.dyi;
-                gh = ((a.zmin - zm) + fz * a.dz) * a.dzi;
-                // array offsets; the 2x2x2 stencil must lie inside the array
-                outside = !(fx >= a.nlo[0] && fx + 1 <= a.nhi[0] && fy >= a.nlo[1] && fy + 1 <= a.nhi[1] &&
-                            fz >= a.nlo[2] && fz + 1 <= a.nhi[2]);
+                // the 2x2x2 stencil must lie inside the array
+                CicCell cc = {0, 0, 0, 0.0, 0.0, 0.0};
+                outside = cic_cell_mode0(a, xm, ym, zm, cc) != 0;
+                ab = cc.ab;
+                de = cc.de;
+                gh = cc.gh;
+                fx = cc.i + a.nlo[0];
+                fy = cc.j + a.nlo[1];
+                fz = cc.k + a.nlo[2];
             } else {
                 fx = floor(__dmul_rn(xm - a.xmin, a.dxi) + a.nlogbl[0]);
                 fy = floor(__dmul_rn(ym - a.ymin, a.dyi) + a.nlogbl[1]);
@@ -134,19 +134,13 @@ template int launch_fixed_to_real<double>(const unsigned long long *, double *, 
 // One particle of the quad deposit: 0 deposited, 1 outside the mesh, 2 non-finite.
 __device__ __forceinline__ int quad_one(const DepositArgs &a, float4 *__restrict__ quad, int64_t plane, double xm,
                                         double ym, double zm, double c) {
-    if (a.check_finite && !(isfinite(xm) && isfinite(ym) && isfinite(zm))) return 2;
-    const double fx = floor(__dmul_rn(xm - a.xmin, a.dxi) + 1);
-    const double fy = floor(__dmul_rn(ym - a.ymin, a.dyi) + 1);
-    const double fz = floor(__dmul_rn(zm - a.zmin, a.dzi) + 1);
-    if (!(fx >= a.nlo[0] && fx + 1 <= a.nhi[0] && fy >= a.nlo[1] && fy + 1 <= a.nhi[1] && fz >= a.nlo[2] &&
-          fz + 1 <= a.nhi[2]))
-        return 1;
-    const double ab = ((a.xmin - xm) + fx * a.dx) * a.dxi;
-    const double de = ((a.ymin - ym) + fy * a.dy) * a.dyi;
-    const double gh = ((a.zmin - zm) + fz * a.dz) * a.dzi;
+    CicCell cc = {0, 0, 0, 0.0, 0.0, 0.0};
+    const int st = cic_cell_mode0(a, xm, ym, zm, cc);
+    if (st) return st;
+    const double ab = cc.ab, de = cc.de, gh = cc.gh;
     const double omab = 1. - ab, omde = 1. - de, omgh = 1. - gh;
     const double lo = gh * c, hi = omgh * c;
-    const int i = (int)fx - a.nlo[0], j = (int)fy - a.nlo[1], k = (int)fz - a.nlo[2];
+    const int i = cc.i, j = cc.j, k = cc.k;
     float4 *q0 = quad + ((int64_t)i + (int64_t)a.nx * j + plane * k);
     red_add(q0, make_float4((float)(ab * de * lo), (float)(omab * de * lo), (float)(ab * omde * lo),
                               (float)(omab * omde * lo)));

@@ -23,6 +23,34 @@ struct DepositArgs {
     int check_finite;
     double fx_scale;  // fixed-point accumulation: units per unit charge
 };
+// Cell and low-node weights of deposit_particles (mode 0; code/open_spacecharge_mod.f90:
+// 259-269): ip = floor((x-xmin)*dxi + 1) with the product rounded before the add, and
+// ab = ((xmin-x) + ip*dx)*dxi with every product and sum rounded separately (no fused
+// multiply-add), as the reference and the oracle evaluate them.  Returns 0 with the cell's
+// array indices (i, j, k) and weights when the 2x2x2 stencil lies inside the array, 1 when
+// it leaves it, 2 for a non-finite coordinate (only when a.check_finite is set; otherwise
+// such a particle lands outside).
+struct CicCell {
+    int i, j, k;
+    double ab, de, gh;
+};
+__device__ __forceinline__ int cic_cell_mode0(const DepositArgs &a, double xm, double ym, double zm, CicCell &c) {
+    if (a.check_finite && !(isfinite(xm) && isfinite(ym) && isfinite(zm))) return 2;
+    const double fx = floor(__dadd_rn(__dmul_rn(xm - a.xmin, a.dxi), 1.0));
+    const double fy = floor(__dadd_rn(__dmul_rn(ym - a.ymin, a.dyi), 1.0));
+    const double fz = floor(__dadd_rn(__dmul_rn(zm - a.zmin, a.dzi), 1.0));
+    if (!(fx >= a.nlo[0] && fx + 1 <= a.nhi[0] && fy >= a.nlo[1] && fy + 1 <= a.nhi[1] && fz >= a.nlo[2] &&
+          fz + 1 <= a.nhi[2]))
+        return 1;
+    c.ab = __dmul_rn(__dadd_rn(a.xmin - xm, __dmul_rn(fx, a.dx)), a.dxi);
+    c.de = __dmul_rn(__dadd_rn(a.ymin - ym, __dmul_rn(fy, a.dy)), a.dyi);
+    c.gh = __dmul_rn(__dadd_rn(a.zmin - zm, __dmul_rn(fz, a.dz)), a.dzi);
+    c.i = (int)fx - a.nlo[0];
+    c.j = (int)fy - a.nlo[1];
+    c.k = (int)fz - a.nlo[2];
+    return 0;
+}
+
 // counters[0] += outside particles, counters[1] += non-finite particles.  TA = float or
 // double: floating-point atomics; TA = unsigned long long: each contribution rounded to
 // a 64-bit fixed-point integer (value * fx_scale), so the sum is exact and independent of

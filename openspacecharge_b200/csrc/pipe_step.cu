@@ -36,7 +36,7 @@ int osc_space_charge_step_rectpipe_dev(osc_ctx *ctx, const osc_mesh3d *mesh, int
     TRY(counters_reset(ctx));
     DepositArgs da = deposit_args(&m, n, np, x, y, z, q, charge1, ctx->check_finite);
     InterpArgs ia = interp_args(&m, n, np, x, y, z);
-    const bool fp32 = precision == OSC_PREC_FP32 && ctx->deposit_mode != OSC_DEPOSIT_DETERMINISTIC;
+    const bool fp32 = precision == OSC_PREC_FP32 && ctx->deposit_mode == OSC_DEPOSIT_ATOMIC;
     if (fp32 && m.npad[0] == 1 && m.npad[1] == 1 && m.npad[2] == 1) {
         // the x transform reads the quad grid; E goes straight from phi to the x-pair grid
         // (and to FP64 planes only when B is wanted)

@@ -24,6 +24,7 @@ __all__ = [
     "space_charge_cathodeimages", "osc_rectpipe_green", "space_charge_rectpipe",
     "osc_write_rectpipe_grn", "osc_read_rectpipe_grn", "interpolate_field",
     "get_mesh_quantities", "depose_rho_scalar", "space_charge_step", "space_charge_step_dev",
+    "sort_particles_dev", "cell_keys",
 ]
 
 
@@ -400,3 +401,37 @@ def space_charge_step_rectpipe_dev(ctx, mesh3d: Mesh3D, x, y, z, E, apipe, bpipe
     tc = None if total_charge is None else ctypes.byref(ctypes.c_double(float(total_charge)))
     ctx.call("osc_space_charge_step_rectpipe_dev", ctypes.byref(m), ctypes.c_int64(x.numel()), _tp(x), _tp(y),
              _tp(z), _tp(qa), tc, ctypes.c_double(apipe), ctypes.c_double(bpipe), int(precision), _tp(E), _tp(B))
+
+
+def cell_keys(mesh3d: Mesh3D, x, y, z) -> np.ndarray:
+    """Host restatement of the cell key osc_sort_particles_dev sorts by: the linear index
+    i + nx*(j + ny*k) of the lowest corner of the particle's deposit cell
+    (deposit_particles' ip = floor((x-xmin)/dx + 1), code/open_spacecharge_mod.f90:259-261),
+    or nx*ny*nz when the particle's 2x2x2 stencil leaves the mesh or a coordinate is not
+    finite.  Used to check and to prepare cell order."""
+    n = mesh3d.shape
+    idx = []
+    inside = np.ones(len(x), dtype=bool)
+    for d, v in enumerate((x, y, z)):
+        with np.errstate(invalid="ignore"):
+            f = np.floor((np.asarray(v, dtype=np.float64) - mesh3d.min[d]) * (1.0 / mesh3d.delta[d]) + 1.0)
+            inside &= (f >= mesh3d.nlo[d]) & (f + 1 <= mesh3d.nhi[d])
+        idx.append(np.where(inside, f, mesh3d.nlo[d]).astype(np.int64) - mesh3d.nlo[d])
+    key = idx[0] + n[0] * (idx[1] + n[1] * idx[2])
+    return np.where(inside, key, n[0] * n[1] * n[2])
+
+
+def sort_particles_dev(ctx, mesh3d: Mesh3D, x, y, z, q=None, want_perm=True):
+    """osc_sort_particles_dev on torch CUDA float64 tensors: returns (xs, ys, zs, qs|None,
+    perm|None, n_outside), the particles in cell order and perm[s] = original index."""
+    import torch
+    ctx = _ctx(ctx)
+    xs, ys, zs = torch.empty_like(x), torch.empty_like(y), torch.empty_like(z)
+    qs = torch.empty_like(q) if q is not None else None
+    perm = torch.empty(x.numel(), dtype=torch.int64, device=x.device) if want_perm else None
+    nout = ctypes.c_int64(0)
+    m = mesh3d.to_c()
+    ctx.call("osc_sort_particles_dev", ctypes.byref(m), ctypes.c_int64(x.numel()), _tp(x), _tp(y), _tp(z), _tp(q),
+             _tp(xs), _tp(ys), _tp(zs), _tp(qs), _tp(perm), ctypes.byref(nout))
+    return xs, ys, zs, qs, perm, int(nout.value)
+

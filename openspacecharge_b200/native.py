@@ -33,6 +33,11 @@ PREC_FP64_PLAIN = 2
 
 DEPOSIT_ATOMIC = 0
 DEPOSIT_DETERMINISTIC = 1
+DEPOSIT_SORTED_SEGMENT = 2
+
+ORDER_ANY = 0
+ORDER_CELL_SORTED = 1
+ORDER_SORT = 2
 
 OPT_PRECISION = 1
 OPT_DEPOSIT_MODE = 2
@@ -41,6 +46,7 @@ OPT_GREEN_CACHE_MB = 4
 OPT_PROFILE = 5
 OPT_CHECK_FINITE = 6
 OPT_TEST_WAIT_TIMEOUT = 7
+OPT_PARTICLE_ORDER = 8
 
 _ERRNAMES = {v: k for k, v in globals().items() if k.startswith("OSC_E_") or k == "OSC_OK"}
 
@@ -106,6 +112,7 @@ SIGNATURES = {
     "osc_launch_count": [_P, _PI64],
     "osc_deposit_particles": [_P, _I64, _P, _P, _P, _P, _P, _I, _PM, _P, _PI64],
     "osc_deposit_particles_dev": [_P, _I64, _P, _P, _P, _P, _P, _I, _PM, _P, _PI64],
+    "osc_sort_particles_dev": [_P, _PM, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _PI64],
     "osc_deposit_particles_dev_noalloc": [_P, _PM, _I64, _P, _P, _P, _P, _D, _P, _PI64, ctypes.c_char_p,
                                           ctypes.c_size_t],
     "osc_get_mesh_quantities": [_P, _I64, _P, _P, _P, _P, _P, _I, _P, _P],

@@ -57,3 +57,36 @@ def test_kernel_bytes_scale_with_particles(np_):
     assert kb1["deposit_f32"] - kb0["deposit_f32"] == 24 * np_
     assert kb1["interp_f32"] - kb0["interp_f32"] == 48 * np_
     assert kb1["fft_z_conv"] == kb0["fft_z_conv"]
+
+
+def test_plan_launch_never_times_one_gpu_for_several():
+    assert bench.plan_launch(1, {}) == ("run", "")
+    assert bench.plan_launch(2, {})[0] == "spawn"
+    assert bench.plan_launch(4, {"WORLD_SIZE": "4"})[0] == "run"
+    assert bench.plan_launch(2, {"WORLD_SIZE": "1"})[0] == "error"
+    assert bench.plan_launch(8, {"WORLD_SIZE": "2"})[0] == "error"
+    assert bench.plan_launch(0, {})[0] == "error"
+
+
+def test_gpus_2_without_a_launcher_spawns_two_ranks():
+    """`bench.py --gpus 2` started bare runs two ranks itself (gloo on 127.0.0.1); the
+    reference arm needs no GPU, so the whole launch path runs here on a tiny workload."""
+    import json
+    import subprocess
+    env = {k: v for k, v in os.environ.items() if k not in ("WORLD_SIZE", "RANK", "LOCAL_RANK", "MASTER_ADDR",
+                                                            "MASTER_PORT")}
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2",
+                        "--np", "20000", "--grid", "16,16,16", "--steps", "1", "--warmup", "1"],
+                       capture_output=True, text=True, timeout=600, env=env)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [json.loads(l) for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1, r.stdout
+    assert lines[0]["impl"] == "reference" and lines[0]["n_gpus"] == 2
+
+
+def test_gpus_mismatching_the_launcher_is_an_error():
+    import subprocess
+    env = dict(os.environ, WORLD_SIZE="1")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2"],
+                       capture_output=True, text=True, timeout=300, env=env)
+    assert r.returncode == 2 and "WORLD_SIZE" in r.stderr

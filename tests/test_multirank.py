@@ -1,8 +1,9 @@
 """The multi-rank path of the batched workload on the CPU: two gloo ranks (127.0.0.1) shard a
-batch of bunches with bench.shard_bunches (no communication), solve their bunches with the
-oracle's deposit + space_charge_3d + interpolate_field, and all-gather the fields; the
-result must equal a single-rank solve of every bunch, the shards must partition the batch,
-and the job time is the maximum over ranks."""
+batch of bunches with the package's ShardedBatch (assignment computed identically on every
+rank, no communication), solve their bunches with the oracle's deposit + space_charge_3d +
+interpolate_field, and gather the fields to rank 0 with ShardedBatch.gather; the result
+must equal a single-rank solve of every bunch in the batch's particle order, the shards must
+partition the batch, and the job time is the maximum over ranks."""
 import os
 import socket
 
@@ -46,21 +47,27 @@ def worker(rank, ws, port, out):
     import datetime
     dist.init_process_group("gloo", rank=rank, world_size=ws, timeout=datetime.timedelta(seconds=60))
     try:
-        import bench
         from oracle import oracle
+        from openspacecharge_b200 import Mesh3D
+        from openspacecharge_b200.multirank import ShardedBatch, max_over_ranks
         oracle.set_threads(1)
         grids, counts, parts = make_bunches()
-        mine = bench.shard_bunches(grids, counts, rank, ws)
-        local = {b: solve(oracle, grids[b], parts[b]) for b in mine}
-        gathered = [None] * ws
-        dist.all_gather_object(gathered, local)
-        t = bench.max_over_ranks(1.0 + rank, dist)
+        meshes = [Mesh3D(nlo=(1, 1, 1), nhi=g, gamma=GAMMA) for g in grids]
+        sb = ShardedBatch(meshes, counts, rank=rank, world_size=ws)
+        full = [np.concatenate([p[d] for p in parts]) for d in range(3)]
+        xl, yl, zl = (sb.select(a) for a in full)
+        rows, o = [], 0
+        for b in sb.mine:  # this rank's bunches, in the order select() concatenates them
+            sl = slice(o, o + counts[b])
+            rows.append(solve(oracle, grids[b], (xl[sl], yl[sl], zl[sl])))
+            o += counts[b]
+        E_local = torch.from_numpy(np.concatenate(rows) if rows else np.zeros((0, 3)))
+        E_full = sb.gather(E_local, dst=0)
+        t = max_over_ranks(1.0 + rank)
         if rank == 0:
-            merged = {}
-            for d in gathered:
-                merged.update(d)
-            out.put((sorted(merged), {b: merged[b] for b in merged}, t,
-                     [bench.shard_bunches(grids, counts, r, ws) for r in range(ws)]))
+            out.put((E_full.numpy(), t, sb.shards))
+        else:
+            assert E_full is None
     finally:
         dist.destroy_process_group()
 
@@ -78,27 +85,38 @@ def test_two_rank_batch_matches_single_rank(oracle):
     procs = [ctx.Process(target=worker, args=(r, 2, port, q)) for r in range(2)]
     for p in procs:
         p.start()
-    keys, fields, t, shards = q.get(timeout=300)
+    E_full, t, shards = q.get(timeout=300)
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
     grids, counts, parts = make_bunches()
-    assert keys == list(range(len(grids)))
     assert sorted(shards[0] + shards[1]) == list(range(len(grids))) and not set(shards[0]) & set(shards[1])
+    assert shards[0] and shards[1]
     assert t == 2.0  # the maximum over ranks
-    for b in range(len(grids)):
-        ref = solve(oracle, grids[b], parts[b])
-        assert np.array_equal(fields[b], ref)
+    ref = np.concatenate([solve(oracle, grids[b], parts[b]) for b in range(len(grids))])
+    assert np.array_equal(E_full, ref)
 
 
 def test_shard_balance():
-    import sys
-    sys.path.insert(0, ROOT)
-    import bench
+    from openspacecharge_b200.multirank import bunch_cost, shard_bunches
     rng = np.random.default_rng(1)
     grids = [tuple(int(rng.choice((32, 48, 64, 96))) for _ in range(3)) for _ in range(256)]
     counts = [int(np.exp(rng.uniform(np.log(1e4), np.log(1e6)))) for _ in range(256)]
-    cost = [g[0] * g[1] * g[2] + 0.35 * n for g, n in zip(grids, counts)]
+    cost = [bunch_cost(g, n) for g, n in zip(grids, counts)]
     for ws in (2, 4, 8):
-        loads = [sum(cost[b] for b in bench.shard_bunches(grids, counts, r, ws)) for r in range(ws)]
+        shards = [shard_bunches(grids, counts, r, ws) for r in range(ws)]
+        assert sorted(sum(shards, [])) == list(range(256))
+        loads = [sum(cost[b] for b in s) for s in shards]
         assert max(loads) <= 1.05 * sum(cost) / ws
+    with pytest.raises(ValueError):
+        shard_bunches(grids, counts, 2, 2)
+
+
+def test_sharded_batch_single_rank_is_the_whole_batch():
+    from openspacecharge_b200 import Mesh3D
+    from openspacecharge_b200.multirank import ShardedBatch, max_over_ranks
+    grids, counts, _ = make_bunches()
+    sb = ShardedBatch([Mesh3D(nlo=(1, 1, 1), nhi=g) for g in grids], counts, rank=0, world_size=1)
+    assert sb.mine == list(range(len(grids)))
+    assert np.array_equal(sb.particle_index(), np.arange(sum(counts)))
+    assert max_over_ranks(3.5) == 3.5  # no process group: the value itself
