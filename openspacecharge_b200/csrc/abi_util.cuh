@@ -165,11 +165,18 @@ inline int cell_sort(osc_ctx *ctx, const DepositArgs &a, double *xs, double *ys,
     CK(cudaMemsetAsync(counts, 0, sizeof(uint32_t) * (size_t)(N + 2), ctx->stream), "memset cell counts");
     // the sort's own outside/non-finite counts go to scratch words 24-25 (the deposit counts)
     CK(cudaMemsetAsync(ctx->d_small + 24, 0, 2 * sizeof(unsigned long long), ctx->stream), "memset sort counters");
-    Launch L_(ctx, "cell_sort", 5);
-    if (launch_cell_keys(a, keys, ranks, counts, ctx->d_small + 24, ctx->stream) ||
-        launch_cell_scan(counts, N + 2, parts, ctx->stream) ||
-        launch_cell_scatter(a.np, keys, ranks, counts, a.x, a.y, a.z, a.q, xs, ys, zs, qs, perm64, inv, ctx->stream))
-        return set_err(ctx, OSC_E_CUDA, "cell sort");
+    {
+        Launch L_(ctx, "cell_keys");
+        if (launch_cell_keys(a, keys, ranks, counts, ctx->d_small + 24, ctx->stream))
+            return set_err(ctx, OSC_E_CUDA, "cell keys");
+    }
+    {
+        Launch L_(ctx, "cell_scan", 3);
+        if (launch_cell_scan(counts, N + 2, parts, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "cell scan");
+    }
+    Launch L_(ctx, "cell_scatter");
+    if (launch_cell_scatter(a.np, keys, ranks, counts, a.x, a.y, a.z, a.q, xs, ys, zs, qs, perm64, inv, ctx->stream))
+        return set_err(ctx, OSC_E_CUDA, "cell scatter");
     return OSC_OK;
 }
 

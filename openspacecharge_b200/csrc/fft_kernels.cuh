@@ -151,8 +151,9 @@ struct SymArgs {
 };
 // row_load: elements of a line are contiguous in the input (load along the line);
 // k_fast_store: outputs of a line are contiguous (store along the line).
-template <typename TO>
-int launch_sym_lines(const double *in, TO *out, const SymArgs &a, const TwPair<cplx<double>> &tw, bool row_load,
+// TC: arithmetic type of the transform (double, or float from octant values rounded once).
+template <typename TC, typename TI, typename TO>
+int launch_sym_lines(const TI *in, TO *out, const SymArgs &a, const TwPair<cplx<TC>> &tw, bool row_load,
                      bool k_fast_store, cudaStream_t st);
 
 template <typename T>

@@ -14,4 +14,6 @@ template int launch_r2c_rows<float, double>(const double *, cplx<float> *, const
 template int launch_c2r_rows<float>(const cplx<float> *, const C2RArgs &, const TwPair<cplx<float>> &, cudaStream_t);
 template int launch_zconv<float>(const cplx<float> *, cplx<float> *, const ZConvArgs &, const TwPair<cplx<float>> &,
                                  int, cudaStream_t);
+template int launch_sym_lines<float, float, float>(const float *, float *, const SymArgs &,
+                                                   const TwPair<cplx<float>> &, bool, bool, cudaStream_t);
 }  // namespace osc

@@ -10,8 +10,6 @@ template int launch_c2r_rows<double>(const cplx<double> *, const C2RArgs &, cons
                                      cudaStream_t);
 template int launch_zconv<double>(const cplx<double> *, cplx<double> *, const ZConvArgs &,
                                   const TwPair<cplx<double>> &, int, cudaStream_t);
-template int launch_sym_lines<double>(const double *, double *, const SymArgs &, const TwPair<cplx<double>> &, bool,
-                                      bool, cudaStream_t);
-template int launch_sym_lines<float>(const double *, float *, const SymArgs &, const TwPair<cplx<double>> &, bool,
-                                     bool, cudaStream_t);
+template int launch_sym_lines<double, double, double>(const double *, double *, const SymArgs &,
+                                                      const TwPair<cplx<double>> &, bool, bool, cudaStream_t);
 }  // namespace osc

@@ -499,11 +499,12 @@ __global__ void __launch_bounds__(E::kLen * 3 * NLC / E::kEPT, sizeof(T) == 4 ? 
 }
 
 // Even/odd real line transforms (Green spectra): two real lines per complex line, the
-// parity extension formed in the load, the halves separated after the transform.
-template <typename TO, int NL, class E, bool LDE, bool STK>
-__global__ void __launch_bounds__(E::kMaxThreads) k_sym_lines(const double *__restrict__ in, TO *__restrict__ out,
-                                                              SymArgs a, const double2 *__restrict__ twg) {
-    typedef double2 V;
+// parity extension formed in the load, the halves separated after the transform.  TC is
+// the arithmetic type (and that of the twiddles), TI the input's, TO the output's.
+template <typename TC, typename TI, typename TO, int NL, class E, bool LDE, bool STK>
+__global__ void __launch_bounds__(E::kMaxThreads) k_sym_lines(const TI *__restrict__ in, TO *__restrict__ out,
+                                                              SymArgs a, const cplx<TC> *__restrict__ twg) {
+    typedef cplx<TC> V;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int64_t bin[2 * NL], bout[2 * NL];
     __shared__ int podd[2 * NL];
@@ -537,17 +538,17 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_sym_lines(const double *__re
         // flight), then writes each value at e and its parity image at L-e
         constexpr int nh = E::kLen / 2, NK = nh + 1, TOT = 2 * NL * NK;
         constexpr int NT = E::kLen * NL / E::kEPT, IT = (TOT + NT - 1) / NT;
-        double v[IT];
+        TC v[IT];
 #pragma unroll
         for (int it = 0; it < IT; ++it) {
             const int idx = tid + it * NT;
-            v[it] = 0.0;
+            v[it] = (TC)0;
             if (idx < TOT) {
                 int rr, e;
                 if (LDE) { rr = idx / NK; e = idx - rr * NK; }
                 else { e = idx / (2 * NL); rr = idx - e * (2 * NL); }
                 const int64_t o = bin[rr];
-                if (o >= 0 && e != nh) v[it] = in[o + (int64_t)e * a.in_es];
+                if (o >= 0 && e != nh) v[it] = (TC)in[o + (int64_t)e * a.in_es];
             }
         }
 #pragma unroll
@@ -557,9 +558,9 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_sym_lines(const double *__re
                 int rr, e;
                 if (LDE) { rr = idx / NK; e = idx - rr * NK; }
                 else { e = idx / (2 * NL); rr = idx - e * (2 * NL); }
-                reinterpret_cast<double *>(&buf[e * lstr + (rr >> 1)])[rr & 1] = v[it];
+                reinterpret_cast<TC *>(&buf[e * lstr + (rr >> 1)])[rr & 1] = v[it];
                 if (e > 0 && e < nh)
-                    reinterpret_cast<double *>(&buf[(E::kLen - e) * lstr + (rr >> 1)])[rr & 1] =
+                    reinterpret_cast<TC *>(&buf[(E::kLen - e) * lstr + (rr >> 1)])[rr & 1] =
                         podd[rr] ? -v[it] : v[it];
             }
         }
@@ -569,13 +570,13 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_sym_lines(const double *__re
             if (LDE) { rr = idx / L; e = idx - rr * L; }
             else { e = idx / (2 * NL); rr = idx - e * (2 * NL); }
             const int64_t o = bin[rr];
-            double v = 0.0;
+            TC v = (TC)0;
             if (o >= 0 && e != n) {
                 const int src = e < n ? e : L - e;
-                v = in[o + (int64_t)src * a.in_es];
+                v = (TC)in[o + (int64_t)src * a.in_es];
                 if (e > n && podd[rr]) v = -v;
             }
-            double *slot = reinterpret_cast<double *>(&buf[e * lstr + (rr >> 1)]);
+            TC *slot = reinterpret_cast<TC *>(&buf[e * lstr + (rr >> 1)]);
             slot[rr & 1] = v;
         }
     }
@@ -591,10 +592,11 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_sym_lines(const double *__re
         const V Z = buf[k * lstr + (rr >> 1)];
         const V Zm = buf[((L - k) % L) * lstr + (rr >> 1)];
         const bool odd = podd[rr];
-        double sv;
-        if ((rr & 1) == 0) sv = !odd ? 0.5 * (Z.x + Zm.x) : 0.5 * (Z.y - Zm.y);
-        else sv = !odd ? 0.5 * (Z.y + Zm.y) : 0.5 * (Zm.x - Z.x);
-        out[o + (int64_t)k * a.out_es] = (TO)(sv * a.scale);
+        TC sv;
+        const TC hf = (TC)0.5;
+        if ((rr & 1) == 0) sv = !odd ? hf * (Z.x + Zm.x) : hf * (Z.y - Zm.y);
+        else sv = !odd ? hf * (Z.y + Zm.y) : hf * (Zm.x - Z.x);
+        out[o + (int64_t)k * a.out_es] = (TO)(sv * (TC)a.scale);
     }
 }
 
@@ -866,28 +868,28 @@ int launch_zconv(const cplx<T> *in, cplx<T> *out, const ZConvArgs &a, const TwPa
     });
 }
 
-template <typename TO>
-int launch_sym_lines(const double *in, TO *out, const SymArgs &a, const TwPair<cplx<double>> &tw, bool row_load,
+template <typename TC, typename TI, typename TO>
+int launch_sym_lines(const TI *in, TO *out, const SymArgs &a, const TwPair<cplx<TC>> &tw, bool row_load,
                      bool k_fast_store, cudaStream_t st) {
     const int L = a.p.L;
     if (L != 2 * a.n) return OSC_E_INVALID;
-    return dispatch_fft_len<double>(L, [&](auto eng) -> int {
+    return dispatch_fft_len<TC>(L, [&](auto eng) -> int {
         using E = decltype(eng);
-        const double2 *twe = eng_tw<E>(tw);
+        const cplx<TC> *twe = eng_tw<E>(tw);
         // static engines: up to 16 line pairs per CTA, so the short lines of small batch
         // groups still give CTAs of several warps
         auto with_sym_nl = [&](auto &&f) -> int {
             if constexpr (E::kLen > 0)
-                return f(std::integral_constant<int, nl_static(E::kLen, 16, (int)sizeof(double2), 1, 100 * 1024,
+                return f(std::integral_constant<int, nl_static(E::kLen, 16, (int)sizeof(cplx<TC>), 1, 100 * 1024,
                                                                E::kEPT)>{});
             else
-                return with_nl<double, E>(L, 1, 8, 0, f);
+                return with_nl<TC, E>(L, 1, 8, 0, f);
         };
         return with_sym_nl([&](auto nlc) -> int {
             constexpr int NL = decltype(nlc)::value;
             const int nt = fft_threads(L, NL, E::kEPT);
             if (nt < 1 || nt > E::kMaxThreads || (L * NL) % E::kEPT) return OSC_E_FFT_SIZE;
-            const size_t sm = sizeof(double2) * ((size_t)L + (size_t)L * (NL + 1));
+            const size_t sm = sizeof(cplx<TC>) * ((size_t)L + (size_t)L * (NL + 1));
             const unsigned nblk = (unsigned)ceil_div(a.nlines, 2 * NL);
             auto go = [&](auto kern) -> int {
                 int rc = set_smem(kern, sm);
@@ -895,9 +897,10 @@ int launch_sym_lines(const double *in, TO *out, const SymArgs &a, const TwPair<c
                 kern<<<nblk, nt, sm, st>>>(in, out, a, twe);
                 return launch_ok();
             };
-            if (row_load) return k_fast_store ? go(k_sym_lines<TO, NL, E, true, true>)
-                                              : go(k_sym_lines<TO, NL, E, true, false>);
-            return k_fast_store ? go(k_sym_lines<TO, NL, E, false, true>) : go(k_sym_lines<TO, NL, E, false, false>);
+            if (row_load) return k_fast_store ? go(k_sym_lines<TC, TI, TO, NL, E, true, true>)
+                                              : go(k_sym_lines<TC, TI, TO, NL, E, true, false>);
+            return k_fast_store ? go(k_sym_lines<TC, TI, TO, NL, E, false, true>)
+                                : go(k_sym_lines<TC, TI, TO, NL, E, false, false>);
         });
     });
 }

@@ -107,7 +107,8 @@ int launch_green_center(const double *F, double2 *cg, const CenterArgs &a, cudaS
 // Octant of the centred kernel for all-symmetric geometries: h[c][b][a] = g at displacement
 // (a, b, c) >= 0, the 8-corner difference of the cell whose corners are a, a+1 (the corner
 // block starts at index n-1 of the doubled grid, so cell a uses corners a and a+1).
-__global__ void k_green_octant(const double *__restrict__ F, double *__restrict__ h, int nx, int ny, int nz) {
+template <typename TH>
+__global__ void k_green_octant(const double *__restrict__ F, TH *__restrict__ h, int nx, int ny, int nz) {
     const int cdx = nx + 1, cdy = ny + 1;
     const int n = nx * ny * nz;  // one member's octant (< 2^31 nodes)
     F += blockIdx.y * ((int64_t)cdx * cdy * (nz + 1));  // batch member
@@ -125,14 +126,17 @@ __global__ void k_green_octant(const double *__restrict__ F, double *__restrict_
         g = g + f0[sz];
         g = g + f0[sy];
         g = g + f0[1];
-        h[idx] = g;
+        h[idx] = (TH)g;
     }
 }
-int launch_green_octant(const double *F, double *h, int nx, int ny, int nz, int nbatch, cudaStream_t st) {
+template <typename TH>
+int launch_green_octant(const double *F, TH *h, int nx, int ny, int nz, int nbatch, cudaStream_t st) {
     const dim3 grid(nblocks((int64_t)nx * ny * nz, 256), (unsigned)nbatch);
-    k_green_octant<<<grid, 256, 0, st>>>(F, h, nx, ny, nz);
+    k_green_octant<TH><<<grid, 256, 0, st>>>(F, h, nx, ny, nz);
     return ok();
 }
+template int launch_green_octant<double>(const double *, double *, int, int, int, int, cudaStream_t);
+template int launch_green_octant<float>(const double *, float *, int, int, int, int, cudaStream_t);
 
 // Corner blocks of several geometries: member blockIdx.y uses args[blockIdx.y] and writes
 // F + blockIdx.y * fstride.

@@ -35,7 +35,9 @@ int launch_green_center(const double *F, double2 *cg, const CenterArgs &a, cudaS
 // All-symmetric geometries: the non-negative octant h[c][b][a] (a < nx, b < ny, c < nz) of
 // the centred kernel from corners F of extent (n+1) per axis starting at index n-1.
 // nbatch members: corner blocks (n+1)^3 apart in F, octants n^3 apart in h.
-int launch_green_octant(const double *F, double *h, int nx, int ny, int nz, int nbatch, cudaStream_t st);
+// h = the 8-corner differences of F (FP64), rounded once to TH.
+template <typename TH>
+int launch_green_octant(const double *F, TH *h, int nx, int ny, int nz, int nbatch, cudaStream_t st);
 // Corner blocks of nbatch geometries (args_dev: device array), fstride apart, npts each.
 int launch_igf_corners_batch(double *F, const CornerArgs *args_dev, int nbatch, int64_t fstride, int64_t npts,
                              cudaStream_t st);

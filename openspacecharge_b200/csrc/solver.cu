@@ -105,26 +105,29 @@ CornerArgs green_corner_args(const int n[3], const double delta[3], double gamma
 // layout (zinner: [ky][kx][kz] with columns zpitch apart, else [kz][ky][kx]) of member b at
 // out + b * out_bstride.  Equals the extraction of the FP64 doubled-grid FFT
 // (osc_get_cgrn_freespace + ccfft3d, code/open_spacecharge_mod.f90:633-705,
-// code/fft_interface_mod.f90:96-143) up to FP64 rounding.
+// code/fft_interface_mod.f90:96-143) up to rounding.  The corner primitives and their
+// 8-corner differences, whose log/atan terms cancel catastrophically at large offsets,
+// are always FP64; the line transforms run in T: FP64 for FP64 spectra, FP32 (from the
+// octant values rounded once) for the FP32 path, whose stored spectrum is FP32 anyway.
 template <typename T>
 int green_sym_lines3(osc_ctx *c, const double *F, int nb, int nx, int ny, int nz, const int odd[3][2], int zinner,
                      int zpitch, T *out, int64_t out_bstride) {
     const int nxh = nx + 1, nyh = ny + 1;
-    double *h, *hx, *hy;
-    TRY(ws_get(c, "green_h", sizeof(double) * (size_t)nb * nx * ny * nz, (void **)&h));
-    TRY(ws_get(c, "green_hx", sizeof(double) * (size_t)nb * nxh * ny * nz, (void **)&hx));
-    TRY(ws_get(c, "green_hy", sizeof(double) * (size_t)nb * nxh * nyh * nz, (void **)&hy));
+    T *h, *hx, *hy;
+    TRY(ws_get(c, "green_h", sizeof(T) * (size_t)nb * nx * ny * nz, (void **)&h));
+    TRY(ws_get(c, "green_hx", sizeof(T) * (size_t)nb * nxh * ny * nz, (void **)&hx));
+    TRY(ws_get(c, "green_hy", sizeof(T) * (size_t)nb * nxh * nyh * nz, (void **)&hy));
     {
         Launch L_(c, "green_octant");
-        TRY(kerr(c, launch_green_octant(F, h, nx, ny, nz, nb, c->stream), "green octant"));
+        TRY(kerr(c, launch_green_octant<T>(F, h, nx, ny, nz, nb, c->stream), "green octant"));
     }
     FFTPlan px, py, pz;
     if (!make_fft_plan(2 * nx, px) || !make_fft_plan(2 * ny, py) || !make_fft_plan(2 * nz, pz))
         return set_err(c, OSC_E_FFT_SIZE, "doubled grid lengths must be 2^a 3^b 5^c");
-    TwPair<cplx<double>> twx, twy, twz;
-    TRY(twiddles<double>(c, 2 * nx, &twx));
-    TRY(twiddles<double>(c, 2 * ny, &twy));
-    TRY(twiddles<double>(c, 2 * nz, &twz));
+    TwPair<cplx<T>> twx, twy, twz;
+    TRY(twiddles<T>(c, 2 * nx, &twx));
+    TRY(twiddles<T>(c, 2 * ny, &twy));
+    TRY(twiddles<T>(c, 2 * nz, &twz));
     Launch L_(c, "green_sym_lines", 3);
     SymArgs a;
     // x: rows h[c][b][0..nx) -> hx[c][b][0..nx]
@@ -133,13 +136,13 @@ int green_sym_lines3(osc_ctx *c, const double *F, int nb, int nx, int ny, int nz
     a.in_ps = (int64_t)ny * nx; a.in_qs = nx; a.in_es = 1; a.in_bs = (int64_t)nx * ny * nz;
     a.out_ps = (int64_t)ny * nxh; a.out_qs = nxh; a.out_es = 1; a.out_bs = (int64_t)nxh * ny * nz;
     a.scale = 1.0;
-    TRY(kerr(c, launch_sym_lines<double>(h, hx, a, twx, true, true, c->stream), "green x"));
+    TRY(kerr(c, launch_sym_lines<T, T, T>(h, hx, a, twx, true, true, c->stream), "green x"));
     // y: lines (c, kx) of hx -> hy[c][ky][kx]
     a.p = py; a.n = ny; a.odd_lo = odd[1][0]; a.odd_hi = odd[1][1]; a.nq = nxh;
     a.npq = (int64_t)nz * nxh; a.nlines = nb * a.npq;
     a.in_ps = (int64_t)ny * nxh; a.in_qs = 1; a.in_es = nxh; a.in_bs = (int64_t)nxh * ny * nz;
     a.out_ps = (int64_t)nyh * nxh; a.out_qs = 1; a.out_es = nxh; a.out_bs = (int64_t)nxh * nyh * nz;
-    TRY(kerr(c, launch_sym_lines<double>(hx, hy, a, twy, false, false, c->stream), "green y"));
+    TRY(kerr(c, launch_sym_lines<T, T, T>(hx, hy, a, twy, false, false, c->stream), "green y"));
     // z: lines (ky, kx) of hy -> stored spectrum, scaled by fpei/M
     a.p = pz; a.n = nz; a.odd_lo = odd[2][0]; a.odd_hi = odd[2][1]; a.nq = nxh;
     a.npq = (int64_t)nyh * nxh; a.nlines = nb * a.npq;
@@ -151,7 +154,7 @@ int green_sym_lines3(osc_ctx *c, const double *F, int nb, int nx, int ny, int nz
     }
     a.out_bs = out_bstride;
     a.scale = fpei_solver2() / (8.0 * nx * ny * nz);
-    TRY(kerr(c, launch_sym_lines<T>(hy, out, a, twz, false, zinner != 0, c->stream), "green z"));
+    TRY(kerr(c, launch_sym_lines<T, T, T>(hy, out, a, twz, false, zinner != 0, c->stream), "green z"));
     return OSC_OK;
 }
 template int green_sym_lines3<float>(osc_ctx *, const double *, int, int, int, int, const int (*)[2], int, int,

@@ -3,8 +3,10 @@
 The loss is L = sum_m q_m |E(x_m)|^2 on a fixed mesh.  Within one cell the deposit and the
 gather are trilinear in a particle's position, so central differences of L are exact up
 to round-off; components whose +-h step would cross a cell face are skipped.  The FP64
-gradients match the differences to 1e-6 (relative to the largest gradient); the FP32 path
-matches FP64 to 1e-4."""
+gradients match central differences of the FP64 oracle's forward chain (deposit_particles,
+space_charge_3d, interpolate_field: the reference algorithm, with no GPU code) and of the
+GPU's own FP64 forward to 1e-6 (relative to the largest gradient); the FP32 path matches
+FP64 to 1e-4, also at the differentiable-step configuration (128^3, 4e6 particles)."""
 import numpy as np
 import pytest
 
@@ -97,6 +99,96 @@ def test_vjp_matches_central_differences(det):
         fd = (Lp - Lm) / (2 * hq)
         full = (E[m] ** 2).sum() + gq[m]
         assert abs(fd - full) <= 1e-6 * abs(full), (m, fd, full)
+
+
+def oracle_loss(oracle, mesh, x, y, z, q):
+    om = oracle.make_mesh((1, 1, 1), mesh.nhi, (1, 1, 1), mesh.min, mesh.max, mesh.delta, mesh.gamma)
+    rho, _ = oracle.deposit_particles(x, y, z, om, qa=q, resize_mesh=False)
+    ef, _ = oracle.space_charge_3d(om, rho)
+    E, _, _ = oracle.interpolate_field(om, ef, x, y, z)
+    return float((q[:, None] * E * E).sum()), E
+
+
+def fd_check(lossf, mesh, x, y, z, q, grads, gq, E, picks, tol, h=1e-7, hq_rel=1e-3):
+    """Central differences of lossf on the picked particles (position steps h, charge steps
+    hq_rel * q) against the gradients."""
+    scale = max(np.abs(g).max() for g in grads)
+    pos = [x, y, z]
+    checked = 0
+    for m in picks:
+        for d in range(3):
+            u = (pos[d][m] - mesh.min[d]) / mesh.delta[d]
+            if min(u - np.floor(u), np.ceil(u) - u) * mesh.delta[d] < 3 * h:
+                continue  # the step would cross a cell face
+            p = [a.copy() for a in pos]
+            p[d][m] += h
+            Lp = lossf(*p, q)
+            p[d][m] -= 2 * h
+            Lm = lossf(*p, q)
+            fd = (Lp - Lm) / (2 * h)
+            assert abs(fd - grads[d][m]) <= tol * scale, (m, d, fd, grads[d][m])
+            checked += 1
+    for m in picks[:16]:
+        hq = hq_rel * q[m]
+        qp = q.copy()
+        qp[m] += hq
+        Lp = lossf(x, y, z, qp)
+        qp[m] -= 2 * hq
+        Lm = lossf(x, y, z, qp)
+        fd = (Lp - Lm) / (2 * hq)
+        full = (E[m] ** 2).sum() + gq[m]
+        assert abs(fd - full) <= tol * abs(full), (m, fd, full)
+    return checked
+
+
+@pytest.mark.parametrize("n", [(16, 16, 16), (16, 16, 24)])
+def test_vjp_matches_oracle_central_differences(ctx, oracle, n):
+    """FP64 reference gradients: central differences of the oracle's forward chain."""
+    x, y, z, q, mesh = setup(ctx, npart=20000, seed=56, n=n)
+    L0, E_orc = oracle_loss(oracle, mesh, x, y, z, q)
+    _, E = loss(ctx, mesh, x, y, z, q, osc.PREC_FP64)
+    assert np.abs(E - E_orc).max() <= 1e-10 * np.abs(E_orc).max()
+    gE = 2 * q[:, None] * E_orc
+    g64 = vjp(ctx, mesh, x, y, z, q, gE, osc.PREC_FP64)
+    picks = np.random.default_rng(8).choice(len(x), 64, replace=False)
+    # the oracle's full complex doubled-grid transforms leave ~1e-13 of L as round-off that
+    # changes with the input, so its differences take steps of 1e-6 m (0.2% of a cell) and 1% of q
+    checked = fd_check(lambda a, b, c, qq: oracle_loss(oracle, mesh, a, b, c, qq)[0], mesh, x, y, z, q,
+                       g64[:3], g64[3], E_orc, picks, 1e-6, h=1e-6, hq_rel=1e-2)
+    assert checked >= 150
+    g32 = vjp(ctx, mesh, x, y, z, q, gE, osc.PREC_FP32)
+    for a, b in zip(g32, g64):
+        assert np.abs(a - b).max() <= 1e-4 * np.abs(b).max()
+
+
+def test_differentiable_step_configuration(det, oracle):
+    """128^3 grid, 4e6 particles (sigma 1 mm, 1 nC): the forward E against the oracle, FP32
+    gradients against FP64 at every particle, FP64 gradients against central differences of
+    the GPU's FP64 forward on 64 particles.  With 4e6 particles one particle's share of L is
+    ~1e-10 of it, so the differences take larger steps (1e-6 m, 1% of q) and a 1e-4
+    tolerance, and the deposits are fixed point (no atomic-order noise in L)."""
+    ctx = det
+    npart = 4_000_000
+    x, y, z = gendist(npart, sigma=(1e-3, 1e-3, 1e-3), seed=1)
+    q = np.full(npart, 1e-9 / npart)
+    n = (128, 128, 128)
+    delta, umin = osc.get_mesh_quantities(ctx, x, y, z, (1, 1, 1), n, 0)
+    mesh = osc.Mesh3D(nlo=(1, 1, 1), nhi=n, min=umin, max=umin + (np.array(n) - 1) * delta, delta=delta,
+                      gamma=GAMMA)
+    _, E_orc = oracle_loss(oracle, mesh, x, y, z, q)
+    _, E = loss(ctx, mesh, x, y, z, q, osc.PREC_FP64)
+    assert np.abs(E - E_orc).max() <= 1e-10 * np.abs(E_orc).max()
+    _, E32 = loss(ctx, mesh, x, y, z, q, osc.PREC_FP32)
+    assert np.abs(E32 - E_orc).max() <= 1e-5 * np.abs(E_orc).max()
+    gE = 2 * q[:, None] * E
+    g64 = vjp(ctx, mesh, x, y, z, q, gE, osc.PREC_FP64)
+    g32 = vjp(ctx, mesh, x, y, z, q, 2 * q[:, None] * E32, osc.PREC_FP32)
+    for a, b in zip(g32, g64):
+        assert np.abs(a - b).max() <= 1e-4 * np.abs(b).max()
+    picks = np.random.default_rng(9).choice(npart, 64, replace=False)
+    checked = fd_check(lambda a, b, c, qq: loss(ctx, mesh, a, b, c, qq, osc.PREC_FP64)[0], mesh, x, y, z, q,
+                       g64[:3], g64[3], E, picks, 1e-4, h=1e-6, hq_rel=1e-2)
+    assert checked >= 120
 
 
 @pytest.mark.parametrize("n", [N, N_SUMMED])
