@@ -227,6 +227,50 @@ def kernel_bytes(nx, ny, nz, npart, at_cathode=False):
     }
 
 
+def green_bytes(nx, ny, nz):
+    """Algorithmic bytes of one FP32 Green build (three E components): FP64 corner blocks
+    written and read once, FP32 octant differences, three FP32 line-transform passes, the
+    stored FP32 spectra written."""
+    c3 = (nx + 1) * (ny + 1) * (nz + 1)
+    return 3 * (8 * c3 + 8 * c3 + 4 * nx * ny * nz + 4 * nx * ny * nz + 4 * (nx + 1) * ny * nz +
+                4 * (nx + 1) * ny * nz + 4 * (nx + 1) * (ny + 1) * nz + 4 * (nx + 1) * (ny + 1) * nz + 4 * c3)
+
+
+def step_bytes(nx, ny, nz, npart):
+    """Algorithmic bytes of one FP32 step (deposit, field with the Green spectra cached,
+    gather), the sum of kernel_bytes."""
+    return sum(kernel_bytes(nx, ny, nz, npart).values())
+
+
+def adjoint_bytes(nx, ny, nz, npart):
+    """Algorithmic bytes of the FP32 forward step plus its adjoint: the forward (deposit,
+    field, gather); the charge and the three dL/dE components deposited into quad grids
+    (coordinates, charges and dL/dE read, four quad grids written); the summed adjoint solve
+    (three quad grids read, one potential written into the x-pair grid's fourth slot); the
+    gradient gather (coordinates, charges, dL/dE and the x-pair grid read, four gradients
+    written)."""
+    n = nx * ny * nz
+    fwd = step_bytes(nx, ny, nz, npart)
+    kb = kernel_bytes(nx, ny, nz, 0)
+    solve = sum(v for k, v in kb.items() if k.startswith("fft_"))
+    dep = 32 * npart + 24 * npart + 4 * 16 * n
+    lam = solve + 2 * 16 * n
+    gather = 32 * npart + 24 * npart + 32 * n + 32 * npart
+    return fwd + dep + lam + gather
+
+
+def pipe_bytes(nx, ny, nz, npart):
+    """Algorithmic bytes of the fused FP32 pipe step: deposit, potential (one input and one
+    output, four cached spectra read as one combined spectrum), FD E written as the x-pair
+    grid, gather; the pipe's kernel is not even or odd, so its spectra are full complex."""
+    n = nx * ny * nz
+    nxh, Ny, Nz = nx + 1, 2 * ny, 2 * nz
+    field = (16 * n + 8 * nxh * ny * nz) + (8 * nxh * ny * nz + 8 * nxh * Ny * nz) + \
+        (8 * nxh * Ny * nz + 8 * nxh * Ny * Nz + 8 * nxh * Ny * nz) + (8 * nxh * Ny * nz + 8 * nxh * ny * nz) + \
+        (8 * nxh * ny * nz + 4 * n) + (4 * n + 32 * n)
+    return 24 * npart + 16 * n + field + 24 * npart + 32 * n + 24 * npart
+
+
 TRAFFIC_DATA = os.path.join(ROOT, "profiles", "dram_traffic_fp32_128x128x256.json")
 
 
@@ -452,6 +496,7 @@ def run_ours(args, ws, rank, local, dist):
             prof_o = kernel_profile(ctx, osc, step_o, 3)
             kbo = kernel_bytes(*grid, npart)
             kbo["deposit_f32_runs"] = kbo["deposit_f32"]
+            kbo["interp_f32_runs"] = kbo["interp_f32"]
             for name, ent in prof_o.items():
                 if name in kbo:
                     ent["alg_bytes"] = kbo[name]
@@ -657,6 +702,18 @@ def run_batch(args, ws, rank, local, dist):
     for _ in range(ke):
         host_step()
     te = maxr((time.perf_counter() - t0) / ke)
+    # algorithmic bytes of this rank's bunches: each bunch's FP32 step plus its Green build
+    # (meshes are refit every step, so every Green set is rebuilt)
+    hbm_peak, peak_src = load_peak()
+    alg = sum(step_bytes(*grids[b], counts[b]) + green_bytes(*grids[b]) for b in mine)
+    ach = alg / (ms * 1e-3) / 1e9
+    roof = {"kernel": "whole batched step (per-bunch deposit, Green build, field, gather)", "bound": "hbm",
+            "achieved": ach, "peak": hbm_peak, "unit": "GB/s", "frac": ach / hbm_peak,
+            "peak_source": peak_src, "traffic": None, "alg_bytes_per_step": alg,
+            "note": "the FP64 IGF corner primitives of the Green build are FP64-pipe bound, not HBM bound"}
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        cpu = cpu_baseline_batch(grids, counts, charges, sb, x, y, z)
     if rank == 0:
         line = {
             "metric": BATCH_METRIC, "value": value, "unit": "bunch solves/s", "n_gpus": ws, "steps": k,
@@ -673,7 +730,8 @@ def run_batch(args, ws, rank, local, dist):
             "e2e": {"value": args.bunches / te, "unit": "bunch solves/s",
                     "h2d_bytes_per_step": 3 * 8 * len(x), "d2h_bytes_per_step": 3 * 8 * len(x),
                     "ms_per_step": te * 1e3, "api": "osc_batch_space_charge_step (C ABI, pinned host buffers)"},
-            "kernels": kernels, "gpu_launches": launches, "clocks": clk.summary(),
+            "kernels": kernels, "gpu_launches": launches, "clocks": clk.summary(), "roofline": roof,
+            "cpu_baseline": cpu,
         }
         print(json.dumps(line))
     ctx.close()
@@ -736,6 +794,25 @@ def run_adjoint(args, ws, rank, local, dist):
     fwd_bwd(osc.PREC_FP64)
     ctx.synchronize()
     err = max(float((a - b).abs().max() / b.abs().max()) for a, b in zip(g32, g))
+    hbm_peak, peak_src = load_peak()
+    alg = adjoint_bytes(*ADJ_GRID, ADJ_NP)
+    ach = alg / (ms * 1e-3) / 1e9
+    roof = {"kernel": "whole forward + adjoint step", "bound": "hbm", "achieved": ach, "peak": hbm_peak,
+            "unit": "GB/s", "frac": ach / hbm_peak, "peak_source": peak_src, "traffic": None,
+            "alg_bytes_per_step": alg}
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        from oracle import oracle as O
+        O.build()
+        om = O.make_mesh((1, 1, 1), ADJ_GRID, (1, 1, 1), mesh.min, mesh.max, mesh.delta, GAMMA)
+        t0 = time.perf_counter()
+        rho, _ = O.deposit_particles(x, y, z, om, qa=q, resize_mesh=False)
+        ef, _ = O.space_charge_3d(om, rho)
+        O.interpolate_field(om, ef, x, y, z)
+        dt = time.perf_counter() - t0
+        cpu = {"value": 1.0 / dt, "unit": "forward steps/s", "cores": O.num_threads(), "kind": "port",
+               "sample": "1 forward step (deposit, solve, interpolation) of the FP64 CPU restatement at 128^3 with "
+                         "4e6 particles; the reference has no adjoint, so a gradient costs at least this"}
     if rank == 0:
         print(json.dumps({
             "metric": ADJ_METRIC, "value": ws * 1000.0 / ms, "unit": "gradients/s", "n_gpus": ws, "steps": k,
@@ -744,7 +821,8 @@ def run_adjoint(args, ws, rank, local, dist):
             "config": {"workload": "loss sum q|E|^2: FP32 step + FP32 adjoint (deposit, field, gather; deposited "
                                    "gradients, three adjoint solves, gradient gather) on a fixed 128^3 mesh, 4e6 "
                                    "particles, sigma = 1 mm", "grid": list(ADJ_GRID), "particles": ADJ_NP},
-            "rel_err_vs_fp64_gradients": err, "kernels": kern, "clocks": clk.summary()}))
+            "rel_err_vs_fp64_gradients": err, "kernels": kern, "clocks": clk.summary(), "roofline": roof,
+            "cpu_baseline": cpu}))
     ctx.close()
 
 
@@ -816,6 +894,25 @@ def run_pipe(args, ws, rank, local, dist):
     ms64 = e0.elapsed_time(e1)
     d = (E32 - E64).abs()
     err = float((d.amax(0) / E64.abs().amax(0)).max())
+    hbm_peak, peak_src = load_peak()
+    alg = pipe_bytes(*n, PIPE_NP)
+    ach = alg / (ms * 1e-3) / 1e9
+    roof = {"kernel": "whole fused pipe step", "bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
+            "frac": ach / hbm_peak, "peak_source": peak_src, "traffic": None, "alg_bytes_per_step": alg}
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        from oracle import oracle as O
+        O.build()
+        grn = O.getgrnpipe(GAMMA, a, b, delta, umin, (1, 1, 1), n)
+        om = O.make_mesh((1, 1, 1), n, (1, 1, 1), umin, umin + (np.array(n) - 1) * delta, delta, GAMMA)
+        t0 = time.perf_counter()
+        rho, _ = O.deposit_particles(x, y, z, om, total_charge=QTOT, resize_mesh=False)
+        _, ef, _ = O.rectpipe_solver(rho, grn, GAMMA, delta, (1, 1, 1), n)
+        O.interpolate_field(om, ef, x, y, z)
+        dt = time.perf_counter() - t0
+        cpu = {"value": 1.0 / dt, "unit": "solves/s", "cores": O.num_threads(), "kind": "port",
+               "sample": "1 pipe step (deposit, rectangular-pipe solve with the Green arrays built beforehand, "
+                         "interpolation) of the FP64 CPU restatement, 64x64x128, 4e6 particles"}
     if rank == 0:
         print(json.dumps({
             "metric": PIPE_METRIC, "value": ws * 1000.0 / ms, "unit": "solves/s", "n_gpus": ws, "steps": k,
@@ -827,8 +924,40 @@ def run_pipe(args, ws, rank, local, dist):
                                    "sigma=(2,1,1) mm centred at (3,-1) mm, pipe rejection",
                        "grid": list(n), "particles": PIPE_NP},
             "fp64_plain": {"ms_per_step": ms64, "speedup_fp32_over_fp64": ms64 / ms},
-            "rel_err_vs_fp64": err, "green_build_s": green_s, "kernels": kern, "clocks": clk.summary()}))
+            "rel_err_vs_fp64": err, "green_build_s": green_s, "kernels": kern, "clocks": clk.summary(),
+            "roofline": roof, "cpu_baseline": cpu}))
     ctx.close()
+
+
+def load_peak():
+    """HBM copy bandwidth (GB/s) of MEASURED_PEAKS.json, else the pool's earlier measurement."""
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(peaks["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except Exception:
+        return 6650.0, "fallback (6.65 TB/s)"
+
+
+def cpu_baseline_batch(grids, counts, charges, sb, x, y, z, nsample=8):
+    """The first nsample of this rank's bunches through the FP64 CPU port, one call each with
+    the mesh refit (deposit_particles with resize_mesh, space_charge_3d, interpolate_field)."""
+    from oracle import oracle as O
+    O.build()
+    t0 = time.perf_counter()
+    o = 0
+    done = 0
+    for i, b in enumerate(sb.mine[:nsample]):
+        sl = slice(o, o + counts[b])
+        om = O.make_mesh((1, 1, 1), grids[b], (1, 1, 1), (0, 0, 0), (0, 0, 0), (0, 0, 0), GAMMA)
+        rho, _ = O.deposit_particles(x[sl], y[sl], z[sl], om, total_charge=charges[b], resize_mesh=True)
+        ef, _ = O.space_charge_3d(om, rho)
+        O.interpolate_field(om, ef, x[sl], y[sl], z[sl])
+        o += counts[b]
+        done += 1
+    dt = time.perf_counter() - t0
+    return {"value": done / dt, "unit": "bunch solves/s", "cores": O.num_threads(), "kind": "port",
+            "sample": f"the first {done} bunches of the batch (particles {sum(counts[b] for b in sb.mine[:done])}), "
+                      f"one FP64 CPU call each with the mesh refit and G rebuilt"}
 
 
 def field_errors(E, ref):

@@ -529,8 +529,11 @@ int osc_space_charge_step_dev(osc_ctx *ctx, osc_mesh3d *mesh, int64_t np, const 
             if (B) TRY(ws_get(ctx, "st_sB", sizeof(double) * 3 * (size_t)np, (void **)&Bo));
         }
         {
-            Launch L_(ctx, "interp_f32");
-            if (launch_interp_pairs(ia, reinterpret_cast<const float4 *>(E8), Eo, ctx->d_small + 2, ctx->stream))
+            Launch L_(ctx, order == OSC_ORDER_ANY ? "interp_f32" : "interp_f32_runs");
+            if ((order == OSC_ORDER_ANY
+                     ? launch_interp_pairs(ia, reinterpret_cast<const float4 *>(E8), Eo, ctx->d_small + 2, ctx->stream)
+                     : launch_interp_pairs_runs(ia, reinterpret_cast<const float4 *>(E8), Eo, ctx->d_small + 2,
+                                                ctx->stream)))
                 return set_err(ctx, OSC_E_CUDA, "interp");
         }
         if (B) {

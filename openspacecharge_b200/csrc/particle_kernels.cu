@@ -351,28 +351,36 @@ __device__ __forceinline__ void ldg_pair(const float4 *p, float4 &lo, float4 &hi
         : "l"(p));
 }
 
+// E at a particle from the four x-pairs of its stencil (rows (j,k), (j+1,k), (j+1,k+1),
+// (j,k+1), each holding nodes i and i+1), with explicit fused multiply-adds so that every
+// gather kernel rounds alike.
+__device__ __forceinline__ void pair_sum(const float4 (&lo)[4], const float4 (&hi)[4], double ab, double de,
+                                         double gh, double &ex, double &ey, double &ez) {
+    const double omab = 1. - ab, omde = 1. - de, omgh = 1. - gh;
+    const double wy[4] = {de * gh, omde * gh, omde * omgh, de * omgh};
+    ex = ey = ez = 0.0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const double w0 = ab * wy[q], w1 = omab * wy[q];
+        ex = __fma_rn((double)lo[q].x, w0, __fma_rn((double)hi[q].x, w1, ex));
+        ey = __fma_rn((double)lo[q].y, w0, __fma_rn((double)hi[q].y, w1, ey));
+        ez = __fma_rn((double)lo[q].z, w0, __fma_rn((double)hi[q].z, w1, ez));
+    }
+}
+
 // One particle of the x-pair gather; returns true when its cell was clamped.
 __device__ __forceinline__ bool interp_pair_one(const InterpArgs &a, const float4 *__restrict__ g8, int64_t plane,
                                                 double xm, double ym, double zm, double *__restrict__ Eo) {
     Cell c;
     const bool fl = locate(a, xm, ym, zm, c);
     const int64_t n0 = c.i + (int64_t)a.nx * c.j + plane * c.k;
-    const double ab = c.ab, de = c.de, gh = c.gh;
-    const double omab = 1. - ab, omde = 1. - de, omgh = 1. - gh;
     // (j,k), (j+1,k), (j+1,k+1), (j,k+1) rows; each pair = nodes i and i+1
     const int64_t rows[4] = {n0, n0 + a.nx, n0 + a.nx + plane, n0 + plane};
-    const double wy[4] = {de * gh, omde * gh, omde * omgh, de * omgh};
     float4 lo[4], hi[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) ldg_pair(g8 + 2 * rows[q], lo[q], hi[q]);
-    double ex = 0, ey = 0, ez = 0;
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const double w0 = ab * wy[q], w1 = omab * wy[q];
-        ex += (double)lo[q].x * w0 + (double)hi[q].x * w1;
-        ey += (double)lo[q].y * w0 + (double)hi[q].y * w1;
-        ez += (double)lo[q].z * w0 + (double)hi[q].z * w1;
-    }
+    double ex, ey, ez;
+    pair_sum(lo, hi, c.ab, c.de, c.gh, ex, ey, ez);
     Eo[0] = ex;
     Eo[1] = ey;
     Eo[2] = ez;
@@ -420,6 +428,87 @@ __global__ void __launch_bounds__(256) k_interp_pairs(InterpArgs a, const float4
         }
         __syncwarp();
     }
+}
+
+// Gather for particles in cell order.  Lane l of warp chunk w owns the kRunG consecutive
+// particles from (32 w + l) kRunG: their coordinates come in as one 256-bit load per array
+// (32-byte aligned arrays), consecutive particles in the same cell reuse the four x-pairs
+// loaded for the first of them, and the lane's 12 consecutive output doubles leave as three
+// 256-bit stores.  Per particle the arithmetic is pair_sum's, as in k_interp_pairs, so E is
+// bit-identical to it for any order.
+constexpr int kRunG = 4;
+__global__ void __launch_bounds__(256) k_interp_pairs_runs(InterpArgs a, const float4 *__restrict__ g8, bool vec,
+                                                           double *__restrict__ E,
+                                                           unsigned long long *__restrict__ nclamp) {
+    const int64_t plane = (int64_t)a.nx * a.ny;
+    const int lane = threadIdx.x & 31;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w * 32 * kRunG < a.np; w += nwarps) {
+        const int64_t m0 = (w * 32 + lane) * kRunG;
+        const bool full = vec && m0 + kRunG <= a.np;
+        double xs[kRunG], ys[kRunG], zs[kRunG];
+        if (full) {
+            asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(xs[0]), "=d"(xs[1]), "=d"(xs[2]), "=d"(xs[3]) : "l"(a.x + m0));
+            asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(ys[0]), "=d"(ys[1]), "=d"(ys[2]), "=d"(ys[3]) : "l"(a.y + m0));
+            asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(zs[0]), "=d"(zs[1]), "=d"(zs[2]), "=d"(zs[3]) : "l"(a.z + m0));
+        } else {
+#pragma unroll
+            for (int t = 0; t < kRunG; ++t) {
+                const bool ok = m0 + t < a.np;
+                xs[t] = ok ? __ldg(a.x + m0 + t) : 0.0;
+                ys[t] = ok ? __ldg(a.y + m0 + t) : 0.0;
+                zs[t] = ok ? __ldg(a.z + m0 + t) : 0.0;
+            }
+        }
+        double out[3 * kRunG];
+        int64_t cur = -1;
+        float4 lo[4], hi[4];
+        unsigned ncl = 0;
+#pragma unroll
+        for (int t = 0; t < kRunG; ++t) {
+            out[3 * t] = out[3 * t + 1] = out[3 * t + 2] = 0.0;
+            if (m0 + t >= a.np) continue;
+            Cell c;
+            ncl += locate(a, xs[t], ys[t], zs[t], c) ? 1u : 0u;
+            const int64_t n0 = c.i + (int64_t)a.nx * c.j + plane * c.k;
+            if (n0 != cur) {
+                const int64_t rows[4] = {n0, n0 + a.nx, n0 + a.nx + plane, n0 + plane};
+#pragma unroll
+                for (int q = 0; q < 4; ++q) ldg_pair(g8 + 2 * rows[q], lo[q], hi[q]);
+                cur = n0;
+            }
+            double ex, ey, ez;
+            pair_sum(lo, hi, c.ab, c.de, c.gh, ex, ey, ez);
+            out[3 * t] = ex;
+            out[3 * t + 1] = ey;
+            out[3 * t + 2] = ez;
+        }
+        double *dst = E + 3 * m0;
+        if (full) {
+#pragma unroll
+            for (int v = 0; v < 3; ++v)
+                asm volatile("st.global.v4.f64 [%0], {%1,%2,%3,%4};" ::"l"(dst + 4 * v), "d"(out[4 * v]),
+                             "d"(out[4 * v + 1]), "d"(out[4 * v + 2]), "d"(out[4 * v + 3])
+                             : "memory");
+        } else {
+#pragma unroll
+            for (int e = 0; e < 3 * kRunG; ++e)
+                if (m0 + e / 3 < a.np) dst[e] = out[e];
+        }
+        ncl = __reduce_add_sync(0xffffffffu, ncl);
+        if (lane == 0 && ncl) atomicAdd(nclamp, (unsigned long long)ncl);
+    }
+}
+
+int launch_interp_pairs_runs(const InterpArgs &a, const float4 *E8, double *E, unsigned long long *nclamp,
+                             cudaStream_t st) {
+    if (a.np <= 0) return OSC_OK;
+    if (reinterpret_cast<uintptr_t>(E8) % 32) return OSC_E_INVALID;
+    auto al = [](const void *p) { return reinterpret_cast<uintptr_t>(p) % 32 == 0; };
+    const bool vec = al(a.x) && al(a.y) && al(a.z) && al(E);
+    const int64_t chunks = (a.np + 32 * kRunG - 1) / (32 * kRunG);
+    k_interp_pairs_runs<<<nblocks(chunks * 32, 256, 148 * 16), 256, 0, st>>>(a, E8, vec, E, nclamp);
+    return ok();
 }
 
 int launch_interp_pairs(const InterpArgs &a, const float4 *E8, double *E, unsigned long long *nclamp,
@@ -477,7 +566,27 @@ __global__ void __launch_bounds__(256) k_bbox(int64_t np, const double *__restri
         }
     }
     for (int off = 16; off; off >>= 1) bad += __shfl_xor_sync(0xffffffffu, bad, off);
+    // the block's warps combine in shared memory, then one thread adds the block's extremes:
+    // seven atomics per block instead of per warp on the same seven words
+    __shared__ unsigned long long sk[8][7];
+    const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            sk[w][2 * d] = lo[d];
+            sk[w][2 * d + 1] = hi[d];
+        }
+        sk[w][6] = bad;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int v = 1; v < nw; ++v)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                lo[d] = sk[v][2 * d] < lo[d] ? sk[v][2 * d] : lo[d];
+                hi[d] = sk[v][2 * d + 1] > hi[d] ? sk[v][2 * d + 1] : hi[d];
+            }
+        for (int v = 1; v < nw; ++v) bad += sk[v][6];
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
             atomicMin(&keys[2 * d], lo[d]);

@@ -91,6 +91,11 @@ int launch_interp_planes(const InterpArgs &a, const double *F, double *out,
 // sector, so the 8 nodes of a particle come from 4 sectors.
 int launch_interp_pairs(const InterpArgs &a, const float4 *E8, double *E, unsigned long long *nclamp,
                         cudaStream_t st);
+// The same gather for particles in cell order: runs of consecutive particles in one cell
+// share their stencil's loads; coordinates and E move as 256-bit vectors.  Bit-identical
+// to launch_interp_pairs for any order.
+int launch_interp_pairs_runs(const InterpArgs &a, const float4 *E8, double *E, unsigned long long *nclamp,
+                             cudaStream_t st);
 
 // Bounding box {xmin,xmax,ymin,ymax,zmin,zmax} of the particles, written to bb (device)
 // through order-preserving 64-bit keys; also counts non-finite coordinates.
