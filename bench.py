@@ -65,6 +65,7 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-refit", action="store_true", help="skip the refit + Green rebuild leg")
     ap.add_argument("--no-order", action="store_true", help="skip the cell-sorted particle-order legs")
+    ap.add_argument("--no-tune", action="store_true", help="built-in launch shapes instead of autotuned ones")
     ap.add_argument("--workload", default="single", choices=["single", "batch", "adjoint", "pipe"],
                     help="single: the headline one-bunch step; batch: 256 bunches of mixed grids per step; "
                          "adjoint: forward + backward of sum q|E|^2 at 128^3, 4e6 particles; "
@@ -334,6 +335,14 @@ def run_ours(args, ws, rank, local, dist):
         osc.space_charge_step_dev(ctx, mesh, tx, ty, tz, out, total_charge=QTOT, resize_mesh=False,
                                   precision=prec)
 
+    # launch shapes from the project's autotuner, timed on this workload before the timed region
+    tuned = None
+    if not args.no_tune:
+        from openspacecharge_b200 import autotune
+        tuned = autotune.tune(ctx, lambda: step(osc.PREC_FP32), grid, order=osc.ORDER_ANY, device=local,
+                              workload=f"{grid} {npart} random order", save=False)
+        tuned = {k: {"value": v, "candidates_ms": t} for k, (v, t) in tuned.items()}
+
     def barrier():
         if dist is not None:
             dist.barrier()
@@ -481,6 +490,11 @@ def run_ours(args, ws, rank, local, dist):
             def step_o(out=E, p=px_):
                 osc.space_charge_step_dev(ctx, mesh, p[0], p[1], p[2], out, total_charge=QTOT, resize_mesh=False,
                                           precision=osc.PREC_FP32)
+            if not args.no_tune and mode == osc.ORDER_CELL_SORTED:
+                from openspacecharge_b200 import autotune
+                tr = autotune.tune(ctx, step_o, grid, order=mode, device=local, save=False,
+                                   workload=f"{grid} {npart} cell order")
+                tuned = dict(tuned or {}, **{k: {"value": v, "candidates_ms": t} for k, (v, t) in tr.items()})
             for _ in range(3):
                 step_o()
             ctx.synchronize()
@@ -574,7 +588,7 @@ def run_ours(args, ws, rank, local, dist):
                        "l2": "inputs larger than L2 (240 MB of particle coordinates per step)",
                        "parallelism": f"{ws} independent replica(s)"},
             "fp64_plain": fp64, "rel_err_vs_fp64": err, "rel_err_vs_oracle": err_oracle,
-            "refit_rebuild": refit, "particle_order": orders,
+            "refit_rebuild": refit, "particle_order": orders, "autotune": tuned,
             "step_alg_bytes": step_bytes, "step_alg_gbs": step_gbs,
             "kernels": kernels, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches, "clocks": clk.summary(),
@@ -636,6 +650,12 @@ def run_batch(args, ws, rank, local, dist):
     def maxr(v):
         return max_over_ranks(v, dist)
 
+    tuned = None
+    if not args.no_tune:
+        from openspacecharge_b200 import autotune
+        lengths = sorted({2 * int(g[1]) for g in grids})
+        tr = autotune.tune_lengths(ctx, step, lengths, device=local, save=False, workload="batch")
+        tuned = {k: {"value": v, "candidates_ms": t} for k, (v, t) in tr.items()}
     for _ in range(max(3, args.warmup)):
         step()
     ctx.synchronize()
@@ -731,7 +751,7 @@ def run_batch(args, ws, rank, local, dist):
                     "h2d_bytes_per_step": 3 * 8 * len(x), "d2h_bytes_per_step": 3 * 8 * len(x),
                     "ms_per_step": te * 1e3, "api": "osc_batch_space_charge_step (C ABI, pinned host buffers)"},
             "kernels": kernels, "gpu_launches": launches, "clocks": clk.summary(), "roofline": roof,
-            "cpu_baseline": cpu,
+            "cpu_baseline": cpu, "autotune": tuned,
         }
         print(json.dumps(line))
     ctx.close()

@@ -119,6 +119,19 @@ OSC_API int osc_ctx_set_stream(osc_ctx *ctx, void *cuda_stream);
 OSC_API int osc_ctx_set_option(osc_ctx *ctx, int option, int64_t value);
 OSC_API int osc_ctx_get_option(osc_ctx *ctx, int option, int64_t *value);
 OSC_API int osc_ctx_synchronize(osc_ctx *ctx);
+/* Launch shapes chosen by an autotuner (openspacecharge_b200.autotune times the candidates
+ * on the GPU and keeps the winners in a JSON cache keyed by GPU, kernel and length); no
+ * reference counterpart.  Keys and values (0 restores the built-in default):
+ *   "deposit_run", "gather_run": particles per lane of the cell-ordered deposit and gather
+ *     (4 or 8);
+ *   "deposit_ctas_per_sm", "gather_ctas_per_sm", "deposit_runs_ctas_per_sm",
+ *   "gather_runs_ctas_per_sm": grid size of the per-particle and run kernels, CTAs per SM
+ *     (4, 8, 16, 32, 64 or 128);
+ *   "lines_nl_div:<f32|f64>:L<length>": 2 halves the lines per CTA of the y transforms of
+ *     that doubled length.
+ * Results are identical for every choice; only the time changes. */
+OSC_API int osc_ctx_set_tuning(osc_ctx *ctx, const char *key, int value);
+OSC_API int osc_ctx_get_tuning(osc_ctx *ctx, const char *key, int *value);
 OSC_API int osc_clear_green_cache(osc_ctx *ctx);
 OSC_API const char *osc_version(void);
 /* Kernel profile (OSC_OPT_PROFILE=1): per kernel name, launches and summed ms. */

@@ -129,6 +129,31 @@ int osc_ctx_get_option(osc_ctx *ctx, int option, int64_t *v) {
     }
 }
 
+// Tuning keys and their allowed values: the launch shapes the kernels accept.
+static bool tuning_value_ok(const std::string &key, int v) {
+    if (key == "deposit_run" || key == "gather_run") return v == 0 || v == 4 || v == 8;
+    if (key == "deposit_ctas_per_sm" || key == "gather_ctas_per_sm" || key == "deposit_runs_ctas_per_sm" ||
+        key == "gather_runs_ctas_per_sm")
+        return v == 0 || v == 4 || v == 8 || v == 16 || v == 32 || v == 64 || v == 128;
+    if (key.rfind("lines_nl_div:", 0) == 0) return v == 0 || v == 1 || v == 2;
+    return false;
+}
+
+int osc_ctx_set_tuning(osc_ctx *ctx, const char *key, int value) {
+    if (!ctx || !key) return OSC_E_INVALID;
+    const std::string k(key);
+    if (!tuning_value_ok(k, value)) return set_err(ctx, OSC_E_INVALID, "tuning %s = %d is not a valid choice", key, value);
+    if (value == 0) ctx->tuning.erase(k);  // the built-in default
+    else ctx->tuning[k] = value;
+    return OSC_OK;
+}
+
+int osc_ctx_get_tuning(osc_ctx *ctx, const char *key, int *value) {
+    if (!ctx || !key || !value) return OSC_E_INVALID;
+    *value = tune_get(ctx, key, 0);
+    return OSC_OK;
+}
+
 int osc_ctx_synchronize(osc_ctx *ctx) {
     if (!ctx) return OSC_E_INVALID;
     return sync(ctx);
@@ -463,6 +488,13 @@ int osc_space_charge_step_dev(osc_ctx *ctx, osc_mesh3d *mesh, int64_t np, const 
     DepositArgs da = deposit_args(mesh, n, np, x, y, z, q, charge1, ctx->check_finite);
     InterpArgs ia = interp_args(mesh, n, np, x, y, z);
     FreeSpaceJob j = fs_job(mesh, n, nullptr, at_cathode, B != nullptr);
+    // launch shapes from the autotuner (per-particle kernels in any order, run kernels in
+    // cell order)
+    const bool runs = ctx->particle_order != OSC_ORDER_ANY;
+    da.tile = tune_get(ctx, "deposit_run");
+    ia.tile = tune_get(ctx, "gather_run");
+    da.ctas = tune_get(ctx, runs ? "deposit_runs_ctas_per_sm" : "deposit_ctas_per_sm");
+    ia.ctas = tune_get(ctx, runs ? "gather_runs_ctas_per_sm" : "gather_ctas_per_sm");
     if (precision == OSC_PREC_FP64_PLAIN) {
         double *rho, *Eg, *Bg = nullptr;
         TRY(ws_get(ctx, "st_rho64", sizeof(double) * N, (void **)&rho));

@@ -185,21 +185,24 @@ int launch_cell_scatter(int64_t np, const uint32_t *keys, const uint32_t *ranks,
 }
 
 // ------------------------------------------------------------------------------------
-// Run-aggregated deposits.  Lane l of warp chunk w owns the kRun consecutive particles
-// starting at (32 w + l) kRun: it loads them (one 256-bit load per coordinate array when
-// the arrays are 32-byte aligned), walks them in order, sums the contributions of
-// consecutive particles in the same cell, and adds a run's sum to the grid when the cell
-// changes and at the end.  Particles outside the mesh are counted and skipped without
-// ending a run.
-constexpr int kRun = 4;
-
+// Run-aggregated deposits.  Lane l of warp chunk w owns the RUN consecutive particles
+// starting at (32 w + l) RUN (RUN = 4 or 8, the deposit tile the autotuner picks): it loads
+// them (256-bit loads when the arrays are 32-byte aligned), walks them in order, sums the
+// contributions of consecutive particles in the same cell, and adds a run's sum to the grid
+// when the cell changes and at the end.  Particles outside the mesh are counted and skipped
+// without ending a run.
+template <int RUN>
 __device__ __forceinline__ void load_run(const double *__restrict__ p, int64_t m0, int64_t np, bool vec,
-                                         double (&v)[kRun]) {
-    if (vec && m0 + kRun <= np) {
-        asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3]) : "l"(p + m0));
+                                         double (&v)[RUN]) {
+    if (vec && m0 + RUN <= np) {
+#pragma unroll
+        for (int u = 0; u < RUN / 4; ++u)
+            asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];"
+                : "=d"(v[4 * u]), "=d"(v[4 * u + 1]), "=d"(v[4 * u + 2]), "=d"(v[4 * u + 3])
+                : "l"(p + m0 + 4 * u));
     } else {
 #pragma unroll
-        for (int t = 0; t < kRun; ++t) v[t] = m0 + t < np ? __ldg(p + m0 + t) : 0.0;
+        for (int t = 0; t < RUN; ++t) v[t] = m0 + t < np ? __ldg(p + m0 + t) : 0.0;
     }
 }
 
@@ -212,6 +215,7 @@ __device__ __forceinline__ void two_sum_add(float &s, float &c, float v) {
     c += e;
 }
 
+template <int kRun>
 __global__ void __launch_bounds__(256) k_deposit_quad_runs(DepositArgs a, float4 *__restrict__ quad, bool vec,
                                                            unsigned long long *__restrict__ counters) {
     const int64_t plane = (int64_t)a.nx * a.ny;
@@ -220,11 +224,11 @@ __global__ void __launch_bounds__(256) k_deposit_quad_runs(DepositArgs a, float4
     for (int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w * 32 * kRun < a.np; w += nwarps) {
         const int64_t m0 = (w * 32 + lane) * kRun;
         double xs[kRun], ys[kRun], zs[kRun], qs[kRun];
-        load_run(a.x, m0, a.np, vec, xs);
-        load_run(a.y, m0, a.np, vec, ys);
-        load_run(a.z, m0, a.np, vec, zs);
+        load_run<kRun>(a.x, m0, a.np, vec, xs);
+        load_run<kRun>(a.y, m0, a.np, vec, ys);
+        load_run<kRun>(a.z, m0, a.np, vec, zs);
         if (a.q) {
-            load_run(a.q, m0, a.np, vec, qs);
+            load_run<kRun>(a.q, m0, a.np, vec, qs);
         } else {
 #pragma unroll
             for (int t = 0; t < kRun; ++t) qs[t] = a.charge1;
@@ -284,15 +288,20 @@ int launch_deposit_quad_runs(const DepositArgs &a, float *quad, unsigned long lo
     if (a.np <= 0) return OSC_OK;
     if (a.mode != 0 || a.lost) return OSC_E_INVALID;
     const bool vec = aligned32(a.x) && aligned32(a.y) && aligned32(a.z) && aligned32(a.q);
-    const int64_t chunks = (a.np + 32 * kRun - 1) / (32 * kRun);
-    k_deposit_quad_runs<<<nblocks(chunks * 32, 256, 148 * 16), 256, 0, st>>>(a, reinterpret_cast<float4 *>(quad), vec,
-                                                                            counters);
+    const int run = a.tile == 8 ? 8 : 4;
+    const int64_t chunks = (a.np + 32 * run - 1) / (32 * run);
+    const unsigned nb = nblocks(chunks * 32, 256, 148 * (int64_t)(a.ctas > 0 ? a.ctas : 16));
+    if (run == 8)
+        k_deposit_quad_runs<8><<<nb, 256, 0, st>>>(a, reinterpret_cast<float4 *>(quad), vec, counters);
+    else
+        k_deposit_quad_runs<4><<<nb, 256, 0, st>>>(a, reinterpret_cast<float4 *>(quad), vec, counters);
     return ok();
 }
 
 // Fixed point: the eight contributions of k_deposit<unsigned long long> (the same double
 // products in the same order, rounded to integers with the same scale), summed per run in
 // 64-bit integers, which is exact, so the node sums are those of the per-particle kernel.
+template <int kRun>
 __global__ void __launch_bounds__(256) k_deposit_fixed_runs(DepositArgs a, unsigned long long *__restrict__ acc,
                                                             bool vec, unsigned long long *__restrict__ counters) {
     const int64_t plane = (int64_t)a.nx * a.ny;
@@ -301,11 +310,11 @@ __global__ void __launch_bounds__(256) k_deposit_fixed_runs(DepositArgs a, unsig
     for (int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w * 32 * kRun < a.np; w += nwarps) {
         const int64_t m0 = (w * 32 + lane) * kRun;
         double xs[kRun], ys[kRun], zs[kRun], qs[kRun];
-        load_run(a.x, m0, a.np, vec, xs);
-        load_run(a.y, m0, a.np, vec, ys);
-        load_run(a.z, m0, a.np, vec, zs);
+        load_run<kRun>(a.x, m0, a.np, vec, xs);
+        load_run<kRun>(a.y, m0, a.np, vec, ys);
+        load_run<kRun>(a.z, m0, a.np, vec, zs);
         if (a.q) {
-            load_run(a.q, m0, a.np, vec, qs);
+            load_run<kRun>(a.q, m0, a.np, vec, qs);
         } else {
 #pragma unroll
             for (int t = 0; t < kRun; ++t) qs[t] = a.charge1;
@@ -369,8 +378,13 @@ int launch_deposit_fixed_runs(const DepositArgs &a, unsigned long long *acc, uns
     if (a.np <= 0) return OSC_OK;
     if (a.mode != 0 || a.lost) return OSC_E_INVALID;
     const bool vec = aligned32(a.x) && aligned32(a.y) && aligned32(a.z) && aligned32(a.q);
-    const int64_t chunks = (a.np + 32 * kRun - 1) / (32 * kRun);
-    k_deposit_fixed_runs<<<nblocks(chunks * 32, 256, 148 * 16), 256, 0, st>>>(a, acc, vec, counters);
+    const int run = a.tile == 8 ? 8 : 4;
+    const int64_t chunks = (a.np + 32 * run - 1) / (32 * run);
+    const unsigned nb = nblocks(chunks * 32, 256, 148 * (int64_t)(a.ctas > 0 ? a.ctas : 16));
+    if (run == 8)
+        k_deposit_fixed_runs<8><<<nb, 256, 0, st>>>(a, acc, vec, counters);
+    else
+        k_deposit_fixed_runs<4><<<nb, 256, 0, st>>>(a, acc, vec, counters);
     return ok();
 }
 

@@ -182,6 +182,11 @@ Launch::~Launch() {
     }
 }
 
+int tune_get(const osc_ctx *c, const std::string &key, int def) {
+    auto it = c->tuning.find(key);
+    return it == c->tuning.end() ? def : it->second;
+}
+
 int prof_flush(osc_ctx *c) {
     if (c->prof_pending.empty()) return OSC_OK;
     cudaStreamSynchronize(c->stream);

@@ -66,6 +66,8 @@ struct osc_ctx {
     int precision = 0;
     int deposit_mode = 0;
     int particle_order = 0;  // OSC_ORDER_*
+    // launch shapes picked by the autotuner (osc_ctx_set_tuning), by key; absent = default
+    std::map<std::string, int> tuning;
     int strict_bounds = 0;
     int profile = 0;
     int check_finite = 0;
@@ -116,6 +118,8 @@ struct Launch {
     ~Launch();
 };
 int prof_flush(osc_ctx *c);
+// Tuned value of `key` (autotuner), or def when none was set.
+int tune_get(const osc_ctx *c, const std::string &key, int def = 0);
 
 // Green-spectrum cache.  A budget of 0 disables it: every solve rebuilds its spectra (the
 // reference's behaviour, code/open_spacecharge_mod.f90:570-573) into reused buffers.

@@ -19,6 +19,7 @@ struct LineArgs {
     int64_t out_pstride, out_cstride, out_estride, out_zstride;
     double scale;
     unsigned flip_mask;  // bit z: component z stores element (L-e) mod L at e (index flip)
+    int nl_div = 0;      // autotuner: 2 halves the lines per CTA of a static engine (0/1: default)
 };
 
 // Forward transform of real rows (length nin, zero-padded to L) packed two per complex

@@ -638,7 +638,8 @@ inline int pick_nl_rt(int L, int nl_max, size_t elem, int nbuf) {
 // Calls f(std::integral_constant<int, NL>) for the engine's lines-per-CTA.  Static engines
 // use a compile-time NL: the widest that fits (one line buffer) or, for the two-buffer
 // z-pass, at most 4 lines in ~48 KB so several CTAs share an SM.
-template <typename T, class E, class F> inline int with_nl(int L, int nbuf, int nl_max, int nl_req, F &&f) {
+template <typename T, class E, class F>
+inline int with_nl(int L, int nbuf, int nl_max, int nl_req, F &&f, int nl_div = 0) {
     if constexpr (E::kLen > 0) {
         (void)L;
         (void)nl_req;
@@ -646,6 +647,9 @@ template <typename T, class E, class F> inline int with_nl(int L, int nbuf, int 
         constexpr int NL1 = nl_static(E::kLen, sizeof(T) == 4 ? 16 : 8, (int)sizeof(cplx<T>), 1, 100 * 1024, E::kEPT);
         constexpr int NL2 = nl_static(E::kLen, 4, (int)sizeof(cplx<T>), 2, 64 * 1024, E::kEPT);
         if (nbuf >= 2) return f(std::integral_constant<int, NL2>{});
+        // the autotuner's alternative tile: half the lines per CTA (more, smaller CTAs)
+        constexpr int NLH = NL1 >= 4 && ((E::kLen * (NL1 / 2)) % E::kEPT) == 0 ? NL1 / 2 : NL1;
+        if (nl_div == 2 && NLH != NL1) return f(std::integral_constant<int, NLH>{});
         return f(std::integral_constant<int, NL1>{});
     } else {
         int nl = nl_req > 0 ? nl_req : pick_nl_rt(L, nl_max, sizeof(cplx<T>), nbuf);
@@ -691,7 +695,7 @@ int launch_lines(const cplx<T> *in, cplx<T> *out, const LineArgs &a, int nplanes
                     return launch_lines_k<T, NL, false, E, 2>(in, out, a, nplanes, ncomp, twe, st);
             }
             return launch_lines_k<T, NL, false, E, 0>(in, out, a, nplanes, ncomp, twe, st);
-        });
+        }, row_mode ? 0 : a.nl_div);
     });
 }
 

@@ -179,7 +179,9 @@ __global__ void __launch_bounds__(256) k_deposit_quad(DepositArgs a, float4 *__r
 
 int launch_deposit_quad(const DepositArgs &a, float *quad, unsigned long long *counters, cudaStream_t st) {
     if (a.np <= 0) return OSC_OK;
-    k_deposit_quad<<<nblocks(a.np, 256, 1 << 20), 256, 0, st>>>(a, reinterpret_cast<float4 *>(quad), counters);
+    // default: one particle per thread; the autotuner may cap the grid at a.ctas CTAs per SM
+    const int64_t cap = a.ctas > 0 ? 148 * (int64_t)a.ctas : (1 << 20);
+    k_deposit_quad<<<nblocks(a.np, 256, cap), 256, 0, st>>>(a, reinterpret_cast<float4 *>(quad), counters);
     return ok();
 }
 
@@ -430,42 +432,49 @@ __global__ void __launch_bounds__(256) k_interp_pairs(InterpArgs a, const float4
     }
 }
 
-// Gather for particles in cell order.  Lane l of warp chunk w owns the kRunG consecutive
-// particles from (32 w + l) kRunG: their coordinates come in as one 256-bit load per array
-// (32-byte aligned arrays), consecutive particles in the same cell reuse the four x-pairs
-// loaded for the first of them, and the lane's 12 consecutive output doubles leave as three
-// 256-bit stores.  Per particle the arithmetic is pair_sum's, as in k_interp_pairs, so E is
-// bit-identical to it for any order.
-constexpr int kRunG = 4;
+// Gather for particles in cell order.  Lane l of warp chunk w owns the RUN consecutive
+// particles from (32 w + l) RUN (RUN = 4 or 8, chosen by the autotuner): their coordinates
+// come in as 256-bit loads (32-byte aligned arrays), consecutive particles in the same cell
+// reuse the four x-pairs loaded for the first of them, and the lane's 3 RUN consecutive
+// output doubles leave as 256-bit stores.  Per particle the arithmetic is pair_sum's, as in
+// k_interp_pairs, so E is bit-identical to it for any order.
+__device__ __forceinline__ void ldg_v4(const double *p, double *v) {
+    asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3]) : "l"(p));
+}
+template <int RUN>
 __global__ void __launch_bounds__(256) k_interp_pairs_runs(InterpArgs a, const float4 *__restrict__ g8, bool vec,
                                                            double *__restrict__ E,
                                                            unsigned long long *__restrict__ nclamp) {
+    static_assert(RUN % 4 == 0, "runs of whole 256-bit vectors");
     const int64_t plane = (int64_t)a.nx * a.ny;
     const int lane = threadIdx.x & 31;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w * 32 * kRunG < a.np; w += nwarps) {
-        const int64_t m0 = (w * 32 + lane) * kRunG;
-        const bool full = vec && m0 + kRunG <= a.np;
-        double xs[kRunG], ys[kRunG], zs[kRunG];
+    for (int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w * 32 * RUN < a.np; w += nwarps) {
+        const int64_t m0 = (w * 32 + lane) * RUN;
+        const bool full = vec && m0 + RUN <= a.np;
+        double xs[RUN], ys[RUN], zs[RUN];
         if (full) {
-            asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(xs[0]), "=d"(xs[1]), "=d"(xs[2]), "=d"(xs[3]) : "l"(a.x + m0));
-            asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(ys[0]), "=d"(ys[1]), "=d"(ys[2]), "=d"(ys[3]) : "l"(a.y + m0));
-            asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(zs[0]), "=d"(zs[1]), "=d"(zs[2]), "=d"(zs[3]) : "l"(a.z + m0));
+#pragma unroll
+            for (int v = 0; v < RUN / 4; ++v) {
+                ldg_v4(a.x + m0 + 4 * v, xs + 4 * v);
+                ldg_v4(a.y + m0 + 4 * v, ys + 4 * v);
+                ldg_v4(a.z + m0 + 4 * v, zs + 4 * v);
+            }
         } else {
 #pragma unroll
-            for (int t = 0; t < kRunG; ++t) {
+            for (int t = 0; t < RUN; ++t) {
                 const bool ok = m0 + t < a.np;
                 xs[t] = ok ? __ldg(a.x + m0 + t) : 0.0;
                 ys[t] = ok ? __ldg(a.y + m0 + t) : 0.0;
                 zs[t] = ok ? __ldg(a.z + m0 + t) : 0.0;
             }
         }
-        double out[3 * kRunG];
+        double out[3 * RUN];
         int64_t cur = -1;
         float4 lo[4], hi[4];
         unsigned ncl = 0;
 #pragma unroll
-        for (int t = 0; t < kRunG; ++t) {
+        for (int t = 0; t < RUN; ++t) {
             out[3 * t] = out[3 * t + 1] = out[3 * t + 2] = 0.0;
             if (m0 + t >= a.np) continue;
             Cell c;
@@ -486,13 +495,13 @@ __global__ void __launch_bounds__(256) k_interp_pairs_runs(InterpArgs a, const f
         double *dst = E + 3 * m0;
         if (full) {
 #pragma unroll
-            for (int v = 0; v < 3; ++v)
+            for (int v = 0; v < 3 * RUN / 4; ++v)
                 asm volatile("st.global.v4.f64 [%0], {%1,%2,%3,%4};" ::"l"(dst + 4 * v), "d"(out[4 * v]),
                              "d"(out[4 * v + 1]), "d"(out[4 * v + 2]), "d"(out[4 * v + 3])
                              : "memory");
         } else {
 #pragma unroll
-            for (int e = 0; e < 3 * kRunG; ++e)
+            for (int e = 0; e < 3 * RUN; ++e)
                 if (m0 + e / 3 < a.np) dst[e] = out[e];
         }
         ncl = __reduce_add_sync(0xffffffffu, ncl);
@@ -506,8 +515,13 @@ int launch_interp_pairs_runs(const InterpArgs &a, const float4 *E8, double *E, u
     if (reinterpret_cast<uintptr_t>(E8) % 32) return OSC_E_INVALID;
     auto al = [](const void *p) { return reinterpret_cast<uintptr_t>(p) % 32 == 0; };
     const bool vec = al(a.x) && al(a.y) && al(a.z) && al(E);
-    const int64_t chunks = (a.np + 32 * kRunG - 1) / (32 * kRunG);
-    k_interp_pairs_runs<<<nblocks(chunks * 32, 256, 148 * 16), 256, 0, st>>>(a, E8, vec, E, nclamp);
+    const int run = a.tile == 8 ? 8 : 4;
+    const int64_t chunks = (a.np + 32 * run - 1) / (32 * run);
+    const unsigned nb = nblocks(chunks * 32, 256, 148 * (int64_t)(a.ctas > 0 ? a.ctas : 16));
+    if (run == 8)
+        k_interp_pairs_runs<8><<<nb, 256, 0, st>>>(a, E8, vec, E, nclamp);
+    else
+        k_interp_pairs_runs<4><<<nb, 256, 0, st>>>(a, E8, vec, E, nclamp);
     return ok();
 }
 
@@ -515,7 +529,8 @@ int launch_interp_pairs(const InterpArgs &a, const float4 *E8, double *E, unsign
                         cudaStream_t st) {
     if (a.np <= 0) return OSC_OK;
     if (reinterpret_cast<uintptr_t>(E8) % 32) return OSC_E_INVALID;
-    k_interp_pairs<<<nblocks(a.np, 256, 148 * 64), 256, 0, st>>>(a, E8, E, nclamp);
+    const int64_t cap = 148 * (int64_t)(a.ctas > 0 ? a.ctas : 64);
+    k_interp_pairs<<<nblocks(a.np, 256, cap), 256, 0, st>>>(a, E8, E, nclamp);
     return ok();
 }
 

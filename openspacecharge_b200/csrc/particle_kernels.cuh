@@ -22,6 +22,10 @@ struct DepositArgs {
     double charge1;  // charge per particle when q == nullptr (mode 0)
     int check_finite;
     double fx_scale;  // fixed-point accumulation: units per unit charge
+    // launch shape chosen by the autotuner (0 = built-in default): particles per lane of the
+    // run-aggregated deposits (4 or 8) and CTAs per SM of the per-particle deposit
+    int tile = 0;
+    int ctas = 0;
 };
 // Cell and low-node weights of deposit_particles (mode 0; code/open_spacecharge_mod.f90:
 // 259-269): ip = floor((x-xmin)*dxi + 1) with the product rounded before the add, and
@@ -77,6 +81,10 @@ struct InterpArgs {
     double min[3], delta[3], hinv[3];
     int nlo[3], nhi[3];
     int nx, ny, nz;
+    // launch shape chosen by the autotuner (0 = built-in default): particles per lane of the
+    // cell-ordered gather (4 or 8) and CTAs per SM of the per-particle gather
+    int tile = 0;
+    int ctas = 0;
 };
 template <typename T>
 int launch_interp_vec4(const InterpArgs &a, const void *E4, double *E, unsigned long long *nclamp,

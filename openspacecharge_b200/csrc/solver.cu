@@ -436,6 +436,7 @@ int freespace_opt(osc_ctx *c, const FreeSpaceJob &j, const TIn *rho) {
     ly.out_zstride = 0;
     ly.scale = 1.0;
     ly.flip_mask = 0;
+    ly.nl_div = tune_get(c, std::string("lines_nl_div:") + (sizeof(T) == 4 ? "f32" : "f64") + ":L" + std::to_string(Ny));
     {
         Launch L_(c, "fft_y_fwd");
         TRY(kerr(c, launch_lines<T>(X1, X2, ly, Bin * nz, 1, false, twy, c->stream), "y forward"));

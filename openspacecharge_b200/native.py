@@ -104,6 +104,8 @@ SIGNATURES = {
     "osc_ctx_set_option": [_P, _I, _I64],
     "osc_ctx_get_option": [_P, _I, _PI64],
     "osc_ctx_synchronize": [_P],
+    "osc_ctx_set_tuning": [_P, ctypes.c_char_p, _I],
+    "osc_ctx_get_tuning": [_P, ctypes.c_char_p, ctypes.POINTER(_I)],
     "osc_clear_green_cache": [_P],
     "osc_version": [],
     "osc_profile_reset": [_P],
@@ -216,6 +218,15 @@ class Context:
     def get_option(self, opt: int) -> int:
         v = ctypes.c_int64()
         self.call("osc_ctx_get_option", int(opt), ctypes.byref(v))
+        return int(v.value)
+
+    def set_tuning(self, key: str, value: int) -> None:
+        """Launch shape `key` (see osc_ctx_set_tuning); 0 restores the default."""
+        self.call("osc_ctx_set_tuning", key.encode(), int(value))
+
+    def get_tuning(self, key: str) -> int:
+        v = ctypes.c_int()
+        self.call("osc_ctx_get_tuning", key.encode(), ctypes.byref(v))
         return int(v.value)
 
     def set_stream(self, stream_ptr: int | None) -> None:
