@@ -124,8 +124,8 @@ def make_bunch(npart):
 
 class ClockSampler:
     """SM clock, its maximum and the throttle reasons of one GPU, read during the timed region:
-    through NVML every 5 ms (read-only queries), or from nvidia-smi every 200 ms when NVML
-    cannot be loaded."""
+    through NVML every millisecond (read-only queries), or from nvidia-smi every 200 ms when
+    NVML cannot be loaded."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -177,7 +177,7 @@ class ClockSampler:
                     self.source = "nvidia-smi"
             except Exception:
                 pass
-            self._stop.wait(0.005 if self._nvml else 0.2)
+            self._stop.wait(0.001 if self._nvml else 0.2)
 
     def __enter__(self):
         self._t = threading.Thread(target=self._run, daemon=True)
