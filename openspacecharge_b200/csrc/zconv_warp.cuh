@@ -61,29 +61,6 @@ template <typename T> constexpr int wbuf_len(int L) {
                : (L + L / 8) + ((2 - (L + L / 8)) % 8 + 8) % 8;
 }
 
-// The R-1 twiddles w^r (r = 1..R-1) of one butterfly, w[r] = table[base + r - 1].  For
-// 8-byte (FP32) values the lanes of a warp read distinct twiddles, two shared-memory
-// wavefronts per load, so only w^1 (and w^(R/2) for R >= 8) are loaded and the others formed
-// as products of at most three factors (a few FP32 ulp, like the table's own rounding);
-// 16-byte (FP64) twiddles are all read from the table.
-template <typename V, int R>
-__device__ __forceinline__ void stage_twiddles(const V *tw, int base, int sign, V (&w)[R]) {
-    w[0] = tw_get(tw, base, sign);  // unused slot, keeps the array fully defined
-    if constexpr (sizeof(V) > 8) {
-#pragma unroll
-        for (int r = 1; r < R; ++r) w[r] = tw_get(tw, base + r - 1, sign);
-    } else {
-        w[1] = w[0];
-#pragma unroll
-        for (int r = 2; r < R; ++r) {
-            if (R >= 8 && r == R / 2) w[r] = tw_get(tw, base + r - 1, sign);
-            else if (R >= 8 && r > R / 2) w[r] = cmul(w[R / 2], w[r - R / 2]);
-            else if (r % 2 == 0) w[r] = cmul(w[r / 2], w[r / 2]);
-            else w[r] = cmul(w[r - 1], w[1]);
-        }
-    }
-}
-
 // One stage of one warp's transform: butterflies j = lane + 32q (j < L/R), input elements
 // j + (L/R) r, outputs (j/Ns) Ns R + j%Ns + Ns r; per-stage twiddles at (Ns-1) + k(R-1) + r-1.
 // Padded positions of a butterfly's R elements are a per-lane base plus compile-time
@@ -114,8 +91,6 @@ template <typename V, int R, int L, int Ns, int LDL = 0, int STL = 0> struct WSt
             const int j = lane + 32 * q, k = j % Ns;
             const int pb = wpadl<V, LDL>(j);
             if (full || j < nb) {
-                V w[R];
-                if (Ns > 1) stage_twiddles<V, R>(tw, (Ns - 1) + k * (R - 1), sign, w);
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
                     V x;
@@ -124,7 +99,7 @@ template <typename V, int R, int L, int Ns, int LDL = 0, int STL = 0> struct WSt
                         x.y = 0;
                     } else {
                         x = wb[ld_lin ? pb + r * ld_step : wpadl<V, LDL>(j + r * nb)];
-                        if (r && Ns > 1) x = cmul(x, w[r]);
+                        if (r && Ns > 1) x = cmul(x, tw_get(tw, (Ns - 1) + k * (R - 1) + (r - 1), sign));
                     }
                     v[q][r] = x;
                 }
