@@ -5,7 +5,9 @@ Every choice gives identical results; only the time changes.  The tuned shapes a
 * the deposit tile of the cell-ordered deposits and gathers: particles per lane (4 or 8);
 * the grid size (CTAs per SM) of the per-particle deposit and gather and of the run kernels;
 * the lines per CTA of the y transforms of each doubled length ("lines_nl_div:<prec>:L<n>":
-  the widest tile that fits, or half of it).
+  the widest tile that fits, or half of it);
+* the transform engine of the z pass at doubled length 512 (one exchange per transform with a
+  16 x 32 split, or the radix-8-8-8 warp engine).
 
 ``tune`` times each candidate on the caller's own workload (the FP32 step through the C ABI,
 per-kernel CUDA-event times from the context profile), keeps the fastest in the context and
@@ -77,6 +79,8 @@ def keys_for(grid, order: int, precision: int = PREC_FP32) -> dict:
     ny = 2 * int(grid[1])
     prec = "f32" if precision == PREC_FP32 else "f64"
     ks = {f"lines_nl_div:{prec}:L{ny}": (("fft_y_fwd", "fft_y_inv"), [1, 2])}
+    if precision == PREC_FP32 and 2 * int(grid[2]) == 512:
+        ks["zconv_engine:f32:L512"] = (("fft_z_conv",), [0, 1])
     if order == ORDER_ANY:
         ks["deposit_ctas_per_sm"] = (("deposit_f32",), CTAS)
         ks["gather_ctas_per_sm"] = (("interp_f32",), CTAS)

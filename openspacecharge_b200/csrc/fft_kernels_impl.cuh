@@ -18,6 +18,7 @@
 
 #include "fft_kernels.cuh"
 #include "zconv_warp.cuh"
+#include "zconv_w512.cuh"
 
 namespace osc {
 
@@ -821,6 +822,17 @@ template <typename T> inline bool zconv_can_stage(const ZConvArgs &a) {
     return zconv_warp_smem<T>(a.p.L, zw_warps<T>(), ZW_STAGED, ns, zp) <= 100 * 1024;
 }
 
+inline int launch_zconv_w512(const float2 *in, float2 *out, const ZConvArgs &a, const float2 *rt, cudaStream_t st) {
+    constexpr int W = 4;
+    const size_t sm = zconv_w512_smem<W>(a.nout, a.g[0].zpitch);
+    auto kern = k_zconv_w512<W>;
+    int rc = set_smem(kern, sm);
+    if (rc) return rc;
+    const dim3 grid((unsigned)ceil_div(a.ncols, W), (unsigned)(a.nbatch > 0 ? a.nbatch : 1));
+    kern<<<grid, W * 32, sm, st>>>(in, out, a, rt);
+    return launch_ok();
+}
+
 template <typename T>
 int launch_zconv(const cplx<T> *in, cplx<T> *out, const ZConvArgs &a, const TwPair<cplx<T>> &tw, int nl,
                  cudaStream_t st) {
@@ -833,6 +845,11 @@ int launch_zconv(const cplx<T> *in, cplx<T> *out, const ZConvArgs &a, const TwPa
         if (tw.wt == tw.rt) return OSC_E_INVALID;
         const bool staged = !img && zconv_can_stage<T>(a);
         if (a.nsum > 0 && (img || !staged || a.nout != 1)) return OSC_E_UNSUPPORTED;
+        if constexpr (sizeof(T) == 4) {
+            if (L == 512 && staged && a.nsum == 0 && a.out_estride == 1 && a.engine != 1 &&
+                zconv_w512_smem<4>(a.nout, a.g[0].zpitch) <= 100 * 1024)
+                return launch_zconv_w512(in, out, a, tw.rt, st);
+        }
         return dispatch_warp_len(L, [&](auto eng) -> int {
             using E = decltype(eng);
             if constexpr (E::kLen > 0) {

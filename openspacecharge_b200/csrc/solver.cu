@@ -459,6 +459,7 @@ int freespace_opt(osc_ctx *c, const FreeSpaceJob &j, const TIn *rho) {
     za.img_phase_mul = nz - 1;
     za.ng = gs->nspec;
     za.fault = c->d_fault;
+    za.engine = tune_get(c, "zconv_engine:" + std::string(sizeof(T) == 4 ? "f32" : "f64") + ":L" + std::to_string(Nz));
     if (c->test_wait_timeout) {  // test only: waits that must run out quickly
         za.poll_limit = 64;
         za.skip_copies = 1;

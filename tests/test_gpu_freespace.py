@@ -98,3 +98,22 @@ def test_green_cache_reuse_is_exact(ctx, oracle):
     ctx.clear_green_cache()
     c, _ = osc.osc_freespace_solver2(ctx, rho, 3.0, delta, precision=osc.PREC_FP32)
     assert np.array_equal(a, c)
+
+
+@pytest.mark.parametrize("n", [(16, 12, 256), (24, 20, 256)])
+def test_z_pass_engines_at_length_512_agree_with_oracle(oracle, n):
+    """Doubled z length 512 with staged Green spectra has two FP32 engines: one exchange per
+    transform (16 x 32 split with a radix-2 lane-pair shuffle, the default) and the radix-8
+    warp engine; both must match the oracle, and each other to FP32 round-off."""
+    rho, delta, _, _ = make_rho(oracle, n, sigma=(1e-3, 1e-3, 3e-3))
+    gamma = 9.784756683727565
+    e_ref, _ = oracle.freespace_solver2(rho, gamma, delta)
+    out = []
+    with osc.Context(0) as c:
+        for engine in (0, 1):
+            c.set_tuning("zconv_engine:f32:L512", engine)
+            e, _ = osc.osc_freespace_solver2(c, rho, gamma, delta, precision=osc.PREC_FP32)
+            mx, rm = field_err(e, e_ref)
+            assert mx <= 1e-5 and rm <= 1e-5, (engine, mx, rm)
+            out.append(e)
+    assert field_err(out[0], out[1])[0] <= 2e-6

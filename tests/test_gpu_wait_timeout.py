@@ -25,7 +25,8 @@ def _rho(oracle, n):
     return rho, delta
 
 
-@pytest.mark.parametrize("n", [(16, 16, 64), (24, 20, 128)])  # z lengths 128 and 256: staged warp z pass
+# z lengths 128 and 256: the radix-8 warp engine; 512: the one-exchange engine
+@pytest.mark.parametrize("n", [(16, 16, 64), (24, 20, 128), (12, 12, 256)])
 def test_z_pass_wait_times_out_then_context_recovers(oracle, n):
     rho, delta = _rho(oracle, n)
     gamma = 2.5
