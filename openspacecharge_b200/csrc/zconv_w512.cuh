@@ -13,8 +13,11 @@
 //   inverse (sign -1), the mirror image: the radix-2 combination of the partner lanes, a
 //   16-point DFT, the twiddles w512^(-(2a+c) k1), one exchange, a 16-point DFT, after which
 //   lane l holds z = l + 32 n1 and stores n1 < 8 (the window z < 256) of its column.
-// Per column that is one exchange per transform instead of two, and no per-stage twiddle
-// table: the w32 factors are constants, the lane twiddles come from the 512-entry table.
+// Per column that is one exchange per transform instead of two.  The w32 factors are
+// constants; the lane twiddles of both transforms are tabulated per CTA lane-contiguous
+// (tf[k1][lane] = w512^(lane k1), ti[a][t] = w512^(-(2a + t/16)(t mod 16))), so that a warp
+// reads 32 consecutive entries per twiddle -- read from the plain 512-entry table, the
+// strides lane*k1 would fall on few banks.
 #pragma once
 
 #include "zconv_warp.cuh"
@@ -47,8 +50,9 @@ __device__ __forceinline__ float2 shfl_xor2(float2 v, int m) {
 }
 
 // Forward transform of this warp's column (buffer wb holds x[z], z < 256, linearly);
-// returns in s[k] the spectrum at kz = (lane & 15) + 16 k + 256 (lane >> 4).
-__device__ __forceinline__ void w512_forward(float2 *wb, const float2 *__restrict__ tw, int lane, float2 (&s)[16]) {
+// returns in s[k] the spectrum at kz = (lane & 15) + 16 k + 256 (lane >> 4).  tf: the
+// forward lane twiddles, [k1][lane].
+__device__ __forceinline__ void w512_forward(float2 *wb, const float2 *__restrict__ tf, int lane, float2 (&s)[16]) {
     float2 v[16];
 #pragma unroll
     for (int m = 0; m < 8; ++m) v[m] = wb[lane + 32 * m];
@@ -56,7 +60,7 @@ __device__ __forceinline__ void w512_forward(float2 *wb, const float2 *__restric
     for (int m = 8; m < 16; ++m) v[m] = make_float2(0.f, 0.f);
     Dft<16>::run(v, +1);
 #pragma unroll
-    for (int k1 = 1; k1 < 16; ++k1) v[k1] = cmul(v[k1], tw[(lane * k1) & 511]);
+    for (int k1 = 1; k1 < 16; ++k1) v[k1] = cmul(v[k1], tf[k1 * 32 + lane]);
     __syncwarp();
 #pragma unroll
     for (int k1 = 0; k1 < 16; ++k1) wb[k1 * W5_PITCH + lane] = v[k1];
@@ -76,8 +80,9 @@ __device__ __forceinline__ void w512_forward(float2 *wb, const float2 *__restric
 }
 
 // Inverse transform of a spectrum in the layout w512_forward returns; stores the window
-// z < 256 of the result at dst[z] (when store is set).
-__device__ __forceinline__ void w512_inverse(float2 *wb, const float2 *__restrict__ tw, int lane, float2 (&s)[16],
+// z < 256 of the result at dst[z] (when store is set).  ti: the inverse lane twiddles,
+// [a][lane].
+__device__ __forceinline__ void w512_inverse(float2 *wb, const float2 *__restrict__ ti, int lane, float2 (&s)[16],
                                              float2 *__restrict__ dst, bool store) {
     const int k1 = lane & 15, c = lane >> 4;
     float2 v[16];
@@ -95,10 +100,7 @@ __device__ __forceinline__ void w512_inverse(float2 *wb, const float2 *__restric
     Dft<16>::run(v, -1);
     // V[a] at n2 = 2a + c, times w512^(-n2 k1)
 #pragma unroll
-    for (int a = 0; a < 16; ++a) {
-        const float2 w = tw[((2 * a + c) * k1) & 511];
-        v[a] = cmul(v[a], make_float2(w.x, -w.y));
-    }
+    for (int a = 0; a < 16; ++a) v[a] = cmul(v[a], ti[a * 32 + lane]);
     __syncwarp();
 #pragma unroll
     for (int a = 0; a < 16; ++a) wb[k1 * W5_PITCH + 2 * a + c] = v[a];
@@ -122,8 +124,9 @@ __global__ void __launch_bounds__(W * 32, 5) k_zconv_w512(const float2 *__restri
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ uint64_t gbar;
     __shared__ int gfail;
-    float2 *tw = reinterpret_cast<float2 *>(smem_raw);
-    float2 *wbufs = tw + L;
+    float2 *tf = reinterpret_cast<float2 *>(smem_raw);  // [16][32]; row 0 unused
+    float2 *ti = tf + 16 * 32;                            // [16][32]
+    float2 *wbufs = ti + 16 * 32;
     float *gst = reinterpret_cast<float *>(wbufs + W * W5_BUF);  // Green columns [W][nout][zpitch]
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int col0 = blockIdx.x * W;
@@ -147,7 +150,12 @@ __global__ void __launch_bounds__(W * 32, 5) k_zconv_w512(const float2 *__restri
             }
         }
     }
-    for (int m = threadIdx.x; m < L; m += W * 32) tw[m] = tw_rt[m];
+    for (int m = threadIdx.x; m < 16 * 32; m += W * 32) {
+        const int r = m >> 5, t = m & 31;
+        tf[m] = tw_rt[(t * r) & (L - 1)];
+        const float2 w = tw_rt[((2 * r + (t >> 4)) * (t & 15)) & (L - 1)];
+        ti[m] = make_float2(w.x, -w.y);
+    }
     // the non-zero half (z < nz) of the W columns, coalesced across the columns
     for (int idx = threadIdx.x; idx < W * a.nz; idx += W * 32) {
         const int e = idx / W, cc = idx - e * W;
@@ -158,7 +166,7 @@ __global__ void __launch_bounds__(W * 32, 5) k_zconv_w512(const float2 *__restri
     }
     __syncthreads();
     float2 s[16];
-    w512_forward(wb, tw, lane, s);
+    w512_forward(wb, tf, lane, s);
     // CTA-wide wait for the staged Green columns (bounded; a give-up is reported)
     if (threadIdx.x == 0) {
         const bool ok = mbar_wait_bounded(&gbar, 0, a.poll_limit);
@@ -195,12 +203,12 @@ __global__ void __launch_bounds__(W * 32, 5) k_zconv_w512(const float2 *__restri
             v[k] = iu ? make_float2(-x.y * sv, x.x * sv) : make_float2(x.x * sv, x.y * sv);
         }
         float2 *dst = out + (int64_t)o * a.out_cstride + (int64_t)(col0 + warp) * a.out_colstride;
-        w512_inverse(wb, tw, lane, v, dst, live);
+        w512_inverse(wb, ti, lane, v, dst, live);
     }
 }
 
 template <int W> inline size_t zconv_w512_smem(int nout, int zp) {
-    return sizeof(float2) * (512 + (size_t)W * W5_BUF) + sizeof(float) * (size_t)W * nout * zp;
+    return sizeof(float2) * (2 * 16 * 32 + (size_t)W * W5_BUF) + sizeof(float) * (size_t)W * nout * zp;
 }
 
 }  // namespace osc
