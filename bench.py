@@ -66,6 +66,8 @@ def parse():
     ap.add_argument("--no-refit", action="store_true", help="skip the refit + Green rebuild leg")
     ap.add_argument("--no-order", action="store_true", help="skip the cell-sorted particle-order legs")
     ap.add_argument("--no-tune", action="store_true", help="built-in launch shapes instead of autotuned ones")
+    ap.add_argument("--tuning", action="append", default=[], metavar="KEY=VALUE",
+                    help="set a launch-shape key (osc_ctx_set_tuning) before the run; implies --no-tune")
     ap.add_argument("--workload", default="single", choices=["single", "batch", "adjoint", "pipe"],
                     help="single: the headline one-bunch step; batch: 256 bunches of mixed grids per step; "
                          "adjoint: forward + backward of sum q|E|^2 at 128^3, 4e6 particles; "
@@ -337,6 +339,12 @@ def run_ours(args, ws, rank, local, dist):
 
     # launch shapes from the project's autotuner, timed on this workload before the timed region
     tuned = None
+    for kv in args.tuning:
+        key, val = kv.split("=", 1)
+        ctx.set_tuning(key, int(val))
+    if args.tuning:
+        args.no_tune = True
+        tuned = {kv.split("=", 1)[0]: {"value": int(kv.split("=", 1)[1]), "set": "--tuning"} for kv in args.tuning}
     if not args.no_tune:
         from openspacecharge_b200 import autotune
         tuned = autotune.tune(ctx, lambda: step(osc.PREC_FP32), grid, order=osc.ORDER_ANY, device=local,

@@ -14,10 +14,11 @@
 //   16-point DFT, the twiddles w512^(-(2a+c) k1), one exchange, a 16-point DFT, after which
 //   lane l holds z = l + 32 n1 and stores n1 < 8 (the window z < 256) of its column.
 // Per column that is one exchange per transform instead of two.  The w32 factors are
-// constants; the lane twiddles of both transforms are tabulated per CTA lane-contiguous
-// (tf[k1][lane] = w512^(lane k1), ti[a][t] = w512^(-(2a + t/16)(t mod 16))), so that a warp
-// reads 32 consecutive entries per twiddle -- read from the plain 512-entry table, the
-// strides lane*k1 would fall on few banks.
+// constants; the lane twiddles of both transforms come from one table per CTA,
+// tf[k1][l] = w512^(l k1) with rows 33 entries apart: the forward reads a row (32
+// consecutive entries), the inverse reads w512^((2a + c) k1) = tf[k1][2a + c] across the rows,
+// which the odd pitch spreads over distinct banks -- read from the plain 512-entry table, the
+// strides l*k1 would fall on few banks.
 #pragma once
 
 #include "zconv_warp.cuh"
@@ -53,6 +54,7 @@ __device__ __forceinline__ float2 shfl_xor2(float2 v, int m) {
 // returns in s[k] the spectrum at kz = (lane & 15) + 16 k + 256 (lane >> 4).  tf: the
 // forward lane twiddles, [k1][lane].
 __device__ __forceinline__ void w512_forward(float2 *wb, const float2 *__restrict__ tf, int lane, float2 (&s)[16]) {
+    constexpr int P = W5_PITCH;
     float2 v[16];
 #pragma unroll
     for (int m = 0; m < 8; ++m) v[m] = wb[lane + 32 * m];
@@ -60,7 +62,7 @@ __device__ __forceinline__ void w512_forward(float2 *wb, const float2 *__restric
     for (int m = 8; m < 16; ++m) v[m] = make_float2(0.f, 0.f);
     Dft<16>::run(v, +1);
 #pragma unroll
-    for (int k1 = 1; k1 < 16; ++k1) v[k1] = cmul(v[k1], tf[k1 * 32 + lane]);
+    for (int k1 = 1; k1 < 16; ++k1) v[k1] = cmul(v[k1], tf[k1 * P + lane]);
     __syncwarp();
 #pragma unroll
     for (int k1 = 0; k1 < 16; ++k1) wb[k1 * W5_PITCH + lane] = v[k1];
@@ -80,27 +82,25 @@ __device__ __forceinline__ void w512_forward(float2 *wb, const float2 *__restric
 }
 
 // Inverse transform of a spectrum in the layout w512_forward returns; stores the window
-// z < 256 of the result at dst[z] (when store is set).  ti: the inverse lane twiddles,
-// [a][lane].
-__device__ __forceinline__ void w512_inverse(float2 *wb, const float2 *__restrict__ ti, int lane, float2 (&s)[16],
+// z < 256 of the result at dst[z] (when store is set).  tf: the twiddle table of
+// w512_forward, read conjugated.
+__device__ __forceinline__ void w512_inverse(float2 *wb, const float2 *__restrict__ tf, int lane, float2 (&s)[16],
                                              float2 *__restrict__ dst, bool store) {
     const int k1 = lane & 15, c = lane >> 4;
     float2 v[16];
     // U[k] = X[k] + X[k+16] (c = 0), (X[k] - X[k+16]) w32^-k (c = 1)
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
+        // branch-free: the two half warps take different sides of the butterfly
         const float2 p = shfl_xor2(s[k], 16);
-        if (c) {
-            const float2 d = csub(p, s[k]);
-            v[k] = cmul(d, make_float2(w32c(k), -w32s(k)));
-        } else {
-            v[k] = cadd(s[k], p);
-        }
+        const float2 d = c ? csub(p, s[k]) : cadd(s[k], p);
+        const float2 w = c ? make_float2(w32c(k), -w32s(k)) : make_float2(1.f, 0.f);
+        v[k] = cmul(d, w);
     }
     Dft<16>::run(v, -1);
     // V[a] at n2 = 2a + c, times w512^(-n2 k1)
 #pragma unroll
-    for (int a = 0; a < 16; ++a) v[a] = cmul(v[a], ti[a * 32 + lane]);
+    for (int a = 0; a < 16; ++a) v[a] = cmulc(v[a], tf[k1 * W5_PITCH + 2 * a + c]);
     __syncwarp();
 #pragma unroll
     for (int a = 0; a < 16; ++a) wb[k1 * W5_PITCH + 2 * a + c] = v[a];
@@ -118,15 +118,14 @@ __device__ __forceinline__ void w512_inverse(float2 *wb, const float2 *__restric
 // column, W warps per CTA; the arguments and outputs are those of
 // k_zconv_warp<float, W, ZW_STAGED, 512, ...> with a kz-innermost output.
 template <int W>
-__global__ void __launch_bounds__(W * 32, 5) k_zconv_w512(const float2 *__restrict__ in, float2 *__restrict__ out,
+__global__ void __launch_bounds__(W * 32, 6) k_zconv_w512(const float2 *__restrict__ in, float2 *__restrict__ out,
                                                           ZConvArgs a, const float2 *__restrict__ tw_rt) {
     constexpr int L = 512;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ uint64_t gbar;
     __shared__ int gfail;
-    float2 *tf = reinterpret_cast<float2 *>(smem_raw);  // [16][32]; row 0 unused
-    float2 *ti = tf + 16 * 32;                            // [16][32]
-    float2 *wbufs = ti + 16 * 32;
+    float2 *tf = reinterpret_cast<float2 *>(smem_raw);  // [16][W5_PITCH]: w512^(l k1)
+    float2 *wbufs = tf + 16 * W5_PITCH;
     float *gst = reinterpret_cast<float *>(wbufs + W * W5_BUF);  // Green columns [W][nout][zpitch]
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int col0 = blockIdx.x * W;
@@ -152,9 +151,7 @@ __global__ void __launch_bounds__(W * 32, 5) k_zconv_w512(const float2 *__restri
     }
     for (int m = threadIdx.x; m < 16 * 32; m += W * 32) {
         const int r = m >> 5, t = m & 31;
-        tf[m] = tw_rt[(t * r) & (L - 1)];
-        const float2 w = tw_rt[((2 * r + (t >> 4)) * (t & 15)) & (L - 1)];
-        ti[m] = make_float2(w.x, -w.y);
+        tf[r * W5_PITCH + t] = tw_rt[(t * r) & (L - 1)];
     }
     // the non-zero half (z < nz) of the W columns, coalesced across the columns
     for (int idx = threadIdx.x; idx < W * a.nz; idx += W * 32) {
@@ -191,24 +188,20 @@ __global__ void __launch_bounds__(W * 32, 5) k_zconv_w512(const float2 *__restri
 #pragma unroll
         for (int k = 0; k < 16; ++k) {
             const int kz = k1 + 16 * k + 256 * c;
-            float sv;
-            if (c == 0) {
-                sv = gc[kz];
-            } else {  // kz >= nz: the value at L - kz, odd spectra change sign (kz = nz excepted)
-                sv = gc[L - kz];
-                if (zodd && kz != a.nz) sv = -sv;
-            }
-            if (yneg) sv = -sv;
+            // kz >= nz (c = 1): the value at L - kz, odd spectra change sign (kz = nz excepted)
+            float sv = gc[c ? L - kz : kz];
+            const bool neg = (c && zodd && kz != a.nz) != yneg;
+            sv = neg ? -sv : sv;
             const float2 x = s[k];
             v[k] = iu ? make_float2(-x.y * sv, x.x * sv) : make_float2(x.x * sv, x.y * sv);
         }
         float2 *dst = out + (int64_t)o * a.out_cstride + (int64_t)(col0 + warp) * a.out_colstride;
-        w512_inverse(wb, ti, lane, v, dst, live);
+        w512_inverse(wb, tf, lane, v, dst, live);
     }
 }
 
 template <int W> inline size_t zconv_w512_smem(int nout, int zp) {
-    return sizeof(float2) * (2 * 16 * 32 + (size_t)W * W5_BUF) + sizeof(float) * (size_t)W * nout * zp;
+    return sizeof(float2) * (16 * W5_PITCH + (size_t)W * W5_BUF) + sizeof(float) * (size_t)W * nout * zp;
 }
 
 }  // namespace osc
