@@ -129,8 +129,8 @@ OSC_API int osc_ctx_synchronize(osc_ctx *ctx);
  *     (4, 8, 16, 32, 64 or 128);
  *   "lines_nl_div:<f32|f64>:L<length>": 2 halves the lines per CTA of the y transforms of
  *     that doubled length;
- *   "zconv_engine:f32:L512": 1 runs the z pass of doubled z length 512 on the radix-8 warp
- *     engine instead of the one-exchange 16 x 32 engine.
+ *   "zconv_engine:f32:L512": 1 runs the z pass of doubled z length 512 on the one-exchange
+ *     16 x 32 engine instead of the radix-8 warp engine.
  * Results are identical for every choice; only the time changes. */
 OSC_API int osc_ctx_set_tuning(osc_ctx *ctx, const char *key, int value);
 OSC_API int osc_ctx_get_tuning(osc_ctx *ctx, const char *key, int *value);

@@ -6,8 +6,8 @@ Every choice gives identical results; only the time changes.  The tuned shapes a
 * the grid size (CTAs per SM) of the per-particle deposit and gather and of the run kernels;
 * the lines per CTA of the y transforms of each doubled length ("lines_nl_div:<prec>:L<n>":
   the widest tile that fits, or half of it);
-* the transform engine of the z pass at doubled length 512 (one exchange per transform with a
-  16 x 32 split, or the radix-8-8-8 warp engine).
+* the transform engine of the z pass at doubled length 512 (the radix-8-8-8 warp engine, or
+  one exchange per transform with a 16 x 32 split).
 
 ``tune`` times each candidate on the caller's own workload (the FP32 step through the C ABI,
 per-kernel CUDA-event times from the context profile), keeps the fastest in the context and

@@ -123,8 +123,8 @@ struct ZConvArgs {
     unsigned poll_limit;  // polls of a bounded mbarrier wait (0: MBAR_POLL_LIMIT)
     int skip_copies;      // test only: arm the Green-column barrier but issue no bulk copy,
                           // so the bounded wait runs out and the fault path is exercised
-    int engine;           // FP32 length 512, staged spectra: 0 the one-exchange 16 x 32
-                          // engine, 1 the radix-8 warp engine (autotuner key zconv_engine)
+    int engine;           // FP32 length 512, staged spectra: 0 the radix-8 warp engine, 1 the
+                          // one-exchange 16 x 32 engine (autotuner key zconv_engine)
     // batches of equal grids (blockIdx.y = member): input, output and spectrum offsets of
     // member b are b*in_bstride, b*out_bstride and b*g_bstride (elements of the spectrum)
     int nbatch;

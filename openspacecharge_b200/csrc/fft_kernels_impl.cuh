@@ -846,7 +846,7 @@ int launch_zconv(const cplx<T> *in, cplx<T> *out, const ZConvArgs &a, const TwPa
         const bool staged = !img && zconv_can_stage<T>(a);
         if (a.nsum > 0 && (img || !staged || a.nout != 1)) return OSC_E_UNSUPPORTED;
         if constexpr (sizeof(T) == 4) {
-            if (L == 512 && staged && a.nsum == 0 && a.out_estride == 1 && a.engine != 1 &&
+            if (L == 512 && staged && a.nsum == 0 && a.out_estride == 1 && a.engine == 1 &&
                 zconv_w512_smem<4>(a.nout, a.g[0].zpitch) <= 100 * 1024)
                 return launch_zconv_w512(in, out, a, tw.rt, st);
         }

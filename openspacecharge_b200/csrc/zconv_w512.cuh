@@ -1,5 +1,6 @@
 // zconv_w512.cuh -- the z pass at length 512 (FP32, staged real Green spectra) with one
-// shared-memory exchange per transform.
+// shared-memory exchange per transform: an alternative engine the autotuner may pick
+// (tuning key zconv_engine:f32:L512 = 1).
 //
 // The radix-8 warp engine (zconv_warp.cuh) moves every value of a 512-point column through
 // shared memory twice per transform.  Here a transform is 512 = 16 x 32:

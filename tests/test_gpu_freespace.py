@@ -102,9 +102,9 @@ def test_green_cache_reuse_is_exact(ctx, oracle):
 
 @pytest.mark.parametrize("n", [(16, 12, 256), (24, 20, 256)])
 def test_z_pass_engines_at_length_512_agree_with_oracle(oracle, n):
-    """Doubled z length 512 with staged Green spectra has two FP32 engines: one exchange per
-    transform (16 x 32 split with a radix-2 lane-pair shuffle, the default) and the radix-8
-    warp engine; both must match the oracle, and each other to FP32 round-off."""
+    """Doubled z length 512 with staged Green spectra has two FP32 engines: the radix-8 warp
+    engine (the default) and one exchange per transform (16 x 32 split with a radix-2
+    lane-pair shuffle); both must match the oracle, and each other to FP32 round-off."""
     rho, delta, _, _ = make_rho(oracle, n, sigma=(1e-3, 1e-3, 3e-3))
     gamma = 9.784756683727565
     e_ref, _ = oracle.freespace_solver2(rho, gamma, delta)
