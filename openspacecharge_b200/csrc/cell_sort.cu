@@ -215,24 +215,20 @@ __device__ __forceinline__ void two_sum_add(float &s, float &c, float v) {
     c += e;
 }
 
-template <int kRun>
-__global__ void __launch_bounds__(256) k_deposit_quad_runs(DepositArgs a, float4 *__restrict__ quad, bool vec,
+template <int kRun, bool HQ>
+__global__ void __launch_bounds__(256, kRun == 4 ? 3 : 2) k_deposit_quad_runs(DepositArgs a, float4 *__restrict__ quad, bool vec,
                                                            unsigned long long *__restrict__ counters) {
     const int64_t plane = (int64_t)a.nx * a.ny;
     const int lane = threadIdx.x & 31;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w * 32 * kRun < a.np; w += nwarps) {
         const int64_t m0 = (w * 32 + lane) * kRun;
-        double xs[kRun], ys[kRun], zs[kRun], qs[kRun];
+        // HQ: charges per particle; otherwise every particle carries a.charge1
+        double xs[kRun], ys[kRun], zs[kRun], qs[HQ ? kRun : 1];
         load_run<kRun>(a.x, m0, a.np, vec, xs);
         load_run<kRun>(a.y, m0, a.np, vec, ys);
         load_run<kRun>(a.z, m0, a.np, vec, zs);
-        if (a.q) {
-            load_run<kRun>(a.q, m0, a.np, vec, qs);
-        } else {
-#pragma unroll
-            for (int t = 0; t < kRun; ++t) qs[t] = a.charge1;
-        }
+        if constexpr (HQ) load_run<kRun>(a.q, m0, a.np, vec, qs);
         int64_t cur = -1;
         float s[8], c[8];
         int nout = 0, nbad = 0;
@@ -248,7 +244,8 @@ __global__ void __launch_bounds__(256) k_deposit_quad_runs(DepositArgs a, float4
             }
             // the quad contributions of deposit_particles' weights (code/open_spacecharge_mod.f90:274-281)
             const double omab = 1. - cc.ab, omde = 1. - cc.de, omgh = 1. - cc.gh;
-            const double lo = cc.gh * qs[t], hi = omgh * qs[t];
+            const double qm = HQ ? qs[HQ ? t : 0] : a.charge1;
+            const double lo = cc.gh * qm, hi = omgh * qm;
             const float v[8] = {(float)(cc.ab * cc.de * lo), (float)(omab * cc.de * lo), (float)(cc.ab * omde * lo),
                                 (float)(omab * omde * lo),   (float)(cc.ab * cc.de * hi), (float)(omab * cc.de * hi),
                                 (float)(cc.ab * omde * hi),  (float)(omab * omde * hi)};
@@ -291,10 +288,14 @@ int launch_deposit_quad_runs(const DepositArgs &a, float *quad, unsigned long lo
     const int run = a.tile == 8 ? 8 : 4;
     const int64_t chunks = (a.np + 32 * run - 1) / (32 * run);
     const unsigned nb = nblocks(chunks * 32, 256, 148 * (int64_t)(a.ctas > 0 ? a.ctas : 16));
-    if (run == 8)
-        k_deposit_quad_runs<8><<<nb, 256, 0, st>>>(a, reinterpret_cast<float4 *>(quad), vec, counters);
-    else
-        k_deposit_quad_runs<4><<<nb, 256, 0, st>>>(a, reinterpret_cast<float4 *>(quad), vec, counters);
+    float4 *q4 = reinterpret_cast<float4 *>(quad);
+    if (run == 8) {
+        if (a.q) k_deposit_quad_runs<8, true><<<nb, 256, 0, st>>>(a, q4, vec, counters);
+        else k_deposit_quad_runs<8, false><<<nb, 256, 0, st>>>(a, q4, vec, counters);
+    } else {
+        if (a.q) k_deposit_quad_runs<4, true><<<nb, 256, 0, st>>>(a, q4, vec, counters);
+        else k_deposit_quad_runs<4, false><<<nb, 256, 0, st>>>(a, q4, vec, counters);
+    }
     return ok();
 }
 

@@ -442,7 +442,7 @@ __device__ __forceinline__ void ldg_v4(const double *p, double *v) {
     asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3]) : "l"(p));
 }
 template <int RUN>
-__global__ void __launch_bounds__(256) k_interp_pairs_runs(InterpArgs a, const float4 *__restrict__ g8, bool vec,
+__global__ void __launch_bounds__(256, RUN == 4 ? 3 : 2) k_interp_pairs_runs(InterpArgs a, const float4 *__restrict__ g8, bool vec,
                                                            double *__restrict__ E,
                                                            unsigned long long *__restrict__ nclamp) {
     static_assert(RUN % 4 == 0, "runs of whole 256-bit vectors");
