@@ -128,7 +128,8 @@ OSC_API int osc_ctx_synchronize(osc_ctx *ctx);
  *   "gather_runs_ctas_per_sm": grid size of the per-particle and run kernels, CTAs per SM
  *     (4, 8, 16, 32, 64 or 128);
  *   "lines_nl_div:<f32|f64>:L<length>": 2 halves the lines per CTA of the y transforms of
- *     that doubled length;
+ *     that doubled length; "r2c_nl_div:..." and "c2r_nl_div:..." the rows per CTA of the
+ *     forward and inverse x transforms;
  *   "zconv_engine:f32:L512": 1 runs the z pass of doubled z length 512 on the one-exchange
  *     16 x 32 engine instead of the radix-8 warp engine.
  * Results are identical for every choice; only the time changes. */

@@ -5,7 +5,8 @@ Every choice gives identical results; only the time changes.  The tuned shapes a
 * the deposit tile of the cell-ordered deposits and gathers: particles per lane (4 or 8);
 * the grid size (CTAs per SM) of the per-particle deposit and gather and of the run kernels;
 * the lines per CTA of the y transforms of each doubled length ("lines_nl_div:<prec>:L<n>":
-  the widest tile that fits, or half of it);
+  the widest tile that fits, or half of it), and the rows per CTA of the x transforms
+  ("r2c_nl_div", "c2r_nl_div");
 * the transform engine of the z pass at doubled length 512 (the radix-8-8-8 warp engine, or
   one exchange per transform with a 16 x 32 split).
 
@@ -78,7 +79,10 @@ def keys_for(grid, order: int, precision: int = PREC_FP32) -> dict:
     profile labels of the kernels it changes and its candidates."""
     ny = 2 * int(grid[1])
     prec = "f32" if precision == PREC_FP32 else "f64"
-    ks = {f"lines_nl_div:{prec}:L{ny}": (("fft_y_fwd", "fft_y_inv"), [1, 2])}
+    nx = 2 * int(grid[0])
+    ks = {f"lines_nl_div:{prec}:L{ny}": (("fft_y_fwd", "fft_y_inv"), [1, 2]),
+          f"r2c_nl_div:{prec}:L{nx}": (("fft_x_r2c",), [1, 2]),
+          f"c2r_nl_div:{prec}:L{nx}": (("fft_x_c2r",), [1, 2])}
     if precision == PREC_FP32 and 2 * int(grid[2]) == 512:
         ks["zconv_engine:f32:L512"] = (("fft_z_conv",), [0, 1])
     if order == ORDER_ANY:

@@ -135,7 +135,8 @@ static bool tuning_value_ok(const std::string &key, int v) {
     if (key == "deposit_ctas_per_sm" || key == "gather_ctas_per_sm" || key == "deposit_runs_ctas_per_sm" ||
         key == "gather_runs_ctas_per_sm")
         return v == 0 || v == 4 || v == 8 || v == 16 || v == 32 || v == 64 || v == 128;
-    if (key.rfind("lines_nl_div:", 0) == 0) return v == 0 || v == 1 || v == 2;
+    if (key.rfind("lines_nl_div:", 0) == 0 || key.rfind("r2c_nl_div:", 0) == 0 || key.rfind("c2r_nl_div:", 0) == 0)
+        return v == 0 || v == 1 || v == 2;
     if (key.rfind("zconv_engine:", 0) == 0) return v == 0 || v == 1;
     return false;
 }

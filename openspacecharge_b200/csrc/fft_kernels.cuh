@@ -31,6 +31,7 @@ struct R2CArgs {
     int64_t in_rstride;   // elements between rows of the real input
     int64_t out_rstride;  // complex elements between output rows
     int qny = 0;          // quad-grid input (float4): rows per plane, for the node sum's y neighbour
+    int nl_div = 0;       // autotuner: 2 halves the rows per CTA (0/1: default)
 };
 
 // Where the real result of one inverse component goes.
@@ -64,6 +65,7 @@ struct C2RArgs {
     // member and zin_ny rows y; row r = (b*ny + y)*nz + z starts at (b*ny + y)*(nx+1)*nz + z
     // with elements nz apart and goes to grid row (b*nz + z)*ny + y ([z][y][x] per member).
     int zin, zin_nz, zin_ny;
+    int nl_div;           // autotuner: 2 halves the rows per CTA (0/1: default)
 };
 
 // Stored Green spectrum of one kernel component on the half-spectrum grid

@@ -731,7 +731,7 @@ int launch_r2c_rows(const TIn *in, cplx<T> *out, const R2CArgs &a, const TwPair<
                 kern<<<nblk, nt, sm, st>>>(in, out, a, twe);
             }
             return launch_ok();
-        });
+        }, a.nl_div);
     });
 }
 
@@ -747,14 +747,21 @@ int launch_c2r_rows(const cplx<T> *in, const C2RArgs &a, const TwPair<cplx<T>> &
             const int rc = dispatch_fft_len<T>(L, [&](auto eng) -> int {
                 using E = decltype(eng);
                 if constexpr (E::kLen > 0) {
+                    auto go = [&](auto nlcc) -> int {
+                        constexpr int NLC = decltype(nlcc)::value;
+                        constexpr int nt = E::kLen * 3 * NLC / E::kEPT;
+                        const size_t sm = sizeof(cplx<T>) * ((size_t)E::kLen + (size_t)E::kLen * (3 * NLC + 1));
+                        auto kern = k_c2r_e8<T, NLC, E>;
+                        int r = set_smem(kern, sm);
+                        if (r) return r;
+                        kern<<<(unsigned)ceil_div(a.nrows, 2 * NLC), nt, sm, st>>>(in, a, tw.st);
+                        return launch_ok();
+                    };
                     constexpr int NLC = c2r_e8_nlc<T, E>();
-                    constexpr int nt = E::kLen * 3 * NLC / E::kEPT;
-                    const size_t sm = sizeof(cplx<T>) * ((size_t)E::kLen + (size_t)E::kLen * (3 * NLC + 1));
-                    auto kern = k_c2r_e8<T, NLC, E>;
-                    int r = set_smem(kern, sm);
-                    if (r) return r;
-                    kern<<<(unsigned)ceil_div(a.nrows, 2 * NLC), nt, sm, st>>>(in, a, tw.st);
-                    return launch_ok();
+                    // the autotuner's alternative tile: half the rows per CTA
+                    constexpr int NLH = NLC >= 2 && (E::kLen * 3 * (NLC / 2)) % E::kEPT == 0 ? NLC / 2 : NLC;
+                    if (a.nl_div == 2 && NLH != NLC) return go(std::integral_constant<int, NLH>{});
+                    return go(std::integral_constant<int, NLC>{});
                 }
                 return -1;  // no static engine: generic kernel
             });

@@ -561,14 +561,29 @@ __global__ void __launch_bounds__(256) k_bbox(int64_t np, const double *__restri
     unsigned long long lo[3] = {~0ull, ~0ull, ~0ull}, hi[3] = {0, 0, 0};
     unsigned long long bad = 0;
     const double *p[3] = {x, y, z};
-    GRID_STRIDE(m, np) {
+    // four particles per thread and trip, their twelve loads issued before any is used
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t m0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; m0 < np; m0 += 4 * stride) {
+        double v[4][3];
 #pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            const double v = p[d][m];
-            if (!isfinite(v)) { ++bad; continue; }
-            const unsigned long long k = ord_key(v);
-            lo[d] = k < lo[d] ? k : lo[d];
-            hi[d] = k > hi[d] ? k : hi[d];
+        for (int u = 0; u < 4; ++u) {
+            const int64_t m = m0 + u * stride;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) v[u][d] = m < np ? __ldg(p[d] + m) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (m0 + u * stride >= np) break;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                if (!isfinite(v[u][d])) {
+                    ++bad;
+                    continue;
+                }
+                const unsigned long long k = ord_key(v[u][d]);
+                lo[d] = k < lo[d] ? k : lo[d];
+                hi[d] = k > hi[d] ? k : hi[d];
+            }
         }
     }
 #pragma unroll

@@ -405,6 +405,8 @@ int freespace_opt(osc_ctx *c, const FreeSpaceJob &j, const TIn *rho) {
     ra.nrows = (int64_t)Bin * ny * nz;
     ra.in_rstride = nx;
     ra.out_rstride = nxh;
+    const std::string tprec = sizeof(T) == 4 ? "f32" : "f64";
+    ra.nl_div = tune_get(c, "r2c_nl_div:" + tprec + ":L" + std::to_string(Nx));
     {
         Launch L_(c, "fft_x_r2c");
         if constexpr (std::is_same<T, float>::value) {
@@ -503,6 +505,7 @@ int freespace_opt(osc_ctx *c, const FreeSpaceJob &j, const TIn *rho) {
     cr.zin_nz = nz;
     cr.zin_ny = ny;
     cr.ncomp = nout;
+    cr.nl_div = tune_get(c, "c2r_nl_div:" + tprec + ":L" + std::to_string(Nx));
     {
         Launch L_(c, "fft_x_c2r");
         TRY(kerr(c, launch_c2r_rows<T>(X4, cr, twx, c->stream), "x c2r"));
