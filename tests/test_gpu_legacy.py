@@ -13,6 +13,10 @@ from conftest import field_err
 pytestmark = pytest.mark.gpu
 
 TOL = {osc.PREC_FP64_PLAIN: 1e-10, osc.PREC_FP64: 1e-10, osc.PREC_FP32: 1e-5}
+# E of the pipe is the central difference of phi (core:588-605), which amplifies phi's
+# normwise error by about max|phi| / (max|E| * delta); FP64 keeps 10x the phi bar, FP32 the
+# accuracy bar of the FP32 path
+E_TOL = {osc.PREC_FP64_PLAIN: 1e-9, osc.PREC_FP64: 1e-9, osc.PREC_FP32: 1e-5}
 
 
 def bunch_mesh(oracle, n, npart=60000, sigma=(1e-3, 1e-3, 0.5e-3), seed=5, centroid=(0, 0, 0), isetzmin=0):
@@ -93,7 +97,8 @@ def test_rectpipe_matches_oracle(ctx, pipe_case, prec):
     osc.space_charge_rectpipe(ctx, m, c["a"], c["b"], direct_field_calc=False, precision=prec)
     pm = np.abs(m.phi - c["phi"]).max() / np.abs(c["phi"]).max()
     mx, _ = field_err(m.efield, c["e"])
-    assert pm <= TOL[prec] and mx <= 10 * TOL[prec], (pm, mx)
+    print(f"pipe prec={prec}: phi {pm:.3e} E {mx:.3e}")
+    assert pm <= TOL[prec] and mx <= E_TOL[prec], (pm, mx)
 
 
 def test_rectpipe_reference_errors(ctx, pipe_case):
@@ -152,9 +157,10 @@ def test_fused_pipe_step_matches_oracle(ctx, oracle, pipe_case, prec):
     om = oracle.make_mesh((1, 1, 1), c["n"], (1, 1, 1), c["umin"], c["umax"], c["delta"], c["gam"])
     E0, B0, _ = oracle.interpolate_field(om, c["e"], c["x"], c["y"], c["z"], bfield=c["bf"])
     mx, _ = field_err(E.cpu().numpy(), E0)
-    assert mx <= 10 * TOL[prec], mx
     bm = np.abs(B.cpu().numpy()[:, :2] - B0[:, :2]).max() / np.abs(B0[:, :2]).max()
-    assert bm <= 10 * TOL[prec], bm
+    print(f"fused pipe prec={prec}: E {mx:.3e} B {bm:.3e}")
+    assert mx <= E_TOL[prec], mx
+    assert bm <= E_TOL[prec], bm
 
 
 def test_fused_pipe_step_without_b(ctx, oracle, pipe_case):
@@ -180,4 +186,4 @@ def test_fused_pipe_step_without_b(ctx, oracle, pipe_case):
     om = oracle.make_mesh((1, 1, 1), c["n"], (1, 1, 1), c["umin"], c["umax"], c["delta"], c["gam"])
     E0, _, _ = oracle.interpolate_field(om, c["e"], c["x"], c["y"], c["z"])
     mx, _ = field_err(E1, E0)
-    assert mx <= 10 * TOL[osc.PREC_FP32], mx
+    assert mx <= E_TOL[osc.PREC_FP32], mx
