@@ -65,6 +65,7 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-refit", action="store_true", help="skip the refit + Green rebuild leg")
     ap.add_argument("--no-order", action="store_true", help="skip the cell-sorted particle-order legs")
+    ap.add_argument("--no-cathode", action="store_true", help="skip the cathode-image leg")
     ap.add_argument("--no-tune", action="store_true", help="built-in launch shapes instead of autotuned ones")
     ap.add_argument("--tuning", action="append", default=[], metavar="KEY=VALUE",
                     help="set a launch-shape key (osc_ctx_set_tuning) before the run; implies --no-tune")
@@ -572,6 +573,51 @@ def run_ours(args, ws, rank, local, dist):
                         "line-transform passes), deposit, field, interpolation on every call",
                  "kernels": prof_r}
 
+    # the cathode-image variant of the same configuration: the bunch centred at z = 3 mm over
+    # a cathode at z = 0, samples at z <= 0 dropped and counted, zmin pinned to 1e-9 as the
+    # reference's test driver does for cathodes (code/test_opensc.f90:141-142); the image term
+    # shares the forward transform (FP32 step with at_cathode)
+    cathode = None
+    if not args.no_cathode:
+        from openspacecharge_b200.bunch import gendist
+        cx, cy, cz = gendist(npart, sigma=SIGMA, cutoff=CUTOFF, disttype=1, seed=SEED, centroid=(0.0, 0.0, 3e-3))
+        keep = cz > 0.0
+        dropped = int((~keep).sum())
+        cx, cy, cz = (np.ascontiguousarray(a[keep]) for a in (cx, cy, cz))
+        cdelta, cumin = osc.get_mesh_quantities(ctx, cx, cy, cz, (1, 1, 1), grid, 1)
+        cumax = cumin + (np.array(grid) - 1) * cdelta
+        cmesh = osc.Mesh3D(nlo=(1, 1, 1), nhi=grid, min=cumin, max=cumax, delta=cdelta, gamma=GAMMA)
+        ctx_, cty, ctz = (torch.from_numpy(a).to(dev) for a in (cx, cy, cz))
+        Ec = torch.empty((len(cx), 3), dtype=torch.float64, device=dev)
+
+        def step_c():
+            osc.space_charge_step_dev(ctx, cmesh, ctx_, cty, ctz, Ec, total_charge=QTOT, resize_mesh=False,
+                                      at_cathode=True, precision=osc.PREC_FP32)
+        for _ in range(3):
+            step_c()
+        ctx.synchronize()
+        kc = max(3, min(args.steps, 20))
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(kc):
+            step_c()
+        e1.record(stream)
+        e1.synchronize()
+        msc = max_over_ranks(e0.elapsed_time(e1) / kc, dist)
+        cathode = {"value": ws * 1000.0 / msc, "unit": "solves/s", "ms_per_step": msc, "steps": kc,
+                   "particles": int(len(cx)), "dropped_behind_cathode": dropped,
+                   "kernels": kernel_profile(ctx, osc, step_c, 3)}
+        if rank == 0 and ws == 1 and not args.no_cpu:
+            from oracle import oracle as O
+            O.build()
+            om = O.make_mesh((1, 1, 1), grid, (1, 1, 1), cumin, cumax, cdelta, GAMMA)
+            rho_c, _ = O.deposit_particles(cx, cy, cz, om, total_charge=QTOT, resize_mesh=False)
+            ef_c, _ = O.space_charge_3d(om, rho_c, at_cathode=True)
+            Ec_orc, _, _ = O.interpolate_field(om, ef_c, cx, cy, cz)
+            cathode["rel_err_vs_oracle"] = field_errors(Ec.cpu().numpy(), Ec_orc)
+        del ctx_, cty, ctz, Ec
+
     cpu = None
     err_oracle = None
     if rank == 0 and ws == 1 and not args.no_cpu:
@@ -596,7 +642,7 @@ def run_ours(args, ws, rank, local, dist):
                        "l2": "inputs larger than L2 (240 MB of particle coordinates per step)",
                        "parallelism": f"{ws} independent replica(s)"},
             "fp64_plain": fp64, "rel_err_vs_fp64": err, "rel_err_vs_oracle": err_oracle,
-            "refit_rebuild": refit, "particle_order": orders, "autotune": tuned,
+            "refit_rebuild": refit, "particle_order": orders, "autotune": tuned, "cathode_image": cathode,
             "step_alg_bytes": step_bytes, "step_alg_gbs": step_gbs,
             "kernels": kernels, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches, "clocks": clk.summary(),
