@@ -551,6 +551,10 @@ def run_ours(args, ws, rank, local, dist):
         def step_refit():
             osc.space_charge_step_dev(ctx, mesh_r, tx, ty, tz, E, total_charge=QTOT, resize_mesh=True,
                                       precision=osc.PREC_FP32)
+        if not args.no_tune:
+            from openspacecharge_b200 import autotune
+            tr = autotune.tune_green(ctx, step_refit, grid, device=local, save=False, workload=f"{grid} refit")
+            tuned = dict(tuned or {}, **{k: {"value": v, "candidates_ms": t} for k, (v, t) in tr.items()})
         for _ in range(3):
             step_refit()
         ctx.synchronize()
@@ -708,7 +712,7 @@ def run_batch(args, ws, rank, local, dist):
     if not args.no_tune:
         from openspacecharge_b200 import autotune
         lengths = sorted({2 * int(g[1]) for g in grids})
-        tr = autotune.tune_lengths(ctx, step, lengths, device=local, save=False, workload="batch")
+        tr = autotune.tune_lengths(ctx, step, lengths, device=local, save=False, workload="batch", green=True)
         tuned = {k: {"value": v, "candidates_ms": t} for k, (v, t) in tr.items()}
     for _ in range(max(3, args.warmup)):
         step()

@@ -131,7 +131,9 @@ OSC_API int osc_ctx_synchronize(osc_ctx *ctx);
  *     that doubled length; "r2c_nl_div:..." and "c2r_nl_div:..." the rows per CTA of the
  *     forward and inverse x transforms;
  *   "zconv_engine:f32:L512": 1 runs the z pass of doubled z length 512 on the one-exchange
- *     16 x 32 engine instead of the radix-8 warp engine.
+ *     16 x 32 engine instead of the radix-8 warp engine;
+ *   "sym_nl_div:<f32|f64>:L<length>": 2 or 4 divides the line pairs per CTA of the Green
+ *     build's even/odd line transforms of that doubled length.
  * Results are identical for every choice; only the time changes. */
 OSC_API int osc_ctx_set_tuning(osc_ctx *ctx, const char *key, int value);
 OSC_API int osc_ctx_get_tuning(osc_ctx *ctx, const char *key, int *value);

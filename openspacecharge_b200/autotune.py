@@ -8,7 +8,9 @@ Every choice gives identical results; only the time changes.  The tuned shapes a
   the widest tile that fits, or half of it), and the rows per CTA of the x transforms
   ("r2c_nl_div", "c2r_nl_div");
 * the transform engine of the z pass at doubled length 512 (the radix-8-8-8 warp engine, or
-  one exchange per transform with a 16 x 32 split).
+  one exchange per transform with a 16 x 32 split);
+* the line-pair tile of the Green build's even/odd transforms of each doubled length
+  ("sym_nl_div", tuned where the spectra are rebuilt: the refit case and the batch).
 
 ``tune`` times each candidate on the caller's own workload (the FP32 step through the C ABI,
 per-kernel CUDA-event times from the context profile), keeps the fastest in the context and
@@ -137,17 +139,11 @@ def tune(ctx, step, grid, order: int = ORDER_ANY, precision: int = PREC_FP32, de
     return result
 
 
-def tune_lengths(ctx, step, lengths, precision: int = PREC_FP32, device: int = 0, path: str | None = None,
-                 reps: int = 2, workload: str = "", save: bool = True) -> dict:
-    """The y-transform tile of every doubled length in `lengths` (a batched step touches
-    several), each timed over the whole step's y passes (the other lengths' passes are the
-    same in every trial)."""
-    prec = "f32" if precision == PREC_FP32 else "f64"
+def _tune_key_set(ctx, step, keys, labels, cands, reps):
     result = {}
-    for n2 in sorted(set(int(v) for v in lengths)):
-        key = f"lines_nl_div:{prec}:L{n2}"
+    for key in keys:
         times = {}
-        for v in (1, 2):
+        for v in cands:
             ctx.set_tuning(key, v)
             step()
             ctx.synchronize()
@@ -157,16 +153,55 @@ def tune_lengths(ctx, step, lengths, precision: int = PREC_FP32, device: int = 0
                 step()
             prof = ctx.profile()
             ctx.set_option(OPT_PROFILE, 0)
-            times[v] = sum(prof[l][1] for l in ("fft_y_fwd", "fft_y_inv") if l in prof) / reps
+            times[v] = sum(prof[l][1] for l in labels if l in prof) / reps
         best = choose(times)
         ctx.set_tuning(key, best)
         result[key] = (best, times)
-    if save:
-        data = load_cache(path)
-        g = data.setdefault(gpu_name(device), {})
-        for key, (best, times) in result.items():
-            g[key] = {"value": int(best), "ms": float(times[best]), "tuned_on": workload,
-                      "candidates_ms": {str(k): float(t) for k, t in times.items()}}
-        save_cache(data, path)
     return result
 
+
+def _save(result, device, path, workload):
+    data = load_cache(path)
+    g = data.setdefault(gpu_name(device), {})
+    for key, (best, times) in result.items():
+        g[key] = {"value": int(best), "ms": float(times[best]), "tuned_on": workload,
+                  "candidates_ms": {str(k): float(t) for k, t in times.items()}}
+    save_cache(data, path)
+
+
+def tune_lengths(ctx, step, lengths, precision: int = PREC_FP32, device: int = 0, path: str | None = None,
+                 reps: int = 2, workload: str = "", save: bool = True, green: bool = False) -> dict:
+    """The y-transform tile of every doubled length in `lengths` (a batched step touches
+    several), each timed over the whole step's y passes (the other lengths' passes are the
+    same in every trial); with `green`, also the line-pair tile of the Green build's
+    even/odd transforms of each length (the step must rebuild its Green spectra)."""
+    prec = "f32" if precision == PREC_FP32 else "f64"
+    ls = sorted(set(int(v) for v in lengths))
+    result = _tune_key_set(ctx, step, [f"lines_nl_div:{prec}:L{n2}" for n2 in ls], ("fft_y_fwd", "fft_y_inv"),
+                           (1, 2), reps)
+    if green:
+        result.update(_tune_key_set(ctx, step, [f"sym_nl_div:{prec}:L{n2}" for n2 in ls], ("green_sym_lines",),
+                                    (1, 2, 4), reps))
+    if save:
+        _save(result, device, path, workload)
+    return result
+
+
+def tune_green(ctx, step, grid, precision: int = PREC_FP32, device: int = 0, path: str | None = None,
+               reps: int = 2, workload: str = "", save: bool = True) -> dict:
+    """The line-pair tile of the Green build's even/odd transforms of each doubled length of
+    `grid`, timed with the Green cache off so that every step rebuilds the spectra (the
+    refit case); the cache budget is restored afterwards."""
+    from .native import OPT_GREEN_CACHE_MB
+    budget = ctx.get_option(OPT_GREEN_CACHE_MB)
+    ctx.set_option(OPT_GREEN_CACHE_MB, 0)
+    try:
+        prec = "f32" if precision == PREC_FP32 else "f64"
+        ls = sorted({2 * int(v) for v in grid})
+        result = _tune_key_set(ctx, step, [f"sym_nl_div:{prec}:L{n2}" for n2 in ls], ("green_sym_lines",),
+                               (1, 2, 4), reps)
+    finally:
+        ctx.set_option(OPT_GREEN_CACHE_MB, budget)
+    if save:
+        _save(result, device, path, workload)
+    return result

@@ -907,11 +907,18 @@ int launch_sym_lines(const TI *in, TO *out, const SymArgs &a, const TwPair<cplx<
         // static engines: up to 16 line pairs per CTA, so the short lines of small batch
         // groups still give CTAs of several warps
         auto with_sym_nl = [&](auto &&f) -> int {
-            if constexpr (E::kLen > 0)
-                return f(std::integral_constant<int, nl_static(E::kLen, 16, (int)sizeof(cplx<TC>), 1, 100 * 1024,
-                                                               E::kEPT)>{});
-            else
+            if constexpr (E::kLen > 0) {
+                constexpr int NL1 = nl_static(E::kLen, 16, (int)sizeof(cplx<TC>), 1, 100 * 1024, E::kEPT);
+                // the autotuner's alternative tiles: a half or a quarter of the line pairs per
+                // CTA (more CTAs for grids whose line count fills barely more than one wave)
+                constexpr int NL2 = NL1 >= 4 && (E::kLen * (NL1 / 2)) % E::kEPT == 0 ? NL1 / 2 : NL1;
+                constexpr int NL4 = NL2 >= 4 && (E::kLen * (NL2 / 2)) % E::kEPT == 0 ? NL2 / 2 : NL2;
+                if (a.nl_div == 4 && NL4 != NL1) return f(std::integral_constant<int, NL4>{});
+                if (a.nl_div >= 2 && NL2 != NL1) return f(std::integral_constant<int, NL2>{});
+                return f(std::integral_constant<int, NL1>{});
+            } else {
                 return with_nl<TC, E>(L, 1, 8, 0, f);
+            }
         };
         return with_sym_nl([&](auto nlc) -> int {
             constexpr int NL = decltype(nlc)::value;

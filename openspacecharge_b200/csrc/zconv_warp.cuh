@@ -340,12 +340,40 @@ __global__ void __launch_bounds__(W * 32, zw_minb<T>()) k_zconv_warp(const cplx<
     forward(rh);
     V *rb = rbufs + warp * WB;
     if (IMG) {
+        // the image spectrum -w^((nz-1) kz) rho_hat(-kz) of this lane's kz, formed once for all
+        // outputs: rho_hat(-kz) is held by another lane, so the spectrum goes through rb, and
+        // rb then keeps each lane's image values at its own positions
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
             const int j = lane + 32 * q;
             if (S0::full || j < NB)
 #pragma unroll
                 for (int r = 0; r < RF; ++r) rb[wpad<V>(j + NB * r)] = rh[q][r];
+        }
+        __syncwarp();
+        V im[Q][RF];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const int j = lane + 32 * q;
+            if (S0::full || j < NB) {
+#pragma unroll
+                for (int r = 0; r < RF; ++r) {
+                    const int e = j + NB * r;
+                    const V rm = rb[wpad<V>(e == 0 ? 0 : L - e)];
+                    // (nz-1)*kz < 2^21: 32-bit index arithmetic
+                    const V ph = __ldg(tw_rt + (int)(((unsigned)a.img_phase_mul * (unsigned)e) % (unsigned)L));
+                    const V ri = cmul(ph, rm);
+                    im[q][r] = mk<T>(-ri.x, -ri.y);
+                }
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const int j = lane + 32 * q;
+            if (S0::full || j < NB)
+#pragma unroll
+                for (int r = 0; r < RF; ++r) rb[wpad<V>(j + NB * r)] = im[q][r];
         }
     }
     if (GS && !wait_green()) return;
@@ -368,12 +396,8 @@ __global__ void __launch_bounds__(W * 32, zw_minb<T>()) k_zconv_warp(const cplx<
                         if (gd >= 0)
                             S = cmul(rh[q][r], g_lookup<T>(a.g[gd], kx, ky, e, a.nxh, a.Ny, a.ny, L, a.nz, goff));
                         if (IMG && gi >= 0) {
-                            // spectrum of -rho flipped in z: -w^((nz-1) kz) * rho_hat(-kz)
-                            const V rm = rb[wpad<V>(e == 0 ? 0 : L - e)];
-                            const V ph = __ldg(tw_rt + (int)(((int64_t)a.img_phase_mul * e) % L));
-                            V ri = cmul(ph, rm);
-                            ri.x = -ri.x * icoef;
-                            ri.y = -ri.y * icoef;
+                            // spectrum of -rho flipped in z, formed above: -w^((nz-1) kz) * rho_hat(-kz)
+                            const V ri = cscale(rb[wpad<V>(e)], icoef);
                             S = cadd(S, cmul(ri, g_lookup<T>(a.g[gi], kx, ky, e, a.nxh, a.Ny, a.ny, L, a.nz, goff)));
                         }
                         v[q][r] = S;
