@@ -74,12 +74,16 @@ struct C2RArgs {
 // meaning s (imag_unit=0) or i*s (imag_unit=1); others store cplx<T>.  Layout [kz][ky][kx],
 // or [ky][kx][kz] when zinner is set (the layout of the warp-per-column z pass), with
 // columns zpitch >= dimz elements apart (a multiple of 16 bytes).
+// herm_img marks a cathode-image spectrum in the layout of the image z pass (zconv_img.cuh):
+// complex, kz-innermost, kz in [0, Nz/2] only (the value at Nz - kz is par_h times the
+// conjugate of the value at kz), the image flip phase -exp(2 pi i (Nz/2 - 1) kz / Nz) applied.
 struct GSpecDev {
     const void *data;
     int real_valued, imag_unit;
     int sym_y, sym_z, par_y, par_z;
     int dimy, dimz;
     int zinner, zpitch;
+    int herm_img = 0, par_h = 1;
 };
 
 // Value of a stored Green spectrum at (kx, ky, kz) of the Nx/2+1 x Ny x Nz half spectrum.
@@ -172,6 +176,9 @@ int launch_c2r_rows(const cplx<T> *in, const C2RArgs &a, const TwPair<cplx<T>> &
 // True when the z pass of length L with nz = L/2 non-zero planes runs the warp-per-column
 // kernel, whose Green spectra must be stored with zinner set.
 bool zconv_warp_ok(int L, int nz, int elem_bytes);
+// True when the cathode-image z pass (zconv_img.cuh) covers length L: the warp-per-column
+// lengths whose first-stage butterfly count L/R is a multiple of 32 or below 32.
+bool zconv_img_ok(int L, int nz, int elem_bytes);
 template <typename T>
 int launch_zconv(const cplx<T> *in, cplx<T> *out, const ZConvArgs &a, const TwPair<cplx<T>> &tw,
                  int nl, cudaStream_t st);

@@ -19,6 +19,7 @@
 #include "fft_kernels.cuh"
 #include "zconv_warp.cuh"
 #include "zconv_w512.cuh"
+#include "zconv_img.cuh"
 
 namespace osc {
 
@@ -39,6 +40,17 @@ bool make_fft_plan(int L, FFTPlan &p) {
 bool zconv_warp_ok(int L, int nz, int elem_bytes) {
     if ((elem_bytes != 4 && elem_bytes != 8) || 2 * nz != L) return false;
     return dispatch_warp_len(L, [](auto eng) -> int { return decltype(eng)::kLen > 0 ? 1 : 0; }) != 0;
+}
+bool zconv_img_ok(int L, int nz, int elem_bytes) {
+    if (!zconv_warp_ok(L, nz, elem_bytes)) return false;
+    return dispatch_warp_len(L, [](auto eng) -> int {
+               using E = decltype(eng);
+               if constexpr (E::kLen > 0) {
+                   constexpr int nb = E::kLen / E::kRad[0];
+                   return nb % 32 == 0 || nb < 32 ? 1 : 0;
+               }
+               return 0;
+           }) != 0;
 }
 #endif
 
@@ -829,6 +841,35 @@ template <typename T> inline bool zconv_can_stage(const ZConvArgs &a) {
     return zconv_warp_smem<T>(a.p.L, zw_warps<T>(), ZW_STAGED, ns, zp) <= 100 * 1024;
 }
 
+// The image z pass: every output has a staged-compatible direct spectrum and a herm_img
+// image spectrum, each kind with one 16-byte column pitch; kz-innermost output.
+template <typename T> inline bool zconv_img_can(const ZConvArgs &a) {
+    if (a.nout < 1 || a.nsum > 0 || a.out_estride != 1 || a.g_bstride != 0) return false;
+    const int zp = a.g[a.gdir[0] >= 0 ? a.gdir[0] : 0].zpitch, zpi = a.g[a.gimg[0] >= 0 ? a.gimg[0] : 0].zpitch;
+    if ((zp * sizeof(T)) % 16 || (zpi * sizeof(cplx<T>)) % 16) return false;
+    for (int o = 0; o < a.nout; ++o) {
+        const int gd = a.gdir[o], gi = a.gimg[o];
+        if (gd < 0 || gi < 0) return false;
+        const GSpecDev &d = a.g[gd], &m = a.g[gi];
+        if (!d.real_valued || !d.sym_z || !d.sym_y || !d.zinner || d.zpitch != zp || d.dimz > zp) return false;
+        if (!m.herm_img || !m.sym_y || !m.zinner || m.zpitch != zpi || m.dimz != a.nz + 1 || m.dimz > zpi) return false;
+        if (reinterpret_cast<uintptr_t>(d.data) % 16 || reinterpret_cast<uintptr_t>(m.data) % 16) return false;
+    }
+    return zconv_img_smem<T>(a.p.L, a.nout, zp, zpi) <= 200 * 1024;
+}
+template <typename T, int L, int... Rs>
+inline int launch_zconv_img(WarpFft<L, Rs...>, const cplx<T> *in, cplx<T> *out, const ZConvArgs &a,
+                            const TwPair<cplx<T>> &tw, cudaStream_t st) {
+    const size_t sm = zconv_img_smem<T>(L, a.nout, a.g[a.gdir[0]].zpitch, a.g[a.gimg[0]].zpitch);
+    auto kern = k_zconv_img<T, L, Rs...>;
+    int rc = set_smem(kern, sm);
+    if (rc) return rc;
+    const int nkp = (a.nxh + 1) / 2;
+    const dim3 grid((unsigned)(nkp * (a.ny + 1)), (unsigned)(a.nbatch > 0 ? a.nbatch : 1));
+    kern<<<grid, ZI_WARPS * 32, sm, st>>>(in, out, a, tw.wt);
+    return launch_ok();
+}
+
 inline int launch_zconv_w512(const float2 *in, float2 *out, const ZConvArgs &a, const float2 *rt, cudaStream_t st) {
     constexpr int W = 4;
     const size_t sm = zconv_w512_smem<W>(a.nout, a.g[0].zpitch);
@@ -847,9 +888,23 @@ int launch_zconv(const cplx<T> *in, cplx<T> *out, const ZConvArgs &a, const TwPa
     if (zconv_warp_ok(L, a.nz, (int)sizeof(T))) {
         for (int i = 0; i < a.ng; ++i)
             if (!a.g[i].zinner) return OSC_E_INVALID;  // spectra stored for the other z pass
-        bool img = false;
-        for (int o = 0; o < a.nout; ++o) img |= a.gimg[o] >= 0;
+        bool img = false, herm = false;
+        for (int o = 0; o < a.nout; ++o) {
+            img |= a.gimg[o] >= 0;
+            herm |= a.gimg[o] >= 0 && a.g[a.gimg[o]].herm_img;
+        }
         if (tw.wt == tw.rt) return OSC_E_INVALID;
+        if (herm) {  // image spectra stored for the image z pass: no other kernel reads them
+            if (!zconv_img_ok(L, a.nz, (int)sizeof(T)) || !zconv_img_can<T>(a)) return OSC_E_INVALID;
+            return dispatch_warp_len(L, [&](auto eng) -> int {
+                using E = decltype(eng);
+                if constexpr (E::kLen > 0) {
+                    constexpr int nb = E::kLen / E::kRad[0];
+                    if constexpr (nb % 32 == 0 || nb < 32) return launch_zconv_img<T>(eng, in, out, a, tw, st);
+                }
+                return OSC_E_INVALID;
+            });
+        }
         const bool staged = !img && zconv_can_stage<T>(a);
         if (a.nsum > 0 && (img || !staged || a.nout != 1)) return OSC_E_UNSUPPORTED;
         if constexpr (sizeof(T) == 4) {

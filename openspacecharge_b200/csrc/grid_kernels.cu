@@ -164,7 +164,8 @@ int launch_igf_corners_batch(double *F, const CornerArgs *args_dev, int nbatch, 
 
 template <typename T>
 __global__ void k_green_extract(const double2 *__restrict__ ghat, void *out, int nx, int Nx, int Ny,
-                                int dimy, int dimz, int real_valued, int imag_unit, double scale, int zpitch) {
+                                int dimy, int dimz, int real_valued, int imag_unit, double scale, int zpitch,
+                                int fold_mul, int Nz) {
     const int nxh = nx + 1;
     const int64_t n = (int64_t)nxh * dimy * (zpitch > 0 ? zpitch : dimz);
     GRID_STRIDE(idx, n) {
@@ -182,22 +183,30 @@ __global__ void k_green_extract(const double2 *__restrict__ ghat, void *out, int
         }
         double2 v = make_double2(0.0, 0.0);
         if (kz < dimz) v = ghat[kx + (int64_t)Nx * (ky + (int64_t)Ny * kz)];
+        if (fold_mul >= 0 && kz < dimz) {
+            // times -exp(2 pi i m kz / Nz), the phase of the image charge's z flip
+            const int64_t ph = ((int64_t)fold_mul * kz) % Nz;
+            double sn, cs;
+            sincospi(2.0 * (double)ph / (double)Nz, &sn, &cs);
+            v = make_double2(-(v.x * cs - v.y * sn), -(v.x * sn + v.y * cs));
+        }
         if (real_valued) reinterpret_cast<T *>(out)[idx] = (T)((imag_unit ? v.y : v.x) * scale);
         else reinterpret_cast<cplx<T> *>(out)[idx] = mk<T>((T)(v.x * scale), (T)(v.y * scale));
     }
 }
 template <typename T>
 int launch_green_extract(const double2 *ghat, void *out, int nx, int Nx, int Ny, int dimy, int dimz,
-                         int real_valued, int imag_unit, double scale, int zpitch, cudaStream_t st) {
+                         int real_valued, int imag_unit, double scale, int zpitch, int fold_mul, int Nz,
+                         cudaStream_t st) {
     const int64_t n = (int64_t)(nx + 1) * dimy * (zpitch > 0 ? zpitch : dimz);
     k_green_extract<T><<<nblocks(n, 256), 256, 0, st>>>(ghat, out, nx, Nx, Ny, dimy, dimz, real_valued,
-                                                        imag_unit, scale, zpitch);
+                                                        imag_unit, scale, zpitch, fold_mul, Nz);
     return ok();
 }
 template int launch_green_extract<float>(const double2 *, void *, int, int, int, int, int, int, int, double, int,
-                                         cudaStream_t);
+                                         int, int, cudaStream_t);
 template int launch_green_extract<double>(const double2 *, void *, int, int, int, int, int, int, int, double, int,
-                                          cudaStream_t);
+                                          int, int, cudaStream_t);
 
 // ------------------------------------------------------------------------------------
 __global__ void k_pad_rho(const double *__restrict__ rho, double2 *__restrict__ crho, int nx, int ny, int nz,

@@ -44,10 +44,12 @@ int launch_igf_corners_batch(double *F, const CornerArgs *args_dev, int nbatch, 
 
 // Stored half-spectrum extraction: kx in [0,nx], ky in [0,dimy), kz in [0,dimz), times scale;
 // layout [kz][ky][kx], or [ky][kx][kz] with columns zpitch elements apart when zpitch > 0
-// (padding zeroed).
+// (padding zeroed).  fold_mul >= 0 multiplies the value at kz by -exp(2 pi i fold_mul kz / Nz)
+// (the image z-flip phase); -1 leaves it.
 template <typename T>
 int launch_green_extract(const double2 *ghat, void *out, int nx, int Nx, int Ny, int dimy, int dimz,
-                         int real_valued, int imag_unit, double scale, int zpitch, cudaStream_t st);
+                         int real_valued, int imag_unit, double scale, int zpitch, int fold_mul, int Nz,
+                         cudaStream_t st);
 // Column pitch (elements) of the kz-innermost layout: dimz rounded up to 16 bytes.
 inline int green_zpitch(int dimz, size_t elem_bytes) {
     const int q = (int)(16 / elem_bytes) > 0 ? (int)(16 / elem_bytes) : 1;

@@ -344,7 +344,7 @@ template <typename T> static int pipe_comb(osc_ctx *c, const LGeom &g) {
                                             zconv_warp_ok(g.period[2], g.n[2], (int)sizeof(T))
                                                 ? green_zpitch(g.period[2], sizeof(cplx<T>))
                                                 : 0,
-                                            c->stream),
+                                            -1, 0, c->stream),
                  "pipe extract"));
     }
     p.comb_prec = prec;

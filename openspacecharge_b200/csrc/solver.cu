@@ -196,7 +196,7 @@ static int green_sym_spectrum(osc_ctx *c, const double *F, int nx, int ny, int n
 // Green spectrum of one component (icomp 0 phi, 1..3 E) with the given offset.
 template <typename T>
 static int build_green_component(osc_ctx *c, int nx, int ny, int nz, const double delta[3], double gamma,
-                                 const double off[3], int icomp, DevBuf &store, GSpecDev &spec) {
+                                 const double off[3], int icomp, bool image, DevBuf &store, GSpecDev &spec) {
     const int n[3] = {nx, ny, nz};
     const int N[3] = {2 * nx, 2 * ny, 2 * nz};
     const int64_t M = (int64_t)N[0] * N[1] * N[2];
@@ -245,6 +245,15 @@ static int build_green_component(osc_ctx *c, int nx, int ny, int nz, const doubl
     spec.dimz = sym[2] ? nz + 1 : N[2];
     spec.zinner = zconv_warp_ok(N[2], nz, (int)sizeof(T)) ? 1 : 0;
     spec.zpitch = spec.zinner ? green_zpitch(spec.dimz, spec.real_valued ? sizeof(T) : sizeof(cplx<T>)) : spec.dimz;
+    // an image spectrum even/odd in x and y: half of z stored, flip phase applied, for the
+    // image z pass (its value at Nz - kz is par_x par_y times the conjugate of that at kz)
+    const bool herm = image && sym[0] && sym[1] && !sym[2] && zconv_img_ok(N[2], nz, (int)sizeof(T));
+    if (herm) {
+        spec.dimz = nz + 1;
+        spec.zpitch = green_zpitch(spec.dimz, sizeof(cplx<T>));
+        spec.herm_img = 1;
+        spec.par_h = par[0] * par[1];
+    }
     const size_t elems = (size_t)(nx + 1) * spec.dimy * spec.zpitch;
     const size_t bytes = elems * (spec.real_valued ? sizeof(T) : sizeof(cplx<T>));
     TRY(green_alloc(c, bytes, store));
@@ -252,7 +261,8 @@ static int build_green_component(osc_ctx *c, int nx, int ny, int nz, const doubl
     {
         Launch L_(c, "green_extract");
         TRY(kerr(c, launch_green_extract<T>(cg, store.p, nx, N[0], N[1], spec.dimy, spec.dimz, spec.real_valued,
-                                            spec.imag_unit, scale, spec.zinner ? spec.zpitch : 0, c->stream),
+                                            spec.imag_unit, scale, spec.zinner ? spec.zpitch : 0, herm ? nz - 1 : -1,
+                                            N[2], c->stream),
                  "green extract"));
     }
     spec.data = store.p;
@@ -285,7 +295,8 @@ static int green_set(osc_ctx *c, const FreeSpaceJob &j, const int *comps, int nc
         if (s == 1) off[2] = off[2] + j.img_zoff;
         for (int i = 0; i < ncomp; ++i) {
             const int k = gs.nspec;
-            int rc = build_green_component<T>(c, j.nx, j.ny, j.nz, j.delta, j.gamma, off, comps[i], gs.buf[k], gs.spec[k]);
+            int rc = build_green_component<T>(c, j.nx, j.ny, j.nz, j.delta, j.gamma, off, comps[i], s == 1,
+                                                       gs.buf[k], gs.spec[k]);
             if (rc) {
                 for (int q = 0; q <= k; ++q) green_release(c, gs.buf[q]);
                 return rc;
