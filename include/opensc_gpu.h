@@ -170,9 +170,9 @@ OSC_API int osc_deposit_particles_dev(osc_ctx *ctx, int64_t np, const double *d_
  * library until the process exits) and writes REAL64 rho.  Meshes with more nodes are
  * rejected with OSC_E_INVALID (the node count is formed in 64-bit arithmetic and checked
  * after every factor, so no mesh can wrap it).  Charges are d_q per particle, or
- * total_charge/np when d_q is NULL: total_charge is used as given (zero deposits zeros, a
- * non-finite value is OSC_E_INVALID), since this signature has no "absent" value for the
- * reference's missing-charge case.  The mesh is not refitted and mesh->charge is not
+ * total_charge/np when d_q is NULL.  With d_q NULL a zero total_charge stands for the
+ * reference's missing charge ("must specify qa or total_charge"): OSC_E_NOCHARGE, rho
+ * untouched; a non-finite total_charge is OSC_E_INVALID.  The mesh is not refitted and mesh->charge is not
  * touched.  *n_outside counts particles outside the mesh plus particles with a non-finite
  * coordinate, the count osc_deposit_particles_dev reports with its default options.  The
  * first call in a CUDA context (normally once per device) looks up the array's device

@@ -126,6 +126,9 @@ int osc_deposit_particles_dev_noalloc(void *cuda_stream, const osc_mesh3d *mesh,
     }
     if (!std::isfinite(total_charge))
         return fail(errbuf, errlen, OSC_E_INVALID, "total_charge must be finite");
+    // the reference's "must specify qa or total_charge" branch (rho untouched)
+    if (!d_q && total_charge == 0.0)
+        return fail(errbuf, errlen, OSC_E_NOCHARGE, "Error, must specify qa or total_charge");
     if (!(mesh->delta[0] > 0 && mesh->delta[1] > 0 && mesh->delta[2] > 0))
         return fail(errbuf, errlen, OSC_E_INVALID, "mesh delta must be positive");
     void *base = nullptr;

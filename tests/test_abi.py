@@ -95,3 +95,9 @@ def test_noalloc_rejects_a_negative_extent_and_a_non_finite_charge():
     assert rc == native.OSC_E_INVALID and "fewer than 2 nodes" in msg
     rc, msg = _noalloc_status((1, 1, 1), (8, 8, 8), total_charge=float("nan"))
     assert rc == native.OSC_E_INVALID and "total_charge" in msg
+
+
+def test_noalloc_without_charges_is_the_missing_charge_error():
+    """d_q NULL and total_charge 0: the reference's "must specify qa or total_charge"."""
+    rc, msg = _noalloc_status((1, 1, 1), (8, 8, 8), total_charge=0.0)
+    assert rc == native.OSC_E_NOCHARGE and "total_charge" in msg
