@@ -130,8 +130,10 @@ OSC_API int osc_ctx_synchronize(osc_ctx *ctx);
  *   "lines_nl_div:<f32|f64>:L<length>": 2 halves the lines per CTA of the y transforms of
  *     that doubled length; "r2c_nl_div:..." and "c2r_nl_div:..." the rows per CTA of the
  *     forward and inverse x transforms;
- *   "zconv_engine:f32:L512": 1 runs the z pass of doubled z length 512 on the one-exchange
- *     16 x 32 engine instead of the radix-8 warp engine;
+ *   "zconv_engine:<f32|f64>:L<length>": the free-space z pass of that doubled z length on
+ *     the radix warp engine (0), the one-exchange 16 x 32 engine (1, FP32 length 512 only),
+ *     or the warp engine with CTAs that pair the rows ky and Ny - ky and fetch their common
+ *     Green columns once (2);
  *   "sym_nl_div:<f32|f64>:L<length>": 2 or 4 divides the line pairs per CTA of the Green
  *     build's even/odd line transforms of that doubled length.
  * Results are identical for every choice; only the time changes. */

@@ -85,8 +85,9 @@ def keys_for(grid, order: int, precision: int = PREC_FP32) -> dict:
     ks = {f"lines_nl_div:{prec}:L{ny}": (("fft_y_fwd", "fft_y_inv"), [1, 2]),
           f"r2c_nl_div:{prec}:L{nx}": (("fft_x_r2c",), [1, 2]),
           f"c2r_nl_div:{prec}:L{nx}": (("fft_x_c2r",), [1, 2])}
-    if precision == PREC_FP32 and 2 * int(grid[2]) == 512:
-        ks["zconv_engine:f32:L512"] = (("fft_z_conv",), [0, 1])
+    nz2 = 2 * int(grid[2])
+    ks[f"zconv_engine:{prec}:L{nz2}"] = (("fft_z_conv",), [0, 1, 2] if precision == PREC_FP32 and nz2 == 512
+                                         else [0, 2])
     if order == ORDER_ANY:
         ks["deposit_ctas_per_sm"] = (("deposit_f32",), CTAS)
         ks["gather_ctas_per_sm"] = (("interp_f32",), CTAS)
@@ -171,14 +172,16 @@ def _save(result, device, path, workload):
 
 def tune_lengths(ctx, step, lengths, precision: int = PREC_FP32, device: int = 0, path: str | None = None,
                  reps: int = 2, workload: str = "", save: bool = True, green: bool = False) -> dict:
-    """The y-transform tile of every doubled length in `lengths` (a batched step touches
-    several), each timed over the whole step's y passes (the other lengths' passes are the
-    same in every trial); with `green`, also the line-pair tile of the Green build's
+    """The y-transform tile and the z-pass engine of every doubled length in `lengths` (a
+    batched step touches several), each timed over the whole step's y or z passes (the other
+    lengths' passes are the same in every trial); with `green`, also the line-pair tile of the Green build's
     even/odd transforms of each length (the step must rebuild its Green spectra)."""
     prec = "f32" if precision == PREC_FP32 else "f64"
     ls = sorted(set(int(v) for v in lengths))
     result = _tune_key_set(ctx, step, [f"lines_nl_div:{prec}:L{n2}" for n2 in ls], ("fft_y_fwd", "fft_y_inv"),
                            (1, 2), reps)
+    result.update(_tune_key_set(ctx, step, [f"zconv_engine:{prec}:L{n2}" for n2 in ls], ("fft_z_conv",), (0, 2),
+                                reps))
     if green:
         result.update(_tune_key_set(ctx, step, [f"sym_nl_div:{prec}:L{n2}" for n2 in ls], ("green_sym_lines",),
                                     (1, 2, 4), reps))

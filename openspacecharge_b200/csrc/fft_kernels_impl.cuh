@@ -857,11 +857,20 @@ template <typename T> inline bool zconv_img_can(const ZConvArgs &a) {
     }
     return zconv_img_smem<T>(a.p.L, a.nout, zp, zpi) <= 200 * 1024;
 }
-template <typename T, int L, int... Rs>
+// The same kernel without images (the staged free-space product, Green columns shared by
+// the rows ky and Ny - ky): staged spectra, all even/odd in y, kz-innermost output; batched
+// members (blockIdx.y) may carry their own spectra g_bstride elements apart.
+template <typename T> inline bool zconv_pair_can(const ZConvArgs &a) {
+    if (a.nout < 1 || a.nsum > 0 || a.out_estride != 1) return false;
+    for (int o = 0; o < a.nout; ++o)
+        if (a.gdir[o] < 0 || !a.g[a.gdir[o]].sym_y) return false;
+    return zconv_img_smem<T>(a.p.L, a.nout, a.g[a.gdir[0]].zpitch, 0) <= 200 * 1024;
+}
+template <typename T, bool IMG, int L, int... Rs>
 inline int launch_zconv_img(WarpFft<L, Rs...>, const cplx<T> *in, cplx<T> *out, const ZConvArgs &a,
                             const TwPair<cplx<T>> &tw, cudaStream_t st) {
-    const size_t sm = zconv_img_smem<T>(L, a.nout, a.g[a.gdir[0]].zpitch, a.g[a.gimg[0]].zpitch);
-    auto kern = k_zconv_img<T, L, Rs...>;
+    const size_t sm = zconv_img_smem<T>(L, a.nout, a.g[a.gdir[0]].zpitch, IMG ? a.g[a.gimg[0]].zpitch : 0);
+    auto kern = k_zconv_img<T, IMG, L, Rs...>;
     int rc = set_smem(kern, sm);
     if (rc) return rc;
     const int nkp = (a.nxh + 1) / 2;
@@ -900,7 +909,7 @@ int launch_zconv(const cplx<T> *in, cplx<T> *out, const ZConvArgs &a, const TwPa
                 using E = decltype(eng);
                 if constexpr (E::kLen > 0) {
                     constexpr int nb = E::kLen / E::kRad[0];
-                    if constexpr (nb % 32 == 0 || nb < 32) return launch_zconv_img<T>(eng, in, out, a, tw, st);
+                    if constexpr (nb % 32 == 0 || nb < 32) return launch_zconv_img<T, true>(eng, in, out, a, tw, st);
                 }
                 return OSC_E_INVALID;
             });
@@ -912,9 +921,14 @@ int launch_zconv(const cplx<T> *in, cplx<T> *out, const ZConvArgs &a, const TwPa
                 zconv_w512_smem<4>(a.nout, a.g[0].zpitch) <= 100 * 1024)
                 return launch_zconv_w512(in, out, a, tw.rt, st);
         }
+        // engine 2: the staged product with Green columns shared by the rows ky and Ny - ky
+        const bool pair = staged && a.engine == 2 && zconv_img_ok(L, a.nz, (int)sizeof(T)) && zconv_pair_can<T>(a);
         return dispatch_warp_len(L, [&](auto eng) -> int {
             using E = decltype(eng);
             if constexpr (E::kLen > 0) {
+                constexpr int nb = E::kLen / E::kRad[0];
+                if constexpr (nb % 32 == 0 || nb < 32)
+                    if (pair) return launch_zconv_img<T, false>(eng, in, out, a, tw, st);
                 if (a.nsum > 0) return launch_zconv_warp<T, ZW_SUM>(eng, in, out, a, tw, st);
                 if (img) return launch_zconv_warp<T, ZW_IMAGE>(eng, in, out, a, tw, st);
                 if (staged) return launch_zconv_warp<T, ZW_STAGED>(eng, in, out, a, tw, st);

@@ -23,9 +23,10 @@
 namespace osc {
 
 constexpr int ZI_WARPS = 4;
-// resident CTAs per SM the register allocation is sized for: FP32 41 KB of shared memory
-// per CTA at L = 512 (5 CTAs), FP64 80 KB (2 CTAs)
-template <typename T> constexpr int zi_minb() { return sizeof(T) == 4 ? 5 : 2; }
+// resident CTAs per SM the register allocation is sized for: with images FP32 holds 41 KB of
+// shared memory per CTA at L = 512 (5 CTAs), FP64 80 KB (2 CTAs); without, FP32 29 KB (6
+// CTAs, the occupancy of the unpaired warp engine)
+template <typename T, bool IMG> constexpr int zi_minb() { return sizeof(T) == 4 ? (IMG ? 5 : 6) : 2; }
 
 template <typename T> __device__ __forceinline__ cplx<T> shfl_c(cplx<T> v, int src) {
     v.x = __shfl_sync(0xffffffffu, v.x, src);
@@ -33,8 +34,10 @@ template <typename T> __device__ __forceinline__ cplx<T> shfl_c(cplx<T> v, int s
     return v;
 }
 
-template <typename T, int L, int... Rs>
-__global__ void __launch_bounds__(ZI_WARPS * 32, zi_minb<T>())
+// IMG false: the free-space product alone (no image spectra staged or read), the same
+// column pairing halving the Green columns each CTA fetches.
+template <typename T, bool IMG, int L, int... Rs>
+__global__ void __launch_bounds__(ZI_WARPS * 32, zi_minb<T, IMG>())
     k_zconv_img(const cplx<T> *__restrict__ in, cplx<T> *__restrict__ out, ZConvArgs a,
                 const cplx<T> *__restrict__ twg) {
     typedef cplx<T> V;
@@ -52,9 +55,9 @@ __global__ void __launch_bounds__(ZI_WARPS * 32, zi_minb<T>())
     V *tw = reinterpret_cast<V *>(smem_raw);
     V *wbufs = tw + L;
     const int nout = a.nout;
-    const int zp = a.g[a.gdir[0]].zpitch, zpi = a.g[a.gimg[0]].zpitch;
+    const int zp = a.g[a.gdir[0]].zpitch, zpi = IMG ? a.g[a.gimg[0]].zpitch : 0;
     T *gdst = reinterpret_cast<T *>(wbufs + W * WB);          // direct columns [2][nout][zp]
-    V *gist = reinterpret_cast<V *>(gdst + 2 * nout * zp);    // image columns [2][nout][zpi]
+    V *gist = reinterpret_cast<V *>(gdst + 2 * nout * zp);    // image columns [2][nout][zpi] (IMG)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nkp = (a.nxh + 1) >> 1;
     const int yy = blockIdx.x / nkp, kx0 = 2 * (blockIdx.x - yy * nkp);
@@ -71,15 +74,17 @@ __global__ void __launch_bounds__(ZI_WARPS * 32, zi_minb<T>())
     if (threadIdx.x == 0) {
         mbar_init(&gbar, 1);
         const int nk = min(2, a.nxh - kx0);
-        mbar_arrive_expect_tx(&gbar, (unsigned)(nk * nout * (zp * (int)sizeof(T) + zpi * (int)sizeof(V))));
+        mbar_arrive_expect_tx(&gbar, (unsigned)(nk * nout * (zp * (int)sizeof(T) + (IMG ? zpi * (int)sizeof(V) : 0))));
         for (int kk = 0; kk < nk; ++kk) {
             const int64_t row = (int64_t)yy * a.nxh + kx0 + kk;
             for (int o = 0; o < nout; ++o) {
-                const T *sd = reinterpret_cast<const T *>(a.g[a.gdir[o]].data) + row * zp;
-                const V *si = reinterpret_cast<const V *>(a.g[a.gimg[o]].data) + row * zpi;
+                const T *sd = reinterpret_cast<const T *>(a.g[a.gdir[o]].data) + blockIdx.y * a.g_bstride + row * zp;
                 if (!a.skip_copies) {
                     bulk_g2s(gdst + (kk * nout + o) * zp, sd, (unsigned)(zp * sizeof(T)), &gbar);
-                    bulk_g2s(gist + (kk * nout + o) * zpi, si, (unsigned)(zpi * sizeof(V)), &gbar);
+                    if (IMG) {
+                        const V *si = reinterpret_cast<const V *>(a.g[a.gimg[o]].data) + row * zpi;
+                        bulk_g2s(gist + (kk * nout + o) * zpi, si, (unsigned)(zpi * sizeof(V)), &gbar);
+                    }
                 }
             }
         }
@@ -124,11 +129,14 @@ __global__ void __launch_bounds__(ZI_WARPS * 32, zi_minb<T>())
     const int partner = S0::full ? ((32 - lane) & 31) : ((NB - lane) & 31);
     for (int o = 0; o < nout; ++o) {
         const GSpecDev &gd = a.g[a.gdir[o]];
-        const GSpecDev &gi = a.g[a.gimg[o]];
         const bool dneg = mrow && gd.par_y < 0, zodd = gd.par_z < 0, iu = gd.imag_unit;
-        T icoef = (T)a.img_coef[o];
-        if (mrow && gi.par_y < 0) icoef = -icoef;
-        const T ph = (T)gi.par_h;
+        T icoef = 0, ph = 0;
+        if (IMG) {
+            const GSpecDev &gi = a.g[a.gimg[o]];
+            icoef = (T)a.img_coef[o];
+            if (mrow && gi.par_y < 0) icoef = -icoef;
+            ph = (T)gi.par_h;
+        }
         const T *gc = gdst + (kk * nout + o) * zp;
         const V *gic = gist + (kk * nout + o) * zpi;
         V v[Q][RF];
@@ -139,27 +147,34 @@ __global__ void __launch_bounds__(ZI_WARPS * 32, zi_minb<T>())
             for (int r = 0; r < RF; ++r) {
                 // rho_hat(L - e): butterfly NB - j, register RF - 1 - r (j > 0); lane 0 keeps
                 // j = 0 (register (RF - r) mod RF) and j = 32q (register Q - q) itself
-                V m = shfl_c<T>(rh[Q - 1 - q][RF - 1 - r], partner);
-                if (lane == 0) m = q == 0 ? rh[0][(RF - r) % RF] : rh[(Q - q) % Q][RF - 1 - r];
+                V m = mk<T>(0, 0);
+                if (IMG) {
+                    m = shfl_c<T>(rh[Q - 1 - q][RF - 1 - r], partner);
+                    if (lane == 0) m = q == 0 ? rh[0][(RF - r) % RF] : rh[(Q - q) % Q][RF - 1 - r];
+                }
                 if (S0::full || j < NB) {
                     const int e = j + NB * r;
                     T sv;
-                    V gv;
+                    V gv = mk<T>(0, 0);
                     if (r < RF / 2) {
                         sv = gc[e];
-                        gv = gic[e];
+                        if (IMG) gv = gic[e];
                     } else {  // kz >= nz: the stored values at L - kz
                         sv = gc[L - e];
                         if (zodd && e != a.nz) sv = -sv;
-                        const V h = gic[L - e];
-                        gv = mk<T>(ph * h.x, -ph * h.y);
+                        if (IMG) {
+                            const V h = gic[L - e];
+                            gv = mk<T>(ph * h.x, -ph * h.y);
+                        }
                     }
                     if (dneg) sv = -sv;
                     const V x = rh[q][r];
                     V s = iu ? mk<T>(-x.y * sv, x.x * sv) : mk<T>(x.x * sv, x.y * sv);
-                    const V t = cmul(m, gv);
-                    s.x += icoef * t.x;
-                    s.y += icoef * t.y;
+                    if (IMG) {
+                        const V t = cmul(m, gv);
+                        s.x += icoef * t.x;
+                        s.y += icoef * t.y;
+                    }
                     v[q][r] = s;
                 }
             }
@@ -186,7 +201,7 @@ __global__ void __launch_bounds__(ZI_WARPS * 32, zi_minb<T>())
 }
 
 // Shared memory bytes of k_zconv_img: zp, zpi = pitches (elements) of the direct (real) and
-// image (complex) Green columns.
+// image (complex) Green columns, zpi = 0 without images.
 template <typename T> inline size_t zconv_img_smem(int L, int nout, int zp, int zpi) {
     return sizeof(cplx<T>) * ((size_t)L + (size_t)ZI_WARPS * wbuf_len<T>(L)) +
            2 * (size_t)nout * (sizeof(T) * (size_t)zp + sizeof(cplx<T>) * (size_t)zpi);

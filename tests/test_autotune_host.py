@@ -24,6 +24,7 @@ def test_keys_depend_on_particle_order_and_length():
     assert "lines_nl_div:f32:L256" in k_any and "deposit_ctas_per_sm" in k_any and "deposit_run" not in k_any
     k_sorted = autotune.keys_for((64, 48, 96), osc.ORDER_CELL_SORTED, osc.PREC_FP64)
     assert "lines_nl_div:f64:L96" in k_sorted and "gather_run" in k_sorted
+    assert k_any["zconv_engine:f32:L512"][1] == [0, 1, 2] and k_sorted["zconv_engine:f64:L192"][1] == [0, 2]
     assert all(cands for _, cands in k_sorted.values())
 
 

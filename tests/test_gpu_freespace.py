@@ -102,18 +102,64 @@ def test_green_cache_reuse_is_exact(ctx, oracle):
 
 @pytest.mark.parametrize("n", [(16, 12, 256), (24, 20, 256)])
 def test_z_pass_engines_at_length_512_agree_with_oracle(oracle, n):
-    """Doubled z length 512 with staged Green spectra has two FP32 engines: the radix-8 warp
-    engine (the default) and one exchange per transform (16 x 32 split with a radix-2
-    lane-pair shuffle); both must match the oracle, and each other to FP32 round-off."""
+    """Doubled z length 512 with staged Green spectra has three FP32 engines: the radix-8 warp
+    engine (the default), one exchange per transform (16 x 32 split with a radix-2 lane-pair
+    shuffle) and the warp engine with rows ky and Ny - ky paired on one CTA; all must match
+    the oracle, and each other to FP32 round-off."""
     rho, delta, _, _ = make_rho(oracle, n, sigma=(1e-3, 1e-3, 3e-3))
     gamma = 9.784756683727565
     e_ref, _ = oracle.freespace_solver2(rho, gamma, delta)
     out = []
     with osc.Context(0) as c:
-        for engine in (0, 1):
+        for engine in (0, 1, 2):
             c.set_tuning("zconv_engine:f32:L512", engine)
             e, _ = osc.osc_freespace_solver2(c, rho, gamma, delta, precision=osc.PREC_FP32)
             mx, rm = field_err(e, e_ref)
             assert mx <= 1e-5 and rm <= 1e-5, (engine, mx, rm)
             out.append(e)
     assert field_err(out[0], out[1])[0] <= 2e-6
+    assert field_err(out[0], out[2])[0] <= 2e-6
+
+
+@pytest.mark.parametrize("nz", [48, 64, 96, 128, 192])
+@pytest.mark.parametrize("prec", [osc.PREC_FP64, osc.PREC_FP32])
+def test_paired_z_engine_matches_oracle(oracle, nz, prec):
+    """Engine 2 of the z pass (one CTA per pair of rows ky, Ny - ky sharing their Green
+    columns) at the warp lengths it covers (doubled z 96, 128, 256, 384; at 192 the pass
+    keeps engine 0), against the oracle and against engine 0."""
+    n = (12, 10, nz)
+    rho, delta, _, _ = make_rho(oracle, n, sigma=(1e-3, 1e-3, 2e-3))
+    gamma = 9.784756683727565
+    e_ref, _ = oracle.freespace_solver2(rho, gamma, delta)
+    tag = "f32" if prec == osc.PREC_FP32 else "f64"
+    out = []
+    with osc.Context(0) as c:
+        for engine in (0, 2):
+            c.set_tuning(f"zconv_engine:{tag}:L{2 * nz}", engine)
+            e, _ = osc.osc_freespace_solver2(c, rho, gamma, delta, precision=prec)
+            mx, rm = field_err(e, e_ref)
+            assert mx <= TOL[prec], (engine, mx, rm)
+            out.append(e)
+    assert field_err(out[0], out[1])[0] <= (2e-6 if prec == osc.PREC_FP32 else 1e-13)
+
+
+@pytest.mark.parametrize("nz", [48, 64, 96, 128, 192])
+@pytest.mark.parametrize("prec", [osc.PREC_FP64, osc.PREC_FP32])
+def test_cathode_image_z_pass_lengths_match_oracle(ctx, oracle, nz, prec):
+    """The image z pass (both Green columns staged, image spectra stored for kz <= nz with
+    the z-flip phase applied, the mirrored spectrum taken by warp shuffles) at every warp
+    length it covers -- doubled z 96, 128, 256, 384 -- and the general image path at 192;
+    with B, whose two extra outputs add the image with the opposite sign."""
+    n = (12, 10, nz)
+    rho, delta, umin, umax = make_rho(oracle, n, sigma=(1e-3, 1e-3, 2e-3), centroid=(0, 0, 6e-3), isetzmin=1)
+    gamma = 9.784756683727565
+    om = oracle.make_mesh((1, 1, 1), n, (1, 1, 1), umin, umax, delta, gamma)
+    e_ref, b_ref = oracle.space_charge_3d(om, rho, at_cathode=True, calc_bfield=True)
+    m = osc.Mesh3D(nlo=(1, 1, 1), nhi=n, min=umin.copy(), max=umax.copy(), delta=delta.copy(), gamma=gamma)
+    m.rho = rho
+    osc.space_charge_3d(ctx, m, at_cathode=True, calc_bfield=True, precision=prec)
+    mx, rm = field_err(m.efield, e_ref)
+    assert mx <= TOL[prec], (mx, rm)
+    for c in range(2):
+        bm = np.abs(m.bfield[..., c] - b_ref[..., c]).max() / np.abs(b_ref[..., c]).max()
+        assert bm <= TOL[prec], (c, bm)
