@@ -89,6 +89,8 @@ extern "C" {
                                        but issues no bulk copy and polls 64 times, so its
                                        bounded wait gives up; the call returns OSC_E_TIMEOUT
                                        and the context stays usable */
+#define OSC_OPT_BATCH_GRAPH 9    /* 1 (default): an FP32 batched step whose call signature
+                                    repeats runs as one CUDA graph launch (0: direct launches) */
 
 typedef struct osc_ctx osc_ctx;
 
@@ -147,6 +149,8 @@ OSC_API int osc_profile_count(osc_ctx *ctx, int *n);
 OSC_API int osc_profile_entry(osc_ctx *ctx, int i, const char **name, int64_t *launches, double *ms);
 /* Number of kernels this library launched on the context since creation. */
 OSC_API int osc_launch_count(osc_ctx *ctx, int64_t *n);
+/* Batched steps of this context that ran as one CUDA graph launch (OSC_OPT_BATCH_GRAPH). */
+OSC_API int osc_graph_launch_count(osc_ctx *ctx, int64_t *n);
 
 /* ---- deposition -------------------------------------------------------------------
  * Replaces deposit_particles (code/open_spacecharge_mod.f90:156-288).  qa may be NULL, then

@@ -46,6 +46,7 @@ int osc_ctx_destroy(osc_ctx *ctx) {
     if (!ctx) return OSC_OK;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    ctx->batch_plans.clear();  // graph executables and their buffers
     for (auto &kv : ctx->ws) cudaFree(kv.second.p);
     for (auto &kv : ctx->tw32) cudaFree(kv.second.p);
     for (auto &kv : ctx->tw64) cudaFree(kv.second.p);
@@ -110,6 +111,7 @@ int osc_ctx_set_option(osc_ctx *ctx, int option, int64_t v) {
     case OSC_OPT_PROFILE: ctx->profile = v ? 1 : 0; return OSC_OK;
     case OSC_OPT_CHECK_FINITE: ctx->check_finite = v ? 1 : 0; return OSC_OK;
     case OSC_OPT_TEST_WAIT_TIMEOUT: ctx->test_wait_timeout = v ? 1 : 0; return OSC_OK;
+    case OSC_OPT_BATCH_GRAPH: ctx->batch_graph = v ? 1 : 0; return OSC_OK;
     default: return bad(ctx, "unknown option");
     }
 }
@@ -125,6 +127,7 @@ int osc_ctx_get_option(osc_ctx *ctx, int option, int64_t *v) {
     case OSC_OPT_PROFILE: *v = ctx->profile; return OSC_OK;
     case OSC_OPT_CHECK_FINITE: *v = ctx->check_finite; return OSC_OK;
     case OSC_OPT_TEST_WAIT_TIMEOUT: *v = ctx->test_wait_timeout; return OSC_OK;
+    case OSC_OPT_BATCH_GRAPH: *v = ctx->batch_graph; return OSC_OK;
     default: return bad(ctx, "unknown option");
     }
 }
@@ -148,6 +151,7 @@ int osc_ctx_set_tuning(osc_ctx *ctx, const char *key, int value) {
     if (!tuning_value_ok(k, value)) return set_err(ctx, OSC_E_INVALID, "tuning %s = %d is not a valid choice", key, value);
     if (value == 0) ctx->tuning.erase(k);  // the built-in default
     else ctx->tuning[k] = value;
+    ++ctx->tune_gen;
     return OSC_OK;
 }
 
@@ -195,6 +199,11 @@ int osc_profile_entry(osc_ctx *ctx, int i, const char **name, int64_t *launches,
 int osc_launch_count(osc_ctx *ctx, int64_t *n) {
     if (!ctx || !n) return OSC_E_INVALID;
     *n = ctx->launches;
+    return OSC_OK;
+}
+int osc_graph_launch_count(osc_ctx *ctx, int64_t *n) {
+    if (!ctx || !n) return OSC_E_INVALID;
+    *n = ctx->graph_launches;
     return OSC_OK;
 }
 

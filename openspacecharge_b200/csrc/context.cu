@@ -28,6 +28,8 @@ int ws_get(osc_ctx *c, const char *name, size_t bytes, void **out) {
     DevBuf &b = c->ws_slot ? c->ws[std::string(name) + "#" + std::to_string(c->ws_slot)] : c->ws[name];
     if (bytes == 0) bytes = 16;
     if (b.bytes < bytes) {
+        if (c->capturing) return set_err(c, OSC_E_UNSUPPORTED, "workspace '%s' would grow during graph capture", name);
+        ++c->ws_gen;
         if (b.p) {
             cudaStreamSynchronize(c->stream);
             cudaFree(b.p);
@@ -116,6 +118,8 @@ static constexpr int kWarpKey = 1 << 20;
 
 template <typename T> int twiddles(osc_ctx *c, int L, TwPair<cplx<T>> *out) {
     auto &tab = sizeof(T) == 4 ? c->tw32 : c->tw64;
+    if (c->capturing && (tab.find(L) == tab.end() || tab.find(-L) == tab.end() || tab.find(L + kWarpKey) == tab.end()))
+        return set_err(c, OSC_E_UNSUPPORTED, "twiddle tables of length %d would be built during graph capture", L);
     if (tab.find(L) == tab.end()) {
         std::vector<cplx<T>> h(L);
         for (int m = 0; m < L; ++m) {

@@ -5,6 +5,7 @@
 #include <cstdio>
 #include <list>
 #include <map>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -72,7 +73,17 @@ struct osc_ctx {
     int profile = 0;
     int check_finite = 0;
     int test_wait_timeout = 0;  // OSC_OPT_TEST_WAIT_TIMEOUT
+    int batch_graph = 1;        // OSC_OPT_BATCH_GRAPH
     size_t gcache_budget = (size_t)4096 << 20;
+    // CUDA-graph capture of a batched step: while capturing, nothing may allocate (ws_get,
+    // twiddles and the auxiliary streams refuse instead); ws_gen counts workspace
+    // (re)allocations and tune_gen tuning changes, so a captured graph whose buffers or
+    // launch shapes went stale is captured again
+    int capturing = 0;
+    uint64_t ws_gen = 0, tune_gen = 0;
+    int64_t graph_launches = 0;  // batched steps run as one graph launch
+    // captured batched steps by call signature (batch.cu), most recently used first
+    std::list<std::shared_ptr<void>> batch_plans;
     // workspaces by name
     std::map<std::string, osc::DevBuf> ws;
     std::map<int, osc::DevBuf> tw32, tw64;

@@ -47,6 +47,7 @@ OPT_PROFILE = 5
 OPT_CHECK_FINITE = 6
 OPT_TEST_WAIT_TIMEOUT = 7
 OPT_PARTICLE_ORDER = 8
+OPT_BATCH_GRAPH = 9
 
 _ERRNAMES = {v: k for k, v in globals().items() if k.startswith("OSC_E_") or k == "OSC_OK"}
 
@@ -112,6 +113,7 @@ SIGNATURES = {
     "osc_profile_count": [_P, ctypes.POINTER(_I)],
     "osc_profile_entry": [_P, _I, ctypes.POINTER(ctypes.c_char_p), _PI64, _PD],
     "osc_launch_count": [_P, _PI64],
+    "osc_graph_launch_count": [_P, _PI64],
     "osc_deposit_particles": [_P, _I64, _P, _P, _P, _P, _P, _I, _PM, _P, _PI64],
     "osc_deposit_particles_dev": [_P, _I64, _P, _P, _P, _P, _P, _I, _PM, _P, _PI64],
     "osc_sort_particles_dev": [_P, _PM, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _PI64],
@@ -243,6 +245,12 @@ class Context:
     def launch_count(self) -> int:
         v = ctypes.c_int64()
         self.call("osc_launch_count", ctypes.byref(v))
+        return int(v.value)
+
+    def graph_launch_count(self) -> int:
+        """Batched steps that ran as one CUDA graph launch (OPT_BATCH_GRAPH)."""
+        v = ctypes.c_int64()
+        self.call("osc_graph_launch_count", ctypes.byref(v))
         return int(v.value)
 
     def profile(self) -> dict[str, tuple[int, float]]:

@@ -103,3 +103,69 @@ def test_batch_dev_matches_host(ctx):
         assert np.array_equal(m1.delta, m2.delta)
     mx, _ = field_err(E.cpu().numpy(), E1)
     assert mx < 2e-6
+
+
+def test_batch_graph_replay(ctx):
+    """A repeated call signature runs the FP32 batched step as one captured CUDA graph (the
+    first call runs directly, the second captures): the replays refit the meshes from the
+    particles' current positions and give the fields of single steps, and equal the direct
+    launches of the same step (OPT_BATCH_GRAPH = 0) to FP32 round-off."""
+    torch = pytest.importorskip("torch")
+    meshes, x, y, z, counts, charges = make_bunches(9, (16, 24, 32), seed=11)
+    dev = torch.device("cuda", 0)
+    tx, ty, tz = (torch.from_numpy(a).to(dev) for a in (x, y, z))
+    E = torch.empty((len(x), 3), dtype=torch.float64, device=dev)
+
+    def run(scale):
+        tx.copy_(torch.from_numpy(x * scale).to(dev))
+        tz.copy_(torch.from_numpy(z + 1e-3 * scale).to(dev))
+        ms = [osc.Mesh3D(nlo=(1, 1, 1), nhi=m.nhi, gamma=GAMMA) for m in meshes]
+        osc.batch_space_charge_step_dev(ctx, ms, tx, ty, tz, counts, E, total_charges=charges)
+        ctx.synchronize()
+        return ms, E.cpu().numpy()
+
+    g0 = ctx.graph_launch_count()
+    results = [run(s) for s in (1.0, 1.0, 1.3, 0.7)]
+    assert ctx.graph_launch_count() - g0 == 3
+    for (ms, Eb), scale in zip(results, (1.0, 1.0, 1.3, 0.7)):
+        off = 0
+        for b, m in enumerate(ms):
+            sl = slice(off, off + counts[b])
+            m1 = osc.Mesh3D(nlo=(1, 1, 1), nhi=m.nhi, gamma=GAMMA)
+            Es, _ = osc.space_charge_step(ctx, m1, x[sl] * scale, y[sl], z[sl] + 1e-3 * scale,
+                                          total_charge=charges[b], resize_mesh=True)
+            assert np.array_equal(m1.min, m.min) and np.array_equal(m1.delta, m.delta) and m1.charge == m.charge
+            mx, _ = field_err(Eb[sl], Es)
+            assert mx <= 2e-6, (scale, b, mx)
+            off += counts[b]
+    ctx.set_option(osc.OPT_BATCH_GRAPH, 0)
+    try:
+        g1 = ctx.graph_launch_count()
+        _, Ed = run(0.7)
+        assert ctx.graph_launch_count() == g1
+    finally:
+        ctx.set_option(osc.OPT_BATCH_GRAPH, 1)
+    assert field_err(results[-1][1], Ed)[0] <= 2e-6
+
+
+def test_batch_graph_recaptures_after_tuning_and_new_signature(ctx):
+    """A tuning change or a different bunch set is a new signature: the step is planned and
+    captured again and still matches single steps."""
+    meshes, x, y, z, counts, charges = make_bunches(5, (16, 32), seed=12)
+    for _ in range(3):
+        E1, _ = osc.batch_space_charge_step(ctx, meshes, x, y, z, counts, total_charges=charges)
+    ctx.set_tuning("zconv_engine:f32:L64", 2)
+    try:
+        g0 = ctx.graph_launch_count()
+        for _ in range(2):
+            E2, _ = osc.batch_space_charge_step(ctx, meshes, x, y, z, counts, total_charges=charges)
+        assert ctx.graph_launch_count() - g0 == 1
+    finally:
+        ctx.set_tuning("zconv_engine:f32:L64", 0)
+    assert field_err(E1, E2)[0] <= 2e-6
+    n2 = counts[:3]
+    m2 = [osc.Mesh3D(nlo=(1, 1, 1), nhi=m.nhi, gamma=GAMMA) for m in meshes[:3]]
+    k = sum(n2)
+    for _ in range(3):
+        E3, _ = osc.batch_space_charge_step(ctx, m2, x[:k], y[:k], z[:k], n2, total_charges=charges[:3])
+    assert field_err(E3, E1[:k])[0] <= 2e-6
