@@ -63,6 +63,7 @@ int osc_ctx_destroy(osc_ctx *ctx) {
     if (ctx->d_partials) cudaFree(ctx->d_partials);
     if (ctx->h_fault) cudaFreeHost(ctx->h_fault);
     for (auto s : ctx->aux) cudaStreamDestroy(s);
+    if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
     for (auto e : ctx->aux_ev) cudaEventDestroy(e);
     if (ctx->switch_ev) cudaEventDestroy(ctx->switch_ev);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);

@@ -45,8 +45,10 @@ inline int sync(osc_ctx *ctx) { return ctx_sync(ctx); }
 // (the last event belongs to the main stream).
 constexpr int kAuxSlots = 4;
 inline int ensure_aux(osc_ctx *ctx) {
-    if (ctx->capturing && ((int)ctx->aux.size() < kAuxSlots || (int)ctx->aux_ev.size() < kAuxSlots + 1))
+    if (ctx->capturing &&
+        ((int)ctx->aux.size() < kAuxSlots || (int)ctx->aux_ev.size() < kAuxSlots + 1 || !ctx->cap_stream))
         return set_err(ctx, OSC_E_UNSUPPORTED, "auxiliary streams would be created during graph capture");
+    if (!ctx->cap_stream) CK(cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking), "capture stream");
     while ((int)ctx->aux.size() < kAuxSlots) {
         cudaStream_t s;
         CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "aux stream");

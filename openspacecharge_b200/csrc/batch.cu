@@ -470,12 +470,22 @@ int batch_issue(osc_ctx *ctx, BatchPlan &P) {
 // that fails leaves the plan without a graph and the step runs directly.
 int batch_capture(osc_ctx *ctx, BatchPlan &P) {
     cudaGraph_t graph = nullptr;
-    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    // captured on the private stream (nothing runs while capturing); launched on the caller's
+    const cudaError_t eb = cudaStreamBeginCapture(ctx->cap_stream, cudaStreamCaptureModeThreadLocal);
+    if (eb != cudaSuccess) {
+        cudaGetLastError();
+        return set_err(ctx, OSC_E_CUDA, "batch graph capture: %s", cudaGetErrorString(eb));
+    }
+    cudaStream_t user = ctx->stream;
+    ctx->stream = ctx->cap_stream;
     ctx->capturing = 1;
     const int64_t l0 = ctx->launches;
     const int rc = batch_issue(ctx, P);
+    const int64_t step_launches = ctx->launches - l0;  // counted when the graph runs
+    ctx->launches = l0;
     ctx->capturing = 0;
-    const cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+    ctx->stream = user;
+    const cudaError_t e = cudaStreamEndCapture(ctx->cap_stream, &graph);
     if (rc || e != cudaSuccess || !graph) {
         if (graph) cudaGraphDestroy(graph);
         cudaGetLastError();
@@ -488,8 +498,7 @@ int batch_capture(osc_ctx *ctx, BatchPlan &P) {
         cudaGetLastError();
         return set_err(ctx, OSC_E_CUDA, "batch graph instantiate: %s", cudaGetErrorString(ei));
     }
-    P.step_launches = ctx->launches - l0;
-    ctx->launches = l0;
+    P.step_launches = step_launches;
     P.ws_gen = ctx->ws_gen;
     return OSC_OK;
 }
@@ -535,7 +544,10 @@ int batch_fp32(osc_ctx *ctx, int nb, osc_bunch *bs, const double *x, const doubl
     // the first call of a signature runs directly; the second captures the step, and that
     // and every later call run it as one graph launch (profiling times launches one by one)
     const bool graph = ctx->batch_graph && !ctx->profile && P->calls >= 1;
-    if (graph && !P->exec && batch_capture(ctx, *P) != OSC_OK) ctx->err.clear();
+    if (graph && !P->exec && batch_capture(ctx, *P) != OSC_OK) {
+        ctx->err.clear();
+        cudaGetLastError();
+    }
     if (graph && P->exec) {
         CK(cudaGraphLaunch(P->exec, ctx->stream), "batch graph launch");
         ctx->launches += P->step_launches;

@@ -230,7 +230,8 @@ static bool gcache_evict_one(osc_ctx *c) {
     auto victim = c->gcache.begin();
     for (auto it = c->gcache.begin(); it != c->gcache.end(); ++it)
         if (it->stamp < victim->stamp) victim = it;
-    for (int i = 0; i < victim->nspec; ++i) c->gpool.push_back(victim->buf[i]);
+    for (int i = 0; i < victim->nspec; ++i)
+        if (victim->buf[i].p) c->gpool.push_back(victim->buf[i]);
     c->gcache.erase(victim);
     return true;
 }

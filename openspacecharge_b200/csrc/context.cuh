@@ -61,6 +61,9 @@ struct osc_ctx {
     std::vector<cudaStream_t> aux;
     std::vector<cudaEvent_t> aux_ev;
     cudaEvent_t switch_ev = nullptr;  // orders a newly set stream after the previous one
+    // private stream that graph captures run on (the caller's stream may be the legacy
+    // default stream, which cannot be captured); the graphs launch on the caller's stream
+    cudaStream_t cap_stream = nullptr;
     int ws_slot = 0;
     std::string err;
     // options

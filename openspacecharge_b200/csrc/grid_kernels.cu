@@ -1,4 +1,5 @@
 // grid_kernels.cu -- Green-function construction (FP64) and grid elementwise kernels.
+#include <algorithm>
 #include "grid_kernels.cuh"
 #include "osc_igf.cuh"
 
@@ -155,6 +156,30 @@ __global__ void k_igf_corners_batch(double *__restrict__ F, const CornerArgs *__
         F[idx] = igf_primitive(a.icomp, u, v, w) * a.factor;
     }
 }
+__global__ void k_igf_corners_set(double *__restrict__ F, CornerSet s, int64_t fstride) {
+    const CornerArgs a = s.a[blockIdx.y];
+    F += blockIdx.y * fstride;
+    const int64_t n = (int64_t)a.cdx * a.cdy * a.cdz;
+    GRID_STRIDE(idx, n) {
+        const int cx = (int)(idx % a.cdx);
+        const int64_t r = idx / a.cdx;
+        const int cy = (int)(r % a.cdy);
+        const int cz = (int)(r / a.cdy);
+        const double u = (a.c0x + cx) * a.dx + a.umin;
+        const double v = (a.c0y + cy) * a.dy + a.vmin;
+        const double w = (a.c0z + cz) * a.dz + a.wmin;
+        F[idx] = igf_primitive(a.icomp, u, v, w) * a.factor;
+    }
+}
+int launch_igf_corners_set(double *F, const CornerSet &s, int64_t fstride, cudaStream_t st) {
+    if (s.n < 1 || s.n > 4) return 1;
+    int64_t npts = 0;
+    for (int i = 0; i < s.n; ++i) npts = std::max(npts, (int64_t)s.a[i].cdx * s.a[i].cdy * s.a[i].cdz);
+    const dim3 grid(nblocks(npts, 256), (unsigned)s.n);
+    k_igf_corners_set<<<grid, 256, 0, st>>>(F, s, fstride);
+    return ok();
+}
+
 int launch_igf_corners_batch(double *F, const CornerArgs *args_dev, int nbatch, int64_t fstride, int64_t npts,
                              cudaStream_t st) {
     const dim3 grid(nblocks(npts, 256), (unsigned)nbatch);

@@ -16,6 +16,13 @@ struct CornerArgs {
     int icomp;
 };
 int launch_igf_corners(double *F, const CornerArgs &a, cudaStream_t st);
+// Corner blocks of up to four components of one geometry in one launch (arguments by
+// value): component i writes F + i * fstride, a[i] cdx*cdy*cdz points each.
+struct CornerSet {
+    CornerArgs a[4];
+    int n;
+};
+int launch_igf_corners_set(double *F, const CornerSet &s, int64_t fstride, cudaStream_t st);
 
 // Reference layout: cgrn(i,j,k) = 8-corner difference for i<N-1.., raw corner value on the
 // last faces, as complex128 over the full (Nx,Ny,Nz) grid (code/open_spacecharge_mod.f90:697-705).

@@ -166,34 +166,68 @@ template int green_sym_lines3<float>(osc_ctx *, const double *, int, int, int, i
 template int green_sym_lines3<double>(osc_ctx *, const double *, int, int, int, int, const int (*)[2], int, int,
                                       double *, int64_t);
 
-// Single geometry: allocates the stored spectrum and fills its descriptor.
+// All components of a geometry with zero offset (even or odd along every axis) at once:
+// the corner blocks of every component in one launch, then the octant differences and the
+// three even/odd line passes with the components as batch members (per axis, the member of
+// that axis' E component is the odd one); one buffer holds the stored spectra of all
+// components, in gs.buf[0], and gs.spec[i] points at component comps[i].
 template <typename T>
-static int green_sym_spectrum(osc_ctx *c, const double *F, int nx, int ny, int nz, const int par[3], int icomp,
-                              DevBuf &store, GSpecDev &spec) {
-    const int nxh = nx + 1, nyh = ny + 1, nzh = nz + 1;
-    spec.real_valued = 1;
-    spec.imag_unit = icomp != 0 ? 1 : 0;
-    spec.sym_y = spec.sym_z = 1;
-    spec.par_y = par[1];
-    spec.par_z = par[2];
-    spec.dimy = nyh;
-    spec.dimz = nzh;
-    spec.zinner = zconv_warp_ok(2 * nz, nz, (int)sizeof(T)) ? 1 : 0;
-    spec.zpitch = spec.zinner ? green_zpitch(nzh, sizeof(T)) : nzh;
-    const size_t bytes = sizeof(T) * (size_t)nxh * nyh * spec.zpitch;
-    TRY(green_alloc(c, bytes, store));
-    spec.data = store.p;
-    if (spec.zinner) TRY(cuda_check(c, cudaMemsetAsync(store.p, 0, bytes, c->stream), "memset spectrum"));
-    int odd[3][2];
-    for (int d = 0; d < 3; ++d) {
-        odd[d][0] = 0;
-        odd[d][1] = par[d] < 0 ? 1 : 0;
+static int green_sym_set(osc_ctx *c, int nx, int ny, int nz, const double delta[3], double gamma, const int *comps,
+                         int ncomp, GreenSet &gs) {
+    const int n[3] = {nx, ny, nz};
+    const double off0[3] = {0.0, 0.0, 0.0};
+    const int64_t fstride = (int64_t)(nx + 1) * (ny + 1) * (nz + 1);
+    double *F;
+    TRY(ws_get(c, "green_F", sizeof(double) * (size_t)ncomp * fstride, (void **)&F));
+    CornerSet cs;
+    cs.n = ncomp;
+    for (int i = 0; i < ncomp; ++i) cs.a[i] = green_corner_args(n, delta, gamma, off0, comps[i]);
+    {
+        Launch L_(c, "green_corners");
+        TRY(kerr(c, launch_igf_corners_set(F, cs, fstride, c->stream), "green corners"));
     }
-    return green_sym_lines3<T>(c, F, 1, nx, ny, nz, odd, spec.zinner, spec.zpitch, reinterpret_cast<T *>(store.p), 0);
+    const int zinner = zconv_warp_ok(2 * nz, nz, (int)sizeof(T)) ? 1 : 0;
+    const int zp = zinner ? green_zpitch(nz + 1, sizeof(T)) : nz + 1;
+    const int64_t per = (int64_t)(nx + 1) * (ny + 1) * zp;
+    DevBuf store;
+    TRY(green_alloc(c, sizeof(T) * (size_t)per * ncomp, store));
+    int odd[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+    for (int i = 0; i < ncomp; ++i)
+        if (comps[i] >= 1) {
+            odd[comps[i] - 1][0] = i;
+            odd[comps[i] - 1][1] = i + 1;
+        }
+    int rc = zinner ? cuda_check(c, cudaMemsetAsync(store.p, 0, store.bytes, c->stream), "memset spectra") : OSC_OK;
+    if (!rc) rc = green_sym_lines3<T>(c, F, ncomp, nx, ny, nz, odd, zinner, zp, reinterpret_cast<T *>(store.p), per);
+    if (rc) {
+        green_release(c, store);
+        return rc;
+    }
+    const int base = gs.nspec;
+    gs.buf[base] = store;
+    gs.bytes += store.bytes;
+    for (int i = 0; i < ncomp; ++i) {
+        GSpecDev &s = gs.spec[base + i];
+        s = GSpecDev{};
+        s.data = reinterpret_cast<T *>(store.p) + i * per;
+        s.real_valued = 1;
+        s.imag_unit = comps[i] != 0 ? 1 : 0;
+        s.sym_y = s.sym_z = 1;
+        s.par_y = comps[i] == 2 ? -1 : 1;
+        s.par_z = comps[i] == 3 ? -1 : 1;
+        s.dimy = ny + 1;
+        s.dimz = nz + 1;
+        s.zinner = zinner;
+        s.zpitch = zp;
+    }
+    gs.nspec += ncomp;
+    return OSC_OK;
 }
 
 // ------------------------------------------------------------------------------------
-// Green spectrum of one component (icomp 0 phi, 1..3 E) with the given offset.
+// Green spectrum of one component (icomp 0 phi, 1..3 E) of a kernel with a non-zero offset
+// on some axis (all-symmetric kernels go through green_sym_set): corners, the centred
+// complex doubled grid, an FP64 3D FFT and the extraction into the stored layout.
 template <typename T>
 static int build_green_component(osc_ctx *c, int nx, int ny, int nz, const double delta[3], double gamma,
                                  const double off[3], int icomp, bool image, DevBuf &store, GSpecDev &spec) {
@@ -214,14 +248,6 @@ static int build_green_component(osc_ctx *c, int nx, int ny, int nz, const doubl
     {
         Launch L_(c, "green_corners");
         TRY(kerr(c, launch_igf_corners(F, ca, c->stream), "green corners"));
-    }
-    const bool all_sym = sym[0] && sym[1] && sym[2];
-    if (all_sym) {
-        // the spectrum of a kernel that is even or odd along every axis is a product of
-        // real even/odd line transforms of its non-negative octant: three passes over
-        // (n+1)^3 reals instead of an FFT of the complex doubled grid
-        TRY(green_sym_spectrum<T>(c, F, nx, ny, nz, par, icomp, store, spec));
-        return OSC_OK;
     }
     TRY(ws_get(c, "green_cg", sizeof(double2) * (size_t)M, (void **)&cg));
     CenterArgs ce;
@@ -293,6 +319,14 @@ static int green_set(osc_ctx *c, const FreeSpaceJob &j, const int *comps, int nc
     for (int s = 0; s < nsets; ++s) {
         double off[3] = {j.offset[0], j.offset[1], j.offset[2]};
         if (s == 1) off[2] = off[2] + j.img_zoff;
+        if (off[0] == 0.0 && off[1] == 0.0 && off[2] == 0.0) {
+            const int rc = green_sym_set<T>(c, j.nx, j.ny, j.nz, j.delta, j.gamma, comps, ncomp, gs);
+            if (rc) {
+                for (int q = 0; q < gs.nspec; ++q) green_release(c, gs.buf[q]);
+                return rc;
+            }
+            continue;
+        }
         for (int i = 0; i < ncomp; ++i) {
             const int k = gs.nspec;
             int rc = build_green_component<T>(c, j.nx, j.ny, j.nz, j.delta, j.gamma, off, comps[i], s == 1,

@@ -105,12 +105,16 @@ def test_batch_dev_matches_host(ctx):
     assert mx < 2e-6
 
 
-def test_batch_graph_replay(ctx):
+@pytest.mark.parametrize("stream", ["own", "legacy_default"])
+def test_batch_graph_replay(ctx, stream):
     """A repeated call signature runs the FP32 batched step as one captured CUDA graph (the
     first call runs directly, the second captures): the replays refit the meshes from the
     particles' current positions and give the fields of single steps, and equal the direct
-    launches of the same step (OPT_BATCH_GRAPH = 0) to FP32 round-off."""
+    launches of the same step (OPT_BATCH_GRAPH = 0) to FP32 round-off.  Also with the
+    context on CUDA's legacy default stream (torch's default), which cannot be captured
+    itself: the capture runs on a private stream and the graph launches on the caller's."""
     torch = pytest.importorskip("torch")
+    ctx.set_stream(0 if stream == "legacy_default" else None)
     meshes, x, y, z, counts, charges = make_bunches(9, (16, 24, 32), seed=11)
     dev = torch.device("cuda", 0)
     tx, ty, tz = (torch.from_numpy(a).to(dev) for a in (x, y, z))
@@ -126,7 +130,9 @@ def test_batch_graph_replay(ctx):
 
     g0 = ctx.graph_launch_count()
     results = [run(s) for s in (1.0, 1.0, 1.3, 0.7)]
-    assert ctx.graph_launch_count() - g0 == 3
+    # 3 replays after the direct first call, 4 when torch handed out the arrays of an
+    # earlier call of this test again (the same signature, its graph reused)
+    assert ctx.graph_launch_count() - g0 >= 3
     for (ms, Eb), scale in zip(results, (1.0, 1.0, 1.3, 0.7)):
         off = 0
         for b, m in enumerate(ms):
@@ -145,6 +151,7 @@ def test_batch_graph_replay(ctx):
         assert ctx.graph_launch_count() == g1
     finally:
         ctx.set_option(osc.OPT_BATCH_GRAPH, 1)
+        ctx.set_stream(None)
     assert field_err(results[-1][1], Ed)[0] <= 2e-6
 
 
