@@ -69,11 +69,14 @@ def parse():
     ap.add_argument("--no-tune", action="store_true", help="built-in launch shapes instead of autotuned ones")
     ap.add_argument("--tuning", action="append", default=[], metavar="KEY=VALUE",
                     help="set a launch-shape key (osc_ctx_set_tuning) before the run; implies --no-tune")
-    ap.add_argument("--workload", default="single", choices=["single", "batch", "adjoint", "pipe"],
+    ap.add_argument("--workload", default="single", choices=["single", "batch", "adjoint", "pipe", "slab"],
                     help="single: the headline one-bunch step; batch: 256 bunches of mixed grids per step; "
                          "adjoint: forward + backward of sum q|E|^2 at 128^3, 4e6 particles; "
-                         "pipe: rectangular-pipe step at 64x64x128, 4e6 particles")
+                         "pipe: rectangular-pipe step at 64x64x128, 4e6 particles; "
+                         "slab: the headline step with its grid split into z slabs over the ranks")
     ap.add_argument("--bunches", type=int, default=BATCH_BUNCHES)
+    ap.add_argument("--slabs", type=int, default=2,
+                    help="slab workload on one GPU: z slabs emulated in this process (exchanges as copies)")
     return ap.parse_args()
 
 
@@ -1007,6 +1010,89 @@ def run_pipe(args, ws, rank, local, dist):
     ctx.close()
 
 
+SLAB_METRIC = "solves/s at 128x128x256, 1e7 ptcl, one grid over z slabs (FP32)"
+
+
+def run_slab(args, ws, rank, local, dist):
+    """The headline step with its grid split into z slabs: deposit with a one-plane halo
+    sum, x and y transforms of each slab, all-to-all to columns, z pass, all-to-all back,
+    inverse transforms, E halo planes, gather (openspacecharge_b200.slab).  With one process
+    the slabs are emulated on its GPU (exchanges as device copies); with N ranks each rank is
+    one slab and the exchanges are NCCL all-to-alls."""
+    import torch
+    import openspacecharge_b200 as osc
+    from openspacecharge_b200 import slab
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    grid = tuple(int(v) for v in args.grid.split(",")) if args.grid else GRID
+    npart = args.np
+    x, y, z = make_bunch(npart)
+    ctx = osc.Context(local)
+    delta, umin = osc.get_mesh_quantities(ctx, x, y, z, (1, 1, 1), grid, 0)
+    mesh = osc.Mesh3D(nlo=(1, 1, 1), nhi=grid, min=umin, max=umin + (np.array(grid) - 1) * delta, delta=delta,
+                      gamma=GAMMA)
+    if ws > 1:
+        import torch.distributed as tdist
+        group = tdist.new_group(backend="nccl")
+        ex = slab.DistExchange(group)
+        how = f"{ws} ranks, one slab each; exchanges: NCCL all_to_all_single"
+    else:
+        ex = slab.LocalExchange(args.slabs)
+        how = f"{args.slabs} slabs emulated on one GPU; exchanges: device copies"
+    own = slab.owner_of(mesh, z, ex.world)
+    parts, idx = {}, {}
+    for r in ex.ranks:
+        idx[r] = np.nonzero(own == r)[0]
+        parts[r] = tuple(torch.from_numpy(a[idx[r]].copy()).to(dev) for a in (x, y, z)) + (None,)
+    solver = slab.SlabSolver(ctx, mesh, ex)
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(max(3, args.warmup)):
+        out = solver.step(parts, total_charge=QTOT)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    k = max(1, args.steps)
+    with ClockSampler(local) as clk:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k):
+            out = solver.step(parts, total_charge=QTOT)
+        e1.record(stream)
+        e1.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1) / k, dist)
+    # the one-GPU step on all particles, for time and error
+    tx, ty, tz = (torch.from_numpy(a).to(dev) for a in (x, y, z))
+    E1 = torch.empty((npart, 3), dtype=torch.float64, device=dev)
+    m1 = osc.Mesh3D(nlo=(1, 1, 1), nhi=grid, min=mesh.min.copy(), max=mesh.max.copy(), delta=mesh.delta.copy(),
+                    gamma=GAMMA)
+    for _ in range(3):
+        osc.space_charge_step_dev(ctx, m1, tx, ty, tz, E1, total_charge=QTOT)
+    e0.record(stream)
+    for _ in range(k):
+        osc.space_charge_step_dev(ctx, m1, tx, ty, tz, E1, total_charge=QTOT)
+    e1.record(stream)
+    e1.synchronize()
+    ms1 = e0.elapsed_time(e1) / k
+    err = 0.0
+    for r in ex.ranks:
+        ref = E1[torch.from_numpy(idx[r]).to(dev)]
+        d = (out[r] - ref).abs().amax(0) / E1.abs().amax(0)
+        err = max(err, float(d.max()))
+    err = max_over_ranks(err, dist)
+    if rank == 0:
+        print(json.dumps({
+            "metric": SLAB_METRIC, "value": 1000.0 / ms, "unit": "solves/s", "n_gpus": ws, "steps": k,
+            "warmup": max(3, args.warmup), "ms_per_step": ms, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "the headline step (128x128x256 grid, 1e7 particles) with the grid split into "
+                                   "z slabs: " + how, "grid": list(grid), "particles": npart,
+                       "slabs": ex.world},
+            "one_gpu_step_ms": ms1, "rel_err_vs_one_gpu_step": err, "clocks": clk.summary()}))
+    ctx.close()
+
+
 def load_peak():
     """HBM copy bandwidth (GB/s) of MEASURED_PEAKS.json, else the pool's earlier measurement."""
     try:
@@ -1122,6 +1208,8 @@ def main():
             run_adjoint(args, ws, rank, local, dist)
         elif args.workload == "pipe":
             run_pipe(args, ws, rank, local, dist)
+        elif args.workload == "slab":
+            run_slab(args, ws, rank, local, dist)
         else:
             run_ours(args, ws, rank, local, dist)
     finally:

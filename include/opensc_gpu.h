@@ -361,6 +361,53 @@ OSC_API int osc_batch_space_charge_step_dev(osc_ctx *ctx, int nbunch, osc_bunch 
                                             const double *d_y, const double *d_z, const double *d_q,
                                             int resize_mesh, int precision, double *d_E);
 
+/* ---- one grid over several GPUs by z slabs (FP32) -------------------------------------
+ * Replaces, for grids that outgrow one GPU, the reference's multi-rank prototype, which
+ * moves the doubled grid between rank layouts with MPI all-to-alls
+ * (mpi_devel/code/open_spacecharge_mod.f90:722-990).  Rank r of P keeps the z planes
+ * [z0, z0 + nzl) of the nx x ny x nz grid (0-based, the mesh's planes nlo[2] + z0 ...) and
+ * the half-spectrum columns [col0, col0 + ncols) (column ky*(nx+1) + kx, ky < 2ny,
+ * kx <= nx); the caller makes the exchanges between the stages (openspacecharge_b200/
+ * slab.py does them with torch.distributed over NCCL):
+ *  1. osc_slab_deposit_dev: the rank's particles (each with its deposit cell in
+ *     [z0, z0 + nzl), see below) into a quad grid of nzl + 1 planes (float4 per node, 16
+ *     bytes; zeroed first).  Its last plane belongs to the next rank: add it into that
+ *     rank's plane 0 (the halo sum; the top slab leaves it zero).  q NULL: charge1 per
+ *     particle (the total charge over the particles of all ranks).  *n_outside (optional,
+ *     synchronises) counts this rank's particles outside the mesh or non-finite.
+ *  2. osc_slab_forward_dev: x and y transforms of the nzl planes of the quad grid into X2,
+ *     complex64 [nzl][2ny][nx+1].
+ *  3. all-to-all: rank s gets, from every rank, the columns [col0_s, col0_s + ncols_s) of
+ *     its planes, assembled as in[nz][ncols_s] (planes in global order).
+ *  4. osc_slab_zpass_dev: the z pass of the rank's columns: out[3][ncols][nz] (complex64,
+ *     the E components, kz innermost), with the Green spectra of the whole grid (built
+ *     once per geometry on every rank, cached); doubled z lengths of the warp engine only
+ *     (96, 128, 192, 256, 384, 512).
+ *  5. all-to-all back: rank s gets out[c][col][z0_s .. z0_s + nzl_s) of every rank's
+ *     columns, assembled as X3[3][2ny][nx+1][nzl_s].
+ *  6. osc_slab_inverse_dev: inverse y and x transforms into the rank's x-pair E grid,
+ *     float4 [nzl][ny][nx][2] (32 bytes per node).
+ *  7. halo: the gather reads planes z0 - 1 (from the previous rank) to z0 + nzl (from the
+ *     next); osc_slab_interp_dev gathers E at the rank's particles from an x-pair grid of
+ *     the planes [p0, p0 + np_planes).
+ * Particle ownership: rank r holds the particles whose deposit cell k = floor((z - zmin) *
+ * (1/dz) + 1) - nlo[2] (the deposit's formula) lies in [z0, z0 + nzl), clamped into
+ * [0, nz - 2] for particles beyond the mesh (as openspacecharge_b200.slab.owner_of does).
+ * The gather's cell can be one lower than the deposit's, hence the plane below the slab.
+ * Results equal osc_space_charge_step_dev's FP32 E to FP32 round-off. */
+OSC_API int osc_slab_deposit_dev(osc_ctx *ctx, const osc_mesh3d *mesh, int z0, int nzl, int64_t np,
+                                 const double *d_x, const double *d_y, const double *d_z, const double *d_q,
+                                 double charge1, float *d_quad, int64_t *n_outside);
+OSC_API int osc_slab_forward_dev(osc_ctx *ctx, const osc_mesh3d *mesh, int z0, int nzl, const float *d_quad,
+                                 void *d_X2);
+OSC_API int osc_slab_zpass_dev(osc_ctx *ctx, const osc_mesh3d *mesh, int col0, int ncols, const void *d_in,
+                               void *d_out);
+OSC_API int osc_slab_inverse_dev(osc_ctx *ctx, const osc_mesh3d *mesh, int z0, int nzl, const void *d_X3,
+                                 float *d_e8);
+OSC_API int osc_slab_interp_dev(osc_ctx *ctx, const osc_mesh3d *mesh, int p0, int np_planes, int64_t np,
+                                const double *d_x, const double *d_y, const double *d_z, const float *d_e8,
+                                double *d_E);
+
 #ifdef __cplusplus
 }
 #endif

@@ -138,6 +138,9 @@ struct ZConvArgs {
     // > 0: the nsum members are the inputs of the single output (warp engine, staged real
     // spectra): out = inverse of sum_s spectrum[gdir[s]] x forward(input s)
     int nsum;
+    // global index of local column 0 (a z slab's share of the columns, warp engine 0): the
+    // Green spectra are read at column col_base + col, input and output at col
+    int col_base;
 };
 
 // Transform of real lines that are even (par = +1) or odd (par = -1) about index 0 on the

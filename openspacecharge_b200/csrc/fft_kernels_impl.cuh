@@ -894,6 +894,8 @@ template <typename T>
 int launch_zconv(const cplx<T> *in, cplx<T> *out, const ZConvArgs &a, const TwPair<cplx<T>> &tw, int nl,
                  cudaStream_t st) {
     const int L = a.p.L;
+    // a column range of a z slab (col_base > 0) runs on the radix warp engine only
+    if (a.col_base != 0 && (!zconv_warp_ok(L, a.nz, (int)sizeof(T)) || a.nsum > 0)) return OSC_E_UNSUPPORTED;
     if (zconv_warp_ok(L, a.nz, (int)sizeof(T))) {
         for (int i = 0; i < a.ng; ++i)
             if (!a.g[i].zinner) return OSC_E_INVALID;  // spectra stored for the other z pass
@@ -904,7 +906,8 @@ int launch_zconv(const cplx<T> *in, cplx<T> *out, const ZConvArgs &a, const TwPa
         }
         if (tw.wt == tw.rt) return OSC_E_INVALID;
         if (herm) {  // image spectra stored for the image z pass: no other kernel reads them
-            if (!zconv_img_ok(L, a.nz, (int)sizeof(T)) || !zconv_img_can<T>(a)) return OSC_E_INVALID;
+            if (a.col_base != 0 || !zconv_img_ok(L, a.nz, (int)sizeof(T)) || !zconv_img_can<T>(a))
+                return OSC_E_INVALID;
             return dispatch_warp_len(L, [&](auto eng) -> int {
                 using E = decltype(eng);
                 if constexpr (E::kLen > 0) {
@@ -917,12 +920,13 @@ int launch_zconv(const cplx<T> *in, cplx<T> *out, const ZConvArgs &a, const TwPa
         const bool staged = !img && zconv_can_stage<T>(a);
         if (a.nsum > 0 && (img || !staged || a.nout != 1)) return OSC_E_UNSUPPORTED;
         if constexpr (sizeof(T) == 4) {
-            if (L == 512 && staged && a.nsum == 0 && a.out_estride == 1 && a.engine == 1 &&
+            if (L == 512 && staged && a.nsum == 0 && a.out_estride == 1 && a.engine == 1 && a.col_base == 0 &&
                 zconv_w512_smem<4>(a.nout, a.g[0].zpitch) <= 100 * 1024)
                 return launch_zconv_w512(in, out, a, tw.rt, st);
         }
         // engine 2: the staged product with Green columns shared by the rows ky and Ny - ky
-        const bool pair = staged && a.engine == 2 && zconv_img_ok(L, a.nz, (int)sizeof(T)) && zconv_pair_can<T>(a);
+        const bool pair = staged && a.engine == 2 && a.col_base == 0 && zconv_img_ok(L, a.nz, (int)sizeof(T)) &&
+                          zconv_pair_can<T>(a);
         return dispatch_warp_len(L, [&](auto eng) -> int {
             using E = decltype(eng);
             if constexpr (E::kLen > 0) {

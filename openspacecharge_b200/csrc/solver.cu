@@ -561,6 +561,146 @@ int freespace_opt(osc_ctx *c, const FreeSpaceJob &j, const TIn *rho) {
     }
     return OSC_OK;
 }
+// ------------------------------------------------------------------------------------
+// z slabs: the passes of freespace_opt<float> with the planes or columns of one rank.
+int slab_forward(osc_ctx *c, int nx, int ny, int nzl, const float4 *quad, cplx<float> *X2) {
+    typedef cplx<float> V;
+    const int Nx = 2 * nx, Ny = 2 * ny, nxh = nx + 1;
+    FFTPlan px, py;
+    if (!make_fft_plan(Nx, px) || !make_fft_plan(Ny, py))
+        return set_err(c, OSC_E_FFT_SIZE, "doubled grid %dx%d: lengths must be 2^a 3^b 5^c", Nx, Ny);
+    if (nzl < 1) return OSC_OK;
+    V *X1;
+    TRY(ws_get(c, "slab_x1", sizeof(V) * (size_t)nxh * ny * nzl, (void **)&X1));
+    TwPair<V> twx, twy;
+    TRY(twiddles<float>(c, Nx, &twx));
+    TRY(twiddles<float>(c, Ny, &twy));
+    R2CArgs ra;
+    ra.p = px;
+    ra.nin = nx;
+    ra.nrows = (int64_t)ny * nzl;
+    ra.in_rstride = nx;
+    ra.out_rstride = nxh;
+    ra.qny = ny;
+    ra.nl_div = tune_get(c, "r2c_nl_div:f32:L" + std::to_string(Nx));
+    {
+        Launch L_(c, "fft_x_r2c");
+        TRY(kerr(c, launch_r2c_rows<float, float4>(quad, X1, ra, twx, c->stream), "x r2c"));
+    }
+    LineArgs ly;
+    ly.p = py;
+    ly.sign = +1;
+    ly.ncols = nxh;
+    ly.in_len = ny;
+    ly.out_lo = 0;
+    ly.out_len = Ny;
+    ly.in_pstride = (int64_t)nxh * ny;
+    ly.in_cstride = 1;
+    ly.in_estride = nxh;
+    ly.in_zstride = 0;
+    ly.out_pstride = (int64_t)nxh * Ny;
+    ly.out_cstride = 1;
+    ly.out_estride = nxh;
+    ly.out_zstride = 0;
+    ly.scale = 1.0;
+    ly.flip_mask = 0;
+    ly.nl_div = tune_get(c, "lines_nl_div:f32:L" + std::to_string(Ny));
+    Launch L_(c, "fft_y_fwd");
+    return kerr(c, launch_lines<float>(X1, X2, ly, nzl, 1, false, twy, c->stream), "y forward");
+}
+
+int slab_zpass(osc_ctx *c, const FreeSpaceJob &j, int col0, int ncols, const cplx<float> *in, cplx<float> *out) {
+    const int nx = j.nx, ny = j.ny, nz = j.nz, nxh = nx + 1, Ny = 2 * ny, Nz = 2 * nz;
+    if (!zconv_warp_ok(Nz, nz, 4))
+        return set_err(c, OSC_E_UNSUPPORTED, "z slabs: doubled z length %d has no warp-per-column z pass", Nz);
+    if (col0 < 0 || ncols < 0 || (int64_t)col0 + ncols > (int64_t)nxh * Ny)
+        return set_err(c, OSC_E_INVALID, "z slabs: columns [%d, %d) outside the %d columns", col0, col0 + ncols,
+                       nxh * Ny);
+    if (ncols == 0) return OSC_OK;
+    FFTPlan pz;
+    if (!make_fft_plan(Nz, pz)) return set_err(c, OSC_E_FFT_SIZE, "doubled z length %d", Nz);
+    const int comps[3] = {1, 2, 3};
+    GreenSet *gs;
+    TRY(green_set<float>(c, j, comps, 3, &gs));
+    TwPair<cplx<float>> twz;
+    TRY(twiddles<float>(c, Nz, &twz));
+    ZConvArgs za;
+    std::memset(&za, 0, sizeof(za));
+    za.p = pz;
+    za.nz = nz;
+    za.ncols = ncols;
+    za.col_base = col0;
+    za.nxh = nxh;
+    za.Ny = Ny;
+    za.ny = ny;
+    za.in_estride = ncols;
+    za.out_estride = 1;
+    za.out_colstride = nz;
+    za.out_cstride = (int64_t)ncols * nz;
+    za.nout = 3;
+    for (int q = 0; q < 3; ++q) {
+        za.gdir[q] = q;
+        za.gimg[q] = -1;
+        za.img_coef[q] = 1.0;
+    }
+    za.ng = gs->nspec;
+    for (int i = 0; i < gs->nspec; ++i) za.g[i] = gs->spec[i];
+    za.fault = c->d_fault;
+    za.nbatch = 1;
+    Launch L_(c, "fft_z_conv");
+    return kerr(c, launch_zconv<float>(in, out, za, twz, 0, c->stream), "z convolution");
+}
+
+int slab_inverse(osc_ctx *c, int nx, int ny, int nzl, const cplx<float> *X3, float4 *e8) {
+    typedef cplx<float> V;
+    const int Nx = 2 * nx, Ny = 2 * ny, nxh = nx + 1;
+    FFTPlan px, py;
+    if (!make_fft_plan(Nx, px) || !make_fft_plan(Ny, py))
+        return set_err(c, OSC_E_FFT_SIZE, "doubled grid %dx%d: lengths must be 2^a 3^b 5^c", Nx, Ny);
+    if (nzl < 1) return OSC_OK;
+    V *X4;
+    TRY(ws_get(c, "slab_x4", sizeof(V) * 3 * (size_t)nxh * ny * nzl, (void **)&X4));
+    TwPair<V> twx, twy;
+    TRY(twiddles<float>(c, Nx, &twx));
+    TRY(twiddles<float>(c, Ny, &twy));
+    // y inverse over the lines (kx, z) with z fastest, window [0, ny)
+    LineArgs li;
+    li.p = py;
+    li.sign = -1;
+    li.ncols = nxh * nzl;
+    li.in_len = Ny;
+    li.out_lo = 0;
+    li.out_len = ny;
+    li.in_cstride = li.out_cstride = 1;
+    li.in_estride = li.out_estride = (int64_t)nxh * nzl;
+    li.in_pstride = li.in_zstride = (int64_t)nxh * Ny * nzl;
+    li.out_pstride = li.out_zstride = (int64_t)nxh * ny * nzl;
+    li.scale = 1.0;
+    li.flip_mask = 0;
+    li.nl_div = tune_get(c, "lines_nl_div:f32:L" + std::to_string(Ny));
+    {
+        Launch L_(c, "fft_y_inv");
+        TRY(kerr(c, launch_lines<float>(X3, X4, li, 1, 3, false, twy, c->stream), "y inverse"));
+    }
+    C2RArgs cr;
+    std::memset(&cr, 0, sizeof(cr));
+    cr.p = px;
+    cr.nout = nx;
+    cr.nrows = (int64_t)ny * nzl;
+    cr.in_rstride = (int64_t)nxh * nzl;
+    cr.in_cstride = (int64_t)nxh * ny * nzl;
+    cr.zin = 1;
+    cr.zin_nz = nzl;
+    cr.zin_ny = ny;
+    cr.ncomp = 3;
+    cr.e8 = e8;
+    for (int q = 0; q < 3; ++q) cr.e8_comp[q] = q;
+    cr.e8_node = 0;
+    cr.nl_div = tune_get(c, "c2r_nl_div:f32:L" + std::to_string(Nx));
+    Launch L_(c, "fft_x_c2r");
+    return kerr(c, launch_c2r_rows<float>(X4, cr, twx, c->stream), "x c2r");
+}
+
 template int freespace_opt<float, float>(osc_ctx *, const FreeSpaceJob &, const float *);
 template int freespace_opt<float, double>(osc_ctx *, const FreeSpaceJob &, const double *);
 template int freespace_opt<double, double>(osc_ctx *, const FreeSpaceJob &, const double *);

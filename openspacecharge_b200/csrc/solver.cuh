@@ -75,6 +75,20 @@ int freespace_opt(osc_ctx *c, const FreeSpaceJob &job, const TIn *rho);
 // The reference algorithm in FP64 (full zero-padded complex FFTs, G rebuilt per call).
 int freespace_plain(osc_ctx *c, const FreeSpaceJob &job, const double *rho);
 
+// ---- one grid over z slabs (FP32) ----------------------------------------------------
+// A rank holding the planes [z0, z0 + nzl) of the nx x ny x nz grid and the half-spectrum
+// columns [col0, col0 + ncols) (column ky*(nx+1) + kx) runs the free-space solve in three
+// stages around two transposes that the caller makes:
+// forward x and y transforms of its planes: quad grid of nzl planes (float4 per node, as
+// the deposit leaves it) -> spectrum planes X2 [nzl][2ny][nx+1];
+int slab_forward(osc_ctx *c, int nx, int ny, int nzl, const float4 *quad, cplx<float> *X2);
+// the z pass of its columns: in [nz][ncols] -> out [3][ncols][nz] (E components, window
+// z < nz), with the cached Green spectra of the whole grid (geometry of j);
+int slab_zpass(osc_ctx *c, const FreeSpaceJob &j, int col0, int ncols, const cplx<float> *in, cplx<float> *out);
+// inverse y and x transforms of its planes: X3 [3][2ny][nx+1][nzl] (kz innermost) -> the
+// x-pair E grid of its planes (float4 [nzl*ny*nx][2], as launch_interp_pairs reads it).
+int slab_inverse(osc_ctx *c, int nx, int ny, int nzl, const cplx<float> *X3, float4 *e8);
+
 // Full in-place C2C transform of an (Nx,Ny,Nz) array with per-axis signs.
 template <typename T>
 int fft3d_full(osc_ctx *c, cplx<T> *a, int Nx, int Ny, int Nz, int sx, int sy, int sz);

@@ -193,7 +193,7 @@ __global__ void __launch_bounds__(W * 32, zw_minb<T>()) k_zconv_warp(const cplx<
             const int ncv = min(W, a.ncols - col0);
             mbar_arrive_expect_tx(&gbar, (unsigned)(ncv * nst * zp * (int)sizeof(T)));
             for (int c = 0; c < ncv; ++c) {
-                const int col = col0 + c, ky = col / a.nxh, kx = col - ky * a.nxh;
+                const int col = a.col_base + col0 + c, ky = col / a.nxh, kx = col - ky * a.nxh;
                 for (int o = 0; o < nst; ++o) {
                     const GSpecDev &g = a.g[a.gdir[o]];
                     const int yy = (g.sym_y && ky > a.ny) ? a.Ny - ky : ky;
@@ -243,7 +243,7 @@ __global__ void __launch_bounds__(W * 32, zw_minb<T>()) k_zconv_warp(const cplx<
         __syncthreads();
         return !gfail;  // CTA-uniform
     };
-    const int colc = min(col0 + warp, a.ncols - 1);
+    const int colc = a.col_base + min(col0 + warp, a.ncols - 1);
     const int ky = colc / a.nxh, kx = colc - ky * a.nxh;
     // v = rh times the staged Green column `slot` of spectrum g (real, even/odd in z)
     auto staged_product = [&](const V (&rh)[Q][RF], int gd, int slot, V (&v)[Q][RF]) {

@@ -142,6 +142,11 @@ SIGNATURES = {
     "osc_space_charge_step_vjp_dev": [_P, _PM, _I64, _P, _P, _P, _P, _D, _I, _P, _P, _P, _P, _P],
     "osc_batch_space_charge_step": [_P, _I, ctypes.POINTER(OscBunch), _P, _P, _P, _P, _I, _I, _P],
     "osc_batch_space_charge_step_dev": [_P, _I, ctypes.POINTER(OscBunch), _P, _P, _P, _P, _I, _I, _P],
+    "osc_slab_deposit_dev": [_P, _PM, _I, _I, _I64, _P, _P, _P, _P, _D, _P, _PI64],
+    "osc_slab_forward_dev": [_P, _PM, _I, _I, _P, _P],
+    "osc_slab_zpass_dev": [_P, _PM, _I, _I, _P, _P],
+    "osc_slab_inverse_dev": [_P, _PM, _I, _I, _P, _P],
+    "osc_slab_interp_dev": [_P, _PM, _I, _I, _I64, _P, _P, _P, _P, _P],
 }
 _RESTYPES = {"osc_last_error": ctypes.c_char_p, "osc_version": ctypes.c_char_p}
 
