@@ -85,8 +85,6 @@ def keys_for(grid, order: int, precision: int = PREC_FP32) -> dict:
     ks = {f"lines_nl_div:{prec}:L{ny}": (("fft_y_fwd", "fft_y_inv"), [1, 2]),
           f"r2c_nl_div:{prec}:L{nx}": (("fft_x_r2c",), [1, 2]),
           f"c2r_nl_div:{prec}:L{nx}": (("fft_x_c2r",), [1, 2])}
-    if precision == PREC_FP32:
-        ks[f"r2c_quad_vec:f32:L{nx}"] = (("fft_x_r2c",), [0, 1])
     nz2 = 2 * int(grid[2])
     ks[f"zconv_engine:{prec}:L{nz2}"] = (("fft_z_conv",), [0, 1, 2] if precision == PREC_FP32 and nz2 == 512
                                          else [0, 2])

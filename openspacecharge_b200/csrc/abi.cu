@@ -142,7 +142,6 @@ static bool tuning_value_ok(const std::string &key, int v) {
     if (key.rfind("lines_nl_div:", 0) == 0 || key.rfind("r2c_nl_div:", 0) == 0 || key.rfind("c2r_nl_div:", 0) == 0)
         return v == 0 || v == 1 || v == 2;
     if (key.rfind("zconv_engine:", 0) == 0) return v == 0 || v == 1 || v == 2;
-    if (key.rfind("r2c_quad_vec:", 0) == 0) return v == 0 || v == 1;
     if (key.rfind("sym_nl_div:", 0) == 0) return v == 0 || v == 1 || v == 2 || v == 4;
     return false;
 }

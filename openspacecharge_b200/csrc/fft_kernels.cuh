@@ -32,9 +32,6 @@ struct R2CArgs {
     int64_t out_rstride;  // complex elements between output rows
     int qny = 0;          // quad-grid input (float4): rows per plane, for the node sum's y neighbour
     int nl_div = 0;       // autotuner: 2 halves the rows per CTA (0/1: default)
-    int quad_vec = 0;     // autotuner, quad input at half-window lengths: 1 loads (x, y) of the
-                          // node's quad and (z, w) of the row below as two 8-byte loads and takes
-                          // the x-1 terms from the previous lane (0: four 4-byte loads per node)
 };
 
 // Where the real result of one inverse component goes.

@@ -142,7 +142,7 @@ __device__ __forceinline__ float r2c_in(const float4 *__restrict__ in, const R2C
     return s;
 }
 
-template <typename T, typename TIn, int NL, class E, bool HIN, bool QV = false>
+template <typename T, typename TIn, int NL, class E, bool HIN>
 __global__ void __launch_bounds__(E::kMaxThreads) k_r2c_rows(const TIn *__restrict__ in, cplx<T> *__restrict__ out,
                                                              R2CArgs a, const cplx<T> *__restrict__ twg) {
     typedef cplx<T> V;
@@ -161,50 +161,12 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_r2c_rows(const TIn *__restri
         constexpr int LDL = HIN ? E::kLen / 2 : E::kLen, NT = E::kLen * NL / E::kEPT;
         constexpr int IT = (2 * NL * LDL + NT - 1) / NT;
         T v[IT];
-        if constexpr (QV && std::is_same<TIn, float4>::value && LDL % 32 == 0 && NT % 32 == 0) {
-            // quad-grid input: (x, y) of the node's own quad and (z, w) of the quad of the
-            // row below, two 8-byte loads; the terms of node i-1 (its y and the row below's
-            // w) come from the previous lane (lane 0 of a row segment loads them), summed in
-            // r2c_in's order
-            const int lane = tid & 31;
-            float2 qa[IT], qb[IT];
 #pragma unroll
-            for (int it = 0; it < IT; ++it) {
-                const int idx = tid + it * NT, rr = idx / LDL, e = idx - rr * LDL;
-                const int64_t row = row0 + rr;
-                const bool ok = idx < 2 * NL * LDL && row < a.nrows && e < a.nin;
-                const bool jn = ok && (row % a.qny) > 0;
-                const float2 *q = reinterpret_cast<const float2 *>(in + row * a.in_rstride + e);
-                qa[it] = ok ? __ldg(q) : make_float2(0.f, 0.f);
-                qb[it] = jn ? __ldg(q - 2 * a.in_rstride + 1) : make_float2(0.f, 0.f);
-            }
-#pragma unroll
-            for (int it = 0; it < IT; ++it) {
-                const int idx = tid + it * NT, rr = idx / LDL, e = idx - rr * LDL;
-                const int64_t row = row0 + rr;
-                const bool ok = idx < 2 * NL * LDL && row < a.nrows && e < a.nin;
-                const bool jn = ok && (row % a.qny) > 0;  // uniform over the warp's row segment
-                float py = __shfl_up_sync(0xffffffffu, qa[it].y, 1);
-                float pw = __shfl_up_sync(0xffffffffu, qb[it].y, 1);
-                if (lane == 0 && ok && e > 0) {
-                    const float4 *q = in + row * a.in_rstride + e;
-                    py = __ldg(&q[-1].y);
-                    pw = jn ? __ldg(&q[-a.in_rstride - 1].w) : 0.f;
-                }
-                float sv = qa[it].x;
-                if (e > 0) sv += py;
-                if (jn) sv += qb[it].x;
-                if (e > 0 && jn) sv += pw;
-                v[it] = ok ? (T)sv : (T)0;
-            }
-        } else {
-#pragma unroll
-            for (int it = 0; it < IT; ++it) {
-                const int idx = tid + it * NT, rr = idx / LDL, e = idx - rr * LDL;
-                const int64_t row = row0 + rr;
-                v[it] = 0;
-                if (idx < 2 * NL * LDL && row < a.nrows && e < a.nin) v[it] = (T)r2c_in(in, a, row, e);
-            }
+        for (int it = 0; it < IT; ++it) {
+            const int idx = tid + it * NT, rr = idx / LDL, e = idx - rr * LDL;
+            const int64_t row = row0 + rr;
+            v[it] = 0;
+            if (idx < 2 * NL * LDL && row < a.nrows && e < a.nin) v[it] = (T)r2c_in(in, a, row, e);
         }
 #pragma unroll
         for (int it = 0; it < IT; ++it) {
@@ -770,9 +732,7 @@ int launch_r2c_rows(const TIn *in, cplx<T> *out, const R2CArgs &a, const TwPair<
             const size_t sm = sizeof(cplx<T>) * ((size_t)L + (size_t)L * (NL + 1));
             const unsigned nblk = (unsigned)ceil_div(a.nrows, 2 * NL);
             if (E::kLen > 0 && 2 * a.nin == L) {
-                // quad-grid input: the autotuner may pick the 8-byte half-quad loads
-                auto kern = (std::is_same<TIn, float4>::value && a.quad_vec == 1) ? k_r2c_rows<T, TIn, NL, E, true, true>
-                                                                                   : k_r2c_rows<T, TIn, NL, E, true>;
+                auto kern = k_r2c_rows<T, TIn, NL, E, true>;
                 int rc = set_smem(kern, sm);
                 if (rc) return rc;
                 kern<<<nblk, nt, sm, st>>>(in, out, a, twe);

@@ -456,7 +456,6 @@ int freespace_opt(osc_ctx *c, const FreeSpaceJob &j, const TIn *rho) {
     ra.out_rstride = nxh;
     const std::string tprec = sizeof(T) == 4 ? "f32" : "f64";
     ra.nl_div = tune_get(c, "r2c_nl_div:" + tprec + ":L" + std::to_string(Nx));
-    ra.quad_vec = tune_get(c, "r2c_quad_vec:" + tprec + ":L" + std::to_string(Nx));
     {
         Launch L_(c, "fft_x_r2c");
         if constexpr (std::is_same<T, float>::value) {
@@ -584,7 +583,6 @@ int slab_forward(osc_ctx *c, int nx, int ny, int nzl, const float4 *quad, cplx<f
     ra.out_rstride = nxh;
     ra.qny = ny;
     ra.nl_div = tune_get(c, "r2c_nl_div:f32:L" + std::to_string(Nx));
-    ra.quad_vec = tune_get(c, "r2c_quad_vec:f32:L" + std::to_string(Nx));
     {
         Launch L_(c, "fft_x_r2c");
         TRY(kerr(c, launch_r2c_rows<float, float4>(quad, X1, ra, twx, c->stream), "x r2c"));
