@@ -18,8 +18,8 @@
 
 namespace osc {
 
-constexpr int SW_WARPS = 4;
-template <typename T> constexpr int sw_minb() { return sizeof(T) == 4 ? 6 : 2; }
+constexpr int SW_WARPS = 8;  // 16 lines per CTA: 64-byte rows of FP32 lines, the twiddle table per 8 pairs
+template <typename T> constexpr int sw_minb() { return sizeof(T) == 4 ? 4 : 1; }
 
 template <typename TC, typename TI, typename TO, bool ROW, bool KF, int L, int... Rs>
 __global__ void __launch_bounds__(SW_WARPS * 32, sw_minb<TC>())
