@@ -136,9 +136,6 @@ OSC_API int osc_ctx_synchronize(osc_ctx *ctx);
  *     the radix warp engine (0), the one-exchange 16 x 32 engine (1, FP32 length 512 only),
  *     or the warp engine with CTAs that pair the rows ky and Ny - ky and fetch their common
  *     Green columns once (2);
- *   "sym_engine:<f32|f64>:L<length>": 1 runs the Green build's even/odd line transforms of
- *     that doubled length on the CTA engine instead of one line pair per warp (lengths 96,
- *     128, 256, 384 and 512 have the warp engine);
  *   "sym_nl_div:<f32|f64>:L<length>": 2 or 4 divides the line pairs per CTA of the Green
  *     build's even/odd line transforms of that doubled length.
  * Results are identical for every choice; only the time changes. */

@@ -9,9 +9,8 @@ Every choice gives identical results; only the time changes.  The tuned shapes a
   ("r2c_nl_div", "c2r_nl_div");
 * the transform engine of the z pass at doubled length 512 (the radix-8-8-8 warp engine, or
   one exchange per transform with a 16 x 32 split);
-* the engine of the Green build's even/odd transforms of each doubled length ("sym_engine":
-  a line pair per warp, or interleaved lines per CTA) and the line-pair tile of the CTA
-  engine ("sym_nl_div"), tuned where the spectra are rebuilt: the refit case and the batch.
+* the line-pair tile of the Green build's even/odd transforms of each doubled length
+  ("sym_nl_div", tuned where the spectra are rebuilt: the refit case and the batch).
 
 ``tune`` times each candidate on the caller's own workload (the FP32 step through the C ABI,
 per-kernel CUDA-event times from the context profile), keeps the fastest in the context and
@@ -184,8 +183,6 @@ def tune_lengths(ctx, step, lengths, precision: int = PREC_FP32, device: int = 0
     result.update(_tune_key_set(ctx, step, [f"zconv_engine:{prec}:L{n2}" for n2 in ls], ("fft_z_conv",), (0, 2),
                                 reps))
     if green:
-        result.update(_tune_key_set(ctx, step, [f"sym_engine:{prec}:L{n2}" for n2 in ls], ("green_sym_lines",),
-                                    (0, 1), reps))
         result.update(_tune_key_set(ctx, step, [f"sym_nl_div:{prec}:L{n2}" for n2 in ls], ("green_sym_lines",),
                                     (1, 2, 4), reps))
     if save:
@@ -195,8 +192,8 @@ def tune_lengths(ctx, step, lengths, precision: int = PREC_FP32, device: int = 0
 
 def tune_green(ctx, step, grid, precision: int = PREC_FP32, device: int = 0, path: str | None = None,
                reps: int = 2, workload: str = "", save: bool = True) -> dict:
-    """The engine and line-pair tile of the Green build's even/odd transforms of each doubled
-    length of `grid`, timed with the Green cache off so that every step rebuilds the spectra (the
+    """The line-pair tile of the Green build's even/odd transforms of each doubled length of
+    `grid`, timed with the Green cache off so that every step rebuilds the spectra (the
     refit case); the cache budget is restored afterwards."""
     from .native import OPT_GREEN_CACHE_MB
     budget = ctx.get_option(OPT_GREEN_CACHE_MB)
@@ -204,10 +201,8 @@ def tune_green(ctx, step, grid, precision: int = PREC_FP32, device: int = 0, pat
     try:
         prec = "f32" if precision == PREC_FP32 else "f64"
         ls = sorted({2 * int(v) for v in grid})
-        result = _tune_key_set(ctx, step, [f"sym_engine:{prec}:L{n2}" for n2 in ls], ("green_sym_lines",),
-                               (0, 1), reps)
-        result.update(_tune_key_set(ctx, step, [f"sym_nl_div:{prec}:L{n2}" for n2 in ls], ("green_sym_lines",),
-                                    (1, 2, 4), reps))
+        result = _tune_key_set(ctx, step, [f"sym_nl_div:{prec}:L{n2}" for n2 in ls], ("green_sym_lines",),
+                               (1, 2, 4), reps)
     finally:
         ctx.set_option(OPT_GREEN_CACHE_MB, budget)
     if save:

@@ -143,7 +143,6 @@ static bool tuning_value_ok(const std::string &key, int v) {
         return v == 0 || v == 1 || v == 2;
     if (key.rfind("zconv_engine:", 0) == 0) return v == 0 || v == 1 || v == 2;
     if (key.rfind("sym_nl_div:", 0) == 0) return v == 0 || v == 1 || v == 2 || v == 4;
-    if (key.rfind("sym_engine:", 0) == 0) return v == 0 || v == 1;
     return false;
 }
 

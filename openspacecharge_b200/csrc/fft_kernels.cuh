@@ -161,7 +161,6 @@ struct SymArgs {
     // batches: lines of member b are the lines [b*npq, (b+1)*npq), offset by b*in_bs, b*out_bs
     int64_t npq, in_bs, out_bs;
     int nl_div = 0;  // autotuner: 2 or 4 divides the line pairs per CTA of a static engine
-    int engine = 0;  // autotuner: 0 the warp engine where the length has one, 1 the CTA engine
 };
 // row_load: elements of a line are contiguous in the input (load along the line);
 // k_fast_store: outputs of a line are contiguous (store along the line).

@@ -20,7 +20,6 @@
 #include "zconv_warp.cuh"
 #include "zconv_w512.cuh"
 #include "zconv_img.cuh"
-#include "sym_warp.cuh"
 
 namespace osc {
 
@@ -970,43 +969,11 @@ int launch_zconv(const cplx<T> *in, cplx<T> *out, const ZConvArgs &a, const TwPa
     });
 }
 
-template <typename TC, typename TI, typename TO, int L, int... Rs>
-inline int launch_sym_warp(WarpFft<L, Rs...>, const TI *in, TO *out, const SymArgs &a, const cplx<TC> *twg,
-                           bool row_load, bool k_fast_store, cudaStream_t st) {
-    const size_t sm = sym_warp_smem<TC>(L);
-    const unsigned nblk = (unsigned)ceil_div(a.nlines, 2 * SW_WARPS);
-    auto go = [&](auto kern) -> int {
-        int rc = set_smem(kern, sm);
-        if (rc) return rc;
-        kern<<<nblk, SW_WARPS * 32, sm, st>>>(in, out, a, twg);
-        return launch_ok();
-    };
-    if (row_load)
-        return k_fast_store ? go(k_sym_warp<TC, TI, TO, true, true, L, Rs...>)
-                            : go(k_sym_warp<TC, TI, TO, true, false, L, Rs...>);
-    return k_fast_store ? go(k_sym_warp<TC, TI, TO, false, true, L, Rs...>)
-                        : go(k_sym_warp<TC, TI, TO, false, false, L, Rs...>);
-}
-
 template <typename TC, typename TI, typename TO>
 int launch_sym_lines(const TI *in, TO *out, const SymArgs &a, const TwPair<cplx<TC>> &tw, bool row_load,
                      bool k_fast_store, cudaStream_t st) {
     const int L = a.p.L;
     if (L != 2 * a.n) return OSC_E_INVALID;
-    if (a.engine == 0 && tw.wt != tw.rt) {
-        // the warp engine for the lengths of the warp registry whose mirror butterflies sit
-        // in one register per lane (L/R a multiple of 32 or below 32)
-        const int rc = dispatch_warp_len(L, [&](auto eng) -> int {
-            using E = decltype(eng);
-            if constexpr (E::kLen > 0) {
-                constexpr int nb = E::kLen / E::kRad[0];
-                if constexpr (nb % 32 == 0 || nb < 32)
-                    return launch_sym_warp<TC, TI, TO>(eng, in, out, a, tw.wt, row_load, k_fast_store, st);
-            }
-            return -1;
-        });
-        if (rc != -1) return rc;
-    }
     return dispatch_fft_len<TC>(L, [&](auto eng) -> int {
         using E = decltype(eng);
         const cplx<TC> *twe = eng_tw<E>(tw);

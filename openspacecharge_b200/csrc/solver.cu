@@ -138,7 +138,6 @@ int green_sym_lines3(osc_ctx *c, const double *F, int nb, int nx, int ny, int nz
     a.out_ps = (int64_t)ny * nxh; a.out_qs = nxh; a.out_es = 1; a.out_bs = (int64_t)nxh * ny * nz;
     a.scale = 1.0;
     a.nl_div = tune_get(c, "sym_nl_div:" + tp + ":L" + std::to_string(2 * nx));
-    a.engine = tune_get(c, "sym_engine:" + tp + ":L" + std::to_string(2 * nx));
     TRY(kerr(c, launch_sym_lines<T, T, T>(h, hx, a, twx, true, true, c->stream), "green x"));
     // y: lines (c, kx) of hx -> hy[c][ky][kx]
     a.p = py; a.n = ny; a.odd_lo = odd[1][0]; a.odd_hi = odd[1][1]; a.nq = nxh;
@@ -146,7 +145,6 @@ int green_sym_lines3(osc_ctx *c, const double *F, int nb, int nx, int ny, int nz
     a.in_ps = (int64_t)ny * nxh; a.in_qs = 1; a.in_es = nxh; a.in_bs = (int64_t)nxh * ny * nz;
     a.out_ps = (int64_t)nyh * nxh; a.out_qs = 1; a.out_es = nxh; a.out_bs = (int64_t)nxh * nyh * nz;
     a.nl_div = tune_get(c, "sym_nl_div:" + tp + ":L" + std::to_string(2 * ny));
-    a.engine = tune_get(c, "sym_engine:" + tp + ":L" + std::to_string(2 * ny));
     TRY(kerr(c, launch_sym_lines<T, T, T>(hx, hy, a, twy, false, false, c->stream), "green y"));
     // z: lines (ky, kx) of hy -> stored spectrum, scaled by fpei/M
     a.p = pz; a.n = nz; a.odd_lo = odd[2][0]; a.odd_hi = odd[2][1]; a.nq = nxh;
@@ -160,7 +158,6 @@ int green_sym_lines3(osc_ctx *c, const double *F, int nb, int nx, int ny, int nz
     a.out_bs = out_bstride;
     a.scale = fpei_solver2() / (8.0 * nx * ny * nz);
     a.nl_div = tune_get(c, "sym_nl_div:" + tp + ":L" + std::to_string(2 * nz));
-    a.engine = tune_get(c, "sym_engine:" + tp + ":L" + std::to_string(2 * nz));
     TRY(kerr(c, launch_sym_lines<T, T, T>(hy, out, a, twz, false, zinner != 0, c->stream), "green z"));
     return OSC_OK;
 }

@@ -163,26 +163,3 @@ def test_cathode_image_z_pass_lengths_match_oracle(ctx, oracle, nz, prec):
     for c in range(2):
         bm = np.abs(m.bfield[..., c] - b_ref[..., c]).max() / np.abs(b_ref[..., c]).max()
         assert bm <= TOL[prec], (c, bm)
-
-
-@pytest.mark.parametrize("prec", [osc.PREC_FP64, osc.PREC_FP32])
-def test_green_line_engines_agree_with_oracle(oracle, prec):
-    """The Green build's even/odd line transforms on the warp engine (a line pair per warp,
-    the default for doubled lengths 96, 128, 256, 384, 512) and on the CTA engine
-    (sym_engine = 1) give the same spectra: both solves match the oracle and each other."""
-    n = (48, 64, 128)
-    rho, delta, _, _ = make_rho(oracle, n, sigma=(1e-3, 1e-3, 2e-3))
-    gamma = 9.784756683727565
-    e_ref, _ = oracle.freespace_solver2(rho, gamma, delta)
-    tag = "f32" if prec == osc.PREC_FP32 else "f64"
-    out = []
-    with osc.Context(0) as c:
-        for engine in (1, 0):
-            for L in (96, 128, 256):
-                c.set_tuning(f"sym_engine:{tag}:L{L}", engine)
-            c.clear_green_cache()
-            e, _ = osc.osc_freespace_solver2(c, rho, gamma, delta, precision=prec)
-            mx, rm = field_err(e, e_ref)
-            assert mx <= TOL[prec], (engine, mx, rm)
-            out.append(e)
-    assert field_err(out[0], out[1])[0] <= (2e-6 if prec == osc.PREC_FP32 else 1e-13)
