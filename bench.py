@@ -251,16 +251,16 @@ def step_bytes(nx, ny, nz, npart):
 
 def adjoint_bytes(nx, ny, nz, npart):
     """Algorithmic bytes of the FP32 forward step plus its adjoint: the forward (deposit,
-    field, gather); the charge and the three dL/dE components deposited into quad grids
-    (coordinates, charges and dL/dE read, four quad grids written); the summed adjoint solve
-    (three quad grids read, one potential written into the x-pair grid's fourth slot); the
-    gradient gather (coordinates, charges, dL/dE and the x-pair grid read, four gradients
+    field, gather); the three dL/dE components deposited into quad grids (coordinates and
+    dL/dE read, three quad grids written; E on the grid is the forward's); the summed adjoint
+    solve (three quad grids read, one potential written into the x-pair grid's fourth slot);
+    the gradient gather (coordinates, charges, dL/dE and the x-pair grid read, four gradients
     written)."""
     n = nx * ny * nz
     fwd = step_bytes(nx, ny, nz, npart)
     kb = kernel_bytes(nx, ny, nz, 0)
     solve = sum(v for k, v in kb.items() if k.startswith("fft_"))
-    dep = 32 * npart + 24 * npart + 4 * 16 * n
+    dep = 24 * npart + 24 * npart + 3 * 16 * n
     lam = solve + 2 * 16 * n
     gather = 32 * npart + 24 * npart + 32 * n + 32 * npart
     return fwd + dep + lam + gather
@@ -847,6 +847,9 @@ def run_adjoint(args, ws, rank, local, dist):
     g = [torch.empty_like(tx) for _ in range(4)]
     P = lambda t: ctypes.c_void_p(t.data_ptr())
 
+    # the backward takes E on the grid from its forward step, as the autograd binding does
+    ctx.set_option(osc.OPT_VJP_REUSE_FORWARD, 1)
+
     def fwd_bwd(prec):
         ctx.call("osc_space_charge_step_dev", ctypes.byref(m), ctypes.c_int64(ADJ_NP), P(tx), P(ty), P(tz), P(tq),
                  None, 0, 0, prec, P(E), None)
@@ -902,7 +905,7 @@ def run_adjoint(args, ws, rank, local, dist):
             "warmup": max(3, args.warmup), "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "loss sum q|E|^2: FP32 step + FP32 adjoint (deposit, field, gather; deposited "
-                                   "gradients, one adjoint solve summing the three components, gradient gather) on a fixed 128^3 mesh, 4e6 "
+                                   "gradients, one adjoint solve summing the three components, gradient gather; the backward reuses the forward's E grid, OSC_OPT_VJP_REUSE_FORWARD) on a fixed 128^3 mesh, 4e6 "
                                    "particles, sigma = 1 mm", "grid": list(ADJ_GRID), "particles": ADJ_NP},
             "rel_err_vs_fp64_gradients": err, "kernels": kern, "gpu_launches": launches, "clocks": clk.summary(),
             "roofline": roof,

@@ -91,6 +91,13 @@ extern "C" {
                                        and the context stays usable */
 #define OSC_OPT_BATCH_GRAPH 9    /* 1 (default): an FP32 batched step whose call signature
                                     repeats runs as one CUDA graph launch (0: direct launches) */
+#define OSC_OPT_VJP_REUSE_FORWARD 10 /* 1: osc_space_charge_step_vjp_dev (FP32) takes E on the
+                                        grid from the last osc_space_charge_step_dev (FP32) of
+                                        this context instead of depositing and solving again,
+                                        when that step had the same mesh, particle and charge
+                                        arrays and particle count and no other step ran since;
+                                        the caller guarantees the arrays' contents did not
+                                        change in between (0, the default: always recompute) */
 
 typedef struct osc_ctx osc_ctx;
 

@@ -4,7 +4,7 @@ grid and interpolation back to particles, as hand-written sm_100a CUDA kernels b
 C ABI (``include/opensc_gpu.h``, ``libopensc_b200.so``).
 """
 from .native import (DEPOSIT_ATOMIC, DEPOSIT_DETERMINISTIC, DEPOSIT_SORTED_SEGMENT, OPT_BATCH_GRAPH, OPT_CHECK_FINITE,
-                     OPT_DEPOSIT_MODE, OPT_GREEN_CACHE_MB, OPT_PARTICLE_ORDER, OPT_PRECISION, OPT_PROFILE,
+                     OPT_DEPOSIT_MODE, OPT_GREEN_CACHE_MB, OPT_PARTICLE_ORDER, OPT_PRECISION, OPT_PROFILE, OPT_VJP_REUSE_FORWARD,
                      OPT_STRICT_BOUNDS, ORDER_ANY, ORDER_CELL_SORTED, ORDER_SORT,
                      PREC_FP32, PREC_FP64, PREC_FP64_PLAIN, Context, OscBunch, OscError, OscMesh3D)
 from .mesh import (Mesh3D, batch_space_charge_step, batch_space_charge_step_dev, depose_rho_scalar, deposit_particles, get_mesh_quantities,

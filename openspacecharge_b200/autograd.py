@@ -3,7 +3,9 @@ positions (and charges), with the backward pass computed by the native adjoint
 (``osc_space_charge_step_vjp_dev``).  The mesh is held fixed (no refit inside the graph).
 
 Both passes run on the caller's current CUDA stream, so they order with the surrounding
-torch work."""
+torch work.  The FP32 backward reuses E on the grid from its forward step when no other step
+ran on the context in between (OPT_VJP_REUSE_FORWARD, set for the backward call only): the
+tensors saved for backward cannot change in between, torch checks their versions."""
 from __future__ import annotations
 
 import ctypes
@@ -11,7 +13,7 @@ import ctypes
 import torch
 
 from .mesh import Mesh3D, _ctx, _tp
-from .native import PREC_FP32
+from .native import OPT_VJP_REUSE_FORWARD, PREC_FP32
 
 
 def _on_stream(octx):
@@ -45,9 +47,14 @@ class _SpaceChargeField(torch.autograd.Function):
         gE = gE.contiguous().to(torch.float64)
         gx, gy, gz = torch.empty_like(x), torch.empty_like(y), torch.empty_like(z)
         gq = torch.empty_like(q) if fctx.needs_input_grad[3] else None
-        octx.call("osc_space_charge_step_vjp_dev", ctypes.byref(fctx.cmesh), ctypes.c_int64(x.numel()), _tp(x),
-                  _tp(y), _tp(z), _tp(q), ctypes.c_double(0.0), int(fctx.precision), _tp(gE), _tp(gx), _tp(gy),
-                  _tp(gz), _tp(gq))
+        prev = octx.get_option(OPT_VJP_REUSE_FORWARD)
+        octx.set_option(OPT_VJP_REUSE_FORWARD, 1)
+        try:
+            octx.call("osc_space_charge_step_vjp_dev", ctypes.byref(fctx.cmesh), ctypes.c_int64(x.numel()),
+                      _tp(x), _tp(y), _tp(z), _tp(q), ctypes.c_double(0.0), int(fctx.precision), _tp(gE), _tp(gx),
+                      _tp(gy), _tp(gz), _tp(gq))
+        finally:
+            octx.set_option(OPT_VJP_REUSE_FORWARD, prev)
         return gx, gy, gz, gq, None, None, None
 
 

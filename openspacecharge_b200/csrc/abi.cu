@@ -113,6 +113,7 @@ int osc_ctx_set_option(osc_ctx *ctx, int option, int64_t v) {
     case OSC_OPT_CHECK_FINITE: ctx->check_finite = v ? 1 : 0; return OSC_OK;
     case OSC_OPT_TEST_WAIT_TIMEOUT: ctx->test_wait_timeout = v ? 1 : 0; return OSC_OK;
     case OSC_OPT_BATCH_GRAPH: ctx->batch_graph = v ? 1 : 0; return OSC_OK;
+    case OSC_OPT_VJP_REUSE_FORWARD: ctx->vjp_reuse = v ? 1 : 0; return OSC_OK;
     default: return bad(ctx, "unknown option");
     }
 }
@@ -129,6 +130,7 @@ int osc_ctx_get_option(osc_ctx *ctx, int option, int64_t *v) {
     case OSC_OPT_CHECK_FINITE: *v = ctx->check_finite; return OSC_OK;
     case OSC_OPT_TEST_WAIT_TIMEOUT: *v = ctx->test_wait_timeout; return OSC_OK;
     case OSC_OPT_BATCH_GRAPH: *v = ctx->batch_graph; return OSC_OK;
+    case OSC_OPT_VJP_REUSE_FORWARD: *v = ctx->vjp_reuse; return OSC_OK;
     default: return bad(ctx, "unknown option");
     }
 }
@@ -489,6 +491,7 @@ int osc_space_charge_step_dev(osc_ctx *ctx, osc_mesh3d *mesh, int64_t np, const 
     if (np <= 0 || !x || !y || !z || !E) return bad(ctx, "step arrays");
     if (!q && !total_charge) return set_err(ctx, OSC_E_NOCHARGE, "Error, must specify qa or total_charge");
     if (!(mesh->gamma >= 1.0)) return set_err(ctx, OSC_E_INVALID, "gamma must be >= 1");
+    ++ctx->step_calls;  // any earlier step's kept E grid is out of date from here on
     if (resize_mesh) TRY(refit_mesh(ctx, np, x, y, z, mesh));
     double charge1 = 0;
     if (q) TRY(set_charge(ctx, np, q, total_charge, mesh, &charge1));
@@ -566,6 +569,24 @@ int osc_space_charge_step_dev(osc_ctx *ctx, osc_mesh3d *mesh, int64_t np, const 
             j.B = Bg;
         }
         TRY(freespace_opt<float, float>(ctx, j, rho));
+        if (!at_cathode) {  // the E grid of this free-space step, for the adjoint
+            osc_ctx::FwdRecord &f = ctx->fwd;
+            f.call = ctx->step_calls;
+            f.np = np;
+            for (int d = 0; d < 3; ++d) {
+                f.nlo[d] = mesh->nlo[d];
+                f.nhi[d] = mesh->nhi[d];
+                f.min[d] = mesh->min[d];
+                f.delta[d] = mesh->delta[d];
+            }
+            f.gamma = mesh->gamma;
+            f.charge1 = charge1;
+            f.x = x;
+            f.y = y;
+            f.z = z;
+            f.q = q;
+            f.e8 = E8;
+        }
         // with the particles sorted here, E and B are gathered in sorted order and then
         // permuted back to the caller's order
         double *Eo = E, *Bo = B;

@@ -34,25 +34,38 @@ int osc_space_charge_step_vjp_dev(osc_ctx *ctx, const osc_mesh3d *mesh, int64_t 
     if (precision == OSC_PREC_FP32 && ctx->deposit_mode == OSC_DEPOSIT_ATOMIC) {
         // FP32: quad-grid deposits (the x transform sums the nodes as it loads them), E and
         // lambda in one x-pair grid, one gather of four 256-bit loads per particle
-        float *quad, *quad3, *e8;
+        float *quad3, *e8;
         double *lam;
-        TRY(ws_get(ctx, "vjp_quad", sizeof(float4) * N, (void **)&quad));
+        // E on the grid: the last FP32 step's, when allowed and it matches this call (its
+        // slot 3 then takes lambda), else deposited and solved here
+        const osc_ctx::FwdRecord &f = ctx->fwd;
+        bool reuse = ctx->vjp_reuse && f.call == ctx->step_calls && f.e8 && f.np == np && f.x == x &&
+                     f.y == y && f.z == z && f.q == q && f.gamma == mesh->gamma && f.charge1 == charge1;
+        for (int d = 0; d < 3 && reuse; ++d)
+            reuse = f.nlo[d] == mesh->nlo[d] && f.nhi[d] == mesh->nhi[d] && f.min[d] == mesh->min[d] &&
+                    f.delta[d] == mesh->delta[d];
         TRY(ws_get(ctx, "vjp_quad3", sizeof(float4) * 3 * N, (void **)&quad3));
-        TRY(ws_get(ctx, "vjp_e8", sizeof(float4) * 2 * N, (void **)&e8));
         TRY(ws_get(ctx, "vjp_lambda", sizeof(double) * N, (void **)&lam));
         TRY(counters_reset(ctx));
-        CK(cudaMemsetAsync(quad, 0, sizeof(float4) * N, ctx->stream), "memset quad");
         CK(cudaMemsetAsync(quad3, 0, sizeof(float4) * 3 * N, ctx->stream), "memset quad3");
         CK(cudaMemsetAsync(lam, 0, sizeof(double) * N, ctx->stream), "memset lambda");  // three-solve path
-        {
-            Launch L_(ctx, "deposit_f32");
-            if (launch_deposit_quad(da, quad, ctx->d_small, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "deposit");
+        if (reuse) {
+            e8 = reinterpret_cast<float *>(f.e8);
+        } else {
+            float *quad;
+            TRY(ws_get(ctx, "vjp_quad", sizeof(float4) * N, (void **)&quad));
+            TRY(ws_get(ctx, "vjp_e8", sizeof(float4) * 2 * N, (void **)&e8));
+            CK(cudaMemsetAsync(quad, 0, sizeof(float4) * N, ctx->stream), "memset quad");
+            {
+                Launch L_(ctx, "deposit_f32");
+                if (launch_deposit_quad(da, quad, ctx->d_small, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "deposit");
+            }
+            FreeSpaceJob j = fs_job(mesh, n, nullptr, 0, 0);
+            j.quad = reinterpret_cast<const float4 *>(quad);
+            j.E4 = e8;
+            j.e4_pairs = 1;
+            TRY(freespace_opt<float, float>(ctx, j, nullptr));
         }
-        FreeSpaceJob j = fs_job(mesh, n, nullptr, 0, 0);
-        j.quad = reinterpret_cast<const float4 *>(quad);
-        j.E4 = e8;
-        j.e4_pairs = 1;
-        TRY(freespace_opt<float, float>(ctx, j, nullptr));
         {
             Launch L_(ctx, "vjp_deposit");
             if (launch_deposit_quad3(da, gE, quad3, ctx->stream)) return set_err(ctx, OSC_E_CUDA, "vjp deposit");

@@ -85,6 +85,17 @@ struct osc_ctx {
     int capturing = 0;
     uint64_t ws_gen = 0, tune_gen = 0;
     int64_t graph_launches = 0;  // batched steps run as one graph launch
+    // the FP32 step's x-pair E grid, kept for the adjoint (OSC_OPT_VJP_REUSE_FORWARD):
+    // every step call counts in step_calls; fwd records the last FP32 step's inputs
+    int vjp_reuse = 0;
+    int64_t step_calls = 0;
+    struct FwdRecord {
+        int64_t call = -1, np = 0;
+        int nlo[3], nhi[3];
+        double min[3], delta[3], gamma, charge1;
+        const double *x, *y, *z, *q;
+        void *e8 = nullptr;
+    } fwd;
     // captured batched steps by call signature (batch.cu), most recently used first
     std::list<std::shared_ptr<void>> batch_plans;
     // workspaces by name

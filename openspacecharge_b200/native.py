@@ -48,6 +48,7 @@ OPT_CHECK_FINITE = 6
 OPT_TEST_WAIT_TIMEOUT = 7
 OPT_PARTICLE_ORDER = 8
 OPT_BATCH_GRAPH = 9
+OPT_VJP_REUSE_FORWARD = 10
 
 _ERRNAMES = {v: k for k, v in globals().items() if k.startswith("OSC_E_") or k == "OSC_OK"}
 

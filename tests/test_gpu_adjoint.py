@@ -244,3 +244,47 @@ def test_autograd_function(ctx):
     for t, ref in ((tx, gx), (ty, gy), (tz, gz)):
         assert np.allclose(t.grad.cpu().numpy(), ref, rtol=0, atol=1e-9 * np.abs(ref).max())
     assert np.allclose(tq.grad.cpu().numpy(), (Ed ** 2).sum(1) + gq, rtol=1e-9, atol=0)
+
+
+@pytest.mark.parametrize("n", [N, N_SUMMED])
+def test_fp32_vjp_reuses_the_forward_grid(ctx, n):
+    """OPT_VJP_REUSE_FORWARD: the FP32 VJP right after the FP32 step on the same arrays takes
+    E on the grid from that step (fewer kernels) and gives the gradients of the recomputing
+    VJP to FP32 round-off; a step in between (other particles) makes it recompute."""
+    import ctypes
+    x, y, z, q, mesh = setup(ctx, npart=60000, seed=55, n=n)
+    dev = torch.device("cuda", 0)
+    tx, ty, tz, tq = (torch.from_numpy(a).to(dev) for a in (x, y, z, q))
+    E = torch.empty((len(x), 3), dtype=torch.float64, device=dev)
+    m = mesh.to_c()
+
+    def step(ax=tx):
+        ms = osc.Mesh3D(nlo=mesh.nlo, nhi=mesh.nhi, min=mesh.min.copy(), max=mesh.max.copy(),
+                        delta=mesh.delta.copy(), gamma=mesh.gamma)
+        osc.space_charge_step_dev(ctx, ms, ax, ty, tz, E, qa=tq, precision=osc.PREC_FP32)
+
+    def vjp32():
+        gE = 2 * tq[:, None] * E
+        g = [torch.empty_like(tx) for _ in range(4)]
+        l0 = ctx.launch_count()
+        ctx.call("osc_space_charge_step_vjp_dev", ctypes.byref(m), ctypes.c_int64(len(x)),
+                 *[ctypes.c_void_p(a.data_ptr()) for a in (tx, ty, tz, tq)], ctypes.c_double(0.0),
+                 int(osc.PREC_FP32), ctypes.c_void_p(gE.data_ptr()), *[ctypes.c_void_p(a.data_ptr()) for a in g])
+        ctx.synchronize()
+        return [a.cpu().numpy() for a in g], ctx.launch_count() - l0
+
+    step()
+    ref, n_ref = vjp32()  # the option is off: recomputed
+    ctx.set_option(osc.OPT_VJP_REUSE_FORWARD, 1)
+    try:
+        step()
+        got, n_got = vjp32()
+        assert n_got < n_ref
+        for a, b in zip(got, ref):
+            assert np.abs(a - b).max() <= 1e-5 * np.abs(b).max()
+        # the last step ran on another x array: its grid is not the one of (tx, ty, tz)
+        step(tx + 0.25 * float(mesh.delta[0]))
+        _, n_other = vjp32()
+        assert n_other == n_ref
+    finally:
+        ctx.set_option(osc.OPT_VJP_REUSE_FORWARD, 0)
