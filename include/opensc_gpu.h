@@ -143,6 +143,9 @@ OSC_API int osc_ctx_synchronize(osc_ctx *ctx);
  *     the radix warp engine (0), the one-exchange 16 x 32 engine (1, FP32 length 512 only),
  *     or the warp engine with CTAs that pair the rows ky and Ny - ky and fetch their common
  *     Green columns once (2);
+ *   "batch_copy_chunks": chunks of bunches the FP32 osc_batch_space_charge_step (host
+ *     arrays) copies in, solves and copies out in a pipeline (1 to 16; 1: one copy in, one
+ *     batched step, one copy out);
  *   "sym_nl_div:<f32|f64>:L<length>": 2 or 4 divides the line pairs per CTA of the Green
  *     build's even/odd line transforms of that doubled length.
  * Results are identical for every choice; only the time changes. */

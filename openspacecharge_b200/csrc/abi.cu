@@ -64,6 +64,9 @@ int osc_ctx_destroy(osc_ctx *ctx) {
     if (ctx->h_fault) cudaFreeHost(ctx->h_fault);
     for (auto s : ctx->aux) cudaStreamDestroy(s);
     if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
+    if (ctx->copy_in) cudaStreamDestroy(ctx->copy_in);
+    if (ctx->copy_out) cudaStreamDestroy(ctx->copy_out);
+    for (auto e : ctx->copy_ev) cudaEventDestroy(e);
     for (auto e : ctx->aux_ev) cudaEventDestroy(e);
     if (ctx->switch_ev) cudaEventDestroy(ctx->switch_ev);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
@@ -145,6 +148,7 @@ static bool tuning_value_ok(const std::string &key, int v) {
         return v == 0 || v == 1 || v == 2;
     if (key.rfind("zconv_engine:", 0) == 0) return v == 0 || v == 1 || v == 2;
     if (key.rfind("sym_nl_div:", 0) == 0) return v == 0 || v == 1 || v == 2 || v == 4;
+    if (key == "batch_copy_chunks") return v >= 0 && v <= 16;
     return false;
 }
 

@@ -520,7 +520,7 @@ int batch_fp32(osc_ctx *ctx, int nb, osc_bunch *bs, const double *x, const doubl
         P->key = key;
         TRY(make_plan(ctx, *P, nb, bs, x, y, z, q, resize, E));
         ctx->batch_plans.push_front(P);
-        constexpr size_t kMaxPlans = 4;
+        constexpr size_t kMaxPlans = 12;  // a host-array call plans each of its chunks
         while (ctx->batch_plans.size() > kMaxPlans) {
             TRY(sync(ctx));
             ctx->batch_plans.pop_back();
@@ -583,6 +583,99 @@ int batch_fp32(osc_ctx *ctx, int nb, osc_bunch *bs, const double *x, const doubl
     return OSC_OK;
 }
 
+// The FP32 batch from host arrays, pipelined over chunks of bunches: every chunk's
+// particles are copied in on one stream as soon as the call starts, each chunk is solved
+// (one batched step) once its copy has landed, and its E rows go back on another stream
+// while the next chunk is solved and later chunks are still coming in, so the two copy
+// directions and the solves overlap.  Chunks are consecutive bunches in offset order with
+// about equal particle counts; a chunk copies the particle range its bunches span.
+constexpr int kCopyChunks = 6;  // default; tuning key batch_copy_chunks (1 to 16)
+
+int batch_host_pipelined(osc_ctx *ctx, int nb, osc_bunch *bs, const double *x, const double *y, const double *z,
+                         const double *q, int resize, int64_t total, double *E) {
+    double *dx, *dy, *dz, *dq = nullptr, *dE;
+    TRY(ws_get(ctx, "h_x", sizeof(double) * (size_t)total, (void **)&dx));
+    TRY(ws_get(ctx, "h_y", sizeof(double) * (size_t)total, (void **)&dy));
+    TRY(ws_get(ctx, "h_z", sizeof(double) * (size_t)total, (void **)&dz));
+    if (q) TRY(ws_get(ctx, "h_q", sizeof(double) * (size_t)total, (void **)&dq));
+    TRY(ws_get(ctx, "h_pE", sizeof(double) * 3 * (size_t)total, (void **)&dE));
+    const int K = std::min(tune_get(ctx, "batch_copy_chunks", kCopyChunks), nb);
+    if (!ctx->copy_in) CK(cudaStreamCreateWithFlags(&ctx->copy_in, cudaStreamNonBlocking), "copy-in stream");
+    if (!ctx->copy_out) CK(cudaStreamCreateWithFlags(&ctx->copy_out, cudaStreamNonBlocking), "copy-out stream");
+    while ((int)ctx->copy_ev.size() < K + 1) {
+        cudaEvent_t e;
+        CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "copy event");
+        ctx->copy_ev.push_back(e);
+    }
+    // chunks of consecutive bunches (offset order), about total/K particles each
+    std::vector<int> order(nb);
+    for (int b = 0; b < nb; ++b) order[b] = b;
+    std::stable_sort(order.begin(), order.end(), [&](int u, int v) { return bs[u].offset < bs[v].offset; });
+    int64_t nall = 0;
+    for (int b = 0; b < nb; ++b) nall += bs[b].np;
+    std::vector<int> first(K + 1, nb);
+    first[0] = 0;
+    {
+        int c = 1;
+        int64_t acc = 0;
+        for (int i = 0; i < nb - 1 && c < K; ++i) {
+            acc += bs[order[i]].np;
+            const int left = nb - (i + 1);  // bunches after this one; every chunk keeps one
+            if ((acc * K >= nall * (int64_t)c && left >= K - c) || left == K - c) first[c++] = i + 1;
+        }
+    }
+    std::vector<int64_t> lo(K), hi(K);
+    for (int c = 0; c < K; ++c) {
+        lo[c] = INT64_MAX;
+        hi[c] = 0;
+        for (int i = first[c]; i < first[c + 1]; ++i) {
+            lo[c] = std::min(lo[c], bs[order[i]].offset);
+            hi[c] = std::max(hi[c], bs[order[i]].offset + bs[order[i]].np);
+        }
+    }
+    // the copy-in stream starts after the work already queued on the context's stream
+    CK(cudaEventRecord(ctx->copy_ev[K], ctx->stream), "record queued work");
+    CK(cudaStreamWaitEvent(ctx->copy_in, ctx->copy_ev[K], 0), "order copies");
+    for (int c = 0; c < K; ++c) {
+        const size_t n = (size_t)(hi[c] - lo[c]), o = (size_t)lo[c];
+        for (const auto &pr : {std::make_pair(dx, x), std::make_pair(dy, y), std::make_pair(dz, z),
+                               std::make_pair(dq, q)})
+            if (pr.second)
+                CK(cudaMemcpyAsync(pr.first + o, pr.second + o, sizeof(double) * n, cudaMemcpyHostToDevice,
+                                   ctx->copy_in),
+                   "H2D copy");
+        CK(cudaEventRecord(ctx->copy_ev[c], ctx->copy_in), "record copy");
+    }
+    auto drain = [&]() {
+        cudaStreamSynchronize(ctx->copy_in);
+        cudaStreamSynchronize(ctx->copy_out);
+    };
+    std::vector<osc_bunch> sub;
+    for (int c = 0; c < K; ++c) {
+        cudaError_t e = cudaStreamWaitEvent(ctx->stream, ctx->copy_ev[c], 0);
+        if (e != cudaSuccess) {
+            drain();
+            return cuda_check(ctx, e, "wait for copy");
+        }
+        sub.clear();
+        for (int i = first[c]; i < first[c + 1]; ++i) sub.push_back(bs[order[i]]);
+        const int rc = batch_fp32(ctx, (int)sub.size(), sub.data(), dx, dy, dz, dq, resize, dE);
+        for (int i = first[c]; i < first[c + 1]; ++i) bs[order[i]] = sub[i - first[c]];
+        if (rc) {
+            drain();
+            return rc;
+        }
+        // batch_fp32 returned after synchronising: the chunk's E rows are final
+        const size_t n = (size_t)(hi[c] - lo[c]), o = (size_t)lo[c];
+        e = cudaMemcpyAsync(E + 3 * o, dE + 3 * o, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, ctx->copy_out);
+        if (e != cudaSuccess) {
+            drain();
+            return cuda_check(ctx, e, "D2H copy");
+        }
+    }
+    return cuda_check(ctx, cudaStreamSynchronize(ctx->copy_out), "copy-out synchronize");
+}
+
 }  // namespace
 
 extern "C" {
@@ -613,6 +706,8 @@ int osc_batch_space_charge_step(osc_ctx *ctx, int nbunch, osc_bunch *bunches, co
     TRY(check_bunches(ctx, nbunch, bunches, x, y, z, E));
     int64_t total = 0;
     for (int b = 0; b < nbunch; ++b) total = std::max(total, bunches[b].offset + bunches[b].np);
+    if (precision == OSC_PREC_FP32 && nbunch >= 2) return batch_host_pipelined(ctx, nbunch, bunches, x, y, z, q,
+                                                                               resize_mesh, total, E);
     double *dx, *dy, *dz, *dq, *dE;
     TRY(stage_in(ctx, "h_x", x, (size_t)total, &dx));
     TRY(stage_in(ctx, "h_y", y, (size_t)total, &dy));

@@ -64,6 +64,10 @@ struct osc_ctx {
     // private stream that graph captures run on (the caller's stream may be the legacy
     // default stream, which cannot be captured); the graphs launch on the caller's stream
     cudaStream_t cap_stream = nullptr;
+    // copy streams of the batched step from host arrays (chunks of bunches copied in and out
+    // while others compute) and their events
+    cudaStream_t copy_in = nullptr, copy_out = nullptr;
+    std::vector<cudaEvent_t> copy_ev;
     int ws_slot = 0;
     std::string err;
     // options
