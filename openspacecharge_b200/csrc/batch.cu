@@ -589,7 +589,7 @@ int batch_fp32(osc_ctx *ctx, int nb, osc_bunch *bs, const double *x, const doubl
 // while the next chunk is solved and later chunks are still coming in, so the two copy
 // directions and the solves overlap.  Chunks are consecutive bunches in offset order with
 // about equal particle counts; a chunk copies the particle range its bunches span.
-constexpr int kCopyChunks = 6;  // default; tuning key batch_copy_chunks (1 to 16)
+constexpr int kCopyChunks = 8;  // default; tuning key batch_copy_chunks (1 to 16)
 
 int batch_host_pipelined(osc_ctx *ctx, int nb, osc_bunch *bs, const double *x, const double *y, const double *z,
                          const double *q, int resize, int64_t total, double *E) {
