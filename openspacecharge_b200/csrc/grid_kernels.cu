@@ -145,7 +145,8 @@ __global__ void k_igf_corners_batch(double *__restrict__ F, const CornerArgs *__
     const CornerArgs a = args[blockIdx.y];
     F += blockIdx.y * fstride;
     const int64_t n = (int64_t)a.cdx * a.cdy * a.cdz;
-    GRID_STRIDE(idx, n) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    auto at = [&](int64_t idx) {
         const int cx = (int)(idx % a.cdx);
         const int64_t r = idx / a.cdx;
         const int cy = (int)(r % a.cdy);
@@ -153,14 +154,22 @@ __global__ void k_igf_corners_batch(double *__restrict__ F, const CornerArgs *__
         const double u = (a.c0x + cx) * a.dx + a.umin;
         const double v = (a.c0y + cy) * a.dy + a.vmin;
         const double w = (a.c0z + cz) * a.dz + a.wmin;
-        F[idx] = igf_primitive(a.icomp, u, v, w) * a.factor;
+        return igf_primitive(a.icomp, u, v, w) * a.factor;
+    };
+    for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += 2 * stride) {
+        const int64_t i1 = i0 + stride;  // two points per thread and trip, as k_igf_corners_set
+        const double f0 = at(i0);
+        const double f1 = i1 < n ? at(i1) : 0.0;
+        F[i0] = f0;
+        if (i1 < n) F[i1] = f1;
     }
 }
 __global__ void k_igf_corners_set(double *__restrict__ F, CornerSet s, int64_t fstride) {
     const CornerArgs a = s.a[blockIdx.y];
     F += blockIdx.y * fstride;
     const int64_t n = (int64_t)a.cdx * a.cdy * a.cdz;
-    GRID_STRIDE(idx, n) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    auto at = [&](int64_t idx) {
         const int cx = (int)(idx % a.cdx);
         const int64_t r = idx / a.cdx;
         const int cy = (int)(r % a.cdy);
@@ -168,21 +177,30 @@ __global__ void k_igf_corners_set(double *__restrict__ F, CornerSet s, int64_t f
         const double u = (a.c0x + cx) * a.dx + a.umin;
         const double v = (a.c0y + cy) * a.dy + a.vmin;
         const double w = (a.c0z + cz) * a.dz + a.wmin;
-        F[idx] = igf_primitive(a.icomp, u, v, w) * a.factor;
+        return igf_primitive(a.icomp, u, v, w) * a.factor;
+    };
+    // two points per thread and trip: the two dependency chains of log/atan evaluations
+    // interleave
+    for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += 2 * stride) {
+        const int64_t i1 = i0 + stride;
+        const double f0 = at(i0);
+        const double f1 = i1 < n ? at(i1) : 0.0;
+        F[i0] = f0;
+        if (i1 < n) F[i1] = f1;
     }
 }
 int launch_igf_corners_set(double *F, const CornerSet &s, int64_t fstride, cudaStream_t st) {
     if (s.n < 1 || s.n > 4) return 1;
     int64_t npts = 0;
     for (int i = 0; i < s.n; ++i) npts = std::max(npts, (int64_t)s.a[i].cdx * s.a[i].cdy * s.a[i].cdz);
-    const dim3 grid(nblocks(npts, 256), (unsigned)s.n);
+    const dim3 grid(nblocks((npts + 1) / 2, 256), (unsigned)s.n);  // two points per thread
     k_igf_corners_set<<<grid, 256, 0, st>>>(F, s, fstride);
     return ok();
 }
 
 int launch_igf_corners_batch(double *F, const CornerArgs *args_dev, int nbatch, int64_t fstride, int64_t npts,
                              cudaStream_t st) {
-    const dim3 grid(nblocks(npts, 256), (unsigned)nbatch);
+    const dim3 grid(nblocks((npts + 1) / 2, 256), (unsigned)nbatch);  // two points per thread
     k_igf_corners_batch<<<grid, 256, 0, st>>>(F, args_dev, fstride);
     return ok();
 }
