@@ -142,8 +142,14 @@ __device__ __forceinline__ float r2c_in(const float4 *__restrict__ in, const R2C
     return s;
 }
 
+// resident CTAs the register allocation of k_r2c_rows is bounded for: 4 (32 registers, no
+// spills) for the FP32 step's quad-grid input on the 8-values-per-thread engine at L = 256,
+// whose loads wait on L2 (35.4 against 40.8 us at 40 registers and 3 CTAs); 1 otherwise
+template <typename T, typename TIn, class E> constexpr int r2c_minb() {
+    return (std::is_same<TIn, float4>::value && E::kLen == 256 && E::kEPT == 8) ? 4 : 1;
+}
 template <typename T, typename TIn, int NL, class E, bool HIN>
-__global__ void __launch_bounds__(E::kMaxThreads) k_r2c_rows(const TIn *__restrict__ in, cplx<T> *__restrict__ out,
+__global__ void __launch_bounds__(E::kMaxThreads, r2c_minb<T, TIn, E>()) k_r2c_rows(const TIn *__restrict__ in, cplx<T> *__restrict__ out,
                                                              R2CArgs a, const cplx<T> *__restrict__ twg) {
     typedef cplx<T> V;
     extern __shared__ __align__(16) unsigned char smem_raw[];
