@@ -20,6 +20,10 @@ struct LineArgs {
     double scale;
     unsigned flip_mask;  // bit z: component z stores element (L-e) mod L at e (index flip)
     int nl_div = 0;      // autotuner: 2 halves the lines per CTA of a static engine (0/1: default)
+    // > 0: the column tiles run over the flat sequence of flat_lines = ncols * nplanes lines
+    // (plane-major), so a tile may end in one plane and continue in the next (column
+    // layouts only, needs ncols >= the lines per CTA); 0: one row of tiles per plane
+    int flat_lines = 0;
 };
 
 // Forward transform of real rows (length nin, zero-padded to L) packed two per complex

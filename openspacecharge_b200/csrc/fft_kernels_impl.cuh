@@ -81,6 +81,31 @@ __global__ void __launch_bounds__(E::kMaxThreads) k_lines(const cplx<T> *in, cpl
         __syncthreads();
         const bool flip = (a.flip_mask >> blockIdx.z) & 1u;
         const T sc = (T)a.scale;
+        if (a.flat_lines > 0) {
+            // tile over the flat line sequence: line col0 + l is column (c0 + l) of plane pl0,
+            // or column (c0 + l - ncols) of plane pl0 + 1 (NL <= ncols, so at most one wrap)
+            const int pl0 = col0 / a.ncols, c0 = col0 - pl0 * a.ncols;
+            const V *src0 = in + (int64_t)blockIdx.z * a.in_zstride + (int64_t)pl0 * a.in_pstride;
+            V *dst0 = out + (int64_t)blockIdx.z * a.out_zstride + (int64_t)pl0 * a.out_pstride;
+            const int64_t in_wrap = a.in_pstride - (int64_t)a.ncols * a.in_cstride;
+            const int64_t out_wrap = a.out_pstride - (int64_t)a.ncols * a.out_cstride;
+            auto ld = [&](int e, int l) -> V {
+                const int c = c0 + l;
+                V v = mk<T>(0, 0);
+                if (e < a.in_len && col0 + l < a.flat_lines)
+                    v = src0[(int64_t)c * a.in_cstride + (c >= a.ncols ? in_wrap : 0) + (int64_t)e * a.in_estride];
+                return v;
+            };
+            auto st = [&](int p, int l, const V &v) {
+                const int c = c0 + l;
+                const int e = (flip ? (L - p) % L : p) - a.out_lo;
+                if (col0 + l < a.flat_lines && e >= 0 && e < a.out_len)
+                    dst0[(int64_t)c * a.out_cstride + (c >= a.ncols ? out_wrap : 0) + (int64_t)e * a.out_estride] =
+                        cscale(v, sc);
+            };
+            E::template run_io<V, NL, MODE == 1, MODE == 2>(buf, a.p, tw, a.sign, ld, st);
+            return;
+        }
         auto ld = [&](int e, int l) -> V {
             const int col = col0 + l;
             V v = mk<T>(0, 0);
@@ -692,8 +717,13 @@ inline int launch_lines_k(const cplx<T> *in, cplx<T> *out, const LineArgs &a, in
     auto kern = k_lines<T, NL, ROW, E, MODE>;
     int rc = set_smem(kern, sm);
     if (rc) return rc;
-    dim3 grid((unsigned)ceil_div(a.ncols, NL), (unsigned)nplanes, (unsigned)ncomp);
-    kern<<<grid, nt, sm, st>>>(in, out, a, tw);
+    // the flat tiling needs a column layout, at most one plane wrap per tile and int line indices
+    const bool flat = !ROW && a.flat_lines > 0 && a.ncols >= NL && (int64_t)a.ncols * nplanes < (1ll << 30);
+    LineArgs af = a;
+    af.flat_lines = flat ? a.ncols * nplanes : 0;
+    dim3 grid(flat ? (unsigned)ceil_div(af.flat_lines, NL) : (unsigned)ceil_div(a.ncols, NL),
+              flat ? 1u : (unsigned)nplanes, (unsigned)ncomp);
+    kern<<<grid, nt, sm, st>>>(in, out, af, tw);
     return launch_ok();
 }
 

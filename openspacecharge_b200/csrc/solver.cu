@@ -488,6 +488,7 @@ int freespace_opt(osc_ctx *c, const FreeSpaceJob &j, const TIn *rho) {
     ly.scale = 1.0;
     ly.flip_mask = 0;
     ly.nl_div = tune_get(c, std::string("lines_nl_div:") + (sizeof(T) == 4 ? "f32" : "f64") + ":L" + std::to_string(Ny));
+    ly.flat_lines = 1;  // tiles over the (z, kx) line sequence: no part-empty tile per plane
     {
         Launch L_(c, "fft_y_fwd");
         TRY(kerr(c, launch_lines<T>(X1, X2, ly, Bin * nz, 1, false, twy, c->stream), "y forward"));
@@ -540,6 +541,8 @@ int freespace_opt(osc_ctx *c, const FreeSpaceJob &j, const TIn *rho) {
         li.in_pstride = (int64_t)nxh * Ny;
         li.out_pstride = (int64_t)nxh * ny;
     }
+    // lines (kx, z) fill whole tiles already; lines kx per plane z tile the flat sequence
+    li.flat_lines = zin ? 0 : 1;
     {
         Launch L_(c, "fft_y_inv");
         TRY(kerr(c, launch_lines<T>(X3, X4, li, zin ? Bout : Bout * nz, nout, false, twy, c->stream), "y inverse"));
