@@ -405,6 +405,7 @@ static int pipe_phi_opt(osc_ctx *c, const LGeom &g, const double *rho, double *p
     ly.out_cstride = 1;
     ly.out_estride = nxh;
     ly.scale = 1.0;
+    ly.flat_lines = 1;  // tiles over the (z, kx) line sequence, in both y passes
     {
         Launch L_(c, "fft_y_fwd");
         TRY(kchk(c, launch_lines<T>(X1, X2, ly, nz, 1, false, twy, c->stream), "y forward"));

@@ -608,6 +608,7 @@ int slab_forward(osc_ctx *c, int nx, int ny, int nzl, const float4 *quad, cplx<f
     ly.scale = 1.0;
     ly.flip_mask = 0;
     ly.nl_div = tune_get(c, "lines_nl_div:f32:L" + std::to_string(Ny));
+    ly.flat_lines = 1;
     Launch L_(c, "fft_y_fwd");
     return kerr(c, launch_lines<float>(X1, X2, ly, nzl, 1, false, twy, c->stream), "y forward");
 }
